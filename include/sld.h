@@ -1,0 +1,174 @@
+/*
+ * sld.h - C ABI of the B200 spin-lattice dynamics step engine.
+ *
+ * The engine runs the per-step hot path of SPILADY 1.0 (-DSLDHL) on one
+ * NVIDIA B200: link-cell relinking, EAM density, forces and energies,
+ * Heisenberg + Landau effective fields with the Suzuki-Trotter colour sweeps,
+ * the lattice updates, Langevin noise, and the electron-temperature
+ * subsystem.  In the reference these are free functions that share global
+ * state (prototype_CPU.h:123-237, called from core(), core.cpp:31-76) and are
+ * swapped for their GPU twins at link time; here each becomes an entry point
+ * on a context that owns the device state.  Plain C types only.
+ *
+ * Conventions
+ *   - every entry point returns SLD_OK (0) or a negative SLD_ERR_* code;
+ *   - one host thread drives one context at a time; several contexts may
+ *     live in one process (each owns its own device memory and stream);
+ *   - units are the reference's (spilady.h:53-62): Angstrom, eV, seconds;
+ *     sld_params holds the variables.in values in their input units
+ *     (temperature in K, atmass in u), converted as read_variables.cpp:256
+ *     does;
+ *   - arrays are row-major, one row per atom in the caller's atom order
+ *     (x, y, z for vectors); the engine reorders internally and always
+ *     returns data in the caller's order;
+ *   - control.h's compile-time switches are the runtime fields spinlang,
+ *     lattlang, eltemp, localcolmot and renormalize_energy.
+ */
+#ifndef SLD_H
+#define SLD_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SLD_OK 0
+#define SLD_ERR_ARG (-1)        /* invalid argument or parameter */
+#define SLD_ERR_CUDA (-2)       /* a CUDA runtime call failed */
+#define SLD_ERR_GEOMETRY (-3)   /* fewer than 3 link cells per axis (the
+                                   reference then double counts neighbours,
+                                   map_cells.cpp:89-121) */
+#define SLD_ERR_CAPACITY (-4)   /* a link cell holds more atoms than the
+                                   kernels support (SLD_MAX_CELL_ATOMS) */
+#define SLD_ERR_TABLE (-5)      /* r or rho outside the potential table
+                                   (the reference reads out of bounds,
+                                   potential_CPU.cpp:172-179) */
+#define SLD_ERR_NAN (-6)        /* a non-finite value was produced */
+#define SLD_ERR_IO (-7)         /* a file could not be read or parsed */
+#define SLD_ERR_STATE (-8)      /* call out of order (e.g. no state loaded) */
+#define SLD_ERR_NOMEM (-9)      /* device allocation failed */
+
+#define SLD_MAX_CELL_ATOMS 64
+
+typedef enum { SLD_FP64 = 0, SLD_SPLIT = 1 } sld_precision;
+
+typedef struct {
+    double box[6];               /* d.xx d.yx d.yy d.zx d.zy d.zz (Angstrom);
+                                    struct.h box_vector, upper-triangular */
+    double step;                 /* time step (s)                 default.h:62 */
+    double temperature;          /* K                             default.h:159 */
+    double atmass;               /* u                             default.h:158 */
+    double gamma_L_over_mass;    /* s^-1 (lattice Langevin)       default.h:166 */
+    double gamma_S_HL;           /* spin Langevin, Heisenberg-Landau  default.h:174 */
+    double rcut_pot;             /* Angstrom                      default.h:200 */
+    double rcut_mag;             /* Angstrom                      default.h:205 */
+    double rcut_max;             /* Angstrom                      default.h:209 */
+    double min_length_link_cell; /* Angstrom                      default.h:217 */
+    double kappa_e;              /* electron thermal conductivity, W/(m K) default.h:96 */
+    int random_seed;             /*                               default.h:161 */
+    int spinlang;                /* control.h:22 */
+    int lattlang;                /* control.h:23 */
+    int eltemp;                  /* control.h:25 */
+    int localcolmot;             /* control.h:28 */
+    int renormalize_energy;      /* control.h:27 */
+    int te_mesh;                 /* 0: Te per link cell as the reference
+                                    (map_cells.cpp:128); n > 0: an n^3 Te
+                                    mesh decoupled from the link cells */
+    int te_nloop;                /* Te substeps per core_dTe call; the
+                                    reference CPU path uses 50
+                                    (core_dTe_CPU.cpp:49) */
+    int interval_of_print_out;   /* energy renormalisation interval
+                                    (check.cpp:33)                default.h:64 */
+    int precision;               /* sld_precision */
+    int device;                  /* CUDA device ordinal */
+} sld_params;
+
+typedef struct sld_ctx sld_ctx;
+
+/* Reference defaults (default.h:44-226 with variables.in's cutoffs). */
+int sld_params_default(sld_params* out);
+
+/* Parse a variables.in file (read_variables.cpp:40-253: whitespace
+   separated key/value pairs, unknown keys ignored) into *inout. */
+int sld_read_variables(const char* path, sld_params* inout);
+
+/* Create a context and load a state: natom atoms, positions r, momenta p
+   (eV s / Angstrom) and spins s, each natom x 3; te_K holds the initial
+   electron temperature per Te cell (NULL: the lattice temperature), the
+   readTe input of map_cells.cpp:33-39,136-150.  Then, as initialize()
+   (initial.cpp:31-106) does: potential tables, link cells and colour groups,
+   rho, forces and energies, cell temperatures, and with renormalize_energy
+   the reference energy of check_energy(-1). */
+int sld_create(sld_ctx** out, const sld_params* prm, int natom,
+               const double* r, const double* p, const double* s,
+               const double* te_K);
+
+/* Read an atoms configuration file in the reference's con- format
+   (read_config.cpp:39-116) and create a context from it; params->box is
+   taken from the file. */
+int sld_create_from_config(sld_ctx** out, const sld_params* prm,
+                           const char* con_path, const char* te_path);
+
+void sld_destroy(sld_ctx* ctx);
+
+/* Replace r, p, s (host arrays, caller order) and recompute rho, forces and
+   energies as after a fresh start. */
+int sld_set_state(sld_ctx* ctx, const double* r, const double* p,
+                  const double* s);
+
+/* The reference's step functions, one for one. */
+int sld_links(sld_ctx* ctx);                       /* links_CPU.cpp:85 */
+int sld_calculate_rho(sld_ctx* ctx);               /* calculate_rho_CPU.cpp:71 */
+int sld_calculate_force_energy(sld_ctx* ctx);      /* calculate_force_energy_CPU.cpp:220 */
+int sld_core_ds(sld_ctx* ctx, double dt);          /* core_ds_CPU.cpp:35 */
+int sld_core_dp(sld_ctx* ctx, double dt);          /* core_dp_CPU.cpp:51 */
+int sld_core_dr(sld_ctx* ctx, double dt);          /* core_dr_CPU.cpp:33 */
+int sld_core_dTe(sld_ctx* ctx, double dt);         /* core_dTe_CPU.cpp:47 */
+int sld_calculate_temperature(sld_ctx* ctx);       /* calculate_temperature_CPU.cpp:35 */
+
+/* nsteps passes of the reference main-loop body (spilady.cpp:50-57):
+   core(); total_time += step; and, when eltemp and renormalize_energy are
+   set, check_energy's renormalisation every interval_of_print_out steps.
+   The step is captured once as a CUDA graph and replayed. */
+int sld_run(sld_ctx* ctx, int nsteps);
+
+/* Copy a field to a host array in caller atom order.  Per-atom fields:
+   "r" "p" "f" "s" (natom x 3), "H" "HL" (Heff_H, Heff_L, natom x 3), "s0"
+   "rho" "pe" "ke" "me" "me0" "vir" "sum_Jij_sj" "local_volume" (natom),
+   "stress" (natom x 6: 11 22 33 12 23 31), "cell" (link cell index).
+   Per-Te-cell fields: "Te" (K) "Ee" "Tl" "Ts_R" "Ts_L" "Gel" "Ges"
+   "count".  Returns the number of doubles written, or a negative code.
+   `capacity` is the size of `out` in doubles. */
+long sld_get(sld_ctx* ctx, const char* field, double* out, long capacity);
+
+/* Cell member lists (atom indices, caller order) head -> tail, cells in
+   index order: natom ints. */
+int sld_get_cell_lists(sld_ctx* ctx, int* out);
+
+/* Averages as check_energy/check_temperature/check_spin compute them:
+   out[0..9] = <pe>, <ke>, <me>, <me0>, <Ee>, Tl (K), <Te> (K), <sx>,
+   <sy>, <sz>. */
+int sld_averages(sld_ctx* ctx, double* out10);
+
+/* out[0..5] = natom, ncells, ngroups, n_te_cells, nx, ny (link cells). */
+int sld_info(sld_ctx* ctx, int* out6);
+
+/* Total virial (sum of the per-atom virials, calculate_force_energy_CPU.cpp:298). */
+int sld_virial(sld_ctx* ctx, double* out);
+
+/* Simulated time (s). */
+int sld_total_time(sld_ctx* ctx, double* out);
+
+/* Block until the device work of this context is done and report any
+   device-side error flag as an SLD_ERR_* code. */
+int sld_sync(sld_ctx* ctx);
+
+/* Milliseconds of device time of the last sld_run call (CUDA events on the
+   context's stream). */
+int sld_last_run_ms(sld_ctx* ctx, double* out);
+
+const char* sld_error_string(int code);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,70 @@
+#!/bin/sh
+# Test infrastructure: compiles the reference's own CPU path (SPILADY 1.0,
+# `-DCPU -DOMP -DSLDHL`, as its make.sh:6 does with g++) from its unmodified
+# sources, for use as a checker and as the timed CPU baseline.
+#
+# The reference selects its physics with #defines in control.h, which
+# spilady.h:45 includes from its own directory.  So for each mode this script
+# makes oracle/_ref/src_<mode>/ holding symbolic links to every reference
+# .cpp/.h file except control.h and spilady.cpp (whose main() is replaced by
+# oracle/ref/harness.cpp), writes that mode's control.h there, and compiles.
+# No reference source is copied; all outputs stay under oracle/_ref/.
+#
+#   nve     NVE spin-lattice (no thermostat)
+#   lang    + spinlang + lattlang        (Langevin spin and lattice)
+#   langte  + eltemp + localcolmot + renormalizeEnergy
+#
+# usage: sh oracle/ref/build.sh [reference_dir]
+set -e
+REF=${1:-/root/reference}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT=$(cd "$HERE/.." && pwd)/_ref
+if [ ! -f "$REF/core.cpp" ]; then
+    echo "reference sources not found at $REF" >&2
+    exit 1
+fi
+mkdir -p "$OUT"
+# the system g++ (an inherited CXX may point at a compiler without libgomp)
+CXX=${ORACLE_CXX:-g++}
+FLAGS="-O3 -fopenmp -U_FORTIFY_SOURCE -D_FORTIFY_SOURCE=0 -DCPU -DOMP -DSLDHL -w"
+
+for mode in nve lang langte; do
+    src="$OUT/src_$mode"
+    obj="$OUT/obj_$mode"
+    mkdir -p "$src" "$obj"
+    find "$src" -maxdepth 1 -type l -delete
+    for f in "$REF"/*.cpp "$REF"/*.h; do
+        b=$(basename "$f")
+        case "$b" in control.h|spilady.cpp) continue ;; esac
+        ln -s "$f" "$src/$b"
+    done
+    {
+        echo "/* control.h for mode $mode, written by oracle/ref/build.sh */"
+        echo "#define readconf"
+        echo "#define runstep"
+        case "$mode" in
+        lang) echo "#define spinlang"; echo "#define lattlang" ;;
+        langte)
+            echo "#define spinlang"; echo "#define lattlang"
+            echo "#define eltemp"; echo "#define localcolmot"
+            echo "#define renormalizeEnergy" ;;
+        esac
+    } > "$src/control.h.new"
+    if ! cmp -s "$src/control.h.new" "$src/control.h"; then
+        mv "$src/control.h.new" "$src/control.h"
+    else
+        rm -f "$src/control.h.new"
+    fi
+    pids=""
+    for f in "$src"/*.cpp "$HERE/harness.cpp"; do
+        b=$(basename "$f" .cpp)
+        o="$obj/$b.o"
+        if [ ! -f "$o" ] || [ "$f" -nt "$o" ] || [ "$src/control.h" -nt "$o" ]; then
+            $CXX $FLAGS -I"$src" -c "$f" -o "$o" &
+            pids="$pids $!"
+        fi
+    done
+    for p in $pids; do wait "$p"; done
+    $CXX -fopenmp "$obj"/*.o -o "$OUT/spilady_ref_$mode" -lm
+done
+echo "built: $OUT/spilady_ref_nve $OUT/spilady_ref_lang $OUT/spilady_ref_langte"

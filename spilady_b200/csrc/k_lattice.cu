@@ -1,0 +1,198 @@
+// Lattice updates: core_dp (core_dp_CPU.cpp:51-312) and core_dr
+// (core_dr_CPU.cpp:33-44).
+//
+// With the lattice thermostat, core_dp is C1(dt/2) B(dt/2) A(dt) B(dt/2)
+// C2(dt/2).  Every one of those touches only the atoms of one link cell (C1
+// and C2 mix the momenta inside a cell, A subtracts the cell mean of the
+// noise, B is per atom), so one thread per cell runs the whole sequence on
+// its atoms in the reference's list order: the momenta are read and written
+// once per core_dp.  rescale_momentum (:268-312) then needs two global sums
+// (total momentum, kinetic energy before/after removing it); they are formed
+// by per-block partials and one finishing block, in a fixed order, so every
+// run gives the same bits.
+#include "sld_common.cuh"
+
+__device__ __forceinline__ void block_partials3(const Dev& D, double a, double b, double c) {
+    __shared__ double sh[32];
+    double ta = block_sum(a, sh);
+    double tb = block_sum(b, sh);
+    double tc = block_sum(c, sh);
+    if (threadIdx.x == 0) {
+        double* o = D.red + 4 * (size_t)blockIdx.x;
+        o[0] = ta; o[1] = tb; o[2] = tc;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_dp_nve(Dev D, double dt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double px = 0, py = 0, pz = 0;
+    if (i < D.natom) {
+        double4 p = D.p[i], f = D.f[i];
+        p.x = p.x + dt * f.x; p.y = p.y + dt * f.y; p.z = p.z + dt * f.z;
+        D.p[i] = p;
+        px = p.x; py = p.y; pz = p.z;
+    }
+    block_partials3(D, px, py, pz);
+}
+
+__device__ __forceinline__ void add3(double4& a, double k, double x, double y, double z) {
+    a.x = a.x + k * x; a.y = a.y + k * y; a.z = a.z + k * z;
+}
+
+// C1 / C2: p_i += gamma/m dt / n (sum_cell p - p_i), Gauss-Seidel in list order
+__device__ __forceinline__ void cell_mix(const Dev& D, const int* a, int n, double dt, bool backward) {
+    double factor = D.gamma_L / D.atmass * dt / n;
+    for (int q = 0; q < n; ++q) {
+        int i = a[backward ? n - 1 - q : q];
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        for (int m = 0; m < n; ++m) {
+            double4 pm = D.p[a[m]];
+            sx = sx + pm.x; sy = sy + pm.y; sz = sz + pm.z;
+        }
+        double4 p = D.p[i];
+        p.x = p.x + factor * (sx - p.x);
+        p.y = p.y + factor * (sy - p.y);
+        p.z = p.z + factor * (sz - p.z);
+        D.p[i] = p;
+    }
+}
+
+__device__ __forceinline__ void friction(const Dev& D, const int* a, int n, double dt) {
+    double e = D.localcolmot ? exp(-D.gamma_L / D.atmass * dt * (1.0 - 1.0 / n))
+                             : exp(-D.gamma_L / D.atmass * dt);
+    for (int m = 0; m < n; ++m) {
+        double4 p = D.p[a[m]];
+        p.x = e * p.x; p.y = e * p.y; p.z = e * p.z;
+        D.p[a[m]] = p;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_dp_lang(Dev D, double dt, int epoch_off) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double px = 0, py = 0, pz = 0;
+    if (c < D.ncells) {
+        int n = D.cell_count[c];
+        const int* a = D.cell_atoms + D.cell_start[c];
+        if (n > 0) {
+            unsigned long long epoch = D.ctl->epoch + (unsigned long long)epoch_off;
+            if (D.localcolmot) cell_mix(D, a, n, dt / 2.0, false);
+            friction(D, a, n, dt / 2.0);
+            double ax = 0.0, ay = 0.0, az = 0.0;
+            for (int m = 0; m < n; ++m) {            // A: force + noise
+                int i = a[m];
+                double T = D.eltemp ? D.Te[D.node[i]] : D.temperature;
+                double amp = sqrt(2.0 * T * D.gamma_L / dt);
+                double3 xi = normals3(D.seed, 0u, (unsigned)D.id[i], epoch);
+                double fx = amp * xi.x, fy = amp * xi.y, fz = amp * xi.z;
+                double4 f = D.f[i], p = D.p[i];
+                p.x = p.x + dt * (f.x + fx); p.y = p.y + dt * (f.y + fy); p.z = p.z + dt * (f.z + fz);
+                D.p[i] = p;
+                ax = ax + fx; ay = ay + fy; az = az + fz;
+            }
+            if (D.localcolmot) {
+                ax = ax / n; ay = ay / n; az = az / n;
+                for (int m = 0; m < n; ++m) {
+                    double4 p = D.p[a[m]];
+                    p.x = p.x - dt * ax; p.y = p.y - dt * ay; p.z = p.z - dt * az;
+                    D.p[a[m]] = p;
+                }
+            }
+            friction(D, a, n, dt / 2.0);
+            if (D.localcolmot) cell_mix(D, a, n, dt / 2.0, true);
+            for (int m = 0; m < n; ++m) {
+                double4 p = D.p[a[m]];
+                px += p.x; py += p.y; pz += p.z;
+            }
+        }
+    }
+    block_partials3(D, px, py, pz);
+}
+
+__global__ void __launch_bounds__(1024) k_avep(Dev D, int nb) {
+    __shared__ double sh[32];
+    double a = 0, b = 0, c = 0;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+        a += D.red[4 * k]; b += D.red[4 * k + 1]; c += D.red[4 * k + 2];
+    }
+    a = block_sum(a, sh);
+    b = block_sum(b, sh);
+    c = block_sum(c, sh);
+    if (threadIdx.x == 0) {
+        D.ctl->avep[0] = a / D.natom;
+        D.ctl->avep[1] = b / D.natom;
+        D.ctl->avep[2] = c / D.natom;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_ke_partials(Dev D) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double ko = 0, kn = 0;
+    if (i < D.natom) {
+        double4 p = D.p[i];
+        ko = (p.x * p.x + p.y * p.y + p.z * p.z) / 2.0 / D.atmass;
+        double x = p.x - D.ctl->avep[0], y = p.y - D.ctl->avep[1], z = p.z - D.ctl->avep[2];
+        kn = (x * x + y * y + z * z) / 2.0 / D.atmass;
+    }
+    __shared__ double sh[32];
+    double a = block_sum(ko, sh);
+    double b = block_sum(kn, sh);
+    if (threadIdx.x == 0) {
+        D.red[4 * (size_t)blockIdx.x] = a;
+        D.red[4 * (size_t)blockIdx.x + 1] = b;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_factor(Dev D, int nb) {
+    __shared__ double sh[32];
+    double a = 0, b = 0;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) { a += D.red[4 * k]; b += D.red[4 * k + 1]; }
+    a = block_sum(a, sh);
+    b = block_sum(b, sh);
+    if (threadIdx.x == 0) {
+        double factor = sqrt(a / b);
+        if (b < 1e-10) factor = 1.0;
+        D.ctl->ke_factor = factor;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_scale(Dev D) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.natom) return;
+    double k = D.ctl->ke_factor;
+    double4 p = D.p[i];
+    p.x = k * (p.x - D.ctl->avep[0]);
+    p.y = k * (p.y - D.ctl->avep[1]);
+    p.z = k * (p.z - D.ctl->avep[2]);
+    D.p[i] = p;
+    D.ke[i] = (p.x * p.x + p.y * p.y + p.z * p.z) / 2.0 / D.atmass;
+}
+
+__global__ void __launch_bounds__(256) k_dr(Dev D, double dt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.natom) return;
+    double k = dt / D.atmass;
+    double4 r = D.r[i], p = D.p[i];
+    double3 x = periodic(D, make_double3(r.x + k * p.x, r.y + k * p.y, r.z + k * p.z));
+    if (!isfinite(x.x + x.y + x.z)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
+    D.r[i] = make_double4(x.x, x.y, x.z, 0.0);
+}
+
+void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off) {
+    int nb;
+    if (D.lattlang) {
+        nb = div_up(D.ncells, 128);
+        k_dp_lang<<<nb, 128, 0, st>>>(D, dt, epoch_off);
+    } else {
+        nb = div_up(D.natom, 256);
+        k_dp_nve<<<nb, 256, 0, st>>>(D, dt);
+    }
+    k_avep<<<1, 1024, 0, st>>>(D, nb);
+    int na = div_up(D.natom, 256);
+    k_ke_partials<<<na, 256, 0, st>>>(D);
+    k_factor<<<1, 1024, 0, st>>>(D, na);
+    k_scale<<<na, 256, 0, st>>>(D);
+}
+
+void launch_dr(const Dev& D, cudaStream_t st, double dt) {
+    k_dr<<<div_up(D.natom, 256), 256, 0, st>>>(D, dt);
+}

@@ -1,0 +1,557 @@
+// C ABI of the step engine (include/sld.h): context set-up, the reference's
+// step functions as entry points, the CUDA-graph main loop and read-outs.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/sld.h"
+#include "potential.h"
+#include "sld_common.cuh"
+#include "sld_host.h"
+
+namespace {
+
+const double kBoltz = 8.617343e-5;
+const double kLight = 299792458e0;
+const double kUtoeV = 931.494028e6 / kLight / kLight;
+
+#define CK(call)                                                   \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) {                                   \
+            std::fprintf(stderr, "sld: %s failed: %s\n", #call,    \
+                         cudaGetErrorString(e_));                  \
+            return SLD_ERR_CUDA;                                   \
+        }                                                          \
+    } while (0)
+
+}  // namespace
+
+struct sld_ctx {
+    sld_params P{};
+    sld::HostGeom G;
+    std::vector<int> id_of_slot, slot_of_id;
+    Dev D{};
+    std::vector<void*> allocs;
+    int* d_gcells = nullptr;
+    int* d_te_gcells = nullptr;
+    int* d_te_gstart = nullptr;
+    double* d_avg = nullptr;
+    cudaStream_t st = nullptr;
+    cudaGraphExec_t step_graph = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0.0;
+    int scan_blocks = 1;
+    int red_cap = 0;
+
+    template <class T>
+    int alloc(T** p, size_t n) {
+        void* q = nullptr;
+        if (n == 0) n = 1;
+        if (cudaMalloc(&q, n * sizeof(T)) != cudaSuccess) return SLD_ERR_NOMEM;
+        cudaMemset(q, 0, n * sizeof(T));
+        allocs.push_back(q);
+        *p = static_cast<T*>(q);
+        return SLD_OK;
+    }
+};
+
+namespace {
+
+int check_flags(sld_ctx* c) {
+    unsigned err = 0;
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaMemcpy(&err, &c->D.ctl->err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (err & SLD_FLAG_CAPACITY) return SLD_ERR_CAPACITY;
+    if (err & SLD_FLAG_TABLE) return SLD_ERR_TABLE;
+    if (err & SLD_FLAG_NAN) return SLD_ERR_NAN;
+    return SLD_OK;
+}
+
+int launch_status() {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "sld: launch failed: %s\n", cudaGetErrorString(e));
+        return SLD_ERR_CUDA;
+    }
+    return SLD_OK;
+}
+
+// One core_ds call: forward sweep, backward sweep.
+void enqueue_ds(sld_ctx* c, double dt, int& eoff) {
+    const auto& G = c->G;
+    double dt_half = dt / 2e0;
+    for (int g = 0; g < G.ngroups; ++g)
+        launch_sweep64(c->D, c->st, c->d_gcells + G.gstart[g], G.gstart[g + 1] - G.gstart[g],
+                       dt_half, false, eoff);
+    if (c->P.spinlang) ++eoff;
+    for (int g = G.ngroups - 1; g >= 0; --g)
+        launch_sweep64(c->D, c->st, c->d_gcells + G.gstart[g], G.gstart[g + 1] - G.gstart[g],
+                       dt_half, true, eoff);
+    if (c->P.spinlang) ++eoff;
+}
+
+void enqueue_dp(sld_ctx* c, double dt, int& eoff) {
+    launch_dp(c->D, c->st, dt, eoff);
+    if (c->P.lattlang) ++eoff;
+}
+
+// core.cpp:31-76 (spin-lattice branch) plus the main-loop bookkeeping
+void enqueue_step(sld_ctx* c) {
+    double dt = c->P.step;
+    int eoff = 0;
+    launch_links(c->D, c->st, false, c->scan_blocks);
+    if (c->P.eltemp) launch_dte(c->D, c->st, dt / 2e0);
+    enqueue_dp(c, dt / 2e0, eoff);
+    enqueue_ds(c, dt / 2e0, eoff);
+    launch_dr(c->D, c->st, dt);
+    launch_rho64(c->D, c->st);
+    enqueue_ds(c, dt / 2e0, eoff);
+    launch_force64(c->D, c->st);
+    enqueue_dp(c, dt / 2e0, eoff);
+    if (c->P.eltemp) {
+        launch_temperature(c->D, c->st);
+        launch_dte(c->D, c->st, dt / 2e0);
+        if (c->P.renormalize_energy) launch_energy_check(c->D, c->st, 1);
+    }
+    launch_advance(c->D, c->st, eoff, 1);
+}
+
+int validate(const sld_params* p) {
+    if (!p) return SLD_ERR_ARG;
+    if (!(p->box[0] > 0 && p->box[2] > 0 && p->box[5] > 0)) return SLD_ERR_ARG;
+    if (!(p->step > 0) || !(p->atmass > 0) || !(p->temperature >= 0)) return SLD_ERR_ARG;
+    if (!(p->rcut_pot > 0 && p->rcut_mag > 0 && p->rcut_max > 0)) return SLD_ERR_ARG;
+    if (p->rcut_pot > p->rcut_max || p->rcut_mag > p->rcut_max) return SLD_ERR_ARG;
+    if (p->eltemp && !(p->spinlang && p->lattlang)) return SLD_ERR_ARG;
+    if (p->localcolmot && !p->lattlang) return SLD_ERR_ARG;
+    if (p->precision != SLD_FP64 && p->precision != SLD_SPLIT) return SLD_ERR_ARG;
+    if (p->te_mesh != 0 && p->te_mesh < 3) return SLD_ERR_ARG;
+    return SLD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* sld_error_string(int code) {
+    switch (code) {
+    case SLD_OK: return "ok";
+    case SLD_ERR_ARG: return "invalid argument";
+    case SLD_ERR_CUDA: return "CUDA runtime error";
+    case SLD_ERR_GEOMETRY: return "fewer than 3 link cells along an axis";
+    case SLD_ERR_CAPACITY: return "a link cell holds more atoms than supported";
+    case SLD_ERR_TABLE: return "r or rho outside the potential table";
+    case SLD_ERR_NAN: return "non-finite value produced";
+    case SLD_ERR_IO: return "file could not be read";
+    case SLD_ERR_STATE: return "call out of order";
+    case SLD_ERR_NOMEM: return "device allocation failed";
+    default: return "unknown error";
+    }
+}
+
+int sld_params_default(sld_params* o) {
+    if (!o) return SLD_ERR_ARG;
+    std::memset(o, 0, sizeof(*o));
+    o->step = 1e-15;
+    o->temperature = 300e0;
+    o->atmass = 55.847e0;
+    o->gamma_L_over_mass = 6e11;
+    o->gamma_S_HL = 5.88e13;
+    o->rcut_pot = 4.1001;
+    o->rcut_mag = 3.7501;
+    o->rcut_max = 4.1001;
+    o->min_length_link_cell = 4.11;
+    o->kappa_e = 80e0;
+    o->random_seed = 1234;
+    o->te_nloop = 50;
+    o->interval_of_print_out = 1;
+    o->precision = SLD_FP64;
+    return SLD_OK;
+}
+
+int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
+               const double* p, const double* s, const double* te_K) {
+    if (!out || !r || !p || !s || natom <= 0) return SLD_ERR_ARG;
+    *out = nullptr;
+    int rc = validate(prm);
+    if (rc) return rc;
+    sld_ctx* c = new (std::nothrow) sld_ctx();
+    if (!c) return SLD_ERR_NOMEM;
+    c->P = *prm;
+    if (c->P.te_nloop <= 0) c->P.te_nloop = 50;
+    if (c->P.interval_of_print_out <= 0) c->P.interval_of_print_out = 1;
+
+    // geometry, link cells, colour groups, initial order (host)
+    std::vector<double> r0(r, r + 3 * (size_t)natom);
+    rc = sld::setup_geometry(c->P, natom, r0, c->G, c->id_of_slot, c->slot_of_id);
+    if (rc) { delete c; return rc; }
+    const auto& G = c->G;
+
+    if (cudaSetDevice(prm->device) != cudaSuccess) { delete c; return SLD_ERR_CUDA; }
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return SLD_ERR_CUDA;
+    }
+    cudaEventCreate(&c->ev0);
+    cudaEventCreate(&c->ev1);
+
+    sld::Tables T;
+    sld::build_tables(T, G.rcut_max);
+
+    Dev& D = c->D;
+    for (int k = 0; k < 6; ++k) { D.d[k] = G.d[k]; D.inv[k] = G.inv[k]; }
+    for (int k = 0; k < 3; ++k) D.box_len[k] = G.box_len[k];
+    D.box_volume = G.box_volume;
+    D.rcut_pot = prm->rcut_pot;
+    D.rcut_mag = prm->rcut_mag;
+    D.rcut_max = G.rcut_max;
+    D.rcut_pot_sq = prm->rcut_pot * prm->rcut_pot;
+    D.rcut_mag_sq = prm->rcut_mag * prm->rcut_mag;
+    D.rcut_max_sq = G.rcut_max * G.rcut_max;
+    D.atmass = prm->atmass * kUtoeV * (1e-10 * 1e-10);
+    D.temperature = prm->temperature * kBoltz;
+    D.gamma_L = prm->gamma_L_over_mass * D.atmass;
+    D.gamma_S_HL = prm->gamma_S_HL;
+    D.step = prm->step;
+    D.inv_r = T.inv_r;
+    D.inv_rho = T.inv_rho;
+    for (int k = 0; k < 4; ++k) D.landau[k] = T.landau[k];
+    D.kappa_e = prm->kappa_e;
+    D.natom = natom;
+    D.nx = G.nx; D.ny = G.ny; D.nz = G.nz; D.ncells = G.ncells;
+    D.tx = G.tx; D.ty = G.ty; D.tz = G.tz; D.nte = G.nte; D.te_mesh = prm->te_mesh;
+    D.seed = (unsigned)prm->random_seed;
+    D.spinlang = prm->spinlang; D.lattlang = prm->lattlang; D.eltemp = prm->eltemp;
+    D.localcolmot = prm->localcolmot; D.renormalize = prm->renormalize_energy;
+    D.print_every = c->P.interval_of_print_out;
+    D.te_nloop = c->P.te_nloop;
+
+    size_t n = (size_t)natom;
+    double* tabs[sld::kTabCount];
+    bool ok = true;
+    for (int k = 0; k < sld::kTabCount; ++k) {
+        ok = ok && c->alloc(&tabs[k], sld::kNInput) == SLD_OK;
+        if (ok) cudaMemcpy(tabs[k], T.t[k].data(), sizeof(double) * sld::kNInput, cudaMemcpyHostToDevice);
+    }
+    if (!ok) { sld_destroy(c); return SLD_ERR_NOMEM; }
+    D.tF = tabs[sld::kF]; D.tdF = tabs[sld::kdF]; D.tf = tabs[sld::kf]; D.tdf = tabs[sld::kdf];
+    D.tphi = tabs[sld::kPhi]; D.tdphi = tabs[sld::kdPhi]; D.tJ = tabs[sld::kJ]; D.tdJ = tabs[sld::kdJ];
+
+    ok = c->alloc(&D.r, n) == 0 && c->alloc(&D.p, n) == 0 && c->alloc(&D.f, n) == 0 &&
+         c->alloc(&D.s, n) == 0 && c->alloc(&D.H, n) == 0 && c->alloc(&D.HL, n) == 0 &&
+         c->alloc(&D.rho, n) == 0 && c->alloc(&D.pe, n) == 0 && c->alloc(&D.ke, n) == 0 &&
+         c->alloc(&D.me, n) == 0 && c->alloc(&D.me0, n) == 0 && c->alloc(&D.vir, n) == 0 &&
+         c->alloc(&D.sumJ, n) == 0 && c->alloc(&D.stress, 6 * n) == 0 &&
+         c->alloc(&D.cell_of, n) == 0 && c->alloc(&D.id, n) == 0 && c->alloc(&D.stamp, n) == 0 &&
+         c->alloc(&D.cell_start, (size_t)G.ncells) == 0 &&
+         c->alloc(&D.cell_count, (size_t)G.ncells) == 0 &&
+         c->alloc(&D.cell_atoms, n) == 0 && c->alloc(&D.cell_fill, (size_t)G.ncells) == 0;
+    c->scan_blocks = div_up(G.ncells, 1024);
+    ok = ok && c->alloc(&D.scan_tmp, (size_t)c->scan_blocks) == 0;
+    if (prm->te_mesh > 0) {
+        ok = ok && c->alloc(&D.node, n) == 0 && c->alloc(&D.te_count, (size_t)G.nte) == 0;
+    } else {
+        D.node = D.cell_of;
+        D.te_count = D.cell_count;
+    }
+    int nte = G.nte;
+    ok = ok && c->alloc(&D.Te, nte) == 0 && c->alloc(&D.Ee, nte) == 0 && c->alloc(&D.Tl, nte) == 0 &&
+         c->alloc(&D.TsR, nte) == 0 && c->alloc(&D.TsL, nte) == 0 && c->alloc(&D.Gel, nte) == 0 &&
+         c->alloc(&D.Ges, nte) == 0 && c->alloc(&D.acc, 9 * (size_t)nte) == 0;
+    c->red_cap = std::max(div_up(natom, 128), div_up(G.ncells, 128)) + 8;
+    ok = ok && c->alloc(&D.red, 8 * (size_t)c->red_cap) == 0;
+    ok = ok && c->alloc(&D.ctl, 1) == 0 && c->alloc(&c->d_avg, 16) == 0;
+    ok = ok && c->alloc(&c->d_gcells, (size_t)G.ncells) == 0;
+    ok = ok && c->alloc(&c->d_te_gcells, (size_t)nte) == 0 &&
+         c->alloc(&c->d_te_gstart, G.te_gstart.size()) == 0;
+    if (!ok) { sld_destroy(c); return SLD_ERR_NOMEM; }
+    cudaMemcpy(c->d_gcells, G.gcells.data(), sizeof(int) * G.ncells, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->d_te_gcells, G.te_gcells.data(), sizeof(int) * nte, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->d_te_gstart, G.te_gstart.data(), sizeof(int) * G.te_gstart.size(),
+               cudaMemcpyHostToDevice);
+    D.te_gcells = c->d_te_gcells;
+    D.te_gstart = c->d_te_gstart;
+    D.te_ngroups = G.te_ngroups;
+
+    // Te per Te cell (map_cells.cpp:128-158), stored in eV as the reference does
+    std::vector<double> te(nte);
+    for (int k = 0; k < nte; ++k) te[k] = te_K ? te_K[k] * kBoltz : D.temperature;
+    cudaMemcpy(D.Te, te.data(), sizeof(double) * nte, cudaMemcpyHostToDevice);
+    std::vector<int> idv(c->id_of_slot);
+    cudaMemcpy(D.id, idv.data(), sizeof(int) * n, cudaMemcpyHostToDevice);
+    // the set-up copies and memsets above ran on the default stream; the
+    // engine's own stream does not order against it
+    if (cudaDeviceSynchronize() != cudaSuccess) { sld_destroy(c); return SLD_ERR_CUDA; }
+
+    rc = sld_set_state(c, r0.data(), p, s);
+    if (rc) { sld_destroy(c); return rc; }
+    *out = c;
+    return SLD_OK;
+}
+
+int sld_set_state(sld_ctx* c, const double* r, const double* p, const double* s) {
+    if (!c || !r || !p || !s) return SLD_ERR_ARG;
+    Dev& D = c->D;
+    size_t n = (size_t)D.natom;
+    std::vector<double4> hr(n), hp(n), hs(n);
+    std::vector<double> hke(n);
+    double m = D.atmass;
+    for (size_t k = 0; k < n; ++k) {
+        int i = c->id_of_slot[k];
+        double x = r[3 * i], y = r[3 * i + 1], z = r[3 * i + 2];
+        sld::host_periodic(c->G, x, y, z);
+        hr[k] = make_double4(x, y, z, 0.0);
+        hp[k] = make_double4(p[3 * i], p[3 * i + 1], p[3 * i + 2], 0.0);
+        double sx = s[3 * i], sy = s[3 * i + 1], sz = s[3 * i + 2];
+        hs[k] = make_double4(sx, sy, sz, std::sqrt(sx * sx + sy * sy + sz * sz));
+        double px = p[3 * i], py = p[3 * i + 1], pz = p[3 * i + 2];
+        hke[k] = (px * px + py * py + pz * pz) / 2e0 / m;
+    }
+    CK(cudaMemcpyAsync(D.r, hr.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(D.p, hp.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(D.s, hs.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(D.ke, hke.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+    Ctl z{};
+    CK(cudaMemcpyAsync(D.ctl, &z, sizeof(Ctl), cudaMemcpyHostToDevice, c->st));
+    // initialize(): links, rho, forces, cell temperatures, reference energy
+    launch_links(D, c->st, true, c->scan_blocks);
+    launch_rho64(D, c->st);
+    launch_force64(D, c->st);
+    if (c->P.eltemp) {
+        launch_temperature(D, c->st);
+        if (c->P.renormalize_energy) launch_energy_check(D, c->st, 0);
+    }
+    int rc = launch_status();
+    if (rc) return rc;
+    return check_flags(c);
+}
+
+void sld_destroy(sld_ctx* c) {
+    if (!c) return;
+    if (c->st) cudaStreamSynchronize(c->st);
+    if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+    for (void* q : c->allocs) cudaFree(q);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+}
+
+int sld_links(sld_ctx* c) {
+    if (!c) return SLD_ERR_ARG;
+    launch_links(c->D, c->st, false, c->scan_blocks);
+    return launch_status();
+}
+
+int sld_calculate_rho(sld_ctx* c) {
+    if (!c) return SLD_ERR_ARG;
+    launch_rho64(c->D, c->st);
+    return launch_status();
+}
+
+int sld_calculate_force_energy(sld_ctx* c) {
+    if (!c) return SLD_ERR_ARG;
+    launch_force64(c->D, c->st);
+    return launch_status();
+}
+
+int sld_core_ds(sld_ctx* c, double dt) {
+    if (!c) return SLD_ERR_ARG;
+    int eoff = 0;
+    enqueue_ds(c, dt, eoff);
+    launch_advance(c->D, c->st, eoff, 0);
+    return launch_status();
+}
+
+int sld_core_dp(sld_ctx* c, double dt) {
+    if (!c) return SLD_ERR_ARG;
+    int eoff = 0;
+    enqueue_dp(c, dt, eoff);
+    launch_advance(c->D, c->st, eoff, 0);
+    return launch_status();
+}
+
+int sld_core_dr(sld_ctx* c, double dt) {
+    if (!c) return SLD_ERR_ARG;
+    launch_dr(c->D, c->st, dt);
+    return launch_status();
+}
+
+int sld_core_dTe(sld_ctx* c, double dt) {
+    if (!c) return SLD_ERR_ARG;
+    if (!c->P.eltemp) return SLD_OK;
+    launch_dte(c->D, c->st, dt);
+    return launch_status();
+}
+
+int sld_calculate_temperature(sld_ctx* c) {
+    if (!c) return SLD_ERR_ARG;
+    if (!c->P.eltemp) return SLD_OK;
+    launch_temperature(c->D, c->st);
+    return launch_status();
+}
+
+int sld_run(sld_ctx* c, int nsteps) {
+    if (!c || nsteps < 0) return SLD_ERR_ARG;
+    if (!c->step_graph) {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+        enqueue_step(c);
+        CK(cudaStreamEndCapture(c->st, &g));
+        CK(cudaGraphInstantiate(&c->step_graph, g, 0));
+        cudaGraphDestroy(g);
+    }
+    CK(cudaEventRecord(c->ev0, c->st));
+    for (int k = 0; k < nsteps; ++k) CK(cudaGraphLaunch(c->step_graph, c->st));
+    CK(cudaEventRecord(c->ev1, c->st));
+    return SLD_OK;
+}
+
+int sld_last_run_ms(sld_ctx* c, double* out) {
+    if (!c || !out) return SLD_ERR_ARG;
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    *out = ms;
+    return SLD_OK;
+}
+
+int sld_sync(sld_ctx* c) {
+    if (!c) return SLD_ERR_ARG;
+    int rc = launch_status();
+    if (rc) return rc;
+    return check_flags(c);
+}
+
+long sld_get(sld_ctx* c, const char* field, double* out, long cap) {
+    if (!c || !field || !out) return SLD_ERR_ARG;
+    Dev& D = c->D;
+    size_t n = (size_t)D.natom;
+    std::string f(field);
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return SLD_ERR_CUDA;
+    auto vec4 = [&](double4* src) -> long {
+        if (cap < (long)(3 * n)) return SLD_ERR_ARG;
+        std::vector<double4> h(n);
+        if (cudaMemcpy(h.data(), src, sizeof(double4) * n, cudaMemcpyDeviceToHost)) return SLD_ERR_CUDA;
+        for (size_t k = 0; k < n; ++k) {
+            int i = c->id_of_slot[k];
+            out[3 * i] = h[k].x; out[3 * i + 1] = h[k].y; out[3 * i + 2] = h[k].z;
+        }
+        return (long)(3 * n);
+    };
+    auto scal = [&](double* src, int width) -> long {
+        if (cap < (long)(width * n)) return SLD_ERR_ARG;
+        std::vector<double> h(width * n);
+        if (cudaMemcpy(h.data(), src, sizeof(double) * width * n, cudaMemcpyDeviceToHost)) return SLD_ERR_CUDA;
+        for (size_t k = 0; k < n; ++k) {
+            int i = c->id_of_slot[k];
+            for (int w = 0; w < width; ++w) out[(size_t)width * i + w] = h[(size_t)width * k + w];
+        }
+        return (long)(width * n);
+    };
+    auto percell = [&](double* src, double scale) -> long {
+        size_t m = (size_t)D.nte;
+        if (cap < (long)m) return SLD_ERR_ARG;
+        if (cudaMemcpy(out, src, sizeof(double) * m, cudaMemcpyDeviceToHost)) return SLD_ERR_CUDA;
+        for (size_t k = 0; k < m; ++k) out[k] *= scale;
+        return (long)m;
+    };
+    if (f == "r") return vec4(D.r);
+    if (f == "p") return vec4(D.p);
+    if (f == "f") return vec4(D.f);
+    if (f == "s") return vec4(D.s);
+    if (f == "H") return vec4(D.H);
+    if (f == "HL") return vec4(D.HL);
+    if (f == "s0") {
+        if (cap < (long)n) return SLD_ERR_ARG;
+        std::vector<double4> h(n);
+        if (cudaMemcpy(h.data(), D.s, sizeof(double4) * n, cudaMemcpyDeviceToHost)) return SLD_ERR_CUDA;
+        for (size_t k = 0; k < n; ++k) out[c->id_of_slot[k]] = h[k].w;
+        return (long)n;
+    }
+    if (f == "rho") return scal(D.rho, 1);
+    if (f == "pe") return scal(D.pe, 1);
+    if (f == "ke") return scal(D.ke, 1);
+    if (f == "me") return scal(D.me, 1);
+    if (f == "me0") return scal(D.me0, 1);
+    if (f == "vir") return scal(D.vir, 1);
+    if (f == "sum_Jij_sj" || f == "sumJ") return scal(D.sumJ, 1);
+    if (f == "stress") return scal(D.stress, 6);
+    if (f == "local_volume") {
+        if (cap < (long)n) return SLD_ERR_ARG;
+        for (size_t k = 0; k < n; ++k) out[k] = D.box_volume / D.natom;
+        return (long)n;
+    }
+    if (f == "cell" || f == "node") {
+        if (cap < (long)n) return SLD_ERR_ARG;
+        std::vector<int> h(n);
+        int* src = f == "cell" ? D.cell_of : D.node;
+        if (cudaMemcpy(h.data(), src, sizeof(int) * n, cudaMemcpyDeviceToHost)) return SLD_ERR_CUDA;
+        for (size_t k = 0; k < n; ++k) out[c->id_of_slot[k]] = h[k];
+        return (long)n;
+    }
+    if (f == "Te") return percell(D.Te, 1.0 / kBoltz);
+    if (f == "Ee") return percell(D.Ee, 1.0);
+    if (f == "Tl") return percell(D.Tl, 1.0);
+    if (f == "Ts_R") return percell(D.TsR, 1.0);
+    if (f == "Ts_L") return percell(D.TsL, 1.0);
+    if (f == "Gel") return percell(D.Gel, 1.0);
+    if (f == "Ges") return percell(D.Ges, 1.0);
+    if (f == "count") {
+        size_t m = (size_t)D.nte;
+        if (cap < (long)m) return SLD_ERR_ARG;
+        std::vector<int> h(m);
+        if (cudaMemcpy(h.data(), D.te_count, sizeof(int) * m, cudaMemcpyDeviceToHost)) return SLD_ERR_CUDA;
+        for (size_t k = 0; k < m; ++k) out[k] = h[k];
+        return (long)m;
+    }
+    return SLD_ERR_ARG;
+}
+
+int sld_get_cell_lists(sld_ctx* c, int* out) {
+    if (!c || !out) return SLD_ERR_ARG;
+    size_t n = (size_t)c->D.natom;
+    CK(cudaStreamSynchronize(c->st));
+    std::vector<int> h(n);
+    CK(cudaMemcpy(h.data(), c->D.cell_atoms, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    for (size_t k = 0; k < n; ++k) out[k] = c->id_of_slot[h[k]];
+    return SLD_OK;
+}
+
+int sld_averages(sld_ctx* c, double* out10) {
+    if (!c || !out10) return SLD_ERR_ARG;
+    launch_averages(c->D, c->st, c->d_avg);
+    CK(cudaMemcpyAsync(out10, c->d_avg, sizeof(double) * 10, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return launch_status();
+}
+
+int sld_virial(sld_ctx* c, double* out) {
+    if (!c || !out) return SLD_ERR_ARG;
+    launch_virial(c->D, c->st);
+    CK(cudaMemcpyAsync(out, &c->D.ctl->virial, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return SLD_OK;
+}
+
+int sld_total_time(sld_ctx* c, double* out) {
+    if (!c || !out) return SLD_ERR_ARG;
+    CK(cudaMemcpyAsync(out, &c->D.ctl->total_time, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return SLD_OK;
+}
+
+int sld_info(sld_ctx* c, int* o) {
+    if (!c || !o) return SLD_ERR_ARG;
+    o[0] = c->D.natom; o[1] = c->G.ncells; o[2] = c->G.ngroups; o[3] = c->G.nte;
+    o[4] = c->G.nx; o[5] = c->G.ny;
+    return SLD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,230 @@
+// Device state and helpers shared by the engine's kernels.
+//
+// Layout in HBM (one system; atoms stored in "slots" sorted by link cell at
+// load time, the caller's atom index kept in `id`):
+//   r, p, f, s, H, HL : double4 per atom (s.w = |s|, the reference's s0)
+//   rho, pe, ke, me, me0, vir, sumJ : double per atom; stress: 6 per atom
+//   cell_of, id, node : int per atom; stamp : int64 insertion key per atom
+//   cell_start/count/atoms : CSR cell member lists in the reference's
+//     linked-list order (head -> tail), rebuilt by links each step
+//   Te ... Ges : double per Te cell (link cell, or a decoupled mesh node)
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define SLD_NINPUT 1000000
+#define SLD_BOLTZ 8.617343e-5
+#define SLD_HBAR 6.58211899e-16
+#define SLD_EVTOJ 1.602176487e-19
+#define SLD_MAXC 64   // == SLD_MAX_CELL_ATOMS in sld.h
+
+// error flag bits in Ctl::err
+#define SLD_FLAG_CAPACITY 1u
+#define SLD_FLAG_TABLE 2u
+#define SLD_FLAG_NAN 4u
+
+struct Ctl {
+    unsigned long long epoch;     // Philox counter: one per noise-drawing sweep
+    long long links_calls;        // stamps of relinked atoms
+    long long steps;              // main-loop steps done
+    unsigned int err;
+    int pad;
+    double initial_ave_energy;
+    double total_time;
+    double avep[3];
+    double ke_factor;
+    double virial;
+    double avg[8];                // last energy averages
+};
+
+struct Dev {
+    // box (struct.h box_vector order: xx yx yy zx zy zz) and inverse
+    double d[6], inv[6];
+    double box_len[3], box_volume;
+    double rcut_pot, rcut_mag, rcut_max, rcut_pot_sq, rcut_mag_sq, rcut_max_sq;
+    double atmass, temperature, gamma_L, gamma_S_HL, step;
+    double inv_r, inv_rho;
+    double landau[4];             // A B C D (the reference's tables are constant)
+    double kappa_e;
+    int natom, nx, ny, nz, ncells;
+    int tx, ty, tz, nte, te_mesh;
+    unsigned seed;
+    int spinlang, lattlang, eltemp, localcolmot, renormalize, print_every;
+    int te_nloop;
+    // tables (potential_CPU.cpp:61-157): F, F', f, f', phi, phi', J, J'
+    const double *tF, *tdF, *tf, *tdf, *tphi, *tdphi, *tJ, *tdJ;
+    // atoms
+    double4 *r, *p, *f, *s, *H, *HL;
+    double *rho, *pe, *ke, *me, *me0, *vir, *sumJ, *stress;
+    int *cell_of, *id, *node;
+    long long* stamp;
+    // cells
+    int *cell_start, *cell_count, *cell_atoms, *cell_fill, *scan_tmp;
+    // Te cells
+    double *Te, *Ee, *Tl, *TsR, *TsL, *Gel, *Ges, *acc;   // acc: 9 per Te cell
+    int* te_count;
+    const int *te_gcells, *te_gstart;
+    int te_ngroups;
+    // control and reduction scratch
+    Ctl* ctl;
+    double* red;                  // partial sums
+    int red_blocks;
+};
+
+// ---------------------------------------------------------------------
+// geometry: periodic_CPU.cpp:31-50, find_image_CPU.cpp:31-53
+
+__device__ __forceinline__ double3 to_frac(const Dev& D, double x, double y, double z) {
+    return make_double3(D.inv[0] * x + D.inv[1] * y + D.inv[3] * z,
+                        D.inv[2] * y + D.inv[4] * z, D.inv[5] * z);
+}
+__device__ __forceinline__ double3 to_cart(const Dev& D, double3 q) {
+    return make_double3(D.d[0] * q.x + D.d[1] * q.y + D.d[3] * q.z,
+                        D.d[2] * q.y + D.d[4] * q.z, D.d[5] * q.z);
+}
+// The reference truncates toward zero, so slightly negative fractional
+// coordinates stay negative; kept as is.
+__device__ __forceinline__ double3 periodic(const Dev& D, double3 r) {
+    double3 q = to_frac(D, r.x, r.y, r.z);
+    int idx = 0;
+    if (q.x < 0.0 || q.x >= 1.0) { q.x -= (double)(int)q.x; ++idx; }
+    if (q.y < 0.0 || q.y >= 1.0) { q.y -= (double)(int)q.y; ++idx; }
+    if (q.z < 0.0 || q.z >= 1.0) { q.z -= (double)(int)q.z; ++idx; }
+    return idx ? to_cart(D, q) : r;
+}
+__device__ __forceinline__ double3 find_image(const Dev& D, double3 rij) {
+    double3 q = to_frac(D, rij.x, rij.y, rij.z);
+    int idx = 0;
+    if (q.x < -0.5) { q.x += 1.0; ++idx; }
+    if (q.x >= 0.5) { q.x -= 1.0; ++idx; }
+    if (q.y < -0.5) { q.y += 1.0; ++idx; }
+    if (q.y >= 0.5) { q.y -= 1.0; ++idx; }
+    if (q.z < -0.5) { q.z += 1.0; ++idx; }
+    if (q.z >= 0.5) { q.z -= 1.0; ++idx; }
+    return idx ? to_cart(D, q) : rij;
+}
+
+// The 26 neighbour cells in the order of map_cells.cpp:96-121 (offsets in
+// x, y, z), then the cell itself.
+static __constant__ signed char kNbr[27][3] = {
+    {1, 0, 0},  {1, 1, 0},   {0, 1, 0},  {-1, 1, 0},  {1, 0, -1},  {1, 1, -1},  {0, 1, -1},
+    {-1, 1, -1}, {1, 0, 1},  {1, 1, 1},  {0, 1, 1},   {-1, 1, 1},  {0, 0, 1},   {-1, 0, 0},
+    {0, -1, 0}, {0, 0, -1},  {1, -1, 0}, {-1, -1, 0}, {-1, 0, 1},  {-1, 0, -1}, {0, -1, 1},
+    {0, -1, -1}, {1, -1, 1}, {1, -1, -1}, {-1, -1, 1}, {-1, -1, -1}, {0, 0, 0}};
+
+__device__ __forceinline__ int nbr_cell(const Dev& D, int cx, int cy, int cz, int k) {
+    int x = cx + kNbr[k][0], y = cy + kNbr[k][1], z = cz + kNbr[k][2];
+    x = x < 0 ? x + D.nx : (x >= D.nx ? x - D.nx : x);
+    y = y < 0 ? y + D.ny : (y >= D.ny ? y - D.ny : y);
+    z = z < 0 ? z + D.nz : (z >= D.nz ? z - D.nz : z);
+    return x + (y + z * D.ny) * D.nx;
+}
+
+// potential_CPU.cpp:172-179: linear interpolation between entries n-1 and n
+// of a 10^6-point table at x_n = (n+1) max / 10^6.  Out-of-range indices are
+// clamped and flagged (the reference reads out of bounds).
+__device__ __forceinline__ double interp(const double* __restrict__ t, double x, double inv,
+                                         unsigned* err) {
+    double fn = x * inv;
+    int n = (int)fn;
+    if (n < 1 || n >= SLD_NINPUT) {
+        atomicOr(err, SLD_FLAG_TABLE);
+        n = n < 1 ? 1 : SLD_NINPUT - 1;
+    }
+    double ratio = (double)(n + 1) - fn;
+    return __ldg(t + n - 1) * ratio + __ldg(t + n) * (1.0 - ratio);
+}
+// the same for a table whose every entry is c
+__device__ __forceinline__ double interp_const(double c, double x, double inv) {
+    double fn = x * inv;
+    int n = (int)fn;
+    double ratio = (double)(n + 1) - fn;
+    return c * ratio + c * (1.0 - ratio);
+}
+
+// ---------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11).  Counter (atom id,
+// epoch lo, epoch hi, tag), key (seed, replica).  One call gives 4 uniforms
+// u = (x + 0.5) 2^-32 and two Box-Muller pairs; three normals are used.
+
+__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int round = 0; round < 10; ++round) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c[0]), lo0 = 0xD2511F53u * c[0];
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]), lo1 = 0xCD9E8D57u * c[2];
+        uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+}
+
+__device__ __forceinline__ double3 normals3(unsigned seed, unsigned replica, unsigned atom,
+                                            unsigned long long epoch) {
+    uint32_t c[4] = {atom, (uint32_t)epoch, (uint32_t)(epoch >> 32), 0x53504e53u};
+    philox4x32_10(c, seed, replica);
+    const double s = 2.3283064365386963e-10;
+    double u0 = ((double)c[0] + 0.5) * s, u1 = ((double)c[1] + 0.5) * s;
+    double u2 = ((double)c[2] + 0.5) * s, u3 = ((double)c[3] + 0.5) * s;
+    double ra = sqrt(-2.0 * log(u0)), rb = sqrt(-2.0 * log(u2));
+    double sa, ca, sb, cb;
+    sincos(6.283185307179586 * u1, &sa, &ca);
+    sincos(6.283185307179586 * u3, &sb, &cb);
+    (void)sb;
+    return make_double3(ra * ca, ra * sa, rb * cb);
+}
+
+// ---------------------------------------------------------------------
+// heat capacity of the electrons: heatcapacity_CPU.cpp:34-57
+__device__ __forceinline__ double te_Ce(double Te) {
+    const double a = 3.0, b = 2e-4 / SLD_BOLTZ;
+    return a * tanh(b * Te);
+}
+__device__ __forceinline__ double te_to_Ee(double Te) {
+    const double a = 3.0, b = 2e-4 / SLD_BOLTZ;
+    return a / b * log(cosh(b * Te));
+}
+__device__ __forceinline__ double Ee_to_te(double Ee) {
+    const double a = 3.0, b = 2e-4 / SLD_BOLTZ;
+    return acosh(exp(b / a * Ee)) / b;
+}
+
+// ---------------------------------------------------------------------
+// reductions (deterministic: fixed shuffle tree, fixed block order)
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+// sums v over the block; result valid in thread 0.  `sh` holds >= 32 doubles.
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (w == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        t = lane < nw ? sh[lane] : 0.0;
+        t = warp_sum(t);
+    }
+    return t;
+}
+
+static inline int div_up(long a, long b) { return (int)((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------
+// launch wrappers (host), one file per kernel family
+void launch_links(const Dev& D, cudaStream_t st, bool initial, int scan_blocks);
+void launch_rho64(const Dev& D, cudaStream_t st);
+void launch_force64(const Dev& D, cudaStream_t st);
+void launch_sweep64(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g, double dt,
+                    bool backward, int epoch_off);
+void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off);
+void launch_dr(const Dev& D, cudaStream_t st, double dt);
+void launch_temperature(const Dev& D, cudaStream_t st);
+void launch_dte(const Dev& D, cudaStream_t st, double dt);
+void launch_energy_check(const Dev& D, cudaStream_t st, int mode);
+void launch_advance(const Dev& D, cudaStream_t st, int epochs, int steps);
+void launch_averages(const Dev& D, cudaStream_t st, double* out_dev);
+void launch_virial(const Dev& D, cudaStream_t st);

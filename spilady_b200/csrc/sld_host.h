@@ -1,0 +1,32 @@
+// Host-side geometry: box, link cells, colour groups, the initial atom order.
+#pragma once
+#include <vector>
+
+#include "../../include/sld.h"
+
+namespace sld {
+
+struct HostGeom {
+    double d[6], inv[6], box_len[3], box_volume;
+    double rcut_max, min_len;
+    int nx, ny, nz, ncells;
+    int tx, ty, tz, nte;
+    int ngroups, te_ngroups;
+    std::vector<int> gstart, gcells;        // link-cell colour groups
+    std::vector<int> te_gstart, te_gcells;  // Te-cell colour groups
+};
+
+// Fills G from the parameters; id_of_slot / slot_of_id give the storage
+// order (atoms sorted by initial link cell, each cell in the reference's
+// initial list order).  r is not modified.
+int setup_geometry(const sld_params& P, int natom, const std::vector<double>& r, HostGeom& G,
+                   std::vector<int>& id_of_slot, std::vector<int>& slot_of_id);
+
+// periodic_CPU.cpp:31-50 on the host
+void host_periodic(const HostGeom& G, double& x, double& y, double& z);
+
+// allocate_cells_CPU.cpp:33-125: greedy colouring of an nx*ny*nz periodic
+// grid with the 26-neighbour stencil, cells scanned in index order
+int colour_grid(int nx, int ny, int nz, std::vector<int>& gstart, std::vector<int>& gcells);
+
+}  // namespace sld

@@ -1,0 +1,221 @@
+"""Python binding of the C ABI in include/sld.h.
+
+``Engine`` mirrors the reference's step functions by name (links,
+calculate_rho, calculate_force_energy, core_ds, core_dp, core_dr, core_dTe,
+calculate_temperature, core) over one device context.  The CUDA library is
+required: importing works without it, but creating an Engine fails loudly
+when ``spilady_b200/_lib/libsld_b200.so`` is missing or no GPU is present.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libsld_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "sld.h")
+
+FP64, SPLIT = 0, 1
+
+ERRORS = {
+    -1: "SLD_ERR_ARG", -2: "SLD_ERR_CUDA", -3: "SLD_ERR_GEOMETRY",
+    -4: "SLD_ERR_CAPACITY", -5: "SLD_ERR_TABLE", -6: "SLD_ERR_NAN",
+    -7: "SLD_ERR_IO", -8: "SLD_ERR_STATE", -9: "SLD_ERR_NOMEM",
+}
+
+
+class SldError(RuntimeError):
+    def __init__(self, code, where):
+        self.code = code
+        super().__init__(f"{where}: {ERRORS.get(code, code)}")
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("box", C.c_double * 6), ("step", C.c_double),
+        ("temperature", C.c_double), ("atmass", C.c_double),
+        ("gamma_L_over_mass", C.c_double), ("gamma_S_HL", C.c_double),
+        ("rcut_pot", C.c_double), ("rcut_mag", C.c_double),
+        ("rcut_max", C.c_double), ("min_length_link_cell", C.c_double),
+        ("kappa_e", C.c_double), ("random_seed", C.c_int),
+        ("spinlang", C.c_int), ("lattlang", C.c_int), ("eltemp", C.c_int),
+        ("localcolmot", C.c_int), ("renormalize_energy", C.c_int),
+        ("te_mesh", C.c_int), ("te_nloop", C.c_int),
+        ("interval_of_print_out", C.c_int), ("precision", C.c_int),
+        ("device", C.c_int),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load the engine library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} not built: run make -C spilady_b200/csrc")
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER(C.c_double)
+        vp = C.c_void_p
+        L.sld_params_default.argtypes = [C.POINTER(Params)]
+        L.sld_read_variables.argtypes = [C.c_char_p, C.POINTER(Params)]
+        L.sld_create.argtypes = [C.POINTER(vp), C.POINTER(Params), C.c_int, P, P, P, P]
+        L.sld_create_from_config.argtypes = [C.POINTER(vp), C.POINTER(Params),
+                                             C.c_char_p, C.c_char_p]
+        L.sld_destroy.argtypes = [vp]
+        L.sld_destroy.restype = None
+        L.sld_set_state.argtypes = [vp, P, P, P]
+        for n in ("sld_links", "sld_calculate_rho", "sld_calculate_force_energy",
+                  "sld_calculate_temperature", "sld_sync"):
+            getattr(L, n).argtypes = [vp]
+        for n in ("sld_core_ds", "sld_core_dp", "sld_core_dr", "sld_core_dTe"):
+            getattr(L, n).argtypes = [vp, C.c_double]
+        L.sld_run.argtypes = [vp, C.c_int]
+        L.sld_get.argtypes = [vp, C.c_char_p, P, C.c_long]
+        L.sld_get.restype = C.c_long
+        L.sld_get_cell_lists.argtypes = [vp, C.POINTER(C.c_int)]
+        L.sld_averages.argtypes = [vp, P]
+        L.sld_info.argtypes = [vp, C.POINTER(C.c_int)]
+        L.sld_virial.argtypes = [vp, P]
+        L.sld_total_time.argtypes = [vp, P]
+        L.sld_last_run_ms.argtypes = [vp, P]
+        L.sld_error_string.argtypes = [C.c_int]
+        L.sld_error_string.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _check(rc, where):
+    if rc != 0:
+        raise SldError(rc, where)
+
+
+def make_params(params, *, spinlang=False, lattlang=False, eltemp=False,
+                localcolmot=False, renormalize=False, te_mesh=0, te_nloop=50,
+                precision=FP64, device=0, interval_of_print_out=1):
+    """sld_params from a variables.in-style dict plus the control switches."""
+    P = Params()
+    lib().sld_params_default(C.byref(P))
+    P.box[:] = list(params["box"])
+    for k in ("step", "temperature", "atmass", "gamma_L_over_mass",
+              "gamma_S_HL", "rcut_pot", "rcut_mag", "rcut_max",
+              "min_length_link_cell", "kappa_e"):
+        if k in params:
+            setattr(P, k, float(params[k]))
+    P.random_seed = int(params.get("random_seed", 1234))
+    P.spinlang, P.lattlang, P.eltemp = int(spinlang), int(lattlang), int(eltemp)
+    P.localcolmot, P.renormalize_energy = int(localcolmot), int(renormalize)
+    P.te_mesh, P.te_nloop = int(te_mesh), int(te_nloop)
+    P.precision, P.device = int(precision), int(device)
+    P.interval_of_print_out = int(interval_of_print_out)
+    return P
+
+
+VEC_FIELDS = {"r": 3, "p": 3, "f": 3, "s": 3, "H": 3, "HL": 3, "stress": 6}
+CELL_FIELDS = ("Te", "Ee", "Tl", "Ts_R", "Ts_L", "Gel", "Ges", "count")
+
+
+class Engine:
+    """One spin-lattice system on one GPU."""
+
+    def __init__(self, params, r, p, s, te=None, **switches):
+        L = lib()
+        self.L = L
+        self.P = make_params(params, **switches)
+        r = np.ascontiguousarray(r, np.float64).reshape(-1, 3)
+        p = np.ascontiguousarray(p, np.float64).reshape(-1, 3)
+        s = np.ascontiguousarray(s, np.float64).reshape(-1, 3)
+        self.natom = r.shape[0]
+        te_arr = None if te is None else np.ascontiguousarray(te, np.float64)
+        h = C.c_void_p()
+        _check(L.sld_create(C.byref(h), C.byref(self.P), self.natom, _dp(r),
+                            _dp(p), _dp(s), None if te_arr is None else _dp(te_arr)),
+               "sld_create")
+        self.h = h
+        info = (C.c_int * 6)()
+        _check(L.sld_info(self.h, info), "sld_info")
+        self.ncells, self.ngroups, self.nte = info[1], info[2], info[3]
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.sld_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    # the reference's step functions
+    def links(self): _check(self.L.sld_links(self.h), "links")
+    def calculate_rho(self): _check(self.L.sld_calculate_rho(self.h), "calculate_rho")
+    def calculate_force_energy(self):
+        _check(self.L.sld_calculate_force_energy(self.h), "calculate_force_energy")
+    def calculate_temperature(self):
+        _check(self.L.sld_calculate_temperature(self.h), "calculate_temperature")
+    def core_ds(self, dt): _check(self.L.sld_core_ds(self.h, dt), "core_ds")
+    def core_dp(self, dt): _check(self.L.sld_core_dp(self.h, dt), "core_dp")
+    def core_dr(self, dt): _check(self.L.sld_core_dr(self.h, dt), "core_dr")
+    def core_dTe(self, dt): _check(self.L.sld_core_dTe(self.h, dt), "core_dTe")
+
+    def run(self, nsteps):
+        _check(self.L.sld_run(self.h, int(nsteps)), "run")
+
+    def core(self):
+        self.run(1)
+
+    def sync(self):
+        _check(self.L.sld_sync(self.h), "sync")
+
+    def set_state(self, r, p, s):
+        r = np.ascontiguousarray(r, np.float64)
+        p = np.ascontiguousarray(p, np.float64)
+        s = np.ascontiguousarray(s, np.float64)
+        _check(self.L.sld_set_state(self.h, _dp(r), _dp(p), _dp(s)), "set_state")
+
+    def get(self, name):
+        width = VEC_FIELDS.get(name, 1)
+        n = (self.nte if name in CELL_FIELDS else self.natom) * width
+        out = np.empty(n, np.float64)
+        got = self.L.sld_get(self.h, name.encode(), _dp(out), n)
+        if got < 0:
+            raise SldError(int(got), f"get({name})")
+        return out.reshape(-1, width) if width > 1 else out
+
+    def cell_lists(self):
+        out = np.empty(self.natom, np.int32)
+        _check(self.L.sld_get_cell_lists(self.h, out.ctypes.data_as(C.POINTER(C.c_int))),
+               "cell_lists")
+        return out
+
+    def averages(self):
+        out = np.empty(10, np.float64)
+        _check(self.L.sld_averages(self.h, _dp(out)), "averages")
+        return dict(zip(["pe", "ke", "me", "me0", "Ee", "Tl", "Te", "sx", "sy", "sz"], out))
+
+    def virial(self):
+        out = np.empty(1, np.float64)
+        _check(self.L.sld_virial(self.h, _dp(out)), "virial")
+        return float(out[0])
+
+    def total_time(self):
+        out = np.empty(1, np.float64)
+        _check(self.L.sld_total_time(self.h, _dp(out)), "total_time")
+        return float(out[0])
+
+    def last_run_ms(self):
+        out = np.empty(1, np.float64)
+        _check(self.L.sld_last_run_ms(self.h, _dp(out)), "last_run_ms")
+        return float(out[0])
+
+
+def header_symbols(path=HEADER):
+    """Entry points declared in include/sld.h."""
+    import re
+    text = open(path).read()
+    return sorted(set(re.findall(r"\b(sld_[a-z_A-Z0-9]+)\s*\(", text)))
