@@ -1,0 +1,286 @@
+#!/usr/bin/env python
+"""Benchmark of the spin-lattice step on B200: atom-steps/s.
+
+Workload (the 4.19M-atom spin-lattice-electron case): bcc Fe, 128^3
+conventional cells (4,194,304 atoms), a = 2.8665 A, DD05 EAM + Fe exchange and
+Landau terms, Langevin lattice and spin thermostats, localcolmot, electron
+temperature on a 16^3 mesh (8^3 unit cells per node) with a Gaussian hot spot
+(3,000 K peak, sigma 2 nm, 300 K background), energy renormalisation every
+step, dt = 0.5 fs.  Synthetic seeded initial state; spins tilted by a
+Gaussian polar angle of 0.35 rad so that the spin temperature starts near
+300 K.  The state (about 1 GB) is far larger than L2, so
+every step streams it from HBM.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--precision fp64|split] [--size 128]
+
+With N > 1 (torchrun) every rank advances its own replica (weak scaling; the
+path has no data exchange).  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atom-steps/s, 4.19M-atom bcc Fe SLD: split-FP32 vs plain FP64 on one B200"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# compulsory HBM bytes per atom for each phase of one step (FP64 form):
+# each atom's own state read/written once per pass, neighbour data reused on
+# chip.  links 28, core_ds (4 visits of r, s, rho in and s out) 320,
+# core_dp (2 kicks incl. rescale) 240, core_dr 72, rho 32, force 80.
+ALGO_BYTES = {"links": 28, "core_ds": 320, "core_dp": 240, "core_dr": 72,
+              "calculate_rho": 32, "calculate_force_energy": 80,
+              "calculate_temperature": 80, "check_energy": 32, "core_dTe": 0,
+              "bookkeeping": 0}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
+    ap.add_argument("--size", type=int, default=128)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(size, seed=2026):
+    from spilady_b200.lattice import hot_spot_te, initial_state
+    params, r, p, s = initial_state(size, seed=seed, tilt=0.35, temperature=300.0)
+    params["step"] = 0.5e-15
+    n_te = max(3, size // 8)
+    te = hot_spot_te(n_te, params["box"][0], peak=3000.0, background=300.0, sigma=20.0)
+    switches = dict(spinlang=True, lattlang=True, eltemp=True, localcolmot=True,
+                    renormalize=True, te_mesh=n_te)
+    return params, r, p, s, te, switches
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ reference
+def reference_sample(steps, threads):
+    """The reference's own CPU build (oracle/_ref) on a bounded sample of the
+    workload: 24^3 cells, same physics, Te on link cells (the reference keeps
+    Te per link cell; it has no decoupled mesh).  Returns (atom-steps/s,
+    natom, seconds)."""
+    from oracle import refjob
+    from spilady_b200.lattice import initial_state
+    params, r, p, s = initial_state(24, seed=2026, tilt=0.35)
+    params["step"] = 0.5e-15
+    ops = [(refjob.OP_CORE, 1), (refjob.OP_CORE, steps), (refjob.OP_DUMP, 0)]
+    d = refjob.run("langte", params, r, p, s, ops=ops, threads=threads)[-1]
+    return r.shape[0] * steps / d.wall, r.shape[0], d.wall
+
+
+def cpu_baseline_block(steps=10):
+    threads = os.cpu_count() or 1
+    from oracle import refjob
+    if refjob.available("langte"):
+        v, n, t = reference_sample(steps, threads)
+        return {"value": v, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
+                "sample": f"reference CPU build, 24^3 cells ({n} atoms), {steps} steps, "
+                          f"same physics with Te on link cells, {t:.1f} s of core()"}
+    return {"value": None, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
+            "sample": "reference build absent (oracle/ref/build.sh not run)"}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(world, x):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+    return x
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    from oracle import refjob
+    if not refjob.available("langte"):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference CPU build missing (sh oracle/ref/build.sh)"}))
+        return
+    v, n, t = reference_sample(args.steps, threads)
+    line = {"metric": METRIC, "value": v, "unit": "atom-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"bcc Fe 24^3 cells ({n} atoms) sample of the 128^3 "
+                                   "spin-lattice-electron workload, Te on link cells",
+                       "parallelism": "OpenMP host threads"},
+            "cpu_baseline": {"value": v, "unit": "atom-steps/s", "cores": threads,
+                             "kind": "reference", "sample": f"{n} atoms x {args.steps} steps"},
+            "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    from spilady_b200 import engine
+    params, r, p, s, te, sw = workload(args.size)
+    prec = engine.SPLIT if args.precision == "split" else engine.FP64
+    e = engine.Engine(params, r, p, s, te=te, device=local, precision=prec, **sw)
+    natom = e.natom
+    e.run(args.warmup)
+    e.sync()
+    import torch
+    torch.cuda.set_device(local)
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    e.run(args.steps)
+    ms = e.last_run_ms()
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    e.sync()
+    ms = allmax(world, ms)
+    value = natom * args.steps * world / (ms / 1e3)
+    kernels_per_step = e.step_kernel_count()
+
+    # per-phase device time (CUDA events on the engine's stream), a few steps
+    prof = {}
+    for _ in range(3):
+        for k, v in e.profile_step().items():
+            prof[k] = prof.get(k, 0.0) + v / 3
+    dom = max(prof, key=prof.get)
+    peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    achieved = ALGO_BYTES.get(dom, 0) * natom / (prof[dom] / 1e3) / 1e9 if prof[dom] > 0 else 0.0
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                "peak_source": "measured" if peaks else "fallback",
+                "phase_ms": {k: round(v, 4) for k, v in prof.items()}}
+
+    # end to end through the public API with host buffers: upload the state,
+    # then every step run it and read the check() averages back
+    e2e = None
+    if not args.no_e2e:
+        k = max(5, min(args.steps, 50))
+        t0 = time.perf_counter()
+        e.set_state(r, p, s)
+        for _ in range(k):
+            e.run(1)
+            e.averages()
+        t1 = time.perf_counter()
+        e2e = {"value": natom * k / (t1 - t0), "unit": "atom-steps/s",
+               "h2d_bytes_per_step": int(natom * 72 / k), "d2h_bytes_per_step": 80,
+               "steps": k}
+    e.close()
+
+    if rank != 0:
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_block()
+    line = {
+        "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if prec == engine.FP64 else "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": f"bcc Fe {args.size}^3 cells ({natom} atoms) spin-lattice-electron,"
+                               f" Langevin spin+lattice, localcolmot, Te mesh {sw['te_mesh']}^3,"
+                               " dt 0.5 fs",
+                   "precision": args.precision, "natom": natom,
+                   "l2": "state (~1 GB) larger than L2; no flush needed",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": kernels_per_step * args.steps, "clocks": clk,
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -166,6 +166,18 @@ int sld_sync(sld_ctx* ctx);
    context's stream). */
 int sld_last_run_ms(sld_ctx* ctx, double* out);
 
+/* Run one main-loop step phase by phase (no graph), timing each phase with
+   CUDA events on the context's stream.  ms_out[SLD_PHASES] receives the
+   device milliseconds of: links, core_dTe (both calls), core_dp (both),
+   core_ds (both), core_dr, calculate_rho, calculate_force_energy,
+   calculate_temperature, energy check, bookkeeping.  The step advances the
+   state exactly as sld_run(ctx, 1) does. */
+#define SLD_PHASES 10
+int sld_profile_step(sld_ctx* ctx, double* ms_out);
+
+/* Number of kernel launches in one captured main-loop step. */
+int sld_step_kernel_count(sld_ctx* ctx, int* out);
+
 const char* sld_error_string(int code);
 
 #ifdef __cplusplus

@@ -1,146 +1,216 @@
-// Spin effective field and the Suzuki-Trotter colour sweeps, FP64 form.
+// Suzuki-Trotter spin sweeps (core_ds_CPU.cpp:35-83), one launch per colour
+// group and direction.
 //
-// core_ds (core_ds_CPU.cpp:35-83) visits every atom twice: colour groups
-// 0..G-1 with each cell walked head -> tail, then groups G-1..0 walked
-// tail -> head.  Cells of one colour share no neighbour, so one launch per
-// (group, direction) updates all cells of the group at once, one thread per
-// cell, each walking its list in the reference's order (the in-cell update
-// is Gauss-Seidel: a later atom sees the spins already rotated before it).
-//
-// A visit (calculate_spin_CPU.cpp:33-199) gathers Heff_H = sum_j J(r_ij) s_j
-// over the 26 neighbour cells and the own cell in the reference's order
-// (inner_spin, :201-235); with the Langevin thermostat it also gathers
-// sum_j J(r_ij) |s_j| (inner_sum_Jij_sj, :238-274) in the same pass, since
-// no neighbour spin changes between the two sums.  NVE visits apply the
-// exact rotation (core_ds_CPU.cpp:90-127); Langevin visits apply the
-// reference's five-part scheme with counter-based normal noise.
-#include "sld_common.cuh"
+// The reference visits the cells of colour group 0..G-1 (then G-1..0), each
+// cell's atoms in list order head -> tail (then tail -> head), and each visit
+// (calculate_spin_CPU.cpp:33-199) evaluates Heff_H = sum_j J(r_ij) s_j with
+// the spins as they are at that moment.  Cells of one colour share no
+// neighbour, so during a group's launch every spin outside the group's cells
+// is frozen and only a cell's own atoms change while it is walked.  Each block
+// takes 32 cells of the group and works in three phases:
+//   A  one thread per atom: from the exchange list, sum the field of the
+//      neighbours outside the atom's cell (frozen), note the in-cell
+//      neighbours, and draw the visit's noise (counter-based, so the draw
+//      does not depend on the order);
+//   B  one thread per cell: walk the cell in the reference's order, add the
+//      in-cell neighbours' current spins (kept in shared memory) and apply the
+//      integrator (FP64);
+//   C  one thread per atom: write the spins back.
+// A block whose cells hold more atoms (or in-cell neighbours) than its
+// shared-memory tables falls back to one thread per cell reading everything
+// from global memory, with the same arithmetic.
+#include "sld_spin.cuh"
 
-__device__ __forceinline__ double3 spin_rotation(double3 H, double3 s, double dt) {
-    double3 w = make_double3(H.x / -SLD_HBAR, H.y / -SLD_HBAR, H.z / -SLD_HBAR);
-    double w0 = sqrt(w.x * w.x + w.y * w.y + w.z * w.z);
-    if (w0 > 0.0) w = make_double3(w.x / w0, w.y / w0, w.z / w0);
-    else w = make_double3(0.0, 0.0, 0.0);
-    double w12 = w.x * w.y, w23 = w.y * w.z, w13 = w.x * w.z;
-    double w1s = w.x * w.x, w2s = w.y * w.y, w3s = w.z * w.z;
-    double A, cw;
-    sincos(w0 * dt, &A, &cw);
-    double B = 1.0 - cw;
-    double3 o;
-    o.x = s.x + (s.x * B * (-w2s - w3s) + s.y * (B * w12 - A * w.z) + s.z * (A * w.y + B * w13));
-    o.y = s.y + (s.y * B * (-w1s - w3s) + s.z * (B * w23 - A * w.x) + s.x * (A * w.z + B * w12));
-    o.z = s.z + (s.z * B * (-w1s - w2s) + s.x * (B * w13 - A * w.y) + s.y * (A * w.x + B * w23));
-    return o;
-}
+#define SW_CPB 32
+#define SW_THREADS 256
+#define SW_MAXA 256
+#define SW_MAXIN 12
 
-// Landau field plus the exchange correction (calculate_spin_CPU.cpp:127-136)
-__device__ __forceinline__ double3 landau_field(const double L[4], double sumJ, double3 x) {
-    double s_sq = x.x * x.x + x.y * x.y + x.z * x.z;
-    double c = -(2.0 * L[0] + 4.0 * L[1] * s_sq + 6.0 * L[2] * (s_sq * s_sq) +
-                 8.0 * L[3] * pow(s_sq, 3.0));
-    double3 HL = make_double3(c * x.x, c * x.y, c * x.z);
-    double s0 = sqrt(s_sq);
-    if (s0 > 0.0) {
-        double k = -sumJ / s0;
-        HL.x += k * x.x; HL.y += k * x.y; HL.z += k * x.z;
+struct SweepShared {
+    double s[SW_MAXA][4];           // current spin, |s|
+    double h[SW_MAXA][4];           // field of the out-of-cell neighbours, sum J|s|
+    double aux[SW_MAXA][5];         // rho, T, noise x y z
+    double inJ[SW_MAXA][SW_MAXIN];  // J of the in-cell neighbours
+    int slot[SW_MAXA];
+    unsigned char inq[SW_MAXA][SW_MAXIN];   // their position in the cell list
+    unsigned char inn[SW_MAXA];
+    int cell[SW_CPB], cell_n[SW_CPB], cell_start[SW_CPB], cell_base[SW_CPB];
+    int total, overflow;
+};
+
+__device__ __forceinline__ void visit_store(const Dev& D, int i, double3 s, double3 H, double3 HL,
+                                            double sumJ, bool fields) {
+    double s0 = sqrt(s.x * s.x + s.y * s.y + s.z * s.z);
+    if (!isfinite(s0)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
+    D.s[i] = make_double4(s.x, s.y, s.z, s0);
+    if (fields) {
+        D.H[i] = make_double4(H.x, H.y, H.z, 0.0);
+        D.HL[i] = make_double4(HL.x, HL.y, HL.z, 0.0);
+        if (D.spinlang) D.sumJ[i] = sumJ;
     }
-    return HL;
 }
 
-__device__ __forceinline__ void cell_xyz(const Dev& D, int c, int& cx, int& cy, int& cz) {
-    cx = c % D.nx;
-    int t = c / D.nx;
-    cy = t % D.ny;
-    cz = t / D.ny;
+// one visit entirely from global memory (the fallback path)
+__device__ void visit_global(const Dev& D, int i, double dt, unsigned long long epoch, bool fields) {
+    const int N = D.natom;
+    double3 H = make_double3(0.0, 0.0, 0.0);
+    double sumJ = 0.0;
+    int nj = D.jl_n[i];
+    for (int e = 0; e < nj; ++e) {
+        int j = D.jl[(size_t)e * N + i];
+        double J = D.jv[(size_t)e * N + i];
+        double4 sj = D.s[j];
+        H.x += J * sj.x; H.y += J * sj.y; H.z += J * sj.z;
+        sumJ += J * sj.w;
+    }
+    double4 s4 = D.s[i];
+    double T = 0.0, rho = 0.0;
+    double3 xi = make_double3(0.0, 0.0, 0.0);
+    if (D.spinlang) {
+        T = D.eltemp ? D.Te[D.node[i]] : D.temperature;
+        rho = D.rho[i];
+        xi = normals3(D.seed, 0u, (unsigned)D.id[i], epoch);
+    }
+    double3 HL;
+    double3 s = spin_integrate(D, make_double3(s4.x, s4.y, s4.z), H, sumJ, rho, T, xi, dt, HL);
+    visit_store(D, i, s, H, HL, sumJ, fields);
 }
 
-// Heff_H and (optionally) sum_j J |s_j| for atom i
-__device__ __forceinline__ void gather_field(const Dev& D, int i, double4 ri, int c0, bool want_sumJ,
-                                             double3& H, double& sumJ, unsigned* err) {
-    int cx, cy, cz;
-    cell_xyz(D, c0, cx, cy, cz);
-    H = make_double3(0.0, 0.0, 0.0);
-    sumJ = 0.0;
-    for (int k = 0; k < 27; ++k) {
-        int c = k == 26 ? c0 : nbr_cell(D, cx, cy, cz, k);
-        int st = D.cell_start[c], n = D.cell_count[c];
-        for (int m = 0; m < n; ++m) {
-            int j = D.cell_atoms[st + m];
-            if (j == i) continue;
-            double4 rj = D.r[j];
-            double3 d = find_image(D, make_double3(ri.x - rj.x, ri.y - rj.y, ri.z - rj.z));
-            double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
-            if (rsq < D.rcut_mag_sq) {
-                double J = interp(D.tJ, sqrt(rsq), D.inv_r, err);
-                double4 sj = D.s[j];
-                H.x += J * sj.x; H.y += J * sj.y; H.z += J * sj.z;
-                if (want_sumJ) sumJ += J * sj.w;
+__global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restrict__ gcells,
+                                                      int ncell_g, double dt, int backward,
+                                                      int epoch_off) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SweepShared& S = *reinterpret_cast<SweepShared*>(smem_raw);
+    const int N = D.natom;
+    const int cbeg = blockIdx.x * SW_CPB;
+    const int ncb = min(SW_CPB, ncell_g - cbeg);
+    const unsigned long long epoch = D.ctl->epoch + (unsigned long long)epoch_off;
+    const bool fields = backward != 0;   // the backward sweep is each atom's last visit
+    if (threadIdx.x < 32) {
+        int lane = threadIdx.x, n = 0, st = 0, c = -1;
+        if (lane < ncb) {
+            c = gcells[cbeg + lane];
+            n = D.cell_count[c];
+            st = D.cell_start[c];
+        }
+        int inc = n;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += t;
+        }
+        if (lane < ncb) {
+            S.cell[lane] = c;
+            S.cell_n[lane] = n;
+            S.cell_start[lane] = st;
+            S.cell_base[lane] = inc - n;
+        }
+        int total = __shfl_sync(0xffffffffu, inc, 31);
+        if (lane == 0) {
+            S.total = total;
+            S.overflow = total > SW_MAXA ? 1 : 0;
+        }
+    }
+    __syncthreads();
+    const int total = S.total;
+    if (!S.overflow) {
+        // phase A
+        for (int a = threadIdx.x; a < total; a += blockDim.x) {
+            int q = 0;
+            while (q + 1 < ncb && S.cell_base[q + 1] <= a) ++q;
+            int i = D.cell_atoms[S.cell_start[q] + (a - S.cell_base[q])];
+            int c = S.cell[q];
+            S.slot[a] = i;
+            double4 si = D.s[i];
+            S.s[a][0] = si.x; S.s[a][1] = si.y; S.s[a][2] = si.z; S.s[a][3] = si.w;
+            double hx = 0, hy = 0, hz = 0, hj = 0;
+            int nin = 0;
+            int nj = D.jl_n[i];
+            for (int e = 0; e < nj; ++e) {
+                int j = D.jl[(size_t)e * N + i];
+                double J = D.jv[(size_t)e * N + i];
+                if (D.cell_of[j] == c) {
+                    int st = S.cell_start[q], n = S.cell_n[q], pos = 0;
+                    while (pos < n && D.cell_atoms[st + pos] != j) ++pos;
+                    if (nin < SW_MAXIN) {
+                        S.inq[a][nin] = (unsigned char)pos;
+                        S.inJ[a][nin] = J;
+                    }
+                    ++nin;
+                } else {
+                    double4 sj = D.s[j];
+                    hx += J * sj.x; hy += J * sj.y; hz += J * sj.z;
+                    hj += J * sj.w;
+                }
             }
+            S.h[a][0] = hx; S.h[a][1] = hy; S.h[a][2] = hz; S.h[a][3] = hj;
+            S.inn[a] = (unsigned char)(nin < SW_MAXIN ? nin : SW_MAXIN);
+            if (nin > SW_MAXIN) S.overflow = 1;
+            if (D.spinlang) {
+                double3 xi = normals3(D.seed, 0u, (unsigned)D.id[i], epoch);
+                S.aux[a][0] = D.rho[i];
+                S.aux[a][1] = D.eltemp ? D.Te[D.node[i]] : D.temperature;
+                S.aux[a][2] = xi.x; S.aux[a][3] = xi.y; S.aux[a][4] = xi.z;
+            }
+        }
+        __syncthreads();
+        if (!S.overflow) {
+            // phase B
+            if (threadIdx.x < ncb) {
+                int q = threadIdx.x, n = S.cell_n[q], b = S.cell_base[q];
+                for (int t = 0; t < n; ++t) {
+                    int a = b + (backward ? n - 1 - t : t);
+                    double3 H = make_double3(S.h[a][0], S.h[a][1], S.h[a][2]);
+                    double sumJ = S.h[a][3];
+                    for (int e = 0; e < S.inn[a]; ++e) {
+                        int a2 = b + S.inq[a][e];
+                        double J = S.inJ[a][e];
+                        H.x += J * S.s[a2][0]; H.y += J * S.s[a2][1]; H.z += J * S.s[a2][2];
+                        sumJ += J * S.s[a2][3];
+                    }
+                    double3 HL;
+                    double3 s = spin_integrate(
+                        D, make_double3(S.s[a][0], S.s[a][1], S.s[a][2]), H, sumJ, S.aux[a][0],
+                        S.aux[a][1], make_double3(S.aux[a][2], S.aux[a][3], S.aux[a][4]), dt, HL);
+                    double s0 = sqrt(s.x * s.x + s.y * s.y + s.z * s.z);
+                    S.s[a][0] = s.x; S.s[a][1] = s.y; S.s[a][2] = s.z; S.s[a][3] = s0;
+                    if (fields) {
+                        int i = S.slot[a];
+                        D.H[i] = make_double4(H.x, H.y, H.z, 0.0);
+                        D.HL[i] = make_double4(HL.x, HL.y, HL.z, 0.0);
+                        if (D.spinlang) D.sumJ[i] = sumJ;
+                    }
+                }
+            }
+            __syncthreads();
+            // phase C
+            for (int a = threadIdx.x; a < total; a += blockDim.x) {
+                double s0 = S.s[a][3];
+                if (!isfinite(s0)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
+                D.s[S.slot[a]] = make_double4(S.s[a][0], S.s[a][1], S.s[a][2], s0);
+            }
+            return;
+        }
+    }
+    // fallback: one thread per cell, from global memory
+    if (threadIdx.x < ncb) {
+        int q = threadIdx.x, n = S.cell_n[q], st = S.cell_start[q];
+        for (int t = 0; t < n; ++t) {
+            int i = D.cell_atoms[st + (backward ? n - 1 - t : t)];
+            visit_global(D, i, dt, epoch, fields);
         }
     }
 }
 
-__device__ void spin_visit(const Dev& D, int i, double dt, unsigned long long epoch) {
-    unsigned* err = &D.ctl->err;
-    double4 ri = D.r[i];
-    double4 s4 = D.s[i];
-    double3 s = make_double3(s4.x, s4.y, s4.z);
-    double3 H;
-    double sumJ;
-    gather_field(D, i, ri, D.cell_of[i], D.spinlang != 0, H, sumJ, err);
-    double3 HL = make_double3(0.0, 0.0, 0.0);
-    if (!D.spinlang) {
-        s = spin_rotation(H, s, dt);
-    } else {
-        double dt_half = dt / 2.0, dt_quad = dt / 4.0, g = D.gamma_S_HL;
-        double rho = D.rho[i];
-        double L[4];
-        for (int k = 0; k < 4; ++k) L[k] = interp_const(D.landau[k], rho, D.inv_rho);
-        s = spin_rotation(H, s, dt_half);                                   // part 1
-        HL = landau_field(L, sumJ, s);                                      // part 2
-        double a = g * dt_quad;
-        double3 t = make_double3(s.x + a * (H.x + HL.x), s.y + a * (H.y + HL.y), s.z + a * (H.z + HL.z));
-        HL = landau_field(L, sumJ, t);
-        a = g * dt_half;
-        s = make_double3(s.x + a * (H.x + HL.x), s.y + a * (H.y + HL.y), s.z + a * (H.z + HL.z));
-        double T = D.eltemp ? D.Te[D.node[i]] : D.temperature;              // part 3
-        double amp = sqrt(2.0 * T * g / dt);
-        double3 xi = normals3(D.seed, 0u, (unsigned)D.id[i], epoch);
-        double3 dS = make_double3(amp * xi.x, amp * xi.y, amp * xi.z);
-        s = make_double3(s.x + dt * dS.x, s.y + dt * dS.y, s.z + dt * dS.z);
-        HL = landau_field(L, sumJ, s);                                      // part 4
-        a = g * dt_quad;
-        t = make_double3(s.x + a * (H.x + HL.x), s.y + a * (H.y + HL.y), s.z + a * (H.z + HL.z));
-        HL = landau_field(L, sumJ, t);
-        a = g * dt_half;
-        s = make_double3(s.x + a * (H.x + HL.x), s.y + a * (H.y + HL.y), s.z + a * (H.z + HL.z));
-        s = spin_rotation(H, s, dt_half);                                   // part 5
-        D.sumJ[i] = sumJ;
-    }
-    double s0 = sqrt(s.x * s.x + s.y * s.y + s.z * s.z);
-    if (!isfinite(s0)) atomicOr(err, SLD_FLAG_NAN);
-    D.s[i] = make_double4(s.x, s.y, s.z, s0);
-    D.H[i] = make_double4(H.x, H.y, H.z, 0.0);
-    D.HL[i] = make_double4(HL.x, HL.y, HL.z, 0.0);
+static size_t sweep_smem() { return sizeof(SweepShared); }
+
+void sweep_init() {
+    cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem());
 }
 
-__global__ void __launch_bounds__(128) k_sweep64(Dev D, const int* __restrict__ gcells, int ncell_g,
-                                                 double dt, int backward, int epoch_off) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ncell_g) return;
-    int c = gcells[t];
-    int st = D.cell_start[c], n = D.cell_count[c];
-    unsigned long long epoch = D.ctl->epoch + (unsigned long long)epoch_off;
-    if (!backward) {
-        for (int m = 0; m < n; ++m) spin_visit(D, D.cell_atoms[st + m], dt, epoch);
-    } else {
-        for (int m = n - 1; m >= 0; --m) spin_visit(D, D.cell_atoms[st + m], dt, epoch);
-    }
-}
-
-void launch_sweep64(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g, double dt,
-                    bool backward, int epoch_off) {
+void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g, double dt,
+                  bool backward, int epoch_off) {
     if (ncell_g <= 0) return;
-    k_sweep64<<<div_up(ncell_g, 128), 128, 0, st>>>(D, gcells, ncell_g, dt, backward ? 1 : 0,
-                                                    epoch_off);
+    k_sweep<<<div_up(ncell_g, SW_CPB), SW_THREADS, sweep_smem(), st>>>(D, gcells, ncell_g, dt,
+                                                                       backward ? 1 : 0, epoch_off);
 }

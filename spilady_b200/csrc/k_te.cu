@@ -11,37 +11,19 @@
 // which a block barrier gives cheaply.
 #include "sld_common.cuh"
 
-__device__ __forceinline__ void cell_xyz_t(const Dev& D, int c, int& cx, int& cy, int& cz) {
-    cx = c % D.nx;
-    int t = c / D.nx;
-    cy = t % D.ny;
-    cz = t / D.ny;
-}
-
-// Heff_H and sum_j J |s_j| as inner_spin / inner_sum_Jij_sj gather them
-__device__ __forceinline__ void gather_field_t(const Dev& D, int i, double3& H, double& sumJ,
-                                               unsigned* err) {
-    double4 ri = D.r[i];
-    int c0 = D.cell_of[i], cx, cy, cz;
-    cell_xyz_t(D, c0, cx, cy, cz);
+// Heff_H and sum_j J |s_j| (inner_spin / inner_sum_Jij_sj) from the
+// exchange list
+__device__ __forceinline__ void gather_field_t(const Dev& D, int i, double3& H, double& sumJ) {
+    const int N = D.natom;
     H = make_double3(0.0, 0.0, 0.0);
     sumJ = 0.0;
-    for (int k = 0; k < 27; ++k) {
-        int c = k == 26 ? c0 : nbr_cell(D, cx, cy, cz, k);
-        int st = D.cell_start[c], n = D.cell_count[c];
-        for (int m = 0; m < n; ++m) {
-            int j = D.cell_atoms[st + m];
-            if (j == i) continue;
-            double4 rj = D.r[j];
-            double3 d = find_image(D, make_double3(ri.x - rj.x, ri.y - rj.y, ri.z - rj.z));
-            double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
-            if (rsq < D.rcut_mag_sq) {
-                double J = interp(D.tJ, sqrt(rsq), D.inv_r, err);
-                double4 sj = D.s[j];
-                H.x += J * sj.x; H.y += J * sj.y; H.z += J * sj.z;
-                sumJ += J * sj.w;
-            }
-        }
+    int nj = D.jl_n[i];
+    for (int e = 0; e < nj; ++e) {
+        int j = D.jl[(size_t)e * N + i];
+        double J = D.jv[(size_t)e * N + i];
+        double4 sj = D.s[j];
+        H.x += J * sj.x; H.y += J * sj.y; H.z += J * sj.z;
+        sumJ += J * sj.w;
     }
 }
 
@@ -49,10 +31,9 @@ __device__ __forceinline__ void gather_field_t(const Dev& D, int i, double3& H, 
 // the five sums (R_up, R_dn, L_up, L_dn) it contributes
 __device__ __forceinline__ void temp_atom(const Dev& D, int i, double& Rup, double& Rdn, double& Lup,
                                           double& Ldn) {
-    unsigned* err = &D.ctl->err;
     double3 H;
     double sumJ;
-    gather_field_t(D, i, H, sumJ, err);
+    gather_field_t(D, i, H, sumJ);
     double4 s4 = D.s[i];
     double3 s = make_double3(s4.x, s4.y, s4.z);
     double cx_ = s.y * H.z - H.y * s.z, cy_ = s.z * H.x - H.z * s.x, cz_ = s.x * H.y - H.x * s.y;

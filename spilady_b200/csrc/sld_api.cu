@@ -48,6 +48,7 @@ struct sld_ctx {
     double last_ms = 0.0;
     int scan_blocks = 1;
     int red_cap = 0;
+    bool lists_stale = false;   // positions moved since the neighbour lists were built
 
     template <class T>
     int alloc(T** p, size_t n) {
@@ -87,12 +88,12 @@ void enqueue_ds(sld_ctx* c, double dt, int& eoff) {
     const auto& G = c->G;
     double dt_half = dt / 2e0;
     for (int g = 0; g < G.ngroups; ++g)
-        launch_sweep64(c->D, c->st, c->d_gcells + G.gstart[g], G.gstart[g + 1] - G.gstart[g],
-                       dt_half, false, eoff);
+        launch_sweep(c->D, c->st, c->d_gcells + G.gstart[g], G.gstart[g + 1] - G.gstart[g],
+                     dt_half, false, eoff);
     if (c->P.spinlang) ++eoff;
     for (int g = G.ngroups - 1; g >= 0; --g)
-        launch_sweep64(c->D, c->st, c->d_gcells + G.gstart[g], G.gstart[g + 1] - G.gstart[g],
-                       dt_half, true, eoff);
+        launch_sweep(c->D, c->st, c->d_gcells + G.gstart[g], G.gstart[g + 1] - G.gstart[g],
+                     dt_half, true, eoff);
     if (c->P.spinlang) ++eoff;
 }
 
@@ -110,9 +111,9 @@ void enqueue_step(sld_ctx* c) {
     enqueue_dp(c, dt / 2e0, eoff);
     enqueue_ds(c, dt / 2e0, eoff);
     launch_dr(c->D, c->st, dt);
-    launch_rho64(c->D, c->st);
+    launch_pairs(c->D, c->st, true);
     enqueue_ds(c, dt / 2e0, eoff);
-    launch_force64(c->D, c->st);
+    launch_force(c->D, c->st);
     enqueue_dp(c, dt / 2e0, eoff);
     if (c->P.eltemp) {
         launch_temperature(c->D, c->st);
@@ -130,7 +131,7 @@ int validate(const sld_params* p) {
     if (p->rcut_pot > p->rcut_max || p->rcut_mag > p->rcut_max) return SLD_ERR_ARG;
     if (p->eltemp && !(p->spinlang && p->lattlang)) return SLD_ERR_ARG;
     if (p->localcolmot && !p->lattlang) return SLD_ERR_ARG;
-    if (p->precision != SLD_FP64 && p->precision != SLD_SPLIT) return SLD_ERR_ARG;
+    if (p->precision != SLD_FP64) return SLD_ERR_ARG;   // the split form is not built yet
     if (p->te_mesh != 0 && p->te_mesh < 3) return SLD_ERR_ARG;
     return SLD_OK;
 }
@@ -194,6 +195,7 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     const auto& G = c->G;
 
     if (cudaSetDevice(prm->device) != cudaSuccess) { delete c; return SLD_ERR_CUDA; }
+    sweep_init();
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
         return SLD_ERR_CUDA;
@@ -231,6 +233,7 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     D.localcolmot = prm->localcolmot; D.renormalize = prm->renormalize_energy;
     D.print_every = c->P.interval_of_print_out;
     D.te_nloop = c->P.te_nloop;
+    D.small_grid = (G.nx < 4 || G.ny < 4 || G.nz < 4) ? 1 : 0;
 
     size_t n = (size_t)natom;
     double* tabs[sld::kTabCount];
@@ -251,7 +254,10 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
          c->alloc(&D.cell_of, n) == 0 && c->alloc(&D.id, n) == 0 && c->alloc(&D.stamp, n) == 0 &&
          c->alloc(&D.cell_start, (size_t)G.ncells) == 0 &&
          c->alloc(&D.cell_count, (size_t)G.ncells) == 0 &&
-         c->alloc(&D.cell_atoms, n) == 0 && c->alloc(&D.cell_fill, (size_t)G.ncells) == 0;
+         c->alloc(&D.cell_atoms, n) == 0 && c->alloc(&D.cell_fill, (size_t)G.ncells) == 0 &&
+         c->alloc(&D.nbr, (size_t)SLD_MAXNB * n) == 0 && c->alloc(&D.nbr_n, n) == 0 &&
+         c->alloc(&D.jl, (size_t)SLD_MAXJ * n) == 0 && c->alloc(&D.jv, (size_t)SLD_MAXJ * n) == 0 &&
+         c->alloc(&D.jl_n, n) == 0;
     c->scan_blocks = div_up(G.ncells, 1024);
     ok = ok && c->alloc(&D.scan_tmp, (size_t)c->scan_blocks) == 0;
     if (prm->te_mesh > 0) {
@@ -321,8 +327,9 @@ int sld_set_state(sld_ctx* c, const double* r, const double* p, const double* s)
     CK(cudaMemcpyAsync(D.ctl, &z, sizeof(Ctl), cudaMemcpyHostToDevice, c->st));
     // initialize(): links, rho, forces, cell temperatures, reference energy
     launch_links(D, c->st, true, c->scan_blocks);
-    launch_rho64(D, c->st);
-    launch_force64(D, c->st);
+    launch_pairs(D, c->st, true);
+    c->lists_stale = false;
+    launch_force(D, c->st);
     if (c->P.eltemp) {
         launch_temperature(D, c->st);
         if (c->P.renormalize_energy) launch_energy_check(D, c->st, 0);
@@ -351,18 +358,29 @@ int sld_links(sld_ctx* c) {
 
 int sld_calculate_rho(sld_ctx* c) {
     if (!c) return SLD_ERR_ARG;
-    launch_rho64(c->D, c->st);
+    launch_pairs(c->D, c->st, true);
+    c->lists_stale = false;
     return launch_status();
+}
+
+// refresh the neighbour lists (not rho) when positions moved since
+static void fresh_lists(sld_ctx* c) {
+    if (c->lists_stale) {
+        launch_pairs(c->D, c->st, false);
+        c->lists_stale = false;
+    }
 }
 
 int sld_calculate_force_energy(sld_ctx* c) {
     if (!c) return SLD_ERR_ARG;
-    launch_force64(c->D, c->st);
+    fresh_lists(c);
+    launch_force(c->D, c->st);
     return launch_status();
 }
 
 int sld_core_ds(sld_ctx* c, double dt) {
     if (!c) return SLD_ERR_ARG;
+    fresh_lists(c);
     int eoff = 0;
     enqueue_ds(c, dt, eoff);
     launch_advance(c->D, c->st, eoff, 0);
@@ -380,6 +398,7 @@ int sld_core_dp(sld_ctx* c, double dt) {
 int sld_core_dr(sld_ctx* c, double dt) {
     if (!c) return SLD_ERR_ARG;
     launch_dr(c->D, c->st, dt);
+    c->lists_stale = true;
     return launch_status();
 }
 
@@ -393,12 +412,14 @@ int sld_core_dTe(sld_ctx* c, double dt) {
 int sld_calculate_temperature(sld_ctx* c) {
     if (!c) return SLD_ERR_ARG;
     if (!c->P.eltemp) return SLD_OK;
+    fresh_lists(c);
     launch_temperature(c->D, c->st);
     return launch_status();
 }
 
 int sld_run(sld_ctx* c, int nsteps) {
     if (!c || nsteps < 0) return SLD_ERR_ARG;
+    fresh_lists(c);
     if (!c->step_graph) {
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
@@ -410,6 +431,65 @@ int sld_run(sld_ctx* c, int nsteps) {
     CK(cudaEventRecord(c->ev0, c->st));
     for (int k = 0; k < nsteps; ++k) CK(cudaGraphLaunch(c->step_graph, c->st));
     CK(cudaEventRecord(c->ev1, c->st));
+    return SLD_OK;
+}
+
+int sld_profile_step(sld_ctx* c, double* ms) {
+    if (!c || !ms) return SLD_ERR_ARG;
+    fresh_lists(c);
+    cudaEvent_t ev[2];
+    CK(cudaEventCreate(&ev[0]));
+    CK(cudaEventCreate(&ev[1]));
+    for (int k = 0; k < SLD_PHASES; ++k) ms[k] = 0.0;
+    auto timed = [&](int slot, auto&& fn) {
+        cudaEventRecord(ev[0], c->st);
+        fn();
+        cudaEventRecord(ev[1], c->st);
+        cudaEventSynchronize(ev[1]);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ev[0], ev[1]);
+        ms[slot] += t;
+    };
+    double dt = c->P.step;
+    int eoff = 0;
+    timed(0, [&] { launch_links(c->D, c->st, false, c->scan_blocks); });
+    if (c->P.eltemp) timed(1, [&] { launch_dte(c->D, c->st, dt / 2e0); });
+    timed(2, [&] { enqueue_dp(c, dt / 2e0, eoff); });
+    timed(3, [&] { enqueue_ds(c, dt / 2e0, eoff); });
+    timed(4, [&] { launch_dr(c->D, c->st, dt); });
+    timed(5, [&] { launch_pairs(c->D, c->st, true); });
+    timed(3, [&] { enqueue_ds(c, dt / 2e0, eoff); });
+    timed(6, [&] { launch_force(c->D, c->st); });
+    timed(2, [&] { enqueue_dp(c, dt / 2e0, eoff); });
+    if (c->P.eltemp) {
+        timed(7, [&] { launch_temperature(c->D, c->st); });
+        timed(1, [&] { launch_dte(c->D, c->st, dt / 2e0); });
+        if (c->P.renormalize_energy) timed(8, [&] { launch_energy_check(c->D, c->st, 1); });
+    }
+    timed(9, [&] { launch_advance(c->D, c->st, eoff, 1); });
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    return launch_status();
+}
+
+int sld_step_kernel_count(sld_ctx* c, int* out) {
+    if (!c || !out) return SLD_ERR_ARG;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(c);
+    CK(cudaStreamEndCapture(c->st, &g));
+    size_t n = 0;
+    CK(cudaGraphGetNodes(g, nullptr, &n));
+    std::vector<cudaGraphNode_t> nodes(n);
+    CK(cudaGraphGetNodes(g, nodes.data(), &n));
+    int k = 0;
+    for (size_t i = 0; i < n; ++i) {
+        cudaGraphNodeType t;
+        cudaGraphNodeGetType(nodes[i], &t);
+        if (t == cudaGraphNodeTypeKernel) ++k;
+    }
+    cudaGraphDestroy(g);
+    *out = k;
     return SLD_OK;
 }
 

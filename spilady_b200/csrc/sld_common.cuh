@@ -17,6 +17,10 @@
 #define SLD_HBAR 6.58211899e-16
 #define SLD_EVTOJ 1.602176487e-19
 #define SLD_MAXC 64   // == SLD_MAX_CELL_ATOMS in sld.h
+#define SLD_MAXNB 48  // neighbours within rcut_max per atom (bcc Fe: 26)
+#define SLD_MAXJ 32   // exchange neighbours within rcut_mag (bcc Fe: 14)
+#define SLD_WRAP (1 << 30)
+#define SLD_JMASK ((1 << 30) - 1)
 
 // error flag bits in Ctl::err
 #define SLD_FLAG_CAPACITY 1u
@@ -51,6 +55,7 @@ struct Dev {
     unsigned seed;
     int spinlang, lattlang, eltemp, localcolmot, renormalize, print_every;
     int te_nloop;
+    int small_grid;               // a link-cell axis of 3: every pair gets the minimum image
     // tables (potential_CPU.cpp:61-157): F, F', f, f', phi, phi', J, J'
     const double *tF, *tdF, *tf, *tdf, *tphi, *tdphi, *tJ, *tdJ;
     // atoms
@@ -65,6 +70,12 @@ struct Dev {
     int* te_count;
     const int *te_gcells, *te_gstart;
     int te_ngroups;
+    // per-step neighbour lists (built after every drift by k_pairs):
+    //   nbr  [SLD_MAXNB][natom]  j | (1<<30 when the pair crosses the box)
+    //        for r_ij < rcut_max, in the reference's traversal order
+    //   jl/jv [SLD_MAXJ][natom]  j and J(r_ij) for r_ij < rcut_mag
+    int *nbr, *nbr_n, *jl, *jl_n;
+    double* jv;
     // control and reduction scratch
     Ctl* ctl;
     double* red;                  // partial sums
@@ -118,6 +129,22 @@ __device__ __forceinline__ int nbr_cell(const Dev& D, int cx, int cy, int cz, in
     y = y < 0 ? y + D.ny : (y >= D.ny ? y - D.ny : y);
     z = z < 0 ? z + D.nz : (z >= D.nz ? z - D.nz : z);
     return x + (y + z * D.ny) * D.nx;
+}
+// the same, also telling whether the neighbour lies across the periodic
+// boundary (only such pairs can need the minimum-image shift)
+__device__ __forceinline__ int nbr_cell_w(const Dev& D, int cx, int cy, int cz, int k, bool& wrap) {
+    int x = cx + kNbr[k][0], y = cy + kNbr[k][1], z = cz + kNbr[k][2];
+    wrap = D.small_grid || x < 0 || x >= D.nx || y < 0 || y >= D.ny || z < 0 || z >= D.nz;
+    x = x < 0 ? x + D.nx : (x >= D.nx ? x - D.nx : x);
+    y = y < 0 ? y + D.ny : (y >= D.ny ? y - D.ny : y);
+    z = z < 0 ? z + D.nz : (z >= D.nz ? z - D.nz : z);
+    return x + (y + z * D.ny) * D.nx;
+}
+__device__ __forceinline__ void cell_xyz(const Dev& D, int c, int& cx, int& cy, int& cz) {
+    cx = c % D.nx;
+    int t = c / D.nx;
+    cy = t % D.ny;
+    cz = t / D.ny;
 }
 
 // potential_CPU.cpp:172-179: linear interpolation between entries n-1 and n
@@ -216,10 +243,11 @@ static inline int div_up(long a, long b) { return (int)((a + b - 1) / b); }
 // ---------------------------------------------------------------------
 // launch wrappers (host), one file per kernel family
 void launch_links(const Dev& D, cudaStream_t st, bool initial, int scan_blocks);
-void launch_rho64(const Dev& D, cudaStream_t st);
-void launch_force64(const Dev& D, cudaStream_t st);
-void launch_sweep64(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g, double dt,
-                    bool backward, int epoch_off);
+void launch_pairs(const Dev& D, cudaStream_t st, bool write_rho);
+void sweep_init();
+void launch_force(const Dev& D, cudaStream_t st);
+void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g, double dt,
+                  bool backward, int epoch_off);
 void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off);
 void launch_dr(const Dev& D, cudaStream_t st, double dt);
 void launch_temperature(const Dev& D, cudaStream_t st);

@@ -82,6 +82,8 @@ def lib():
         L.sld_virial.argtypes = [vp, P]
         L.sld_total_time.argtypes = [vp, P]
         L.sld_last_run_ms.argtypes = [vp, P]
+        L.sld_profile_step.argtypes = [vp, P]
+        L.sld_step_kernel_count.argtypes = [vp, C.POINTER(C.c_int)]
         L.sld_error_string.argtypes = [C.c_int]
         L.sld_error_string.restype = C.c_char_p
         _lib = L
@@ -207,6 +209,20 @@ class Engine:
         out = np.empty(1, np.float64)
         _check(self.L.sld_total_time(self.h, _dp(out)), "total_time")
         return float(out[0])
+
+    PHASES = ("links", "core_dTe", "core_dp", "core_ds", "core_dr", "calculate_rho",
+              "calculate_force_energy", "calculate_temperature", "check_energy", "bookkeeping")
+
+    def profile_step(self):
+        """One step run phase by phase; device ms per phase (CUDA events)."""
+        out = np.zeros(10, np.float64)
+        _check(self.L.sld_profile_step(self.h, _dp(out)), "profile_step")
+        return dict(zip(self.PHASES, out))
+
+    def step_kernel_count(self):
+        n = C.c_int()
+        _check(self.L.sld_step_kernel_count(self.h, C.byref(n)), "step_kernel_count")
+        return n.value
 
     def last_run_ms(self):
         out = np.empty(1, np.float64)
