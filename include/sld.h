@@ -49,7 +49,12 @@ extern "C" {
 
 #define SLD_MAX_CELL_ATOMS 64
 
-typedef enum { SLD_FP64 = 0, SLD_SPLIT = 1 } sld_precision;
+/* SLD_FP64: the reference's arithmetic (FP64, interpolated 10^6-point
+   tables); SLD_SPLIT: FP32 pair terms from the analytic potential with
+   compensated sums, FP64 integration and reductions; SLD_FP64_ANALYTIC: the
+   split form's kernels evaluated in FP64 (the error reference for
+   SLD_SPLIT). */
+typedef enum { SLD_FP64 = 0, SLD_SPLIT = 1, SLD_FP64_ANALYTIC = 2 } sld_precision;
 
 typedef struct {
     double box[6];               /* d.xx d.yx d.yy d.zx d.zy d.zz (Angstrom);

@@ -39,21 +39,25 @@ __device__ __forceinline__ void add3(double4& a, double k, double x, double y, d
     a.x = a.x + k * x; a.y = a.y + k * y; a.z = a.z + k * z;
 }
 
-// C1 / C2: p_i += gamma/m dt / n (sum_cell p - p_i), Gauss-Seidel in list order
+// C1 / C2: p_i += gamma/m dt / n (sum_cell p - p_i), Gauss-Seidel in list
+// order.  The reference re-adds the cell's momenta for every atom; here the
+// cell sum is carried along and corrected by each update (the same sum up to
+// rounding), so the pass is linear in the cell's size.
 __device__ __forceinline__ void cell_mix(const Dev& D, const int* a, int n, double dt, bool backward) {
     double factor = D.gamma_L / D.atmass * dt / n;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int m = 0; m < n; ++m) {
+        double4 pm = D.p[a[m]];
+        sx = sx + pm.x; sy = sy + pm.y; sz = sz + pm.z;
+    }
     for (int q = 0; q < n; ++q) {
         int i = a[backward ? n - 1 - q : q];
-        double sx = 0.0, sy = 0.0, sz = 0.0;
-        for (int m = 0; m < n; ++m) {
-            double4 pm = D.p[a[m]];
-            sx = sx + pm.x; sy = sy + pm.y; sz = sz + pm.z;
-        }
         double4 p = D.p[i];
-        p.x = p.x + factor * (sx - p.x);
-        p.y = p.y + factor * (sy - p.y);
-        p.z = p.z + factor * (sz - p.z);
-        D.p[i] = p;
+        double nx = p.x + factor * (sx - p.x);
+        double ny = p.y + factor * (sy - p.y);
+        double nz = p.z + factor * (sz - p.z);
+        sx += nx - p.x; sy += ny - p.y; sz += nz - p.z;
+        D.p[i] = make_double4(nx, ny, nz, 0.0);
     }
 }
 

@@ -14,9 +14,21 @@
 // image is applied with the reference's arithmetic (find_image) and only to
 // pairs whose cells are neighbours across the periodic boundary; for all
 // other pairs the reference's find_image leaves the vector unchanged.
-#include "sld_common.cuh"
+#include "sld_pot32.cuh"
 
+// pair vector (FP64, minimum image with the reference's arithmetic)
+__device__ __forceinline__ double3 pair_d(const Dev& D, double4 ri, int pk) {
+    double4 rj = D.r[pk & SLD_JMASK];
+    double3 d = make_double3(ri.x - rj.x, ri.y - rj.y, ri.z - rj.z);
+    if (pk & SLD_WRAP) d = find_image(D, d);
+    return d;
+}
+
+// MODE 0: FP64 tables (the reference's arithmetic); 1: split form (FP32
+// analytic); 2: the analytic forms in FP64
+template <int MODE>
 __global__ void __launch_bounds__(128) k_pairs(Dev D, int write_rho) {
+    constexpr bool SPLIT = MODE == 1;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= D.natom) return;
     unsigned* err = &D.ctl->err;
@@ -25,92 +37,113 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, int write_rho) {
     int c0 = D.cell_of[i], cx, cy, cz;
     cell_xyz(D, c0, cx, cy, cz);
     double rho = 0.0;
+    Kahan rho32;
+    const float rmax2f = (float)D.rcut_max_sq, rmag2f = (float)D.rcut_mag_sq;
+    const float rpotf = (float)D.rcut_pot;
     int nn = 0, nj = 0;
     for (int k = 0; k < 27; ++k) {
         bool wrap = false;
         int c = k == 26 ? c0 : nbr_cell_w(D, cx, cy, cz, k, wrap);
         int st = D.cell_start[c], n = D.cell_count[c];
-        for (int m = 0; m < n; ++m) {
-            int j = D.cell_atoms[st + m];
-            if (j == i) continue;
-            double4 rj = D.r[j];
+        for (int m0 = 0; m0 < n; m0 += SLD_GB) {
+          int jb[SLD_GB];
+          double4 rb[SLD_GB];
+#pragma unroll
+          for (int u = 0; u < SLD_GB; ++u) jb[u] = m0 + u < n ? D.cell_atoms[st + m0 + u] : -1;
+#pragma unroll
+          for (int u = 0; u < SLD_GB; ++u) rb[u] = jb[u] >= 0 ? D.r[jb[u]] : ri;
+#pragma unroll
+          for (int u = 0; u < SLD_GB; ++u) {
+            int j = jb[u];
+            if (j < 0 || j == i) continue;
+            double4 rj = rb[u];
             double3 d = make_double3(ri.x - rj.x, ri.y - rj.y, ri.z - rj.z);
             if (wrap) d = find_image(D, d);
-            double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
-            if (rsq >= D.rcut_max_sq) continue;
-            if (nn < SLD_MAXNB) D.nbr[(size_t)nn * N + i] = j | (wrap ? SLD_WRAP : 0);
-            ++nn;
-            double r0 = sqrt(rsq);
-            if (r0 < D.rcut_pot) rho += interp(D.tf, r0, D.inv_r, err);
-            if (rsq < D.rcut_mag_sq) {
-                if (nj < SLD_MAXJ) {
-                    D.jl[(size_t)nj * N + i] = j;
-                    D.jv[(size_t)nj * N + i] = interp(D.tJ, r0, D.inv_r, err);
+            if constexpr (!SPLIT) {
+                double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
+                if (rsq >= D.rcut_max_sq) continue;
+                if (nn < SLD_MAXNB) D.nbr[(size_t)nn * N + i] = j | (wrap ? SLD_WRAP : 0);
+                ++nn;
+                double r0 = sqrt(rsq);
+                if (r0 < D.rcut_pot) {
+                    if constexpr (MODE == 0) {
+                        rho += interp(D.tf, r0, D.inv_r, err);
+                    } else {
+                        double f, df;
+                        dens64(D, r0, f, df);
+                        rho += f;
+                    }
                 }
-                ++nj;
+                if (rsq < D.rcut_mag_sq) {
+                    if (nj < SLD_MAXJ) {
+                        D.jl[(size_t)nj * N + i] = j;
+                        double J, dJ;
+                        if constexpr (MODE == 0) J = interp(D.tJ, r0, D.inv_r, err);
+                        else exch64(r0, J, dJ);
+                        D.jv[(size_t)nj * N + i] = J;
+                    }
+                    ++nj;
+                }
+            } else {
+                float dx = (float)d.x, dy = (float)d.y, dz = (float)d.z;
+                float rsq = dx * dx + dy * dy + dz * dz;
+                if (rsq >= rmax2f) continue;
+                if (nn < SLD_MAXNB) D.nbr[(size_t)nn * N + i] = j | (wrap ? SLD_WRAP : 0);
+                ++nn;
+                double r64 = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
+                float f, df;
+                if ((float)r64 < rpotf) {
+                    dens32r(D, r64, f, df);
+                    rho32.add(f);
+                }
+                if (rsq < rmag2f) {
+                    if (nj < SLD_MAXJ) {
+                        float J, dJ;
+                        exch32r(r64, J, dJ);
+                        D.jl[(size_t)nj * N + i] = j;
+                        D.jvf[(size_t)nj * N + i] = J;
+                    }
+                    ++nj;
+                }
             }
+          }
         }
     }
     if (nn > SLD_MAXNB || nj > SLD_MAXJ) atomicOr(err, SLD_FLAG_CAPACITY);
     D.nbr_n[i] = nn < SLD_MAXNB ? nn : SLD_MAXNB;
     D.jl_n[i] = nj < SLD_MAXJ ? nj : SLD_MAXJ;
-    if (write_rho) D.rho[i] = rho;
+    if (write_rho) D.rho[i] = SPLIT ? rho32.value() : rho;
 }
 
-__global__ void __launch_bounds__(128) k_force(Dev D) {
+// F'(rho) per atom (the force pass needs it for both atoms of every pair)
+template <int MODE>
+__global__ void __launch_bounds__(256) k_embed(Dev D) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= D.natom) return;
-    unsigned* err = &D.ctl->err;
-    const int N = D.natom;
-    double4 ri = D.r[i];
-    double4 si = D.s[i];
-    double si_sq = si.x * si.x + si.y * si.y + si.z * si.z;
-    double rho_i = D.rho[i];
-    double dF_i = interp(D.tdF, rho_i, D.inv_rho, err);
-    double fx = 0, fy = 0, fz = 0, pe = 0, me = 0, me0 = 0, vir = 0;
-    double s11 = 0, s22 = 0, s33 = 0, s12 = 0, s23 = 0, s31 = 0;
-    int nn = D.nbr_n[i];
-    for (int e = 0; e < nn; ++e) {
-        int pk = D.nbr[(size_t)e * N + i];
-        int j = pk & SLD_JMASK;
-        double4 rj = D.r[j];
-        double3 d = make_double3(ri.x - rj.x, ri.y - rj.y, ri.z - rj.z);
-        if (pk & SLD_WRAP) d = find_image(D, d);
-        double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
-        double r0 = sqrt(rsq);
-        double dudr = 0.0, dudr_spin = 0.0;
-        if (r0 < D.rcut_pot) {
-            double df = interp(D.tdf, r0, D.inv_r, err);
-            double dF_j = interp(D.tdF, D.rho[j], D.inv_rho, err);
-            dudr = (dF_i + dF_j) * df + interp(D.tdphi, r0, D.inv_r, err);
-            // the Landau tables are rho-independent: their derivative
-            // tables are zero and add nothing to dudr
-            pe += 0.5 * interp(D.tphi, r0, D.inv_r, err);
-        }
-        if (r0 < D.rcut_mag) {
-            double4 sj = D.s[j];
-            double sj_sq = sj.x * sj.x + sj.y * sj.y + sj.z * sj.z;
-            double dot = si.x * sj.x + si.y * sj.y + si.z * sj.z;
-            double times = sqrt(si_sq * sj_sq);
-            dudr_spin = -interp(D.tdJ, r0, D.inv_r, err) * (dot - times);
-            double Jh = interp(D.tJ, r0, D.inv_r, err) / 2.0;
-            me0 += Jh * times;
-            me += -Jh * dot;
-        }
-        dudr += dudr_spin;
-        double force = -dudr / r0;
-        double gx = force * d.x, gy = force * d.y, gz = force * d.z;
-        fx += gx; fy += gy; fz += gz;
-        s11 += gx * d.x; s22 += gy * d.y; s33 += gz * d.z;
-        s12 += gx * d.y; s23 += gy * d.z; s31 += gz * d.x;
-        vir += -force * rsq;
+    if constexpr (MODE == 1) {
+        float F, dF;
+        emb32((float)D.rho[i], F, dF);
+        D.dF[i] = (double)dF;
+    } else if constexpr (MODE == 2) {
+        double F, dF;
+        emb64(D.rho[i], F, dF);
+        D.dF[i] = dF;
+    } else {
+        D.dF[i] = interp(D.tdF, D.rho[i], D.inv_rho, &D.ctl->err);
     }
-    pe += interp(D.tF, rho_i, D.inv_rho, err);
+}
+
+// on-site terms and outputs common to both forms
+__device__ __forceinline__ void force_finish(const Dev& D, int i, double si_sq, double rho_i,
+                                             double F_i, double fx, double fy, double fz, double pe,
+                                             double me, double me0, double vir, const double st6[6]) {
+    pe += F_i;
     double A = interp_const(D.landau[0], rho_i, D.inv_rho);
     double B = interp_const(D.landau[1], rho_i, D.inv_rho);
     double C = interp_const(D.landau[2], rho_i, D.inv_rho);
     double Dd = interp_const(D.landau[3], rho_i, D.inv_rho);
-    me += A * si_sq + B * (si_sq * si_sq) + C * pow(si_sq, 3.0) + Dd * pow(si_sq, 4.0);
+    double s4 = si_sq * si_sq;
+    me += A * si_sq + B * s4 + C * (s4 * si_sq) + Dd * (s4 * s4);
     D.f[i] = make_double4(fx, fy, fz, 0.0);
     D.pe[i] = pe;
     D.me[i] = me;
@@ -120,18 +153,180 @@ __global__ void __launch_bounds__(128) k_force(Dev D) {
     double4 p = D.p[i];
     double m = D.atmass, V = D.box_volume / D.natom;
     double* out = D.stress + 6 * (size_t)i;
-    out[0] = ((p.x * p.x) / m + s11 / 2.0) / V;
-    out[1] = ((p.y * p.y) / m + s22 / 2.0) / V;
-    out[2] = ((p.z * p.z) / m + s33 / 2.0) / V;
-    out[3] = ((p.x * p.y) / m + s12 / 2.0) / V;
-    out[4] = ((p.y * p.z) / m + s23 / 2.0) / V;
-    out[5] = ((p.z * p.x) / m + s31 / 2.0) / V;
-    if (!isfinite(fx + fy + fz + pe + me)) atomicOr(err, SLD_FLAG_NAN);
+    out[0] = ((p.x * p.x) / m + st6[0] / 2.0) / V;
+    out[1] = ((p.y * p.y) / m + st6[1] / 2.0) / V;
+    out[2] = ((p.z * p.z) / m + st6[2] / 2.0) / V;
+    out[3] = ((p.x * p.y) / m + st6[3] / 2.0) / V;
+    out[4] = ((p.y * p.z) / m + st6[4] / 2.0) / V;
+    out[5] = ((p.z * p.x) / m + st6[5] / 2.0) / V;
+    if (!isfinite(fx + fy + fz + pe + me)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
+}
+
+// FP64 force pass; AN: the analytic forms instead of the tables
+template <bool AN>
+__global__ void __launch_bounds__(128) k_force64(Dev D) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.natom) return;
+    unsigned* err = &D.ctl->err;
+    const int N = D.natom;
+    double4 ri = D.r[i];
+    double4 si = D.s[i];
+    double si_sq = si.x * si.x + si.y * si.y + si.z * si.z;
+    double rho_i = D.rho[i];
+    double dF_i = D.dF[i];
+    double fx = 0, fy = 0, fz = 0, pe = 0, me = 0, me0 = 0, vir = 0;
+    double st6[6] = {0, 0, 0, 0, 0, 0};
+    int nn = D.nbr_n[i];
+    for (int e0 = 0; e0 < nn; e0 += 4) {
+      int pkb[4];
+      double4 rjb[4];
+      double dFb[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) pkb[u] = e0 + u < nn ? D.nbr[(size_t)(e0 + u) * N + i] : -1;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+          int j = pkb[u] & SLD_JMASK;
+          rjb[u] = pkb[u] >= 0 ? D.r[j] : ri;
+          dFb[u] = pkb[u] >= 0 ? D.dF[j] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        int pk = pkb[u];
+        if (pk < 0) continue;
+        int j = pk & SLD_JMASK;
+        double3 d = make_double3(ri.x - rjb[u].x, ri.y - rjb[u].y, ri.z - rjb[u].z);
+        if (pk & SLD_WRAP) d = find_image(D, d);
+        double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
+        double r0 = sqrt(rsq);
+        double dudr = 0.0, dudr_spin = 0.0;
+        if (r0 < D.rcut_pot) {
+            double df, dphi, phi;
+            if constexpr (AN) {
+                double f;
+                dens64(D, r0, f, df);
+                pair64(D, r0, phi, dphi);
+            } else {
+                df = interp(D.tdf, r0, D.inv_r, err);
+                dphi = interp(D.tdphi, r0, D.inv_r, err);
+                phi = interp(D.tphi, r0, D.inv_r, err);
+            }
+            dudr = (dF_i + dFb[u]) * df + dphi;
+            // the Landau tables are rho-independent: their derivative
+            // tables are zero and add nothing to dudr
+            pe += 0.5 * phi;
+        }
+        if (r0 < D.rcut_mag) {
+            double4 sj = D.s[j];
+            double sj_sq = sj.x * sj.x + sj.y * sj.y + sj.z * sj.z;
+            double dot = si.x * sj.x + si.y * sj.y + si.z * sj.z;
+            double times = sqrt(si_sq * sj_sq);
+            double J, dJ;
+            if constexpr (AN) {
+                exch64(r0, J, dJ);
+            } else {
+                dJ = interp(D.tdJ, r0, D.inv_r, err);
+                J = interp(D.tJ, r0, D.inv_r, err);
+            }
+            dudr_spin = -dJ * (dot - times);
+            double Jh = J / 2.0;
+            me0 += Jh * times;
+            me += -Jh * dot;
+        }
+        dudr += dudr_spin;
+        double force = -dudr / r0;
+        double gx = force * d.x, gy = force * d.y, gz = force * d.z;
+        fx += gx; fy += gy; fz += gz;
+        st6[0] += gx * d.x; st6[1] += gy * d.y; st6[2] += gz * d.z;
+        st6[3] += gx * d.y; st6[4] += gy * d.z; st6[5] += gz * d.x;
+        vir += -force * rsq;
+      }
+    }
+    double F_i;
+    if constexpr (AN) {
+        double dF_unused;
+        emb64(rho_i, F_i, dF_unused);
+    } else {
+        F_i = interp(D.tF, rho_i, D.inv_rho, err);
+    }
+    force_finish(D, i, si_sq, rho_i, F_i, fx, fy, fz, pe, me, me0,
+                 vir, st6);
+}
+
+// split form: FP32 pair terms from the analytic potential, Kahan sums
+__global__ void __launch_bounds__(128) k_force32(Dev D) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.natom) return;
+    const int N = D.natom;
+    double4 ri = D.r[i];
+    double4 si = D.s[i];
+    double si_sq = si.x * si.x + si.y * si.y + si.z * si.z;
+    float sx = (float)si.x, sy = (float)si.y, sz = (float)si.z;
+    float si_sqf = sx * sx + sy * sy + sz * sz;
+    double rho_i = D.rho[i];
+    float dF_i = (float)D.dF[i];
+    const float rpot = (float)D.rcut_pot, rmag = (float)D.rcut_mag;
+    Kahan fx, fy, fz, pe, me, me0;
+    float vir = 0.f, st6f[6] = {0, 0, 0, 0, 0, 0};
+    int nn = D.nbr_n[i];
+    for (int e = 0; e < nn; ++e) {
+        int pk = D.nbr[(size_t)e * N + i];
+        int j = pk & SLD_JMASK;
+        double3 dd = pair_d(D, ri, pk);
+        float dx = (float)dd.x, dy = (float)dd.y, dz = (float)dd.z;
+        double r64 = sqrt(dd.x * dd.x + dd.y * dd.y + dd.z * dd.z);
+        float r0 = (float)r64, rsq = r0 * r0;
+        float dudr = 0.f;
+        if (r0 < rpot) {
+            float f, df, phi, dphi;
+            dens32r(D, r64, f, df);
+            pair32r(D, r64, phi, dphi);
+            dudr = (dF_i + (float)D.dF[j]) * df + dphi;
+            pe.add(0.5f * phi);
+        }
+        if (r0 < rmag) {
+            double4 sj4 = D.s[j];
+            float tx = (float)sj4.x, ty = (float)sj4.y, tz = (float)sj4.z;
+            float sj_sq = tx * tx + ty * ty + tz * tz;
+            float dot = sx * tx + sy * ty + sz * tz;
+            float times = sqrtf(si_sqf * sj_sq);
+            float J, dJ;
+            exch32r(r64, J, dJ);
+            dudr += -dJ * (dot - times);
+            float Jh = 0.5f * J;
+            me0.add(Jh * times);
+            me.add(-Jh * dot);
+        }
+        float force = -dudr / r0;
+        float gx = force * dx, gy = force * dy, gz = force * dz;
+        fx.add(gx); fy.add(gy); fz.add(gz);
+        st6f[0] += gx * dx; st6f[1] += gy * dy; st6f[2] += gz * dz;
+        st6f[3] += gx * dy; st6f[4] += gy * dz; st6f[5] += gz * dx;
+        vir += -force * rsq;
+    }
+    float F, dF;
+    emb32((float)rho_i, F, dF);
+    double st6[6];
+    for (int k = 0; k < 6; ++k) st6[k] = st6f[k];
+    force_finish(D, i, si_sq, rho_i, (double)F, fx.value(), fy.value(), fz.value(), pe.value(),
+                 me.value(), me0.value(), (double)vir, st6);
 }
 
 void launch_pairs(const Dev& D, cudaStream_t st, bool write_rho) {
-    k_pairs<<<div_up(D.natom, 128), 128, 0, st>>>(D, write_rho ? 1 : 0);
+    int nb = div_up(D.natom, 128), w = write_rho ? 1 : 0;
+    if (D.split) k_pairs<1><<<nb, 128, 0, st>>>(D, w);
+    else if (D.analytic) k_pairs<2><<<nb, 128, 0, st>>>(D, w);
+    else k_pairs<0><<<nb, 128, 0, st>>>(D, w);
+}
+void launch_embed(const Dev& D, cudaStream_t st) {
+    int nb = div_up(D.natom, 256);
+    if (D.split) k_embed<1><<<nb, 256, 0, st>>>(D);
+    else if (D.analytic) k_embed<2><<<nb, 256, 0, st>>>(D);
+    else k_embed<0><<<nb, 256, 0, st>>>(D);
 }
 void launch_force(const Dev& D, cudaStream_t st) {
-    k_force<<<div_up(D.natom, 128), 128, 0, st>>>(D);
+    launch_embed(D, st);
+    int nb = div_up(D.natom, 128);
+    if (D.split) k_force32<<<nb, 128, 0, st>>>(D);
+    else if (D.analytic) k_force64<true><<<nb, 128, 0, st>>>(D);
+    else k_force64<false><<<nb, 128, 0, st>>>(D);
 }

@@ -19,6 +19,9 @@
 // A block whose cells hold more atoms (or in-cell neighbours) than its
 // shared-memory tables falls back to one thread per cell reading everything
 // from global memory, with the same arithmetic.
+#include <cstdlib>
+
+#include "sld_pot32.cuh"
 #include "sld_spin.cuh"
 
 #define SW_CPB 32
@@ -52,17 +55,9 @@ __device__ __forceinline__ void visit_store(const Dev& D, int i, double3 s, doub
 
 // one visit entirely from global memory (the fallback path)
 __device__ void visit_global(const Dev& D, int i, double dt, unsigned long long epoch, bool fields) {
-    const int N = D.natom;
-    double3 H = make_double3(0.0, 0.0, 0.0);
-    double sumJ = 0.0;
-    int nj = D.jl_n[i];
-    for (int e = 0; e < nj; ++e) {
-        int j = D.jl[(size_t)e * N + i];
-        double J = D.jv[(size_t)e * N + i];
-        double4 sj = D.s[j];
-        H.x += J * sj.x; H.y += J * sj.y; H.z += J * sj.z;
-        sumJ += J * sj.w;
-    }
+    double3 H;
+    double sumJ;
+    exchange_field(D, i, H, sumJ, [](int) { return false; }, [](int, double) {});
     double4 s4 = D.s[i];
     double T = 0.0, rho = 0.0;
     double3 xi = make_double3(0.0, 0.0, 0.0);
@@ -81,7 +76,6 @@ __global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restri
                                                       int epoch_off) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SweepShared& S = *reinterpret_cast<SweepShared*>(smem_raw);
-    const int N = D.natom;
     const int cbeg = blockIdx.x * SW_CPB;
     const int ncb = min(SW_CPB, ncell_g - cbeg);
     const unsigned long long epoch = D.ctl->epoch + (unsigned long long)epoch_off;
@@ -123,27 +117,22 @@ __global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restri
             S.slot[a] = i;
             double4 si = D.s[i];
             S.s[a][0] = si.x; S.s[a][1] = si.y; S.s[a][2] = si.z; S.s[a][3] = si.w;
-            double hx = 0, hy = 0, hz = 0, hj = 0;
             int nin = 0;
-            int nj = D.jl_n[i];
-            for (int e = 0; e < nj; ++e) {
-                int j = D.jl[(size_t)e * N + i];
-                double J = D.jv[(size_t)e * N + i];
-                if (D.cell_of[j] == c) {
-                    int st = S.cell_start[q], n = S.cell_n[q], pos = 0;
-                    while (pos < n && D.cell_atoms[st + pos] != j) ++pos;
+            const int cst = S.cell_start[q], cn = S.cell_n[q];
+            double3 Ho;
+            double hjo;
+            exchange_field(
+                D, i, Ho, hjo, [&](int j) { return D.cell_of[j] == c; },
+                [&](int j, double J) {
+                    int pos = 0;
+                    while (pos < cn && D.cell_atoms[cst + pos] != j) ++pos;
                     if (nin < SW_MAXIN) {
                         S.inq[a][nin] = (unsigned char)pos;
                         S.inJ[a][nin] = J;
                     }
                     ++nin;
-                } else {
-                    double4 sj = D.s[j];
-                    hx += J * sj.x; hy += J * sj.y; hz += J * sj.z;
-                    hj += J * sj.w;
-                }
-            }
-            S.h[a][0] = hx; S.h[a][1] = hy; S.h[a][2] = hz; S.h[a][3] = hj;
+                });
+            S.h[a][0] = Ho.x; S.h[a][1] = Ho.y; S.h[a][2] = Ho.z; S.h[a][3] = hjo;
             S.inn[a] = (unsigned char)(nin < SW_MAXIN ? nin : SW_MAXIN);
             if (nin > SW_MAXIN) S.overflow = 1;
             if (D.spinlang) {
@@ -202,15 +191,40 @@ __global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restri
     }
 }
 
+// one thread per cell for the whole visit, reading the spins from global
+// memory (no shared-memory phases)
+__global__ void __launch_bounds__(128) k_sweep_cell(Dev D, const int* __restrict__ gcells,
+                                                    int ncell_g, double dt, int backward,
+                                                    int epoch_off) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ncell_g) return;
+    int c = gcells[t];
+    int st = D.cell_start[c], n = D.cell_count[c];
+    unsigned long long epoch = D.ctl->epoch + (unsigned long long)epoch_off;
+    bool fields = backward != 0;
+    for (int m = 0; m < n; ++m) {
+        int i = D.cell_atoms[st + (backward ? n - 1 - m : m)];
+        visit_global(D, i, dt, epoch, fields);
+    }
+}
+
 static size_t sweep_smem() { return sizeof(SweepShared); }
+static int g_sweep_mode = 1;   // 0: two-level (shared memory), 1: one thread per cell
 
 void sweep_init() {
     cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem());
+    const char* v = getenv("SLD_SWEEP_MODE");
+    if (v && (v[0] == '0' || v[0] == '1')) g_sweep_mode = v[0] - '0';
 }
 
 void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g, double dt,
                   bool backward, int epoch_off) {
     if (ncell_g <= 0) return;
+    if (g_sweep_mode == 1) {
+        k_sweep_cell<<<div_up(ncell_g, 128), 128, 0, st>>>(D, gcells, ncell_g, dt, backward ? 1 : 0,
+                                                          epoch_off);
+        return;
+    }
     k_sweep<<<div_up(ncell_g, SW_CPB), SW_THREADS, sweep_smem(), st>>>(D, gcells, ncell_g, dt,
                                                                        backward ? 1 : 0, epoch_off);
 }

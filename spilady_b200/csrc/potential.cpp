@@ -136,4 +136,53 @@ double pot_f(double r) { return dens_f(r); }
 double pot_phi(double r) { return pair_phi(r); }
 double pot_J(double r) { return exch_J(r); }
 
+void pot_join_data(double o[7]) {
+    const double x1 = 1.8, x2 = 2.0, h = 1e-7;
+    o[0] = zbl(x1);
+    o[1] = (zbl(x1 + h) - zbl(x1 - h)) / 2e-7;
+    o[2] = (zbl(x1 + h) + zbl(x1 - h) - 2e0 * zbl(x1)) / std::pow(h, 2);
+    o[3] = pair_knots(x2, 0);
+    o[4] = pair_knots(x2, 1);
+    o[5] = pair_knots(x2, 2);
+    o[6] = 0.88535e0 * 0.52917720859e0 / (2e0 * std::pow(26e0, 0.23));
+}
+
+static void cubic_pieces(const double* a, const double* k, int n, float* K, float* C, double* K64,
+                         double* C64) {
+    // knots ascending (the arrays here are given descending)
+    std::vector<int> ord(n);
+    for (int i = 0; i < n; ++i) ord[i] = n - 1 - i;
+    for (int i = 0; i < n; ++i) {
+        K[i] = (float)k[ord[i]];
+        K64[i] = (double)K[i];
+    }
+    for (int m = 0; m <= n; ++m) {
+        double c[4] = {0, 0, 0, 0};
+        if (m < n) {
+            double base = (double)(m == 0 ? K[0] : K[m - 1]);
+            for (int q = 0; q < n; ++q) {
+                int i = ord[q];
+                if (q < m) continue;          // knot at or below the interval: inactive
+                double dl = k[i] - base;
+                c[0] += a[i] * dl * dl * dl;
+                c[1] += -3e0 * a[i] * dl * dl;
+                c[2] += 3e0 * a[i] * dl;
+                c[3] += -a[i];
+            }
+        }
+        for (int q = 0; q < 4; ++q) {
+            C[4 * m + q] = (float)c[q];
+            C64[4 * m + q] = c[q];
+        }
+    }
+}
+
+void pot_cubic_tables(float out[kCubicFloats], double o64[kCubicFloats]) {
+    static const double da[6] = {0.9332056681088162, -1.162558782567700, -0.3502026949249225,
+                                 0.4287820835430028, 4.907925057809273, -5.307049068415304};
+    static const double dk[6] = {3.0, 2.8666666666666666, 2.7333333333333333, 2.6, 2.4, 2.3};
+    cubic_pieces(kPV, kPK, 8, out, out + 8, o64, o64 + 8);
+    cubic_pieces(da, dk, 6, out + 44, out + 50, o64 + 44, o64 + 50);
+}
+
 }  // namespace sld

@@ -18,5 +18,17 @@ double pot_F(double rho);
 double pot_f(double r);
 double pot_phi(double r);
 double pot_J(double r);
+// Hermite data of the pair term's 1.8-2.0 A join: y, y', y'' of the ZBL core
+// at 1.8 A and of the cubic knots at 2.0 A, then the ZBL screening length
+void pot_join_data(double out[7]);
+
+// Piecewise-cubic form of the DD05 pair term (r > 2 A) and density: between
+// consecutive knots each is one cubic, written here in t = r - base with the
+// base stored as FP32.  Layout (floats): pair knots [0,8), pair coefficients
+// [8,44) (9 intervals x c0..c3), density knots [44,50), density coefficients
+// [50,78) (7 intervals).  Interval m holds r with m knots <= r; its base is
+// knot m-1 (knot 0 for m = 0); the last interval is zero.
+constexpr int kCubicFloats = 78;
+void pot_cubic_tables(float out[kCubicFloats], double out64[kCubicFloats]);
 
 }  // namespace sld

@@ -41,6 +41,7 @@ struct sld_ctx {
     int* d_gcells = nullptr;
     int* d_te_gcells = nullptr;
     int* d_te_gstart = nullptr;
+    unsigned char* d_te_color = nullptr;
     double* d_avg = nullptr;
     cudaStream_t st = nullptr;
     cudaGraphExec_t step_graph = nullptr;
@@ -131,7 +132,9 @@ int validate(const sld_params* p) {
     if (p->rcut_pot > p->rcut_max || p->rcut_mag > p->rcut_max) return SLD_ERR_ARG;
     if (p->eltemp && !(p->spinlang && p->lattlang)) return SLD_ERR_ARG;
     if (p->localcolmot && !p->lattlang) return SLD_ERR_ARG;
-    if (p->precision != SLD_FP64) return SLD_ERR_ARG;   // the split form is not built yet
+    if (p->precision != SLD_FP64 && p->precision != SLD_SPLIT &&
+        p->precision != SLD_FP64_ANALYTIC)
+        return SLD_ERR_ARG;
     if (p->te_mesh != 0 && p->te_mesh < 3) return SLD_ERR_ARG;
     return SLD_OK;
 }
@@ -196,6 +199,7 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
 
     if (cudaSetDevice(prm->device) != cudaSuccess) { delete c; return SLD_ERR_CUDA; }
     sweep_init();
+    dte_init(prm->device);
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
         return SLD_ERR_CUDA;
@@ -234,6 +238,17 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     D.print_every = c->P.interval_of_print_out;
     D.te_nloop = c->P.te_nloop;
     D.small_grid = (G.nx < 4 || G.ny < 4 || G.nz < 4) ? 1 : 0;
+    D.split = prm->precision == SLD_SPLIT ? 1 : 0;
+    D.analytic = prm->precision == SLD_FP64_ANALYTIC ? 1 : 0;
+    {
+        double jd[7];
+        sld::pot_join_data(jd);
+        D.pot32 = Pot32{(float)jd[0], (float)jd[1], (float)jd[2], (float)jd[3],
+                        (float)jd[4], (float)jd[5], (float)jd[6]};
+    }
+    float cubic_h[sld::kCubicFloats];
+    double cubic64_h[sld::kCubicFloats];
+    sld::pot_cubic_tables(cubic_h, cubic64_h);
 
     size_t n = (size_t)natom;
     double* tabs[sld::kTabCount];
@@ -256,8 +271,21 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
          c->alloc(&D.cell_count, (size_t)G.ncells) == 0 &&
          c->alloc(&D.cell_atoms, n) == 0 && c->alloc(&D.cell_fill, (size_t)G.ncells) == 0 &&
          c->alloc(&D.nbr, (size_t)SLD_MAXNB * n) == 0 && c->alloc(&D.nbr_n, n) == 0 &&
-         c->alloc(&D.jl, (size_t)SLD_MAXJ * n) == 0 && c->alloc(&D.jv, (size_t)SLD_MAXJ * n) == 0 &&
-         c->alloc(&D.jl_n, n) == 0;
+         c->alloc(&D.jl, (size_t)SLD_MAXJ * n) == 0 && c->alloc(&D.jl_n, n) == 0 &&
+         c->alloc(&D.dF, n) == 0;
+    {
+        float* cub = nullptr;
+        double* cub64 = nullptr;
+        ok = ok && c->alloc(&cub, sld::kCubicFloats) == 0 && c->alloc(&cub64, sld::kCubicFloats) == 0;
+        if (ok) {
+            cudaMemcpy(cub, cubic_h, sizeof(cubic_h), cudaMemcpyHostToDevice);
+            cudaMemcpy(cub64, cubic64_h, sizeof(cubic64_h), cudaMemcpyHostToDevice);
+        }
+        D.cubic = cub;
+        D.cubic64 = cub64;
+    }
+    if (prm->precision == SLD_SPLIT) ok = ok && c->alloc(&D.jvf, (size_t)SLD_MAXJ * n) == 0;
+    else ok = ok && c->alloc(&D.jv, (size_t)SLD_MAXJ * n) == 0;
     c->scan_blocks = div_up(G.ncells, 1024);
     ok = ok && c->alloc(&D.scan_tmp, (size_t)c->scan_blocks) == 0;
     if (prm->te_mesh > 0) {
@@ -275,12 +303,21 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     ok = ok && c->alloc(&D.ctl, 1) == 0 && c->alloc(&c->d_avg, 16) == 0;
     ok = ok && c->alloc(&c->d_gcells, (size_t)G.ncells) == 0;
     ok = ok && c->alloc(&c->d_te_gcells, (size_t)nte) == 0 &&
-         c->alloc(&c->d_te_gstart, G.te_gstart.size()) == 0;
+         c->alloc(&c->d_te_gstart, G.te_gstart.size()) == 0 &&
+         c->alloc(&c->d_te_color, (size_t)nte) == 0;
     if (!ok) { sld_destroy(c); return SLD_ERR_NOMEM; }
     cudaMemcpy(c->d_gcells, G.gcells.data(), sizeof(int) * G.ncells, cudaMemcpyHostToDevice);
     cudaMemcpy(c->d_te_gcells, G.te_gcells.data(), sizeof(int) * nte, cudaMemcpyHostToDevice);
     cudaMemcpy(c->d_te_gstart, G.te_gstart.data(), sizeof(int) * G.te_gstart.size(),
                cudaMemcpyHostToDevice);
+    {
+        std::vector<unsigned char> col(nte, 0);
+        for (int g = 0; g < G.te_ngroups; ++g)
+            for (int m = G.te_gstart[g]; m < G.te_gstart[g + 1]; ++m)
+                col[G.te_gcells[m]] = (unsigned char)g;
+        cudaMemcpy(c->d_te_color, col.data(), nte, cudaMemcpyHostToDevice);
+        D.te_color = c->d_te_color;
+    }
     D.te_gcells = c->d_te_gcells;
     D.te_gstart = c->d_te_gstart;
     D.te_ngroups = G.te_ngroups;

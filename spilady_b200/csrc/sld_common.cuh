@@ -41,6 +41,13 @@ struct Ctl {
     double avg[8];                // last energy averages
 };
 
+// data of the quintic that joins the ZBL core to the cubic knots of the
+// DD05 pair term between 1.8 and 2.0 A (split form)
+struct Pot32 {
+    float zbl_y1, zbl_d1, zbl_c1, knot_y2, knot_d2, knot_c2;
+    float zbl_as;   // ZBL screening length
+};
+
 struct Dev {
     // box (struct.h box_vector order: xx yx yy zx zy zz) and inverse
     double d[6], inv[6];
@@ -56,6 +63,11 @@ struct Dev {
     int spinlang, lattlang, eltemp, localcolmot, renormalize, print_every;
     int te_nloop;
     int small_grid;               // a link-cell axis of 3: every pair gets the minimum image
+    int split;                    // 1: split-precision form (FP32 pair terms)
+    int analytic;                 // 1: the split form's kernels in FP64
+    Pot32 pot32;
+    const float* cubic;           // piecewise-cubic pair and density coefficients
+    const double* cubic64;        // the same in FP64 (analytic FP64 form)
     // tables (potential_CPU.cpp:61-157): F, F', f, f', phi, phi', J, J'
     const double *tF, *tdF, *tf, *tdf, *tphi, *tdphi, *tJ, *tdJ;
     // atoms
@@ -69,13 +81,16 @@ struct Dev {
     double *Te, *Ee, *Tl, *TsR, *TsL, *Gel, *Ges, *acc;   // acc: 9 per Te cell
     int* te_count;
     const int *te_gcells, *te_gstart;
+    const unsigned char* te_color;   // colour group of each Te cell
     int te_ngroups;
     // per-step neighbour lists (built after every drift by k_pairs):
     //   nbr  [SLD_MAXNB][natom]  j | (1<<30 when the pair crosses the box)
     //        for r_ij < rcut_max, in the reference's traversal order
     //   jl/jv [SLD_MAXJ][natom]  j and J(r_ij) for r_ij < rcut_mag
     int *nbr, *nbr_n, *jl, *jl_n;
-    double* jv;
+    double* jv;                   // FP64 form
+    float* jvf;                   // split form
+    double* dF;                   // F'(rho) per atom, refreshed after each rho pass
     // control and reduction scratch
     Ctl* ctl;
     double* red;                  // partial sums
@@ -240,18 +255,84 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 
 static inline int div_up(long a, long b) { return (int)((a + b - 1) / b); }
 
+// Exchange field of atom i from its J list: H = sum J_ij s_j and
+// sumJ = sum J_ij |s_j| in list order.  The list is read in batches of 8
+// (indices and J first, then the 8 spins) so that a batch costs two memory
+// latencies instead of two per neighbour; the additions stay in list order.
+// Entries whose neighbour satisfies skip(j) are left out (and reported to
+// on_skip(j, J)).  FP64 form: FP64 products and sums; split form: FP32
+// products with compensated FP32 sums.
+#define SLD_GB 8
+template <class Skip, class OnSkip>
+__device__ __forceinline__ void exchange_field(const Dev& D, int i, double3& H, double& sumJ,
+                                               Skip skip, OnSkip on_skip) {
+    const int N = D.natom;
+    const int nj = D.jl_n[i];
+    double hx = 0, hy = 0, hz = 0, hj = 0;
+    float ks[4] = {0, 0, 0, 0}, kc[4] = {0, 0, 0, 0};   // Kahan sums (split form)
+    for (int e0 = 0; e0 < nj; e0 += SLD_GB) {
+        int jj[SLD_GB];
+        double Jv[SLD_GB];
+#pragma unroll
+        for (int u = 0; u < SLD_GB; ++u) {
+            int e = e0 + u;
+            jj[u] = e < nj ? D.jl[(size_t)e * N + i] : -1;
+            Jv[u] = e < nj ? (D.split ? (double)D.jvf[(size_t)e * N + i] : D.jv[(size_t)e * N + i])
+                           : 0.0;
+        }
+        double4 sj[SLD_GB];
+#pragma unroll
+        for (int u = 0; u < SLD_GB; ++u)
+            sj[u] = jj[u] >= 0 ? D.s[jj[u]] : make_double4(0, 0, 0, 0);
+#pragma unroll
+        for (int u = 0; u < SLD_GB; ++u) {
+            if (jj[u] < 0) continue;
+            if (skip(jj[u])) {
+                on_skip(jj[u], Jv[u]);
+                continue;
+            }
+            if (!D.split) {
+                double J = Jv[u];
+                hx += J * sj[u].x; hy += J * sj[u].y; hz += J * sj[u].z;
+                hj += J * sj[u].w;
+            } else {
+                float J = (float)Jv[u];
+                float v[4] = {J * (float)sj[u].x, J * (float)sj[u].y, J * (float)sj[u].z,
+                              J * (float)sj[u].w};
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    float y = v[q] - kc[q];
+                    float t = ks[q] + y;
+                    kc[q] = (t - ks[q]) - y;
+                    ks[q] = t;
+                }
+            }
+        }
+    }
+    if (D.split) {
+        hx = (double)ks[0] - (double)kc[0];
+        hy = (double)ks[1] - (double)kc[1];
+        hz = (double)ks[2] - (double)kc[2];
+        hj = (double)ks[3] - (double)kc[3];
+    }
+    H = make_double3(hx, hy, hz);
+    sumJ = hj;
+}
+
 // ---------------------------------------------------------------------
 // launch wrappers (host), one file per kernel family
 void launch_links(const Dev& D, cudaStream_t st, bool initial, int scan_blocks);
 void launch_pairs(const Dev& D, cudaStream_t st, bool write_rho);
 void sweep_init();
 void launch_force(const Dev& D, cudaStream_t st);
+void launch_embed(const Dev& D, cudaStream_t st);
 void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g, double dt,
                   bool backward, int epoch_off);
 void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off);
 void launch_dr(const Dev& D, cudaStream_t st, double dt);
 void launch_temperature(const Dev& D, cudaStream_t st);
 void launch_dte(const Dev& D, cudaStream_t st, double dt);
+int dte_init(int device);
 void launch_energy_check(const Dev& D, cudaStream_t st, int mode);
 void launch_advance(const Dev& D, cudaStream_t st, int epochs, int steps);
 void launch_averages(const Dev& D, cudaStream_t st, double* out_dev);

@@ -24,7 +24,7 @@ __device__ __forceinline__ double3 spin_rotation(double3 H, double3 s, double dt
 __device__ __forceinline__ double3 landau_field(const double L[4], double sumJ, double3 x) {
     double s_sq = x.x * x.x + x.y * x.y + x.z * x.z;
     double c = -(2.0 * L[0] + 4.0 * L[1] * s_sq + 6.0 * L[2] * (s_sq * s_sq) +
-                 8.0 * L[3] * pow(s_sq, 3.0));
+                 8.0 * L[3] * (s_sq * s_sq * s_sq));
     double3 HL = make_double3(c * x.x, c * x.y, c * x.z);
     double s0 = sqrt(s_sq);
     if (s0 > 0.0) {

@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libsld_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "sld.h")
 
-FP64, SPLIT = 0, 1
+FP64, SPLIT, FP64_ANALYTIC = 0, 1, 2
 
 ERRORS = {
     -1: "SLD_ERR_ARG", -2: "SLD_ERR_CUDA", -3: "SLD_ERR_GEOMETRY",
