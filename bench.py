@@ -51,10 +51,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
+    ap.add_argument("--precision", default="split", choices=["fp64", "split", "fp64-analytic"])
     ap.add_argument("--size", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--small", action="store_true",
+                    help="short run for profiler captures: no CPU baseline, no e2e leg, "
+                         "one phase-profile step")
     return ap.parse_args()
 
 
@@ -202,13 +205,17 @@ def run_reference(args, world, rank):
 
 def main():
     args = parse()
+    if args.small:
+        args.no_cpu_baseline = True
+        args.no_e2e = True
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
         return
     from spilady_b200 import engine
     params, r, p, s, te, sw = workload(args.size)
-    prec = engine.SPLIT if args.precision == "split" else engine.FP64
+    prec = {"fp64": engine.FP64, "split": engine.SPLIT,
+            "fp64-analytic": engine.FP64_ANALYTIC}[args.precision]
     e = engine.Engine(params, r, p, s, te=te, device=local, precision=prec, **sw)
     natom = e.natom
     e.run(args.warmup)
@@ -231,9 +238,10 @@ def main():
 
     # per-phase device time (CUDA events on the engine's stream), a few steps
     prof = {}
-    for _ in range(3):
+    nprof = 1 if args.small else 3
+    for _ in range(nprof):
         for k, v in e.profile_step().items():
-            prof[k] = prof.get(k, 0.0) + v / 3
+            prof[k] = prof.get(k, 0.0) + v / nprof
     dom = max(prof, key=prof.get)
     peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
     hbm = peaks.get("hbm_gbs", 6650.0)
@@ -268,7 +276,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if prec == engine.FP64 else "f32+f64",
+        "dtype": "f32+f64" if prec == engine.SPLIT else "f64",
         "data": "synthetic",
         "config": {"workload": f"bcc Fe {args.size}^3 cells ({natom} atoms) spin-lattice-electron,"
                                f" Langevin spin+lattice, localcolmot, Te mesh {sw['te_mesh']}^3,"

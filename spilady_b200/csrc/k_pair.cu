@@ -14,6 +14,8 @@
 // image is applied with the reference's arithmetic (find_image) and only to
 // pairs whose cells are neighbours across the periodic boundary; for all
 // other pairs the reference's find_image leaves the vector unchanged.
+#include <cstdlib>
+
 #include "sld_pot32.cuh"
 
 // pair vector (FP64, minimum image with the reference's arithmetic)
@@ -27,10 +29,8 @@ __device__ __forceinline__ double3 pair_d(const Dev& D, double4 ri, int pk) {
 // MODE 0: FP64 tables (the reference's arithmetic); 1: split form (FP32
 // analytic); 2: the analytic forms in FP64
 template <int MODE>
-__global__ void __launch_bounds__(128) k_pairs(Dev D, int write_rho) {
+__device__ void pairs_one(const Dev& D, int i, int write_rho) {
     constexpr bool SPLIT = MODE == 1;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= D.natom) return;
     unsigned* err = &D.ctl->err;
     const int N = D.natom;
     double4 ri = D.r[i];
@@ -45,18 +45,11 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, int write_rho) {
         bool wrap = false;
         int c = k == 26 ? c0 : nbr_cell_w(D, cx, cy, cz, k, wrap);
         int st = D.cell_start[c], n = D.cell_count[c];
-        for (int m0 = 0; m0 < n; m0 += SLD_GB) {
-          int jb[SLD_GB];
-          double4 rb[SLD_GB];
-#pragma unroll
-          for (int u = 0; u < SLD_GB; ++u) jb[u] = m0 + u < n ? D.cell_atoms[st + m0 + u] : -1;
-#pragma unroll
-          for (int u = 0; u < SLD_GB; ++u) rb[u] = jb[u] >= 0 ? D.r[jb[u]] : ri;
-#pragma unroll
-          for (int u = 0; u < SLD_GB; ++u) {
-            int j = jb[u];
-            if (j < 0 || j == i) continue;
-            double4 rj = rb[u];
+        for (int m = 0; m < n; ++m) {
+          {
+            int j = D.cell_atoms[st + m];
+            if (j == i) continue;
+            double4 rj = D.r[j];
             double3 d = make_double3(ri.x - rj.x, ri.y - rj.y, ri.z - rj.z);
             if (wrap) d = find_image(D, d);
             if constexpr (!SPLIT) {
@@ -76,11 +69,11 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, int write_rho) {
                 }
                 if (rsq < D.rcut_mag_sq) {
                     if (nj < SLD_MAXJ) {
-                        D.jl[(size_t)nj * N + i] = j;
+                        D.jl[(size_t)i * SLD_MAXJ + nj] = j;
                         double J, dJ;
                         if constexpr (MODE == 0) J = interp(D.tJ, r0, D.inv_r, err);
                         else exch64(r0, J, dJ);
-                        D.jv[(size_t)nj * N + i] = J;
+                        D.jv[(size_t)i * SLD_MAXJ + nj] = J;
                     }
                     ++nj;
                 }
@@ -100,8 +93,8 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, int write_rho) {
                     if (nj < SLD_MAXJ) {
                         float J, dJ;
                         exch32r(r64, J, dJ);
-                        D.jl[(size_t)nj * N + i] = j;
-                        D.jvf[(size_t)nj * N + i] = J;
+                        D.jl[(size_t)i * SLD_MAXJ + nj] = j;
+                        D.jvf[(size_t)i * SLD_MAXJ + nj] = J;
                     }
                     ++nj;
                 }
@@ -113,6 +106,153 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, int write_rho) {
     D.nbr_n[i] = nn < SLD_MAXNB ? nn : SLD_MAXNB;
     D.jl_n[i] = nj < SLD_MAXJ ? nj : SLD_MAXJ;
     if (write_rho) D.rho[i] = SPLIT ? rho32.value() : rho;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(128) k_pairs(Dev D, int write_rho) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < D.natom) pairs_one<MODE>(D, i, write_rho);
+}
+
+// One warp per link cell: the cell's 27-cell candidate set (positions, atom
+// indices, a flag for pairs across the box) is staged once in shared memory
+// in the reference's traversal order, then every atom of the cell is tested
+// against it 32 candidates at a time.  List entries are placed with a warp
+// ballot, so each list keeps the traversal order.  A cell whose candidate
+// set does not fit falls back to one thread per atom.
+#define PW_WARPS 4
+#define PW_CAP 384
+template <int MODE>
+__global__ void __launch_bounds__(PW_WARPS * 32) k_pairs_warp(Dev D, int write_rho) {
+    constexpr bool SPLIT = MODE == 1;
+    __shared__ double s_rx[PW_WARPS][PW_CAP], s_ry[PW_WARPS][PW_CAP], s_rz[PW_WARPS][PW_CAP];
+    __shared__ int s_j[PW_WARPS][PW_CAP];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * PW_WARPS + warp;
+    if (c >= D.ncells) return;
+    unsigned* err = &D.ctl->err;
+    const int N = D.natom;
+    int cx, cy, cz;
+    cell_xyz(D, c, cx, cy, cz);
+    int nc = c, cnt = 0, st = 0;
+    bool wr = false;
+    if (lane < 27) {
+        nc = lane == 26 ? c : nbr_cell_w(D, cx, cy, cz, lane, wr);
+        cnt = D.cell_count[nc];
+        st = D.cell_start[nc];
+    }
+    int inc = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    const int off = inc - cnt;
+    const int T = __shfl_sync(0xffffffffu, inc, 31);
+    const int own_off = __shfl_sync(0xffffffffu, off, 26);
+    const int own_n = __shfl_sync(0xffffffffu, cnt, 26);
+    if (T > PW_CAP) {   // too dense for the staging area
+        int own_st = __shfl_sync(0xffffffffu, st, 26);
+        for (int h = lane; h < own_n; h += 32) pairs_one<MODE>(D, D.cell_atoms[own_st + h], write_rho);
+        return;
+    }
+    const unsigned wrap_lanes = __ballot_sync(0xffffffffu, wr);
+    for (int k = 0; k < 27; ++k) {
+        int stk = __shfl_sync(0xffffffffu, st, k), ck = __shfl_sync(0xffffffffu, cnt, k);
+        int ok = __shfl_sync(0xffffffffu, off, k);
+        for (int m = lane; m < ck; m += 32) {
+            int j = D.cell_atoms[stk + m];
+            double4 r = D.r[j];
+            s_j[warp][ok + m] = j | (((wrap_lanes >> k) & 1u) ? SLD_WRAP : 0);
+            s_rx[warp][ok + m] = r.x;
+            s_ry[warp][ok + m] = r.y;
+            s_rz[warp][ok + m] = r.z;
+        }
+    }
+    __syncwarp();
+    const float rmax2f = (float)D.rcut_max_sq, rmag2f = (float)D.rcut_mag_sq;
+    const float rpotf = (float)D.rcut_pot;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int h = 0; h < own_n; ++h) {
+        const int ci = own_off + h;
+        const int i = s_j[warp][ci] & SLD_JMASK;
+        const double rix = s_rx[warp][ci], riy = s_ry[warp][ci], riz = s_rz[warp][ci];
+        int nn = 0, nj = 0;
+        double rho = 0.0;
+        Kahan rho32;
+        for (int base = 0; base < T; base += 32) {
+            const int idx = base + lane;
+            int pk = idx < T ? s_j[warp][idx] : -1;
+            int j = pk & SLD_JMASK;
+            bool in_max = false, in_mag = false;
+            double r64 = 0.0;
+            if (pk >= 0 && j != i) {
+                double3 d = make_double3(rix - s_rx[warp][idx], riy - s_ry[warp][idx],
+                                         riz - s_rz[warp][idx]);
+                if (pk & SLD_WRAP) d = find_image(D, d);
+                if constexpr (!SPLIT) {
+                    double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
+                    in_max = rsq < D.rcut_max_sq;
+                    in_mag = rsq < D.rcut_mag_sq;
+                    r64 = sqrt(rsq);
+                } else {
+                    float dx = (float)d.x, dy = (float)d.y, dz = (float)d.z;
+                    float rsq = dx * dx + dy * dy + dz * dz;
+                    in_max = rsq < rmax2f;
+                    in_mag = rsq < rmag2f;
+                    if (in_max) r64 = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
+                }
+            }
+            unsigned bm = __ballot_sync(0xffffffffu, in_max);
+            if (in_max) {
+                int pos = nn + __popc(bm & lt);
+                if (pos < SLD_MAXNB) D.nbr[(size_t)pos * N + i] = pk;
+                if constexpr (MODE == 0) {
+                    if (r64 < D.rcut_pot) rho += interp(D.tf, r64, D.inv_r, err);
+                } else if constexpr (MODE == 2) {
+                    if (r64 < D.rcut_pot) {
+                        double f, df;
+                        dens64(D, r64, f, df);
+                        rho += f;
+                    }
+                } else {
+                    if ((float)r64 < rpotf) {
+                        float f, df;
+                        dens32r(D, r64, f, df);
+                        rho32.add(f);
+                    }
+                }
+            }
+            nn += __popc(bm);
+            unsigned bj = __ballot_sync(0xffffffffu, in_mag && in_max);
+            if (in_mag && in_max) {
+                int pj = nj + __popc(bj & lt);
+                if (pj < SLD_MAXJ) {
+                    D.jl[(size_t)i * SLD_MAXJ + pj] = j;
+                    if constexpr (MODE == 0) {
+                        D.jv[(size_t)i * SLD_MAXJ + pj] = interp(D.tJ, r64, D.inv_r, err);
+                    } else if constexpr (MODE == 2) {
+                        double J, dJ;
+                        exch64(r64, J, dJ);
+                        D.jv[(size_t)i * SLD_MAXJ + pj] = J;
+                    } else {
+                        float J, dJ;
+                        exch32r(r64, J, dJ);
+                        D.jvf[(size_t)i * SLD_MAXJ + pj] = J;
+                    }
+                }
+            }
+            nj += __popc(bj);
+        }
+        double rsum = SPLIT ? rho32.value() : rho;
+        rsum = warp_sum(rsum);
+        if (lane == 0) {
+            if (nn > SLD_MAXNB || nj > SLD_MAXJ) atomicOr(err, SLD_FLAG_CAPACITY);
+            D.nbr_n[i] = nn < SLD_MAXNB ? nn : SLD_MAXNB;
+            D.jl_n[i] = nj < SLD_MAXJ ? nj : SLD_MAXJ;
+            if (write_rho) D.rho[i] = rsum;
+        }
+    }
 }
 
 // F'(rho) per atom (the force pass needs it for both atoms of every pair)
@@ -133,47 +273,68 @@ __global__ void __launch_bounds__(256) k_embed(Dev D) {
     }
 }
 
-// on-site terms and outputs common to both forms
+// Parts of the force pass.  The lattice (EAM) terms do not depend on the
+// spins, the magnetic ones do; the step runs the EAM part beside the spin
+// sweeps and adds the magnetic part after them (the sum is the reference's
+// dudr = dudr_EAM + dudr_spin per pair, added in two passes).
+enum { PART_ALL = 3, PART_EAM = 1, PART_MAG = 2 };
+
+// on-site terms and outputs
+template <int PART>
 __device__ __forceinline__ void force_finish(const Dev& D, int i, double si_sq, double rho_i,
                                              double F_i, double fx, double fy, double fz, double pe,
                                              double me, double me0, double vir, const double st6[6]) {
-    pe += F_i;
-    double A = interp_const(D.landau[0], rho_i, D.inv_rho);
-    double B = interp_const(D.landau[1], rho_i, D.inv_rho);
-    double C = interp_const(D.landau[2], rho_i, D.inv_rho);
-    double Dd = interp_const(D.landau[3], rho_i, D.inv_rho);
-    double s4 = si_sq * si_sq;
-    me += A * si_sq + B * s4 + C * (s4 * si_sq) + Dd * (s4 * s4);
+    double m = D.atmass, V = D.box_volume / D.natom;
+    double* out = D.stress + 6 * (size_t)i;
+    if (PART & PART_EAM) {
+        pe += F_i;
+        D.pe[i] = pe;
+    }
+    if (PART & PART_MAG) {
+        double A = interp_const(D.landau[0], rho_i, D.inv_rho);
+        double B = interp_const(D.landau[1], rho_i, D.inv_rho);
+        double C = interp_const(D.landau[2], rho_i, D.inv_rho);
+        double Dd = interp_const(D.landau[3], rho_i, D.inv_rho);
+        double s4 = si_sq * si_sq;
+        me += A * si_sq + B * s4 + C * (s4 * si_sq) + Dd * (s4 * s4);
+        D.me[i] = me;
+        D.me0[i] = me0;
+    }
+    if (PART == PART_MAG) {
+        // add to what the EAM part wrote
+        double4 f = D.f[i];
+        D.f[i] = make_double4(f.x + fx, f.y + fy, f.z + fz, 0.0);
+        D.vir[i] += 0.5 * vir;
+        for (int k = 0; k < 6; ++k) out[k] += st6[k] / 2.0 / V;
+        if (!isfinite(fx + fy + fz + me)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
+        return;
+    }
     D.f[i] = make_double4(fx, fy, fz, 0.0);
-    D.pe[i] = pe;
-    D.me[i] = me;
-    D.me0[i] = me0;
     D.vir[i] = 0.5 * vir;   // each pair's virial split evenly between its atoms
     // calculate_force_energy_CPU.cpp:262-296: local volume V/N, kinetic part
     double4 p = D.p[i];
-    double m = D.atmass, V = D.box_volume / D.natom;
-    double* out = D.stress + 6 * (size_t)i;
     out[0] = ((p.x * p.x) / m + st6[0] / 2.0) / V;
     out[1] = ((p.y * p.y) / m + st6[1] / 2.0) / V;
     out[2] = ((p.z * p.z) / m + st6[2] / 2.0) / V;
     out[3] = ((p.x * p.y) / m + st6[3] / 2.0) / V;
     out[4] = ((p.y * p.z) / m + st6[4] / 2.0) / V;
     out[5] = ((p.z * p.x) / m + st6[5] / 2.0) / V;
-    if (!isfinite(fx + fy + fz + pe + me)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
+    if (!isfinite(fx + fy + fz + pe)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
 }
 
 // FP64 force pass; AN: the analytic forms instead of the tables
-template <bool AN>
+template <bool AN, int PART>
 __global__ void __launch_bounds__(128) k_force64(Dev D) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= D.natom) return;
     unsigned* err = &D.ctl->err;
     const int N = D.natom;
     double4 ri = D.r[i];
-    double4 si = D.s[i];
+    // the EAM part runs beside the spin sweeps and must not read the spins
+    double4 si = (PART & PART_MAG) ? D.s[i] : make_double4(0, 0, 0, 0);
     double si_sq = si.x * si.x + si.y * si.y + si.z * si.z;
     double rho_i = D.rho[i];
-    double dF_i = D.dF[i];
+    double dF_i = (PART & PART_EAM) ? D.dF[i] : 0.0;
     double fx = 0, fy = 0, fz = 0, pe = 0, me = 0, me0 = 0, vir = 0;
     double st6[6] = {0, 0, 0, 0, 0, 0};
     int nn = D.nbr_n[i];
@@ -187,7 +348,7 @@ __global__ void __launch_bounds__(128) k_force64(Dev D) {
       for (int u = 0; u < 4; ++u) {
           int j = pkb[u] & SLD_JMASK;
           rjb[u] = pkb[u] >= 0 ? D.r[j] : ri;
-          dFb[u] = pkb[u] >= 0 ? D.dF[j] : 0.0;
+          dFb[u] = (pkb[u] >= 0 && (PART & PART_EAM)) ? D.dF[j] : 0.0;
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
@@ -199,7 +360,7 @@ __global__ void __launch_bounds__(128) k_force64(Dev D) {
         double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
         double r0 = sqrt(rsq);
         double dudr = 0.0, dudr_spin = 0.0;
-        if (r0 < D.rcut_pot) {
+        if ((PART & PART_EAM) && r0 < D.rcut_pot) {
             double df, dphi, phi;
             if constexpr (AN) {
                 double f;
@@ -215,7 +376,7 @@ __global__ void __launch_bounds__(128) k_force64(Dev D) {
             // tables are zero and add nothing to dudr
             pe += 0.5 * phi;
         }
-        if (r0 < D.rcut_mag) {
+        if ((PART & PART_MAG) && r0 < D.rcut_mag) {
             double4 sj = D.s[j];
             double sj_sq = sj.x * sj.x + sj.y * sj.y + sj.z * sj.z;
             double dot = si.x * sj.x + si.y * sj.y + si.z * sj.z;
@@ -233,6 +394,7 @@ __global__ void __launch_bounds__(128) k_force64(Dev D) {
             me += -Jh * dot;
         }
         dudr += dudr_spin;
+        if (dudr == 0.0 && PART != PART_ALL) continue;
         double force = -dudr / r0;
         double gx = force * d.x, gy = force * d.y, gz = force * d.z;
         fx += gx; fy += gy; fz += gz;
@@ -241,29 +403,31 @@ __global__ void __launch_bounds__(128) k_force64(Dev D) {
         vir += -force * rsq;
       }
     }
-    double F_i;
-    if constexpr (AN) {
-        double dF_unused;
-        emb64(rho_i, F_i, dF_unused);
-    } else {
-        F_i = interp(D.tF, rho_i, D.inv_rho, err);
+    double F_i = 0.0;
+    if (PART & PART_EAM) {
+        if constexpr (AN) {
+            double dF_unused;
+            emb64(rho_i, F_i, dF_unused);
+        } else {
+            F_i = interp(D.tF, rho_i, D.inv_rho, err);
+        }
     }
-    force_finish(D, i, si_sq, rho_i, F_i, fx, fy, fz, pe, me, me0,
-                 vir, st6);
+    force_finish<PART>(D, i, si_sq, rho_i, F_i, fx, fy, fz, pe, me, me0, vir, st6);
 }
 
 // split form: FP32 pair terms from the analytic potential, Kahan sums
+template <int PART>
 __global__ void __launch_bounds__(128) k_force32(Dev D) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= D.natom) return;
     const int N = D.natom;
     double4 ri = D.r[i];
-    double4 si = D.s[i];
+    double4 si = (PART & PART_MAG) ? D.s[i] : make_double4(0, 0, 0, 0);
     double si_sq = si.x * si.x + si.y * si.y + si.z * si.z;
     float sx = (float)si.x, sy = (float)si.y, sz = (float)si.z;
     float si_sqf = sx * sx + sy * sy + sz * sz;
     double rho_i = D.rho[i];
-    float dF_i = (float)D.dF[i];
+    float dF_i = (PART & PART_EAM) ? (float)D.dF[i] : 0.f;
     const float rpot = (float)D.rcut_pot, rmag = (float)D.rcut_mag;
     Kahan fx, fy, fz, pe, me, me0;
     float vir = 0.f, st6f[6] = {0, 0, 0, 0, 0, 0};
@@ -276,14 +440,14 @@ __global__ void __launch_bounds__(128) k_force32(Dev D) {
         double r64 = sqrt(dd.x * dd.x + dd.y * dd.y + dd.z * dd.z);
         float r0 = (float)r64, rsq = r0 * r0;
         float dudr = 0.f;
-        if (r0 < rpot) {
+        if ((PART & PART_EAM) && r0 < rpot) {
             float f, df, phi, dphi;
             dens32r(D, r64, f, df);
             pair32r(D, r64, phi, dphi);
             dudr = (dF_i + (float)D.dF[j]) * df + dphi;
             pe.add(0.5f * phi);
         }
-        if (r0 < rmag) {
+        if ((PART & PART_MAG) && r0 < rmag) {
             double4 sj4 = D.s[j];
             float tx = (float)sj4.x, ty = (float)sj4.y, tz = (float)sj4.z;
             float sj_sq = tx * tx + ty * ty + tz * tz;
@@ -296,6 +460,7 @@ __global__ void __launch_bounds__(128) k_force32(Dev D) {
             me0.add(Jh * times);
             me.add(-Jh * dot);
         }
+        if (dudr == 0.f && PART != PART_ALL) continue;
         float force = -dudr / r0;
         float gx = force * dx, gy = force * dy, gz = force * dz;
         fx.add(gx); fy.add(gy); fz.add(gz);
@@ -303,16 +468,38 @@ __global__ void __launch_bounds__(128) k_force32(Dev D) {
         st6f[3] += gx * dy; st6f[4] += gy * dz; st6f[5] += gz * dx;
         vir += -force * rsq;
     }
-    float F, dF;
-    emb32((float)rho_i, F, dF);
+    float F = 0.f, dF;
+    if (PART & PART_EAM) emb32((float)rho_i, F, dF);
     double st6[6];
     for (int k = 0; k < 6; ++k) st6[k] = st6f[k];
-    force_finish(D, i, si_sq, rho_i, (double)F, fx.value(), fy.value(), fz.value(), pe.value(),
-                 me.value(), me0.value(), (double)vir, st6);
+    force_finish<PART>(D, i, si_sq, rho_i, (double)F, fx.value(), fy.value(), fz.value(),
+                       pe.value(), me.value(), me0.value(), (double)vir, st6);
 }
 
+template <int PART>
+static void launch_force_part(const Dev& D, cudaStream_t st) {
+    int nb = div_up(D.natom, 128);
+    if (D.split) k_force32<PART><<<nb, 128, 0, st>>>(D);
+    else if (D.analytic) k_force64<true, PART><<<nb, 128, 0, st>>>(D);
+    else k_force64<false, PART><<<nb, 128, 0, st>>>(D);
+}
+
+static int g_pairs_mode = -1;   // 0: one thread per atom (default), 1: one warp per cell
+
 void launch_pairs(const Dev& D, cudaStream_t st, bool write_rho) {
-    int nb = div_up(D.natom, 128), w = write_rho ? 1 : 0;
+    if (g_pairs_mode < 0) {
+        const char* v = getenv("SLD_PAIRS_MODE");
+        g_pairs_mode = (v && v[0] == '1') ? 1 : 0;
+    }
+    int w = write_rho ? 1 : 0;
+    if (g_pairs_mode == 1) {
+        int nb = div_up(D.ncells, PW_WARPS);
+        if (D.split) k_pairs_warp<1><<<nb, PW_WARPS * 32, 0, st>>>(D, w);
+        else if (D.analytic) k_pairs_warp<2><<<nb, PW_WARPS * 32, 0, st>>>(D, w);
+        else k_pairs_warp<0><<<nb, PW_WARPS * 32, 0, st>>>(D, w);
+        return;
+    }
+    int nb = div_up(D.natom, 128);
     if (D.split) k_pairs<1><<<nb, 128, 0, st>>>(D, w);
     else if (D.analytic) k_pairs<2><<<nb, 128, 0, st>>>(D, w);
     else k_pairs<0><<<nb, 128, 0, st>>>(D, w);
@@ -325,8 +512,10 @@ void launch_embed(const Dev& D, cudaStream_t st) {
 }
 void launch_force(const Dev& D, cudaStream_t st) {
     launch_embed(D, st);
-    int nb = div_up(D.natom, 128);
-    if (D.split) k_force32<<<nb, 128, 0, st>>>(D);
-    else if (D.analytic) k_force64<true><<<nb, 128, 0, st>>>(D);
-    else k_force64<false><<<nb, 128, 0, st>>>(D);
+    launch_force_part<PART_ALL>(D, st);
 }
+void launch_force_eam(const Dev& D, cudaStream_t st) {
+    launch_embed(D, st);
+    launch_force_part<PART_EAM>(D, st);
+}
+void launch_force_mag(const Dev& D, cudaStream_t st) { launch_force_part<PART_MAG>(D, st); }

@@ -53,6 +53,31 @@ __device__ __forceinline__ void visit_store(const Dev& D, int i, double3 s, doub
     }
 }
 
+// The normals of both sweeps of one core_ds call, drawn for every atom in
+// one parallel pass before the sweeps (the draw is counter-based, so it does
+// not depend on when it is made); the sweeps' serial chains only read them.
+__global__ void __launch_bounds__(256) k_spin_noise(Dev D, int epoch_off) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.natom) return;
+    unsigned long long e0 = D.ctl->epoch + (unsigned long long)epoch_off;
+    for (int v = 0; v < 2; ++v) {
+        double3 x = normals3(D.seed, 0u, (unsigned)D.id[i], e0 + v);
+        double* o = D.xi + 6 * (size_t)i + 3 * v;
+        o[0] = x.x;
+        o[1] = x.y;
+        o[2] = x.z;
+    }
+}
+
+void launch_spin_noise(const Dev& D, cudaStream_t st, int epoch_off) {
+    k_spin_noise<<<div_up(D.natom, 256), 256, 0, st>>>(D, epoch_off);
+}
+
+__device__ __forceinline__ double3 spin_noise_at(const Dev& D, int i, int sweep) {
+    const double* x = D.xi + 6 * (size_t)i + 3 * sweep;
+    return make_double3(x[0], x[1], x[2]);
+}
+
 // one visit entirely from global memory (the fallback path)
 __device__ void visit_global(const Dev& D, int i, double dt, unsigned long long epoch, bool fields) {
     double3 H;
@@ -64,7 +89,8 @@ __device__ void visit_global(const Dev& D, int i, double dt, unsigned long long 
     if (D.spinlang) {
         T = D.eltemp ? D.Te[D.node[i]] : D.temperature;
         rho = D.rho[i];
-        xi = normals3(D.seed, 0u, (unsigned)D.id[i], epoch);
+        xi = spin_noise_at(D, i, fields ? 1 : 0);
+        (void)epoch;
     }
     double3 HL;
     double3 s = spin_integrate(D, make_double3(s4.x, s4.y, s4.z), H, sumJ, rho, T, xi, dt, HL);
@@ -136,7 +162,7 @@ __global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restri
             S.inn[a] = (unsigned char)(nin < SW_MAXIN ? nin : SW_MAXIN);
             if (nin > SW_MAXIN) S.overflow = 1;
             if (D.spinlang) {
-                double3 xi = normals3(D.seed, 0u, (unsigned)D.id[i], epoch);
+                double3 xi = spin_noise_at(D, i, fields ? 1 : 0);
                 S.aux[a][0] = D.rho[i];
                 S.aux[a][1] = D.eltemp ? D.Te[D.node[i]] : D.temperature;
                 S.aux[a][2] = xi.x; S.aux[a][3] = xi.y; S.aux[a][4] = xi.z;

@@ -590,8 +590,119 @@ __global__ void __launch_bounds__(1024) k_dte_block(Dev D, double dt) {
     for (int k = threadIdx.x; k < n; k += blockDim.x) D.Te[k] = sT[k];
 }
 
+// Cluster "hub" form: every CTA of a 4-CTA cluster does the cell-local A and
+// B parts for its share of the cells in parallel; CTA 0 holds all Te and
+// Te_to_Ee(Te) in its shared memory (the others read and write them through
+// distributed shared memory) and runs C's colour phases with block barriers.
+// Two cluster barriers per substep instead of one per colour phase.
+#define HUB_CL 4
+__global__ void __launch_bounds__(1024) k_dte_hub(Dev D, double dt, int per) {
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ __align__(16) double hsm[];
+    const int n = D.nte;
+    const int rank = (int)cl.block_rank();
+    double* hT = cl.map_shared_rank(hsm, 0);   // the hub's arrays
+    double* hE = hT + n;
+    double* hfac = hT + 2 * n;
+    __shared__ double sh[32];
+    const int k0 = rank * per, k1 = min(n, k0 + per);
+    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        double T = D.Te[k];
+        hT[k] = T;
+        hE[k] = te_to_Ee(T);
+    }
+    cl.sync();
+    int nloop = D.te_nloop > 0 ? D.te_nloop : 50;
+    double h = dt / nloop, hh = h / 2.0;
+    double cond = D.kappa_e / SLD_EVTOJ / 1e10;
+    double lx = D.box_len[0] / D.tx, ly = D.box_len[1] / D.ty, lz = D.box_len[2] / D.tz;
+    double dx2 = lx * lx, dy2 = ly * ly, dz2 = lz * lz;
+    double atomic_volume = D.box_volume / (double)D.natom;
+    double volume_factor = atomic_volume / ((double)D.natom / (double)D.nte);
+    double pre = h / 2.0 * cond * volume_factor / SLD_BOLTZ;
+    const int tx = D.tx, ty = D.ty, tz = D.tz;
+    double lastE[4];   // this thread's last A-step energies (per = 1024 -> <= 1 per thread)
+    for (int it = 0; it < nloop; ++it) {
+        for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {   // A(h/2), B(h/2)
+            double dE = 0.0;
+            dE += D.Gel[k] * D.Tl[k];
+            dE += D.Ges[k] * D.TsL[k];
+            double T = Ee_to_te(hE[k] + hh * dE);
+            double g = 0.0;
+            g += D.Gel[k];
+            g += D.Ges[k];
+            g *= hh / SLD_BOLTZ;
+            T = dte_rk4(T, g, hh);
+            hT[k] = T;
+            hE[k] = te_to_Ee(T);
+        }
+        cl.sync();
+        if (rank == 0) {   // C(h) on the hub
+            double acc = 0.0;
+            for (int k = threadIdx.x; k < n; k += blockDim.x) acc += hsm[n + k];
+            double t = block_sum(acc, sh);
+            __shared__ double tot;
+            if (threadIdx.x == 0) tot = t;
+            __syncthreads();
+            double start = tot;
+            for (int pass = 0; pass < 2; ++pass) {
+                for (int gg = 0; gg < D.te_ngroups; ++gg) {
+                    int g = pass == 0 ? gg : D.te_ngroups - 1 - gg;
+                    int b = D.te_gstart[g], e = D.te_gstart[g + 1];
+                    for (int m = b + threadIdx.x; m < e; m += blockDim.x) {
+                        int k = D.te_gcells[m];
+                        int x = k % tx, y = (k / tx) % ty, z = k / (tx * ty);
+                        int xp = x + 1 == tx ? 0 : x + 1, xm = x == 0 ? tx - 1 : x - 1;
+                        int yp = y + 1 == ty ? 0 : y + 1, ym = y == 0 ? ty - 1 : y - 1;
+                        int zp = z + 1 == tz ? 0 : z + 1, zm = z == 0 ? tz - 1 : z - 1;
+                        const double* sT = hsm;
+                        double T = sT[k];
+                        double ex = sT[xp + (y + z * ty) * tx] + sT[xm + (y + z * ty) * tx] - 2.0 * T;
+                        double ey = sT[x + (yp + z * ty) * tx] + sT[x + (ym + z * ty) * tx] - 2.0 * T;
+                        double ez = sT[x + (y + zp * ty) * tx] + sT[x + (y + zm * ty) * tx] - 2.0 * T;
+                        T = Ee_to_te(hsm[n + k] + pre * (ex / dx2 + ey / dy2 + ez / dz2));
+                        hsm[k] = T;
+                        hsm[n + k] = te_to_Ee(T);
+                    }
+                    __syncthreads();
+                }
+            }
+            acc = 0.0;
+            for (int k = threadIdx.x; k < n; k += blockDim.x) acc += hsm[n + k];
+            t = block_sum(acc, sh);
+            if (threadIdx.x == 0) hsm[2 * n] = start / t;
+        }
+        cl.sync();
+        double fac = *hfac;
+        int q = 0;
+        for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x, ++q) {   // rescale, B, A
+            double T = Ee_to_te(hE[k] * fac);
+            double g = 0.0;
+            g += D.Gel[k];
+            g += D.Ges[k];
+            g *= hh / SLD_BOLTZ;
+            T = dte_rk4(T, g, hh);
+            double dE = 0.0;
+            dE += D.Gel[k] * D.Tl[k];
+            dE += D.Ges[k] * D.TsL[k];
+            double Ee = te_to_Ee(T) + hh * dE;
+            T = Ee_to_te(Ee);
+            hT[k] = T;
+            hE[k] = te_to_Ee(T);
+            if (q < 4) lastE[q] = Ee;
+        }
+    }
+    int q = 0;
+    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x, ++q) {
+        D.Te[k] = hT[k];
+        if (q < 4) D.Ee[k] = lastE[q];
+    }
+    cl.sync();   // keep the hub's shared memory alive until every CTA is done
+}
+
 static int g_dte_cluster = 0;   // cluster size in use, 0: single block
-static int g_dte_mode = 0;      // 0: one CTA, shared memory; 1: cluster
+static int g_dte_mode = 2;      // 0: one CTA; 1: cluster, cells spread; 2: cluster hub
+static bool g_hub_ok = false;
 static const int kDsmMaxPer = 12000;   // Te cells per CTA held in shared memory
 
 int dte_init(int device) {
@@ -600,7 +711,25 @@ int dte_init(int device) {
     cudaFuncSetAttribute(k_dte_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(sizeof(double) * 2 * kBlockMaxCells));
     const char* m = getenv("SLD_DTE_MODE");
-    if (m && (m[0] == '0' || m[0] == '1')) g_dte_mode = m[0] - '0';
+    if (m && (m[0] == '0' || m[0] == '1' || m[0] == '2')) g_dte_mode = m[0] - '0';
+    cudaFuncSetAttribute(k_dte_hub, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(sizeof(double) * (2 * kBlockMaxCells + 2)));
+    {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(HUB_CL);
+        cfg.blockDim = dim3(1024);
+        cfg.dynamicSmemBytes = sizeof(double) * (2 * kBlockMaxCells + 2);
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = HUB_CL;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int nclu = 0;
+        g_hub_ok = cudaOccupancyMaxActiveClusters(&nclu, k_dte_hub, &cfg) == cudaSuccess && nclu > 0;
+        cudaGetLastError();
+    }
     const char* v = getenv("SLD_DTE_SINGLE");
     if (v && v[0] == '1') return 0;
     cudaFuncSetAttribute(k_dte_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
@@ -629,6 +758,23 @@ int dte_init(int device) {
 }
 
 void launch_dte(const Dev& D, cudaStream_t st, double dt) {
+    int hub_per = (D.nte + HUB_CL - 1) / HUB_CL;
+    if (g_dte_mode == 2 && g_hub_ok && D.nte <= kBlockMaxCells && hub_per <= 4 * 1024) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(HUB_CL);
+        cfg.blockDim = dim3(1024);
+        cfg.dynamicSmemBytes = sizeof(double) * (2 * D.nte + 2);
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = HUB_CL;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, k_dte_hub, D, dt, hub_per);
+        return;
+    }
     if ((g_dte_mode == 0 || g_dte_cluster == 0) && D.nte <= kBlockMaxCells) {
         k_dte_block<<<1, 1024, sizeof(double) * 2 * D.nte, st>>>(D, dt);
         return;

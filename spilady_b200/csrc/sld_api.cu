@@ -44,7 +44,18 @@ struct sld_ctx {
     unsigned char* d_te_color = nullptr;
     double* d_avg = nullptr;
     cudaStream_t st = nullptr;
+    cudaStream_t st2 = nullptr;        // second branch of the step graph
+    cudaEvent_t fork_ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaGraphExec_t step_graph = nullptr;
+    cudaGraphExec_t step_graphs[2] = {nullptr, nullptr};   // by current buffer set
+    // exchange lists and rho are double buffered: the list pass of a step
+    // writes the other set while the first spin sweep still reads this one
+    int cur = 0;
+    int* jl_set[2] = {nullptr, nullptr};
+    int* jln_set[2] = {nullptr, nullptr};
+    double* jv_set[2] = {nullptr, nullptr};
+    float* jvf_set[2] = {nullptr, nullptr};
+    double* rho_set[2] = {nullptr, nullptr};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
     int scan_blocks = 1;
@@ -64,6 +75,22 @@ struct sld_ctx {
 };
 
 namespace {
+
+// the device state with buffer set k of the exchange lists and rho
+Dev dev_set(const sld_ctx* c, int k) {
+    Dev D = c->D;
+    D.jl = c->jl_set[k];
+    D.jl_n = c->jln_set[k];
+    D.jv = c->jv_set[k];
+    D.jvf = c->jvf_set[k];
+    D.rho = c->rho_set[k];
+    return D;
+}
+
+void use_set(sld_ctx* c, int k) {
+    c->cur = k;
+    c->D = dev_set(c, k);
+}
 
 int check_flags(sld_ctx* c) {
     unsigned err = 0;
@@ -85,43 +112,71 @@ int launch_status() {
 }
 
 // One core_ds call: forward sweep, backward sweep.
-void enqueue_ds(sld_ctx* c, double dt, int& eoff) {
+void enqueue_ds(sld_ctx* c, const Dev& D, double dt, int& eoff) {
     const auto& G = c->G;
     double dt_half = dt / 2e0;
+    if (c->P.spinlang) launch_spin_noise(D, c->st, eoff);
     for (int g = 0; g < G.ngroups; ++g)
-        launch_sweep(c->D, c->st, c->d_gcells + G.gstart[g], G.gstart[g + 1] - G.gstart[g],
+        launch_sweep(D, c->st, c->d_gcells + G.gstart[g], G.gstart[g + 1] - G.gstart[g],
                      dt_half, false, eoff);
     if (c->P.spinlang) ++eoff;
     for (int g = G.ngroups - 1; g >= 0; --g)
-        launch_sweep(c->D, c->st, c->d_gcells + G.gstart[g], G.gstart[g + 1] - G.gstart[g],
+        launch_sweep(D, c->st, c->d_gcells + G.gstart[g], G.gstart[g + 1] - G.gstart[g],
                      dt_half, true, eoff);
     if (c->P.spinlang) ++eoff;
 }
+void enqueue_ds(sld_ctx* c, double dt, int& eoff) { enqueue_ds(c, c->D, dt, eoff); }
 
-void enqueue_dp(sld_ctx* c, double dt, int& eoff) {
-    launch_dp(c->D, c->st, dt, eoff);
+void enqueue_dp(sld_ctx* c, const Dev& D, double dt, int& eoff) {
+    launch_dp(D, c->st, dt, eoff);
     if (c->P.lattlang) ++eoff;
 }
+void enqueue_dp(sld_ctx* c, double dt, int& eoff) { enqueue_dp(c, c->D, dt, eoff); }
 
-// core.cpp:31-76 (spin-lattice branch) plus the main-loop bookkeeping
+// core.cpp:31-76 (spin-lattice branch) plus the main-loop bookkeeping, as
+// two branches of one graph.  The second branch runs what does not read the
+// spins beside the sweeps:
+//   main:   links | dp(dt/2) | ds(dt/2) ........ | ds(dt/2) | force(magnetic) | dp(dt/2) | Te ...
+//   second:  core_dTe(dt/2) |  dr | rho + lists | force(EAM)
+// The lists and rho of this step go to the other buffer set, so the first
+// sweep still reads the previous ones; the step ends with that set current.
 void enqueue_step(sld_ctx* c) {
     double dt = c->P.step;
     int eoff = 0;
-    launch_links(c->D, c->st, false, c->scan_blocks);
-    if (c->P.eltemp) launch_dte(c->D, c->st, dt / 2e0);
-    enqueue_dp(c, dt / 2e0, eoff);
-    enqueue_ds(c, dt / 2e0, eoff);
-    launch_dr(c->D, c->st, dt);
-    launch_pairs(c->D, c->st, true);
-    enqueue_ds(c, dt / 2e0, eoff);
-    launch_force(c->D, c->st);
-    enqueue_dp(c, dt / 2e0, eoff);
+    const Dev Dc = dev_set(c, c->cur), Dn = dev_set(c, 1 - c->cur);
+    static const bool one_stream = getenv("SLD_ONE_STREAM") && getenv("SLD_ONE_STREAM")[0] == '1';
+    cudaStream_t M = c->st, A = one_stream ? c->st : c->st2;
+    cudaEvent_t* ev = c->fork_ev;
     if (c->P.eltemp) {
-        launch_temperature(c->D, c->st);
-        launch_dte(c->D, c->st, dt / 2e0);
-        if (c->P.renormalize_energy) launch_energy_check(c->D, c->st, 1);
+        cudaEventRecord(ev[0], M);
+        cudaStreamWaitEvent(A, ev[0], 0);
+        launch_dte(Dc, A, dt / 2e0);
+        cudaEventRecord(ev[1], A);
+        launch_links(Dc, M, false, c->scan_blocks);
+        cudaStreamWaitEvent(M, ev[1], 0);
+    } else {
+        launch_links(Dc, M, false, c->scan_blocks);
     }
-    launch_advance(c->D, c->st, eoff, 1);
+    enqueue_dp(c, Dc, dt / 2e0, eoff);
+    cudaEventRecord(ev[0], M);
+    cudaStreamWaitEvent(A, ev[0], 0);
+    launch_dr(Dc, A, dt);
+    launch_pairs(Dn, A, true);
+    cudaEventRecord(ev[2], A);
+    launch_force_eam(Dn, A);
+    cudaEventRecord(ev[3], A);
+    enqueue_ds(c, Dc, dt / 2e0, eoff);
+    cudaStreamWaitEvent(M, ev[2], 0);
+    enqueue_ds(c, Dn, dt / 2e0, eoff);
+    cudaStreamWaitEvent(M, ev[3], 0);
+    launch_force_mag(Dn, M);
+    enqueue_dp(c, Dn, dt / 2e0, eoff);
+    if (c->P.eltemp) {
+        launch_temperature(Dn, M);
+        launch_dte(Dn, M, dt / 2e0);
+        if (c->P.renormalize_energy) launch_energy_check(Dn, M, 1);
+    }
+    launch_advance(Dn, M, eoff, 1);
 }
 
 int validate(const sld_params* p) {
@@ -200,12 +255,21 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     if (cudaSetDevice(prm->device) != cudaSuccess) { delete c; return SLD_ERR_CUDA; }
     sweep_init();
     dte_init(prm->device);
-    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+    // the main branch (spin sweeps: few, latency-bound blocks) gets the
+    // highest priority so that the side branch's wide grids fill in around it
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    if (cudaStreamCreateWithPriority(&c->st, cudaStreamNonBlocking, prio_hi) != cudaSuccess) {
         delete c;
         return SLD_ERR_CUDA;
     }
     cudaEventCreate(&c->ev0);
     cudaEventCreate(&c->ev1);
+    if (cudaStreamCreateWithPriority(&c->st2, cudaStreamNonBlocking, prio_lo) != cudaSuccess) {
+        sld_destroy(c);
+        return SLD_ERR_CUDA;
+    }
+    for (int k = 0; k < 4; ++k) cudaEventCreateWithFlags(&c->fork_ev[k], cudaEventDisableTiming);
 
     sld::Tables T;
     sld::build_tables(T, G.rcut_max);
@@ -263,7 +327,8 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
 
     ok = c->alloc(&D.r, n) == 0 && c->alloc(&D.p, n) == 0 && c->alloc(&D.f, n) == 0 &&
          c->alloc(&D.s, n) == 0 && c->alloc(&D.H, n) == 0 && c->alloc(&D.HL, n) == 0 &&
-         c->alloc(&D.rho, n) == 0 && c->alloc(&D.pe, n) == 0 && c->alloc(&D.ke, n) == 0 &&
+         c->alloc(&c->rho_set[0], n) == 0 && c->alloc(&c->rho_set[1], n) == 0 &&
+         c->alloc(&D.pe, n) == 0 && c->alloc(&D.ke, n) == 0 &&
          c->alloc(&D.me, n) == 0 && c->alloc(&D.me0, n) == 0 && c->alloc(&D.vir, n) == 0 &&
          c->alloc(&D.sumJ, n) == 0 && c->alloc(&D.stress, 6 * n) == 0 &&
          c->alloc(&D.cell_of, n) == 0 && c->alloc(&D.id, n) == 0 && c->alloc(&D.stamp, n) == 0 &&
@@ -271,8 +336,11 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
          c->alloc(&D.cell_count, (size_t)G.ncells) == 0 &&
          c->alloc(&D.cell_atoms, n) == 0 && c->alloc(&D.cell_fill, (size_t)G.ncells) == 0 &&
          c->alloc(&D.nbr, (size_t)SLD_MAXNB * n) == 0 && c->alloc(&D.nbr_n, n) == 0 &&
-         c->alloc(&D.jl, (size_t)SLD_MAXJ * n) == 0 && c->alloc(&D.jl_n, n) == 0 &&
+         c->alloc(&c->jl_set[0], (size_t)SLD_MAXJ * n) == 0 &&
+         c->alloc(&c->jl_set[1], (size_t)SLD_MAXJ * n) == 0 &&
+         c->alloc(&c->jln_set[0], n) == 0 && c->alloc(&c->jln_set[1], n) == 0 &&
          c->alloc(&D.dF, n) == 0;
+    if (prm->spinlang) ok = ok && c->alloc(&D.xi, 6 * n) == 0;
     {
         float* cub = nullptr;
         double* cub64 = nullptr;
@@ -284,8 +352,11 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
         D.cubic = cub;
         D.cubic64 = cub64;
     }
-    if (prm->precision == SLD_SPLIT) ok = ok && c->alloc(&D.jvf, (size_t)SLD_MAXJ * n) == 0;
-    else ok = ok && c->alloc(&D.jv, (size_t)SLD_MAXJ * n) == 0;
+    for (int k = 0; k < 2 && ok; ++k) {
+        if (prm->precision == SLD_SPLIT) ok = c->alloc(&c->jvf_set[k], (size_t)SLD_MAXJ * n) == 0;
+        else ok = c->alloc(&c->jv_set[k], (size_t)SLD_MAXJ * n) == 0;
+    }
+    if (ok) use_set(c, 0);
     c->scan_blocks = div_up(G.ncells, 1024);
     ok = ok && c->alloc(&D.scan_tmp, (size_t)c->scan_blocks) == 0;
     if (prm->te_mesh > 0) {
@@ -380,6 +451,11 @@ void sld_destroy(sld_ctx* c) {
     if (!c) return;
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+    for (int k = 0; k < 2; ++k)
+        if (c->step_graphs[k]) cudaGraphExecDestroy(c->step_graphs[k]);
+    for (int k = 0; k < 4; ++k)
+        if (c->fork_ev[k]) cudaEventDestroy(c->fork_ev[k]);
+    if (c->st2) cudaStreamDestroy(c->st2);
     for (void* q : c->allocs) cudaFree(q);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -457,16 +533,23 @@ int sld_calculate_temperature(sld_ctx* c) {
 int sld_run(sld_ctx* c, int nsteps) {
     if (!c || nsteps < 0) return SLD_ERR_ARG;
     fresh_lists(c);
-    if (!c->step_graph) {
+    for (int k = 0; k < 2; ++k) {
+        if (c->step_graphs[k]) continue;
+        int saved = c->cur;
+        use_set(c, k);
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
         enqueue_step(c);
         CK(cudaStreamEndCapture(c->st, &g));
-        CK(cudaGraphInstantiate(&c->step_graph, g, 0));
+        CK(cudaGraphInstantiate(&c->step_graphs[k], g, 0));
         cudaGraphDestroy(g);
+        use_set(c, saved);
     }
     CK(cudaEventRecord(c->ev0, c->st));
-    for (int k = 0; k < nsteps; ++k) CK(cudaGraphLaunch(c->step_graph, c->st));
+    for (int k = 0; k < nsteps; ++k) {
+        CK(cudaGraphLaunch(c->step_graphs[c->cur], c->st));
+        use_set(c, 1 - c->cur);
+    }
     CK(cudaEventRecord(c->ev1, c->st));
     return SLD_OK;
 }
@@ -489,21 +572,23 @@ int sld_profile_step(sld_ctx* c, double* ms) {
     };
     double dt = c->P.step;
     int eoff = 0;
-    timed(0, [&] { launch_links(c->D, c->st, false, c->scan_blocks); });
-    if (c->P.eltemp) timed(1, [&] { launch_dte(c->D, c->st, dt / 2e0); });
-    timed(2, [&] { enqueue_dp(c, dt / 2e0, eoff); });
-    timed(3, [&] { enqueue_ds(c, dt / 2e0, eoff); });
-    timed(4, [&] { launch_dr(c->D, c->st, dt); });
-    timed(5, [&] { launch_pairs(c->D, c->st, true); });
-    timed(3, [&] { enqueue_ds(c, dt / 2e0, eoff); });
-    timed(6, [&] { launch_force(c->D, c->st); });
-    timed(2, [&] { enqueue_dp(c, dt / 2e0, eoff); });
+    const Dev Dc = dev_set(c, c->cur), Dn = dev_set(c, 1 - c->cur);
+    timed(0, [&] { launch_links(Dc, c->st, false, c->scan_blocks); });
+    if (c->P.eltemp) timed(1, [&] { launch_dte(Dc, c->st, dt / 2e0); });
+    timed(2, [&] { enqueue_dp(c, Dc, dt / 2e0, eoff); });
+    timed(3, [&] { enqueue_ds(c, Dc, dt / 2e0, eoff); });
+    timed(4, [&] { launch_dr(Dc, c->st, dt); });
+    timed(5, [&] { launch_pairs(Dn, c->st, true); });
+    timed(3, [&] { enqueue_ds(c, Dn, dt / 2e0, eoff); });
+    timed(6, [&] { launch_force(Dn, c->st); });
+    timed(2, [&] { enqueue_dp(c, Dn, dt / 2e0, eoff); });
     if (c->P.eltemp) {
-        timed(7, [&] { launch_temperature(c->D, c->st); });
-        timed(1, [&] { launch_dte(c->D, c->st, dt / 2e0); });
-        if (c->P.renormalize_energy) timed(8, [&] { launch_energy_check(c->D, c->st, 1); });
+        timed(7, [&] { launch_temperature(Dn, c->st); });
+        timed(1, [&] { launch_dte(Dn, c->st, dt / 2e0); });
+        if (c->P.renormalize_energy) timed(8, [&] { launch_energy_check(Dn, c->st, 1); });
     }
-    timed(9, [&] { launch_advance(c->D, c->st, eoff, 1); });
+    timed(9, [&] { launch_advance(Dn, c->st, eoff, 1); });
+    use_set(c, 1 - c->cur);
     cudaEventDestroy(ev[0]);
     cudaEventDestroy(ev[1]);
     return launch_status();
@@ -512,6 +597,7 @@ int sld_profile_step(sld_ctx* c, double* ms) {
 int sld_step_kernel_count(sld_ctx* c, int* out) {
     if (!c || !out) return SLD_ERR_ARG;
     cudaGraph_t g = nullptr;
+    fresh_lists(c);
     CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
     enqueue_step(c);
     CK(cudaStreamEndCapture(c->st, &g));

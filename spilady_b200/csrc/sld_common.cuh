@@ -85,12 +85,16 @@ struct Dev {
     int te_ngroups;
     // per-step neighbour lists (built after every drift by k_pairs):
     //   nbr  [SLD_MAXNB][natom]  j | (1<<30 when the pair crosses the box)
-    //        for r_ij < rcut_max, in the reference's traversal order
-    //   jl/jv [SLD_MAXJ][natom]  j and J(r_ij) for r_ij < rcut_mag
+    //        for r_ij < rcut_max, in the reference's traversal order; entry
+    //        major, as its readers take atoms in storage order
+    //   jl/jv [natom][SLD_MAXJ]  j and J(r_ij) for r_ij < rcut_mag; atom
+    //        major, as the spin sweeps visit atoms of cells scattered over
+    //        the box and each visit should read one contiguous row
     int *nbr, *nbr_n, *jl, *jl_n;
     double* jv;                   // FP64 form
     float* jvf;                   // split form
     double* dF;                   // F'(rho) per atom, refreshed after each rho pass
+    double* xi;                   // [natom][2 sweeps][3] spin-noise normals of one core_ds
     // control and reduction scratch
     Ctl* ctl;
     double* red;                  // partial sums
@@ -266,7 +270,6 @@ static inline int div_up(long a, long b) { return (int)((a + b - 1) / b); }
 template <class Skip, class OnSkip>
 __device__ __forceinline__ void exchange_field(const Dev& D, int i, double3& H, double& sumJ,
                                                Skip skip, OnSkip on_skip) {
-    const int N = D.natom;
     const int nj = D.jl_n[i];
     double hx = 0, hy = 0, hz = 0, hj = 0;
     float ks[4] = {0, 0, 0, 0}, kc[4] = {0, 0, 0, 0};   // Kahan sums (split form)
@@ -276,8 +279,9 @@ __device__ __forceinline__ void exchange_field(const Dev& D, int i, double3& H, 
 #pragma unroll
         for (int u = 0; u < SLD_GB; ++u) {
             int e = e0 + u;
-            jj[u] = e < nj ? D.jl[(size_t)e * N + i] : -1;
-            Jv[u] = e < nj ? (D.split ? (double)D.jvf[(size_t)e * N + i] : D.jv[(size_t)e * N + i])
+            size_t at = (size_t)i * SLD_MAXJ + e;
+            jj[u] = e < nj ? D.jl[at] : -1;
+            Jv[u] = e < nj ? (D.split ? (double)D.jvf[at] : D.jv[at])
                            : 0.0;
         }
         double4 sj[SLD_GB];
@@ -326,8 +330,11 @@ void launch_pairs(const Dev& D, cudaStream_t st, bool write_rho);
 void sweep_init();
 void launch_force(const Dev& D, cudaStream_t st);
 void launch_embed(const Dev& D, cudaStream_t st);
+void launch_force_eam(const Dev& D, cudaStream_t st);   // lattice terms (no spins)
+void launch_force_mag(const Dev& D, cudaStream_t st);   // adds the magnetic terms
 void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g, double dt,
                   bool backward, int epoch_off);
+void launch_spin_noise(const Dev& D, cudaStream_t st, int epoch_off);
 void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off);
 void launch_dr(const Dev& D, cudaStream_t st, double dt);
 void launch_temperature(const Dev& D, cudaStream_t st);

@@ -3,16 +3,55 @@
 #include "sld_common.cuh"
 
 // core_ds_CPU.cpp:90-127: exact rotation of s about -Heff/hbar by |w| dt
+// sin x and 1 - cos x.  The rotation angle |w| dt of one visit is a small
+// fraction of a radian, where the Taylor series of sin and of 1 - cos
+// (truncated after x^15 and x^16: the next terms are below 1e-17 relative for
+// |x| < 0.5) are far shorter than the general routine; larger angles use
+// sincos.  1 - cos x from its own series also avoids the cancellation of
+// 1 - cos(x) near zero.
+__device__ __forceinline__ void sin_1mcos(double x, double& sn, double& omc) {
+    if (fabs(x) < 0.5) {
+        double x2 = x * x;
+        // sin x = x (1 - x^2/3! + x^4/5! - ...)
+        double p = -1.0 / 1307674368000.0;                 // -1/15!
+        p = p * x2 + 1.0 / 6227020800.0;                   //  1/13!
+        p = p * x2 - 1.0 / 39916800.0;                     // -1/11!
+        p = p * x2 + 1.0 / 362880.0;                       //  1/9!
+        p = p * x2 - 1.0 / 5040.0;                         // -1/7!
+        p = p * x2 + 1.0 / 120.0;                          //  1/5!
+        p = p * x2 - 1.0 / 6.0;                            // -1/3!
+        sn = x + x * (x2 * p);
+        // 1 - cos x = x^2 (1/2! - x^2/4! + x^4/6! - ...)
+        double q = 1.0 / 20922789888000.0;                 //  1/16!
+        q = q * x2 - 1.0 / 87178291200.0;                  // -1/14!
+        q = q * x2 + 1.0 / 479001600.0;                    //  1/12!
+        q = q * x2 - 1.0 / 3628800.0;                      // -1/10!
+        q = q * x2 + 1.0 / 40320.0;                        //  1/8!
+        q = q * x2 - 1.0 / 720.0;                          // -1/6!
+        q = q * x2 + 1.0 / 24.0;                           //  1/4!
+        q = q * x2 - 0.5;                                  // -1/2!
+        omc = -(x2 * q);
+        return;
+    }
+    double c;
+    sincos(x, &sn, &c);
+    omc = 1.0 - c;
+}
+
+// (w = -H/hbar is formed with one reciprocal and |w| with one reciprocal
+// square root: the reference divides each component, which differs in the
+// last bit at most)
 __device__ __forceinline__ double3 spin_rotation(double3 H, double3 s, double dt) {
-    double3 w = make_double3(H.x / -SLD_HBAR, H.y / -SLD_HBAR, H.z / -SLD_HBAR);
-    double w0 = sqrt(w.x * w.x + w.y * w.y + w.z * w.z);
-    if (w0 > 0.0) w = make_double3(w.x / w0, w.y / w0, w.z / w0);
-    else w = make_double3(0.0, 0.0, 0.0);
+    const double k = -1.0 / SLD_HBAR;
+    double3 w = make_double3(H.x * k, H.y * k, H.z * k);
+    double w2 = w.x * w.x + w.y * w.y + w.z * w.z;
+    double iw = w2 > 0.0 ? rsqrt(w2) : 0.0;
+    double w0 = w2 * iw;
+    w = make_double3(w.x * iw, w.y * iw, w.z * iw);
     double w12 = w.x * w.y, w23 = w.y * w.z, w13 = w.x * w.z;
     double w1s = w.x * w.x, w2s = w.y * w.y, w3s = w.z * w.z;
-    double A, cw;
-    sincos(w0 * dt, &A, &cw);
-    double B = 1.0 - cw;
+    double A, B;
+    sin_1mcos(w0 * dt, A, B);
     double3 o;
     o.x = s.x + (s.x * B * (-w2s - w3s) + s.y * (B * w12 - A * w.z) + s.z * (A * w.y + B * w13));
     o.y = s.y + (s.y * B * (-w1s - w3s) + s.z * (B * w23 - A * w.x) + s.x * (A * w.z + B * w12));
@@ -26,9 +65,8 @@ __device__ __forceinline__ double3 landau_field(const double L[4], double sumJ, 
     double c = -(2.0 * L[0] + 4.0 * L[1] * s_sq + 6.0 * L[2] * (s_sq * s_sq) +
                  8.0 * L[3] * (s_sq * s_sq * s_sq));
     double3 HL = make_double3(c * x.x, c * x.y, c * x.z);
-    double s0 = sqrt(s_sq);
-    if (s0 > 0.0) {
-        double k = -sumJ / s0;
+    if (s_sq > 0.0) {
+        double k = -sumJ * rsqrt(s_sq);
         HL.x += k * x.x; HL.y += k * x.y; HL.z += k * x.z;
     }
     return HL;
