@@ -185,6 +185,31 @@ int sld_step_kernel_count(sld_ctx* ctx, int* out);
 
 const char* sld_error_string(int code);
 
+/* Allocation-free averages.  This entry point has no counterpart in the
+   reference; it exists for callers that cannot let a library allocate
+   device memory (a code that gives all device memory to its own pool, or
+   cannot afford cudaFree, which waits for all device work, during its
+   stream-ordered work).  It computes out[0..7] = <pe>, <ke>, <me>, <me0>,
+   Tl (K), <sx>, <sy>, <sz>, the same values as out[0,1,2,3,5,7,8,9] of
+   the context-based averages entry point, from caller-owned device arrays
+   pe, ke, me, me0 (natom each) and s (3 * natom, xyz per atom), and writes
+   them to the device array out8, all on `stream` (a cudaStream_t; NULL is
+   the default stream).  It calls no cudaMalloc or cudaFree: its scratch
+   is a fixed device array compiled into the library, large enough for
+   SLD_AVERAGES_STATIC_MAX_ATOMS atoms (2 MiB); larger natom is refused
+   with SLD_ERR_CAPACITY before any launch.
+   - The first call on each device (the device current at the call) looks
+     up that array's device address (cudaGetSymbolAddress) and keeps it;
+     make that first call before capturing any stream.
+   - There is one scratch array per device, so calls that overlap on one
+     device (on different streams, or from different host threads without
+     ordering) race on it and can return wrong averages.  Order them on one
+     stream or with events. */
+#define SLD_AVERAGES_STATIC_MAX_ATOMS 8388608
+int sld_averages_static(const double* pe, const double* ke, const double* me,
+                        const double* me0, const double* s, int natom, double* out8,
+                        void* stream);
+
 #ifdef __cplusplus
 }
 #endif
