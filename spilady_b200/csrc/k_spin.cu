@@ -20,6 +20,7 @@
 // shared-memory tables falls back to one thread per cell reading everything
 // from global memory, with the same arithmetic.
 #include <cstdlib>
+#include <type_traits>
 
 #include "sld_pot32.cuh"
 #include "sld_spin.cuh"
@@ -32,7 +33,7 @@
 struct SweepShared {
     double s[SW_MAXA][4];           // current spin, |s|
     double h[SW_MAXA][4];           // field of the out-of-cell neighbours, sum J|s|
-    double aux[SW_MAXA][5];         // rho, T, noise x y z
+    double aux[SW_MAXA][4];         // rho, noise increment x y z
     double inJ[SW_MAXA][SW_MAXIN];  // J of the in-cell neighbours
     int slot[SW_MAXA];
     unsigned char inq[SW_MAXA][SW_MAXIN];   // their position in the cell list
@@ -46,6 +47,7 @@ __device__ __forceinline__ void visit_store(const Dev& D, int i, double3 s, doub
     double s0 = sqrt(s.x * s.x + s.y * s.y + s.z * s.z);
     if (!isfinite(s0)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
     D.s[i] = make_double4(s.x, s.y, s.z, s0);
+    if (D.split) D.s32[i] = make_float4((float)s.x, (float)s.y, (float)s.z, (float)s0);
     if (fields) {
         D.H[i] = make_double4(H.x, H.y, H.z, 0.0);
         D.HL[i] = make_double4(HL.x, HL.y, HL.z, 0.0);
@@ -53,15 +55,18 @@ __device__ __forceinline__ void visit_store(const Dev& D, int i, double3 s, doub
     }
 }
 
-// The normals of both sweeps of one core_ds call, drawn for every atom in
-// one parallel pass before the sweeps (the draw is counter-based, so it does
-// not depend on when it is made); the sweeps' serial chains only read them.
-__global__ void __launch_bounds__(256) k_spin_noise(Dev D, int epoch_off) {
+// The noise increments of both sweeps of one core_ds call, drawn for every
+// atom in one parallel pass before the sweeps (the draw is counter-based, so
+// it does not depend on when it is made, and the temperature does not change
+// during core_ds); the sweeps' serial chains only read them.  Stored atom
+// major: [natom][sweep][3], dS = sqrt(2 T gamma_S_HL / dt) xi.
+__global__ void __launch_bounds__(256) k_spin_noise(Dev D, int epoch_off, double dt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= D.natom) return;
     unsigned long long e0 = D.ctl->epoch + (unsigned long long)epoch_off;
+    double T = D.eltemp ? D.Te[D.node[i]] : D.temperature;
     for (int v = 0; v < 2; ++v) {
-        double3 x = normals3(D.seed, 0u, (unsigned)D.id[i], e0 + v);
+        double3 x = spin_noise_dS(D, T, normals3(D.seed, 0u, (unsigned)D.id[i], e0 + v), dt);
         double* o = D.xi + 6 * (size_t)i + 3 * v;
         o[0] = x.x;
         o[1] = x.y;
@@ -69,8 +74,20 @@ __global__ void __launch_bounds__(256) k_spin_noise(Dev D, int epoch_off) {
     }
 }
 
-void launch_spin_noise(const Dev& D, cudaStream_t st, int epoch_off) {
-    k_spin_noise<<<div_up(D.natom, 256), 256, 0, st>>>(D, epoch_off);
+void launch_spin_noise(const Dev& D, cudaStream_t st, int epoch_off, double dt) {
+    k_spin_noise<<<div_up(D.natom, 256), 256, 0, st>>>(D, epoch_off, dt);
+}
+
+// s32 = (float)s for every atom, after the spins are loaded from the host
+__global__ void __launch_bounds__(256) k_spin32(Dev D) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.natom) return;
+    double4 s = D.s[i];
+    D.s32[i] = make_float4((float)s.x, (float)s.y, (float)s.z, (float)s.w);
+}
+
+void launch_spin32(const Dev& D, cudaStream_t st) {
+    k_spin32<<<div_up(D.natom, 256), 256, 0, st>>>(D);
 }
 
 __device__ __forceinline__ double3 spin_noise_at(const Dev& D, int i, int sweep) {
@@ -79,32 +96,28 @@ __device__ __forceinline__ double3 spin_noise_at(const Dev& D, int i, int sweep)
 }
 
 // one visit entirely from global memory (the fallback path)
-__device__ void visit_global(const Dev& D, int i, double dt, unsigned long long epoch, bool fields) {
+__device__ void visit_global(const Dev& D, int i, double dt, bool fields) {
     double3 H;
     double sumJ;
     exchange_field(D, i, H, sumJ, [](int) { return false; }, [](int, double) {});
     double4 s4 = D.s[i];
-    double T = 0.0, rho = 0.0;
-    double3 xi = make_double3(0.0, 0.0, 0.0);
+    double rho = 0.0;
+    double3 dS = make_double3(0.0, 0.0, 0.0);
     if (D.spinlang) {
-        T = D.eltemp ? D.Te[D.node[i]] : D.temperature;
         rho = D.rho[i];
-        xi = spin_noise_at(D, i, fields ? 1 : 0);
-        (void)epoch;
+        dS = spin_noise_at(D, i, fields ? 1 : 0);
     }
     double3 HL;
-    double3 s = spin_integrate(D, make_double3(s4.x, s4.y, s4.z), H, sumJ, rho, T, xi, dt, HL);
+    double3 s = spin_integrate_dS(D, make_double3(s4.x, s4.y, s4.z), H, sumJ, rho, dS, dt, HL);
     visit_store(D, i, s, H, HL, sumJ, fields);
 }
 
 __global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restrict__ gcells,
-                                                      int ncell_g, double dt, int backward,
-                                                      int epoch_off) {
+                                                      int ncell_g, double dt, int backward) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SweepShared& S = *reinterpret_cast<SweepShared*>(smem_raw);
     const int cbeg = blockIdx.x * SW_CPB;
     const int ncb = min(SW_CPB, ncell_g - cbeg);
-    const unsigned long long epoch = D.ctl->epoch + (unsigned long long)epoch_off;
     const bool fields = backward != 0;   // the backward sweep is each atom's last visit
     if (threadIdx.x < 32) {
         int lane = threadIdx.x, n = 0, st = 0, c = -1;
@@ -162,10 +175,9 @@ __global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restri
             S.inn[a] = (unsigned char)(nin < SW_MAXIN ? nin : SW_MAXIN);
             if (nin > SW_MAXIN) S.overflow = 1;
             if (D.spinlang) {
-                double3 xi = spin_noise_at(D, i, fields ? 1 : 0);
+                double3 dS = spin_noise_at(D, i, fields ? 1 : 0);
                 S.aux[a][0] = D.rho[i];
-                S.aux[a][1] = D.eltemp ? D.Te[D.node[i]] : D.temperature;
-                S.aux[a][2] = xi.x; S.aux[a][3] = xi.y; S.aux[a][4] = xi.z;
+                S.aux[a][1] = dS.x; S.aux[a][2] = dS.y; S.aux[a][3] = dS.z;
             }
         }
         __syncthreads();
@@ -184,9 +196,9 @@ __global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restri
                         sumJ += J * S.s[a2][3];
                     }
                     double3 HL;
-                    double3 s = spin_integrate(
+                    double3 s = spin_integrate_dS(
                         D, make_double3(S.s[a][0], S.s[a][1], S.s[a][2]), H, sumJ, S.aux[a][0],
-                        S.aux[a][1], make_double3(S.aux[a][2], S.aux[a][3], S.aux[a][4]), dt, HL);
+                        make_double3(S.aux[a][1], S.aux[a][2], S.aux[a][3]), dt, HL);
                     double s0 = sqrt(s.x * s.x + s.y * s.y + s.z * s.z);
                     S.s[a][0] = s.x; S.s[a][1] = s.y; S.s[a][2] = s.z; S.s[a][3] = s0;
                     if (fields) {
@@ -203,6 +215,9 @@ __global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restri
                 double s0 = S.s[a][3];
                 if (!isfinite(s0)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
                 D.s[S.slot[a]] = make_double4(S.s[a][0], S.s[a][1], S.s[a][2], s0);
+                if (D.split)
+                    D.s32[S.slot[a]] = make_float4((float)S.s[a][0], (float)S.s[a][1],
+                                                   (float)S.s[a][2], (float)s0);
             }
             return;
         }
@@ -212,7 +227,7 @@ __global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restri
         int q = threadIdx.x, n = S.cell_n[q], st = S.cell_start[q];
         for (int t = 0; t < n; ++t) {
             int i = D.cell_atoms[st + (backward ? n - 1 - t : t)];
-            visit_global(D, i, dt, epoch, fields);
+            visit_global(D, i, dt, fields);
         }
     }
 }
@@ -220,37 +235,256 @@ __global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restri
 // one thread per cell for the whole visit, reading the spins from global
 // memory (no shared-memory phases)
 __global__ void __launch_bounds__(128) k_sweep_cell(Dev D, const int* __restrict__ gcells,
-                                                    int ncell_g, double dt, int backward,
-                                                    int epoch_off) {
+                                                    int ncell_g, double dt, int backward) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ncell_g) return;
     int c = gcells[t];
     int st = D.cell_start[c], n = D.cell_count[c];
-    unsigned long long epoch = D.ctl->epoch + (unsigned long long)epoch_off;
     bool fields = backward != 0;
     for (int m = 0; m < n; ++m) {
         int i = D.cell_atoms[st + (backward ? n - 1 - m : m)];
-        visit_global(D, i, dt, epoch, fields);
+        visit_global(D, i, dt, fields);
+    }
+}
+
+// ---------------------------------------------------------------------
+// One thread per cell, software-pipelined.  A visit's inputs sit behind a
+// chain of dependent loads (cell list -> atom -> exchange row -> neighbour
+// spins), and a thread walks its cell's atoms one after another, so without
+// overlap every visit pays that chain in full.  Here the loads of later
+// visits are issued before visit m is integrated:
+//   - the atom index three visits ahead;
+//   - the first SC_PJ exchange-list indices of the atom two visits ahead
+//     (split form; the FP64 form, short of registers, loads them one visit
+//     ahead and waits for them);
+//   - for the next atom: its couplings J, the spins of its first SC_PJ
+//     exchange neighbours, its own spin, rho and noise increment.
+// During visit m only atom m's spin changes (cells of one colour group share
+// no neighbour), so a prefetched neighbour spin is stale only if that
+// neighbour is atom m; it is replaced by atom m's new spin right after the
+// store.  Entries beyond SC_PJ (rare in bcc Fe) are read when used.  The
+// field is summed in exchange-list order with exchange_field's arithmetic,
+// so the result is the one of k_sweep_cell.  The split form gathers the FP32
+// copy of the spins (16 bytes per neighbour, the values its FP32 sums use).
+#define SC_PJ 16
+
+// the exchange-list indices of one atom, as loaded (not yet masked by nj)
+struct RowIdx {
+    int i, nj;
+    int4 w[SC_PJ / 4];
+};
+
+__device__ __forceinline__ void row_load(const Dev& D, int i, RowIdx& r) {
+    r.i = i;
+    r.nj = __ldg(D.jl_n + i);
+    const int4* jl4 = reinterpret_cast<const int4*>(D.jl + (size_t)i * SLD_MAXJ);
+#pragma unroll
+    for (int q = 0; q < SC_PJ / 4; ++q) r.w[q] = __ldg(jl4 + q);
+}
+
+template <bool SPLIT>
+struct VisitRegs {
+    using JT = typename std::conditional<SPLIT, float, double>::type;
+    using ST = typename std::conditional<SPLIT, float4, double4>::type;
+    int i, nj;
+    int jj[SC_PJ];
+    JT J[SC_PJ];
+    ST sj[SC_PJ];
+    double4 si;
+    double rho;
+    double3 dS;
+};
+
+template <bool SPLIT>
+__device__ __forceinline__ typename VisitRegs<SPLIT>::ST spin_reg(const double4& s) {
+    if constexpr (SPLIT) {
+        return make_float4((float)s.x, (float)s.y, (float)s.z, (float)s.w);
+    } else {
+        return s;
+    }
+}
+
+// everything of one visit but the indices: couplings, neighbour spins, the
+// atom's own spin, rho and noise increment
+template <bool SPLIT>
+__device__ __forceinline__ void visit_fetch(const Dev& D, const RowIdx& r, int sweep,
+                                            VisitRegs<SPLIT>& v) {
+    const int i = r.i, nj = r.nj;
+    v.i = i;
+    v.nj = nj;
+#pragma unroll
+    for (int q = 0; q < SC_PJ / 4; ++q) {
+        v.jj[4 * q + 0] = 4 * q + 0 < nj ? r.w[q].x : -1;
+        v.jj[4 * q + 1] = 4 * q + 1 < nj ? r.w[q].y : -1;
+        v.jj[4 * q + 2] = 4 * q + 2 < nj ? r.w[q].z : -1;
+        v.jj[4 * q + 3] = 4 * q + 3 < nj ? r.w[q].w : -1;
+    }
+    const size_t row = (size_t)i * SLD_MAXJ;
+    if constexpr (SPLIT) {
+        const float4* j4 = reinterpret_cast<const float4*>(D.jvf + row);
+#pragma unroll
+        for (int q = 0; q < SC_PJ / 4; ++q) {
+            float4 w = __ldg(j4 + q);
+            v.J[4 * q + 0] = w.x; v.J[4 * q + 1] = w.y; v.J[4 * q + 2] = w.z; v.J[4 * q + 3] = w.w;
+        }
+#pragma unroll
+        for (int u = 0; u < SC_PJ; ++u)
+            v.sj[u] = v.jj[u] >= 0 ? D.s32[v.jj[u]] : make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+        const double2* j2 = reinterpret_cast<const double2*>(D.jv + row);
+#pragma unroll
+        for (int q = 0; q < SC_PJ / 2; ++q) {
+            double2 w = __ldg(j2 + q);
+            v.J[2 * q + 0] = w.x; v.J[2 * q + 1] = w.y;
+        }
+#pragma unroll
+        for (int u = 0; u < SC_PJ; ++u)
+            v.sj[u] = v.jj[u] >= 0 ? D.s[v.jj[u]] : make_double4(0, 0, 0, 0);
+    }
+    v.si = D.s[i];
+    if (D.spinlang) {
+        v.rho = __ldg(D.rho + i);
+        const double* x = D.xi + 6 * (size_t)i + 3 * sweep;
+        v.dS = make_double3(__ldg(x), __ldg(x + 1), __ldg(x + 2));
+    } else {
+        v.rho = 0.0;
+        v.dS = make_double3(0.0, 0.0, 0.0);
+    }
+}
+
+// sum_j J s_j and sum_j J |s_j| in exchange-list order (exchange_field's
+// arithmetic: FP64, or FP32 products in Kahan sums for the split form)
+template <bool SPLIT>
+__device__ __forceinline__ void visit_field(const Dev& D, const VisitRegs<SPLIT>& v, double3& H,
+                                            double& sumJ) {
+    double hx = 0, hy = 0, hz = 0, hj = 0;
+    float ks[4] = {0, 0, 0, 0}, kc[4] = {0, 0, 0, 0};
+    auto add32 = [&](float J, float4 s) {
+        float w[4] = {J * s.x, J * s.y, J * s.z, J * s.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float y = w[q] - kc[q];
+            float t = ks[q] + y;
+            kc[q] = (t - ks[q]) - y;
+            ks[q] = t;
+        }
+    };
+    auto add64 = [&](double J, double4 s) {
+        hx += J * s.x; hy += J * s.y; hz += J * s.z;
+        hj += J * s.w;
+    };
+#pragma unroll
+    for (int u = 0; u < SC_PJ; ++u) {
+        if (u < v.nj) {
+            if constexpr (SPLIT) add32(v.J[u], v.sj[u]);
+            else add64(v.J[u], v.sj[u]);
+        }
+    }
+    for (int e = SC_PJ; e < v.nj; ++e) {
+        const size_t at = (size_t)v.i * SLD_MAXJ + e;
+        const int j = D.jl[at];
+        if constexpr (SPLIT) add32(D.jvf[at], D.s32[j]);
+        else add64(D.jv[at], D.s[j]);
+    }
+    if constexpr (SPLIT) {
+        hx = (double)ks[0] - (double)kc[0];
+        hy = (double)ks[1] - (double)kc[1];
+        hz = (double)ks[2] - (double)kc[2];
+        hj = (double)ks[3] - (double)kc[3];
+    }
+    H = make_double3(hx, hy, hz);
+    sumJ = hj;
+}
+
+template <bool SPLIT>
+__global__ void __launch_bounds__(128) k_sweep_pipe(Dev D, const int* __restrict__ gcells,
+                                                    int ncell_g, double dt, int backward) {
+    constexpr bool kDeep = SPLIT;   // indices two visits ahead
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ncell_g) return;
+    const int c = gcells[t];
+    const int n = D.cell_count[c];
+    if (n <= 0) return;
+    const int* ca = D.cell_atoms + D.cell_start[c];
+    const bool fields = backward != 0;   // the backward sweep is each atom's last visit
+    const int sweep = fields ? 1 : 0;
+    auto atom_at = [&](int m) { return __ldg(ca + (backward ? n - 1 - m : m)); };
+    VisitRegs<SPLIT> v;
+    RowIdx r;
+    row_load(D, atom_at(0), r);
+    visit_fetch<SPLIT>(D, r, sweep, v);
+    int i_after;          // the atom whose indices are loaded next
+    if (kDeep) {
+        if (n > 1) row_load(D, atom_at(1), r);
+        i_after = n > 2 ? atom_at(2) : -1;
+    } else {
+        i_after = n > 1 ? atom_at(1) : -1;
+    }
+    for (int m = 0; m < n; ++m) {
+        const int i = v.i;
+        double3 H;
+        double sumJ;
+        visit_field<SPLIT>(D, v, H, sumJ);
+        const double3 s_old = make_double3(v.si.x, v.si.y, v.si.z);
+        const double rho = v.rho;
+        const double3 dS = v.dS;
+        const bool more = m + 1 < n;
+        if (more) {
+            if (kDeep) {
+                visit_fetch<SPLIT>(D, r, sweep, v);        // r: indices of atom m+1
+                if (m + 2 < n) row_load(D, i_after, r);    // indices of atom m+2
+                i_after = m + 3 < n ? atom_at(m + 3) : -1;
+            } else {
+                row_load(D, i_after, r);
+                visit_fetch<SPLIT>(D, r, sweep, v);
+                i_after = m + 2 < n ? atom_at(m + 2) : -1;
+            }
+        }
+        double3 HL;
+        double3 s = spin_integrate_dS(D, s_old, H, sumJ, rho, dS, dt, HL);
+        double s0 = sqrt(s.x * s.x + s.y * s.y + s.z * s.z);
+        if (!isfinite(s0)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
+        const double4 s4 = make_double4(s.x, s.y, s.z, s0);
+        D.s[i] = s4;
+        const auto sr = spin_reg<SPLIT>(s4);
+        if constexpr (SPLIT) D.s32[i] = sr;
+        if (fields) {
+            D.H[i] = make_double4(H.x, H.y, H.z, 0.0);
+            D.HL[i] = make_double4(HL.x, HL.y, HL.z, 0.0);
+            if (D.spinlang) D.sumJ[i] = sumJ;
+        }
+        if (more) {
+#pragma unroll
+            for (int u = 0; u < SC_PJ; ++u)
+                if (v.jj[u] == i) v.sj[u] = sr;
+        }
     }
 }
 
 static size_t sweep_smem() { return sizeof(SweepShared); }
-static int g_sweep_mode = 1;   // 0: two-level (shared memory), 1: one thread per cell
+static int g_sweep_mode = 2;   // 0: two-level (shared memory), 1: one thread per cell,
+                               // 2: one thread per cell, pipelined
 
 void sweep_init() {
     cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem());
     const char* v = getenv("SLD_SWEEP_MODE");
-    if (v && (v[0] == '0' || v[0] == '1')) g_sweep_mode = v[0] - '0';
+    if (v && v[0] >= '0' && v[0] <= '2') g_sweep_mode = v[0] - '0';
 }
 
 void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g, double dt,
-                  bool backward, int epoch_off) {
+                  bool backward) {
     if (ncell_g <= 0) return;
-    if (g_sweep_mode == 1) {
-        k_sweep_cell<<<div_up(ncell_g, 128), 128, 0, st>>>(D, gcells, ncell_g, dt, backward ? 1 : 0,
-                                                          epoch_off);
+    const int b = backward ? 1 : 0;
+    if (g_sweep_mode == 2) {
+        if (D.split)
+            k_sweep_pipe<true><<<div_up(ncell_g, 128), 128, 0, st>>>(D, gcells, ncell_g, dt, b);
+        else
+            k_sweep_pipe<false><<<div_up(ncell_g, 128), 128, 0, st>>>(D, gcells, ncell_g, dt, b);
         return;
     }
-    k_sweep<<<div_up(ncell_g, SW_CPB), SW_THREADS, sweep_smem(), st>>>(D, gcells, ncell_g, dt,
-                                                                       backward ? 1 : 0, epoch_off);
+    if (g_sweep_mode == 1) {
+        k_sweep_cell<<<div_up(ncell_g, 128), 128, 0, st>>>(D, gcells, ncell_g, dt, b);
+        return;
+    }
+    k_sweep<<<div_up(ncell_g, SW_CPB), SW_THREADS, sweep_smem(), st>>>(D, gcells, ncell_g, dt, b);
 }

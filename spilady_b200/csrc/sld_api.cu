@@ -115,14 +115,14 @@ int launch_status() {
 void enqueue_ds(sld_ctx* c, const Dev& D, double dt, int& eoff) {
     const auto& G = c->G;
     double dt_half = dt / 2e0;
-    if (c->P.spinlang) launch_spin_noise(D, c->st, eoff);
+    if (c->P.spinlang) launch_spin_noise(D, c->st, eoff, dt_half);
     for (int g = 0; g < G.ngroups; ++g)
         launch_sweep(D, c->st, c->d_gcells + G.gstart[g], G.gstart[g + 1] - G.gstart[g],
-                     dt_half, false, eoff);
+                     dt_half, false);
     if (c->P.spinlang) ++eoff;
     for (int g = G.ngroups - 1; g >= 0; --g)
         launch_sweep(D, c->st, c->d_gcells + G.gstart[g], G.gstart[g + 1] - G.gstart[g],
-                     dt_half, true, eoff);
+                     dt_half, true);
     if (c->P.spinlang) ++eoff;
 }
 void enqueue_ds(sld_ctx* c, double dt, int& eoff) { enqueue_ds(c, c->D, dt, eoff); }
@@ -341,6 +341,7 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
          c->alloc(&c->jln_set[0], n) == 0 && c->alloc(&c->jln_set[1], n) == 0 &&
          c->alloc(&D.dF, n) == 0;
     if (prm->spinlang) ok = ok && c->alloc(&D.xi, 6 * n) == 0;
+    if (prm->precision == SLD_SPLIT) ok = ok && c->alloc(&D.s32, n) == 0;
     {
         float* cub = nullptr;
         double* cub64 = nullptr;
@@ -430,6 +431,7 @@ int sld_set_state(sld_ctx* c, const double* r, const double* p, const double* s)
     CK(cudaMemcpyAsync(D.r, hr.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(D.p, hp.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(D.s, hs.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, c->st));
+    if (D.split) launch_spin32(D, c->st);
     CK(cudaMemcpyAsync(D.ke, hke.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
     Ctl z{};
     CK(cudaMemcpyAsync(D.ctl, &z, sizeof(Ctl), cudaMemcpyHostToDevice, c->st));

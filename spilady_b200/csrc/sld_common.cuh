@@ -72,6 +72,8 @@ struct Dev {
     const double *tF, *tdF, *tf, *tdf, *tphi, *tdphi, *tJ, *tdJ;
     // atoms
     double4 *r, *p, *f, *s, *H, *HL;
+    float4* s32;                  // split form: s rounded to FP32, written with s by every
+                                  // spin writer; the FP32 exchange sums gather it
     double *rho, *pe, *ke, *me, *me0, *vir, *sumJ, *stress;
     int *cell_of, *id, *node;
     long long* stamp;
@@ -333,8 +335,9 @@ void launch_embed(const Dev& D, cudaStream_t st);
 void launch_force_eam(const Dev& D, cudaStream_t st);   // lattice terms (no spins)
 void launch_force_mag(const Dev& D, cudaStream_t st);   // adds the magnetic terms
 void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g, double dt,
-                  bool backward, int epoch_off);
-void launch_spin_noise(const Dev& D, cudaStream_t st, int epoch_off);
+                  bool backward);
+void launch_spin_noise(const Dev& D, cudaStream_t st, int epoch_off, double dt);
+void launch_spin32(const Dev& D, cudaStream_t st);
 void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off);
 void launch_dr(const Dev& D, cudaStream_t st, double dt);
 void launch_temperature(const Dev& D, cudaStream_t st);

@@ -73,11 +73,12 @@ __device__ __forceinline__ double3 landau_field(const double L[4], double sumJ, 
 }
 
 // One visit with field H (and sum_j J |s_j|): NVE rotation, or the five-part
-// Langevin Heisenberg-Landau scheme with normal noise xi at temperature T (eV).
-// Returns the new spin; HL receives the last Landau field.
-__device__ __forceinline__ double3 spin_integrate(const Dev& D, double3 s, double3 H, double sumJ,
-                                                  double rho, double T, double3 xi, double dt,
-                                                  double3& HL) {
+// Langevin Heisenberg-Landau scheme with the noise increment dS (eV/s, the
+// normals times sqrt(2 T gamma_S / dt)).  Returns the new spin; HL receives
+// the last Landau field.
+__device__ __forceinline__ double3 spin_integrate_dS(const Dev& D, double3 s, double3 H,
+                                                     double sumJ, double rho, double3 dS,
+                                                     double dt, double3& HL) {
     HL = make_double3(0.0, 0.0, 0.0);
     if (!D.spinlang) return spin_rotation(H, s, dt);
     double dt_half = dt / 2.0, dt_quad = dt / 4.0, g = D.gamma_S_HL;
@@ -90,9 +91,7 @@ __device__ __forceinline__ double3 spin_integrate(const Dev& D, double3 s, doubl
     HL = landau_field(L, sumJ, t);
     a = g * dt_half;
     s = make_double3(s.x + a * (H.x + HL.x), s.y + a * (H.y + HL.y), s.z + a * (H.z + HL.z));
-    double amp = sqrt(2.0 * T * g / dt);                                // part 3
-    double3 dS = make_double3(amp * xi.x, amp * xi.y, amp * xi.z);
-    s = make_double3(s.x + dt * dS.x, s.y + dt * dS.y, s.z + dt * dS.z);
+    s = make_double3(s.x + dt * dS.x, s.y + dt * dS.y, s.z + dt * dS.z);    // part 3
     HL = landau_field(L, sumJ, s);                                      // part 4
     a = g * dt_quad;
     t = make_double3(s.x + a * (H.x + HL.x), s.y + a * (H.y + HL.y), s.z + a * (H.z + HL.z));
@@ -100,4 +99,11 @@ __device__ __forceinline__ double3 spin_integrate(const Dev& D, double3 s, doubl
     a = g * dt_half;
     s = make_double3(s.x + a * (H.x + HL.x), s.y + a * (H.y + HL.y), s.z + a * (H.z + HL.z));
     return spin_rotation(H, s, dt_half);                                // part 5
+}
+
+// The noise increment of one visit at temperature T (eV): the normals xi
+// scaled by sqrt(2 T gamma_S_HL / dt) (calculate_spin_CPU.cpp:157-167).
+__device__ __forceinline__ double3 spin_noise_dS(const Dev& D, double T, double3 xi, double dt) {
+    double amp = sqrt(2.0 * T * D.gamma_S_HL / dt);
+    return make_double3(amp * xi.x, amp * xi.y, amp * xi.z);
 }
