@@ -46,6 +46,9 @@ extern "C" {
 #define SLD_ERR_IO (-7)         /* a file could not be read or parsed */
 #define SLD_ERR_STATE (-8)      /* call out of order (e.g. no state loaded) */
 #define SLD_ERR_NOMEM (-9)      /* device allocation failed */
+#define SLD_ERR_TIMEOUT (-10)   /* a bounded device-side wait ran out (the
+                                   spin sweeps' cell-by-cell schedule); the
+                                   state is no longer valid */
 
 #define SLD_MAX_CELL_ATOMS 64
 

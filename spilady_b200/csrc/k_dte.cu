@@ -1,0 +1,458 @@
+// core_dTe (core_dTe_CPU.cpp:47-200): nloop substeps of
+// A(h/2) B(h/2) C(h) B(h/2) A(h/2) on the electron-temperature cells.
+//   A  C dTe/dt = Gel Tl + Ges Ts_L     (cell-local)
+//   B  C dTe/dt = -(Gel + Ges) Te       (cell-local, RK4)
+//   C  C dTe/dt = kappa Laplacian Te    (colour sweep forward and back over
+//      the cells, then the total Ee rescaled to its value before the sweep)
+// Three kernels, by mesh size:
+//   k_dte_hub      meshes up to kHubMaxCells: a 4-CTA cluster, the sweep on
+//                  one CTA's shared memory, with the colour lists and a
+//                  neighbour table there too (the default);
+//   k_dte_cluster  any mesh: the cells spread over a cluster, Te in global
+//                  memory, a cluster barrier per colour phase;
+//   k_dte          any mesh, one CTA, global memory (no clusters).
+// Each is compiled with the reference's heat-capacity expressions (FP64
+// form) and with the fitted ones (sld_te.cuh; split form and its FP64 twin).
+#include <cooperative_groups.h>
+
+#include <cstdlib>
+
+#include "sld_te.cuh"
+
+namespace cg = cooperative_groups;
+
+struct DteGeom {
+    double dx2, dy2, dz2, pre;   // squared Te-cell edges; C's prefactor for a step h
+    double idx2, idy2, idz2;     // their reciprocals (fitted form)
+};
+
+__device__ __forceinline__ DteGeom dte_geom(const Dev& D, double h) {
+    DteGeom g;
+    double cond = D.kappa_e / SLD_EVTOJ / 1e10;
+    double lx = D.box_len[0] / D.tx, ly = D.box_len[1] / D.ty, lz = D.box_len[2] / D.tz;
+    g.dx2 = lx * lx;
+    g.dy2 = ly * ly;
+    g.dz2 = lz * lz;
+    double atomic_volume = D.box_volume / (double)D.natom;
+    double volume_factor = atomic_volume / ((double)D.natom / (double)D.nte);
+    g.pre = h / 2.0 * cond * volume_factor / SLD_BOLTZ;
+    g.idx2 = 1.0 / g.dx2;
+    g.idy2 = 1.0 / g.dy2;
+    g.idz2 = 1.0 / g.dz2;
+    return g;
+}
+
+// the six face neighbours of Te cell k (periodic)
+struct Nbr6 {
+    int xp, xm, yp, ym, zp, zm;
+};
+__device__ __forceinline__ Nbr6 te_nbr6(const Dev& D, int k) {
+    const int tx = D.tx, ty = D.ty, tz = D.tz;
+    int x = k % tx, y = (k / tx) % ty, z = k / (tx * ty);
+    int xp = x + 1 == tx ? 0 : x + 1, xm = x == 0 ? tx - 1 : x - 1;
+    int yp = y + 1 == ty ? 0 : y + 1, ym = y == 0 ? ty - 1 : y - 1;
+    int zp = z + 1 == tz ? 0 : z + 1, zm = z == 0 ? tz - 1 : z - 1;
+    return {xp + (y + z * ty) * tx, xm + (y + z * ty) * tx, x + (yp + z * ty) * tx,
+            x + (ym + z * ty) * tx, x + (y + zp * ty) * tx, x + (y + zm * ty) * tx};
+}
+
+// core_dTe_CPU.cpp:158-171: the Laplacian term of one cell (the fitted
+// form multiplies by the reciprocal squared edges instead of dividing)
+template <bool FAST>
+__device__ __forceinline__ double te_lap(const DteGeom& g, double T, double xp, double xm,
+                                         double yp, double ym, double zp, double zm) {
+    double ex = xp + xm - 2.0 * T;
+    double ey = yp + ym - 2.0 * T;
+    double ez = zp + zm - 2.0 * T;
+    if constexpr (FAST) return g.pre * (ex * g.idx2 + ey * g.idy2 + ez * g.idz2);
+    else return g.pre * (ex / g.dx2 + ey / g.dy2 + ez / g.dz2);
+}
+
+// Gel Tl + Ges Ts_L and (Gel + Ges) hh / boltz of cell k
+__device__ __forceinline__ double te_src(const Dev& D, int k) {
+    double dE = 0.0;
+    dE += D.Gel[k] * D.Tl[k];
+    dE += D.Ges[k] * D.TsL[k];
+    return dE;
+}
+__device__ __forceinline__ double te_rate(const Dev& D, int k, double hh) {
+    double g = 0.0;
+    g += D.Gel[k];
+    g += D.Ges[k];
+    g *= hh / SLD_BOLTZ;
+    return g;
+}
+
+// ---------------------------------------------------------------------
+// one CTA, global memory
+
+template <bool FAST>
+__device__ __forceinline__ void dte_A(const Dev& D, double dt) {
+    for (int k = threadIdx.x; k < D.nte; k += blockDim.x) {
+        double Ee = te_E<FAST>(D.Te[k]);
+        Ee += dt * te_src(D, k);
+        D.Ee[k] = Ee;
+        D.Te[k] = te_T<FAST>(Ee);
+    }
+}
+
+template <bool FAST>
+__device__ __forceinline__ void dte_B(const Dev& D, double dt) {
+    for (int k = threadIdx.x; k < D.nte; k += blockDim.x)
+        D.Te[k] = te_rk4<FAST>(D.Te[k], te_rate(D, k, dt), dt);
+}
+
+template <bool FAST>
+__device__ __forceinline__ double dte_total_Ee(const Dev& D, double* sh) {
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < D.nte; k += blockDim.x) {
+        double e = te_E<FAST>(D.Te[k]);
+        D.Ee[k] = e;
+        acc += e;
+    }
+    double t = block_sum(acc, sh);
+    __shared__ double tot;
+    if (threadIdx.x == 0) tot = t;
+    __syncthreads();
+    return tot;
+}
+
+template <bool FAST>
+__device__ __forceinline__ void dte_C(const Dev& D, double dt, double* sh) {
+    double start = dte_total_Ee<FAST>(D, sh);
+    const DteGeom gm = dte_geom(D, dt);
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int gg = 0; gg < D.te_ngroups; ++gg) {
+            int g = pass == 0 ? gg : D.te_ngroups - 1 - gg;
+            int b = D.te_gstart[g], e = D.te_gstart[g + 1];
+            for (int m = b + threadIdx.x; m < e; m += blockDim.x) {
+                int k = D.te_gcells[m];
+                const Nbr6 q = te_nbr6(D, k);
+                const double* Te = D.Te;
+                double T = Te[k];
+                double Ee = te_E<FAST>(T);
+                Ee += te_lap<FAST>(gm, T, Te[q.xp], Te[q.xm], Te[q.yp], Te[q.ym], Te[q.zp], Te[q.zm]);
+                D.Ee[k] = Ee;
+                D.Te[k] = te_T<FAST>(Ee);
+            }
+            __syncthreads();
+        }
+    }
+    double end = dte_total_Ee<FAST>(D, sh);
+    double fac = start / end;
+    for (int k = threadIdx.x; k < D.nte; k += blockDim.x) {
+        double Ee = D.Ee[k] * fac;
+        D.Ee[k] = Ee;
+        D.Te[k] = te_T<FAST>(Ee);
+    }
+    __syncthreads();
+}
+
+template <bool FAST>
+__global__ void __launch_bounds__(1024) k_dte(Dev D, double dt) {
+    __shared__ double sh[32];
+    int nloop = D.te_nloop > 0 ? D.te_nloop : 50;
+    double h = dt / nloop;
+    for (int it = 0; it < nloop; ++it) {
+        dte_A<FAST>(D, h / 2.0);
+        __syncthreads();
+        dte_B<FAST>(D, h / 2.0);
+        __syncthreads();
+        dte_C<FAST>(D, h, sh);
+        dte_B<FAST>(D, h / 2.0);
+        __syncthreads();
+        dte_A<FAST>(D, h / 2.0);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------
+// core_dTe on a thread-block cluster: the Te cells are split over the
+// cluster's CTAs (each thread owns the same cells in every phase, so A and B
+// need no barrier); the colour phases of the diffusion sweep and the two
+// energy sums of C synchronise the cluster with its hardware barrier.  Te is
+// read across CTAs through L2 (ld.global.cg) after the barrier.
+
+__device__ __forceinline__ double cl_total(double v, double* sh, double* slot_base,
+                                           cg::cluster_group& cl) {
+    double t = block_sum(v, sh);
+    if (threadIdx.x == 0) __stcg(slot_base + cl.block_rank(), t);
+    cl.sync();
+    double tot = 0.0;
+    for (unsigned r = 0; r < cl.num_blocks(); ++r) tot += __ldcg(slot_base + r);
+    return tot;
+}
+
+template <bool FAST>
+__global__ void __launch_bounds__(256) k_dte_cluster(Dev D, double dt) {
+    cg::cluster_group cl = cg::this_cluster();
+    __shared__ double sh[32];
+    const int nb = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    const int per = (D.nte + nb - 1) / nb;
+    const int k0 = rank * per, k1 = min(D.nte, k0 + per);
+    int nloop = D.te_nloop > 0 ? D.te_nloop : 50;
+    const double h = dt / nloop, hh = h / 2.0;
+    const DteGeom gm = dte_geom(D, h);
+    double* slots = D.red;   // 2 x num_blocks partial sums
+    for (int it = 0; it < nloop; ++it) {
+        for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {   // A(h/2), B(h/2)
+            double Ee = te_E<FAST>(__ldcg(D.Te + k));
+            Ee += hh * te_src(D, k);
+            double T = te_T<FAST>(Ee);
+            __stcg(D.Te + k, te_rk4<FAST>(T, te_rate(D, k, hh), hh));
+        }
+        // C(h): start sum, colour sweep forward and back, end sum, rescale
+        double part = 0.0;
+        for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) part += te_E<FAST>(__ldcg(D.Te + k));
+        double start = cl_total(part, sh, slots, cl);
+        for (int pass = 0; pass < 2; ++pass) {
+            for (int gg = 0; gg < D.te_ngroups; ++gg) {
+                int g = pass == 0 ? gg : D.te_ngroups - 1 - gg;
+                for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+                    if (D.te_color[k] != g) continue;
+                    const Nbr6 q = te_nbr6(D, k);
+                    double T = __ldcg(D.Te + k);
+                    double Ee = te_E<FAST>(T);
+                    Ee += te_lap<FAST>(gm, T, __ldcg(D.Te + q.xp), __ldcg(D.Te + q.xm),
+                                 __ldcg(D.Te + q.yp), __ldcg(D.Te + q.ym), __ldcg(D.Te + q.zp),
+                                 __ldcg(D.Te + q.zm));
+                    __stcg(D.Te + k, te_T<FAST>(Ee));
+                }
+                cl.sync();
+            }
+        }
+        part = 0.0;
+        for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) part += te_E<FAST>(__ldcg(D.Te + k));
+        double end = cl_total(part, sh, slots + nb, cl);
+        double fac = start / end;
+        for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {   // rescale, B(h/2), A(h/2)
+            double T = te_T<FAST>(te_E<FAST>(__ldcg(D.Te + k)) * fac);
+            T = te_rk4<FAST>(T, te_rate(D, k, hh), hh);
+            double Ee = te_E<FAST>(T) + hh * te_src(D, k);
+            D.Ee[k] = Ee;
+            __stcg(D.Te + k, te_T<FAST>(Ee));
+        }
+        cl.sync();   // the next substep reads neighbours' Te and reuses the slots
+    }
+}
+
+// ---------------------------------------------------------------------
+#define HUB_CL 4
+// Cluster "hub" form: every CTA of a 4-CTA cluster does the cell-local A and
+// B parts for its share of the cells in parallel; CTA 0 holds all Te and
+// Te_to_Ee(Te) in its shared memory (the others read and write them through
+// distributed shared memory) and runs C's colour phases with block barriers.
+// Two cluster barriers per substep instead of one per colour phase.
+//   - Each CTA keeps its cells' coupling source Gel Tl + Ges Ts_L and rate
+//     (Gel + Ges) h/2/boltz in its own shared memory: they do not change
+//     during core_dTe, so the substeps read no global memory.
+//   - In a colour phase, half of the hub's threads update the Te of the
+//     phase's cells (the chain the next phase waits for) while the other
+//     half evaluate Te_to_Ee for the cells of the previous phase, which no
+//     cell of this phase reads.  The one exception is the last forward
+//     colour, updated again right away by the backward pass: its Te_to_Ee is
+//     evaluated in place.  Every value is the one of the plain sequence.
+static const int kHubMaxCells = 6400;    // 8 (2 n + 2 + 2 n / 4) + 16 n bytes of shared memory
+
+template <bool FAST>
+__global__ void __launch_bounds__(1024) k_dte_hub(Dev D, double dt, int per) {
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ __align__(16) double hsm[];
+    const int n = D.nte;
+    const int rank = (int)cl.block_rank();
+    double* hT = cl.map_shared_rank(hsm, 0);   // the hub's arrays
+    double* hE = hT + n;
+    double* hfac = hT + 2 * n;
+    double* mySrc = hsm + 2 * n + 2;           // this CTA's own cells
+    double* myG = mySrc + per;
+    int* sGc = reinterpret_cast<int*>(myG + per);                        // hub: colour lists
+    unsigned short* sNb = reinterpret_cast<unsigned short*>(sGc + n);    // hub: 6 neighbours
+    __shared__ double sh[32];
+    const int k0 = rank * per, k1 = min(n, k0 + per);
+    int nloop = D.te_nloop > 0 ? D.te_nloop : 50;
+    double h = dt / nloop, hh = h / 2.0;
+    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        double T = D.Te[k];
+        hT[k] = T;
+        hE[k] = te_E<FAST>(T);
+        mySrc[k - k0] = te_src(D, k);
+        myG[k - k0] = te_rate(D, k, hh);
+    }
+    if (rank == 0) {
+        for (int m = threadIdx.x; m < n; m += blockDim.x) {
+            sGc[m] = D.te_gcells[m];
+            const Nbr6 q = te_nbr6(D, m);
+            unsigned short* o = sNb + 6 * m;
+            o[0] = (unsigned short)q.xp; o[1] = (unsigned short)q.xm; o[2] = (unsigned short)q.yp;
+            o[3] = (unsigned short)q.ym; o[4] = (unsigned short)q.zp; o[5] = (unsigned short)q.zm;
+        }
+    }
+    cl.sync();
+    const DteGeom gm = dte_geom(D, h);
+    double lastE[4];   // this thread's last A-step energies (per <= 4096 -> <= 4 per thread)
+    for (int it = 0; it < nloop; ++it) {
+        for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {   // A(h/2), B(h/2)
+            double T = te_T<FAST>(hE[k] + hh * mySrc[k - k0]);
+            T = te_rk4<FAST>(T, myG[k - k0], hh);
+            hT[k] = T;
+            hE[k] = te_E<FAST>(T);
+        }
+        cl.sync();
+        if (rank == 0) {   // C(h) on the hub
+            double acc = 0.0;
+            for (int k = threadIdx.x; k < n; k += blockDim.x) acc += hsm[n + k];
+            double t = block_sum(acc, sh);
+            __shared__ double tot;
+            if (threadIdx.x == 0) tot = t;
+            __syncthreads();
+            double start = tot;
+            const int G = D.te_ngroups, half = blockDim.x / 2;
+            const bool worker = threadIdx.x < half;
+            const int lane = worker ? threadIdx.x : threadIdx.x - half;
+            int pb = 0, pe = 0;   // cells of the previous phase whose Te_to_Ee is due
+            for (int p = 0; p < 2 * G; ++p) {
+                const int g = p < G ? p : 2 * G - 1 - p;
+                const int b = D.te_gstart[g], e = D.te_gstart[g + 1];
+                if (worker) {
+                    for (int m = b + lane; m < e; m += half) {
+                        int k = sGc[m];
+                        const unsigned short* q = sNb + 6 * k;
+                        const double* sT = hsm;
+                        double T = sT[k];
+                        T = te_T<FAST>(hsm[n + k] + te_lap<FAST>(gm, T, sT[q[0]], sT[q[1]], sT[q[2]],
+                                                                 sT[q[3]], sT[q[4]], sT[q[5]]));
+                        hsm[k] = T;
+                        if (p == G - 1) hsm[n + k] = te_E<FAST>(T);
+                    }
+                } else {
+                    for (int m = pb + lane; m < pe; m += half) {
+                        int k = sGc[m];
+                        hsm[n + k] = te_E<FAST>(hsm[k]);
+                    }
+                }
+                __syncthreads();
+                pb = p == G - 1 ? 0 : b;
+                pe = p == G - 1 ? 0 : e;
+            }
+            for (int m = pb + threadIdx.x; m < pe; m += blockDim.x) {
+                int k = sGc[m];
+                hsm[n + k] = te_E<FAST>(hsm[k]);
+            }
+            __syncthreads();
+            acc = 0.0;
+            for (int k = threadIdx.x; k < n; k += blockDim.x) acc += hsm[n + k];
+            t = block_sum(acc, sh);
+            if (threadIdx.x == 0) hsm[2 * n] = start / t;
+        }
+        cl.sync();
+        double fac = *hfac;
+        int q = 0;
+        for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x, ++q) {   // rescale, B, A
+            double T = te_T<FAST>(hE[k] * fac);
+            T = te_rk4<FAST>(T, myG[k - k0], hh);
+            double Ee = te_E<FAST>(T) + hh * mySrc[k - k0];
+            T = te_T<FAST>(Ee);
+            hT[k] = T;
+            hE[k] = te_E<FAST>(T);
+            if (q < 4) lastE[q] = Ee;
+        }
+    }
+    int q = 0;
+    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x, ++q) {
+        D.Te[k] = hT[k];
+        if (q < 4) D.Ee[k] = lastE[q];
+    }
+    cl.sync();   // keep the hub's shared memory alive until every CTA is done
+}
+
+// ---------------------------------------------------------------------
+// launch
+
+static bool g_dte_inited = false;
+static int g_dte_cluster = 0;   // cluster size of k_dte_cluster, 0: clusters unavailable
+static int g_dte_mode = 2;      // 2: hub when the mesh fits; 1: cluster; 0: one CTA
+static bool g_hub_ok = false;
+
+// dynamic shared memory of k_dte_hub for n Te cells: the hub's Te, f(Te) and
+// factor, and each CTA's own source and rate
+static size_t hub_smem(int n) {
+    const int per = (n + HUB_CL - 1) / HUB_CL;
+    return sizeof(double) * (2 * (size_t)n + 2 + 2 * (size_t)per) + sizeof(int) * (size_t)n +
+           sizeof(unsigned short) * 6 * (size_t)n;
+}
+
+static cudaLaunchConfig_t cluster_cfg(int cs, int threads, size_t smem, cudaStream_t st,
+                                      cudaLaunchAttribute* at) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+template <bool FAST>
+static void dte_attributes() {
+    cudaFuncSetAttribute(k_dte_hub<FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)hub_smem(kHubMaxCells));
+    cudaFuncSetAttribute(k_dte_cluster<FAST>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+
+int dte_init(int device) {
+    (void)device;
+    if (g_dte_inited) return g_dte_cluster;
+    g_dte_inited = true;
+    dte_attributes<false>();
+    dte_attributes<true>();
+    const char* m = getenv("SLD_DTE_MODE");
+    if (m && m[0] >= '0' && m[0] <= '2') g_dte_mode = m[0] - '0';
+    cudaLaunchAttribute at[1];
+    {
+        cudaLaunchConfig_t cfg = cluster_cfg(HUB_CL, 1024, hub_smem(kHubMaxCells), nullptr, at);
+        int nclu = 0, nclu2 = 0;
+        g_hub_ok = cudaOccupancyMaxActiveClusters(&nclu, k_dte_hub<false>, &cfg) == cudaSuccess &&
+                   nclu > 0 &&
+                   cudaOccupancyMaxActiveClusters(&nclu2, k_dte_hub<true>, &cfg) == cudaSuccess &&
+                   nclu2 > 0;
+        cudaGetLastError();
+    }
+    for (int cs : {16, 8, 4}) {
+        cudaLaunchConfig_t cfg = cluster_cfg(cs, 256, 0, nullptr, at);
+        int n = 0, n2 = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, k_dte_cluster<false>, &cfg) == cudaSuccess && n > 0 &&
+            cudaOccupancyMaxActiveClusters(&n2, k_dte_cluster<true>, &cfg) == cudaSuccess && n2 > 0) {
+            g_dte_cluster = cs;
+            break;
+        }
+        cudaGetLastError();
+    }
+    return g_dte_cluster;
+}
+
+template <bool FAST>
+static void launch_dte_form(const Dev& D, cudaStream_t st, double dt) {
+    cudaLaunchAttribute at[1];
+    const int hub_per = (D.nte + HUB_CL - 1) / HUB_CL;
+    if (g_dte_mode == 2 && g_hub_ok && D.nte <= kHubMaxCells && hub_per <= 4 * 1024) {
+        cudaLaunchConfig_t cfg = cluster_cfg(HUB_CL, 1024, hub_smem(D.nte), st, at);
+        cudaLaunchKernelEx(&cfg, k_dte_hub<FAST>, D, dt, hub_per);
+        return;
+    }
+    if (g_dte_mode >= 1 && g_dte_cluster > 0) {
+        cudaLaunchConfig_t cfg = cluster_cfg(g_dte_cluster, 256, 0, st, at);
+        cudaLaunchKernelEx(&cfg, k_dte_cluster<FAST>, D, dt);
+        return;
+    }
+    k_dte<FAST><<<1, 1024, 0, st>>>(D, dt);
+}
+
+void launch_dte(const Dev& D, cudaStream_t st, double dt) {
+    if (D.split || D.analytic) launch_dte_form<true>(D, st, dt);
+    else launch_dte_form<false>(D, st, dt);
+}

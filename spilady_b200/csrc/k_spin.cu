@@ -304,9 +304,28 @@ __device__ __forceinline__ typename VisitRegs<SPLIT>::ST spin_reg(const double4&
     }
 }
 
+// Spin loads.  CG: through L2 only (ld.global.cg), for a kernel in which
+// other blocks update spins while it runs, so that no stale copy in this
+// SM's L1 is read.
+template <bool CG>
+__device__ __forceinline__ double4 ld_spin(const double4* p) {
+    if constexpr (CG) {
+        const double2* q = reinterpret_cast<const double2*>(p);
+        double2 a = __ldcg(q), b = __ldcg(q + 1);
+        return make_double4(a.x, a.y, b.x, b.y);
+    } else {
+        return *p;
+    }
+}
+template <bool CG>
+__device__ __forceinline__ float4 ld_spin(const float4* p) {
+    if constexpr (CG) return __ldcg(p);
+    else return *p;
+}
+
 // everything of one visit but the indices: couplings, neighbour spins, the
 // atom's own spin, rho and noise increment
-template <bool SPLIT>
+template <bool SPLIT, bool CG>
 __device__ __forceinline__ void visit_fetch(const Dev& D, const RowIdx& r, int sweep,
                                             VisitRegs<SPLIT>& v) {
     const int i = r.i, nj = r.nj;
@@ -329,7 +348,7 @@ __device__ __forceinline__ void visit_fetch(const Dev& D, const RowIdx& r, int s
         }
 #pragma unroll
         for (int u = 0; u < SC_PJ; ++u)
-            v.sj[u] = v.jj[u] >= 0 ? D.s32[v.jj[u]] : make_float4(0.f, 0.f, 0.f, 0.f);
+            v.sj[u] = v.jj[u] >= 0 ? ld_spin<CG>(D.s32 + v.jj[u]) : make_float4(0.f, 0.f, 0.f, 0.f);
     } else {
         const double2* j2 = reinterpret_cast<const double2*>(D.jv + row);
 #pragma unroll
@@ -339,9 +358,9 @@ __device__ __forceinline__ void visit_fetch(const Dev& D, const RowIdx& r, int s
         }
 #pragma unroll
         for (int u = 0; u < SC_PJ; ++u)
-            v.sj[u] = v.jj[u] >= 0 ? D.s[v.jj[u]] : make_double4(0, 0, 0, 0);
+            v.sj[u] = v.jj[u] >= 0 ? ld_spin<CG>(D.s + v.jj[u]) : make_double4(0, 0, 0, 0);
     }
-    v.si = D.s[i];
+    v.si = ld_spin<CG>(D.s + i);
     if (D.spinlang) {
         v.rho = __ldg(D.rho + i);
         const double* x = D.xi + 6 * (size_t)i + 3 * sweep;
@@ -354,25 +373,13 @@ __device__ __forceinline__ void visit_fetch(const Dev& D, const RowIdx& r, int s
 
 // sum_j J s_j and sum_j J |s_j| in exchange-list order (exchange_field's
 // arithmetic: FP64, or FP32 products in Kahan sums for the split form)
-template <bool SPLIT>
+template <bool SPLIT, bool CG>
 __device__ __forceinline__ void visit_field(const Dev& D, const VisitRegs<SPLIT>& v, double3& H,
                                             double& sumJ) {
     double hx = 0, hy = 0, hz = 0, hj = 0;
     float ks[4] = {0, 0, 0, 0}, kc[4] = {0, 0, 0, 0};
-    auto add32 = [&](float J, float4 s) {
-        float w[4] = {J * s.x, J * s.y, J * s.z, J * s.w};
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            float y = w[q] - kc[q];
-            float t = ks[q] + y;
-            kc[q] = (t - ks[q]) - y;
-            ks[q] = t;
-        }
-    };
-    auto add64 = [&](double J, double4 s) {
-        hx += J * s.x; hy += J * s.y; hz += J * s.z;
-        hj += J * s.w;
-    };
+    auto add32 = [&](float J, float4 s) { exch_add32(ks, kc, J, s); };
+    auto add64 = [&](double J, double4 s) { exch_add64(hx, hy, hz, hj, J, s); };
 #pragma unroll
     for (int u = 0; u < SC_PJ; ++u) {
         if (u < v.nj) {
@@ -383,8 +390,8 @@ __device__ __forceinline__ void visit_field(const Dev& D, const VisitRegs<SPLIT>
     for (int e = SC_PJ; e < v.nj; ++e) {
         const size_t at = (size_t)v.i * SLD_MAXJ + e;
         const int j = D.jl[at];
-        if constexpr (SPLIT) add32(D.jvf[at], D.s32[j]);
-        else add64(D.jv[at], D.s[j]);
+        if constexpr (SPLIT) add32(D.jvf[at], ld_spin<CG>(D.s32 + j));
+        else add64(D.jv[at], ld_spin<CG>(D.s + j));
     }
     if constexpr (SPLIT) {
         hx = (double)ks[0] - (double)kc[0];
@@ -396,13 +403,10 @@ __device__ __forceinline__ void visit_field(const Dev& D, const VisitRegs<SPLIT>
     sumJ = hj;
 }
 
-template <bool SPLIT>
-__global__ void __launch_bounds__(128) k_sweep_pipe(Dev D, const int* __restrict__ gcells,
-                                                    int ncell_g, double dt, int backward) {
+// the walk of one cell c in the reference's order (backward: tail -> head)
+template <bool SPLIT, bool CG>
+__device__ __forceinline__ void cell_walk(const Dev& D, int c, double dt, int backward) {
     constexpr bool kDeep = SPLIT;   // indices two visits ahead
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ncell_g) return;
-    const int c = gcells[t];
     const int n = D.cell_count[c];
     if (n <= 0) return;
     const int* ca = D.cell_atoms + D.cell_start[c];
@@ -412,7 +416,7 @@ __global__ void __launch_bounds__(128) k_sweep_pipe(Dev D, const int* __restrict
     VisitRegs<SPLIT> v;
     RowIdx r;
     row_load(D, atom_at(0), r);
-    visit_fetch<SPLIT>(D, r, sweep, v);
+    visit_fetch<SPLIT, CG>(D, r, sweep, v);
     int i_after;          // the atom whose indices are loaded next
     if (kDeep) {
         if (n > 1) row_load(D, atom_at(1), r);
@@ -424,19 +428,19 @@ __global__ void __launch_bounds__(128) k_sweep_pipe(Dev D, const int* __restrict
         const int i = v.i;
         double3 H;
         double sumJ;
-        visit_field<SPLIT>(D, v, H, sumJ);
+        visit_field<SPLIT, CG>(D, v, H, sumJ);
         const double3 s_old = make_double3(v.si.x, v.si.y, v.si.z);
         const double rho = v.rho;
         const double3 dS = v.dS;
         const bool more = m + 1 < n;
         if (more) {
             if (kDeep) {
-                visit_fetch<SPLIT>(D, r, sweep, v);        // r: indices of atom m+1
+                visit_fetch<SPLIT, CG>(D, r, sweep, v);        // r: indices of atom m+1
                 if (m + 2 < n) row_load(D, i_after, r);    // indices of atom m+2
                 i_after = m + 3 < n ? atom_at(m + 3) : -1;
             } else {
                 row_load(D, i_after, r);
-                visit_fetch<SPLIT>(D, r, sweep, v);
+                visit_fetch<SPLIT, CG>(D, r, sweep, v);
                 i_after = m + 2 < n ? atom_at(m + 2) : -1;
             }
         }
@@ -461,21 +465,165 @@ __global__ void __launch_bounds__(128) k_sweep_pipe(Dev D, const int* __restrict
     }
 }
 
+template <bool SPLIT>
+__global__ void __launch_bounds__(128) k_sweep_pipe(Dev D, const int* __restrict__ gcells,
+                                                    int ncell_g, double dt, int backward) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ncell_g) return;
+    cell_walk<SPLIT, false>(D, gcells[t], dt, backward);
+}
+
+// ---------------------------------------------------------------------
+// Both sweeps of one core_ds call in one persistent launch, scheduled by
+// data flow instead of a grid-wide barrier per colour group.
+//
+// The reference's order gives each visit of a cell c of group g a fixed view
+// of its 26 neighbour cells:
+//   forward:  neighbours of groups < g already swept forward, of groups > g
+//             not yet;
+//   backward: neighbours of groups > g already swept backward, of groups < g
+//             swept forward but not yet backward.
+// Any schedule that keeps these views gives the reference's result bit for
+// bit.  Work is handed out in the reference's order (forward groups 0..G-1,
+// then backward G-1..0) in tasks of at most 32 cells of one group (one warp
+// each), through an atomic counter.  A cell's flag holds the tag of its last
+// finished sweep (tagF = forward of this call, tagB = backward); before a
+// warp walks its cells it waits until
+//   forward:  every neighbour of a lower group shows tagF;
+//   backward: the cell itself shows tagF, every neighbour of a higher group
+//             tagB and every one of a lower group tagF.
+// A neighbour that must not have moved yet cannot have: its own wait needs
+// this cell's flag.  Every task depends only on earlier tasks, and a task is
+// taken only by a running warp, so the earliest unfinished task can always
+// proceed.  The waits are bounded: a wait that runs out sets SLD_FLAG_WAIT
+// and every warp leaves; the host reports SLD_ERR_TIMEOUT.
+// Tags grow by 2 per call (sync[0]); flags and tags are never reset, so
+// stale flags from earlier calls are always below this call's tags.
+#define FLOW_POLLS (1 << 21)     // polls of one cell's waits (~0.2 s with the sleeps)
+
+__device__ __forceinline__ int ld_flag(const int* p) {
+    return *reinterpret_cast<const volatile int*>(p);
+}
+
+__device__ __forceinline__ bool flow_wait_one(const Dev& D, const int* flag, int need, int& budget) {
+    while (ld_flag(flag) < need) {
+        if (--budget <= 0) return false;
+        if ((budget & 255) == 0 &&
+            (*reinterpret_cast<const volatile unsigned*>(&D.ctl->err) & SLD_FLAG_WAIT))
+            return false;
+        __nanosleep(64);
+    }
+    return true;
+}
+
+// The waits of one cell: all its flags and groups are read at once, and only
+// the flags not yet set are polled.
+__device__ bool flow_wait(const Dev& D, const SweepFlow& F, int c, int g, bool bwd, int tagF,
+                          int tagB) {
+    int budget = FLOW_POLLS;
+    int cx, cy, cz;
+    cell_xyz(D, c, cx, cy, cz);
+    int nb[26], fl[26], gr[26];
+#pragma unroll
+    for (int k = 0; k < 26; ++k) nb[k] = nbr_cell(D, cx, cy, cz, k);
+#pragma unroll
+    for (int k = 0; k < 26; ++k) {
+        fl[k] = ld_flag(F.cell_flag + nb[k]);
+        gr[k] = __ldg(F.cell_group + nb[k]);
+    }
+    if (bwd && !flow_wait_one(D, F.cell_flag + c, tagF, budget)) return false;
+#pragma unroll
+    for (int k = 0; k < 26; ++k) {
+        int need;
+        if (!bwd) {
+            if (gr[k] > g) continue;
+            need = tagF;
+        } else {
+            need = gr[k] > g ? tagB : tagF;
+        }
+        if (fl[k] < need && !flow_wait_one(D, F.cell_flag + nb[k], need, budget)) return false;
+    }
+    return true;
+}
+
+template <bool SPLIT>
+__global__ void __launch_bounds__(128) k_sweep_flow(Dev D, SweepFlow F, double dt) {
+    const int lane = threadIdx.x & 31;
+    const int tagF = F.sync[0] + 1, tagB = tagF + 1;
+    int task = 0;
+    if (lane == 0) task = atomicAdd(F.sync + 1, 1);
+    task = __shfl_sync(0xffffffffu, task, 0);
+    while (task < F.ntasks) {
+        const bool stop =
+            (*reinterpret_cast<const volatile unsigned*>(&D.ctl->err) & SLD_FLAG_WAIT) != 0;
+        if (__any_sync(0xffffffffu, stop)) break;
+        // the warp's next task, taken now so that the atomic's round trip
+        // overlaps this task (tasks stay in order per warp, so the earliest
+        // unfinished task can still always proceed)
+        int next = 0;
+        if (lane == 0) next = atomicAdd(F.sync + 1, 1);
+        const int4 tk = __ldg(F.tasks + task);   // backward, first, count, group
+        const bool bwd = tk.x != 0;
+        const int c = lane < tk.z ? __ldg(F.gcells + tk.y + lane) : -1;
+        bool ok = c < 0 || flow_wait(D, F, c, tk.w, bwd, tagF, tagB);
+        if (!__all_sync(0xffffffffu, ok)) {
+            if (lane == 0) atomicOr(&D.ctl->err, SLD_FLAG_WAIT);
+            break;
+        }
+        if (c >= 0) {
+            __threadfence();                  // the flags above before the spins below
+            cell_walk<SPLIT, true>(D, c, dt, bwd ? 1 : 0);
+            __threadfence();                  // this cell's spins before its flag
+            atomicExch(F.cell_flag + c, bwd ? tagB : tagF);
+        }
+        task = __shfl_sync(0xffffffffu, next, 0);
+    }
+}
+
+// after a flow launch: the next call's tags, and the task counter back to 0
+__global__ void k_flow_next(SweepFlow F) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        F.sync[0] += 2;
+        F.sync[1] = 0;
+    }
+}
+
+static int g_flow_blocks[2] = {0, 0};
+
+void launch_sweep_flow(const Dev& D, cudaStream_t st, const SweepFlow& F, double dt) {
+    const int k = D.split ? 1 : 0;
+    if (D.split)
+        k_sweep_flow<true><<<g_flow_blocks[k], 128, 0, st>>>(D, F, dt);
+    else
+        k_sweep_flow<false><<<g_flow_blocks[k], 128, 0, st>>>(D, F, dt);
+    k_flow_next<<<1, 32, 0, st>>>(F);
+}
+
 static size_t sweep_smem() { return sizeof(SweepShared); }
 static int g_sweep_mode = 2;   // 0: two-level (shared memory), 1: one thread per cell,
-                               // 2: one thread per cell, pipelined
+                               // 2: one thread per cell, pipelined; one launch per group
+                               // 3: the pipelined walk, scheduled by data flow
 
 void sweep_init() {
     cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem());
     const char* v = getenv("SLD_SWEEP_MODE");
-    if (v && v[0] >= '0' && v[0] <= '2') g_sweep_mode = v[0] - '0';
+    if (v && v[0] >= '0' && v[0] <= '3') g_sweep_mode = v[0] - '0';
+    int dev = 0, sms = 0, b0 = 0, b1 = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_sweep_flow<false>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_sweep_flow<true>, 128, 0);
+    g_flow_blocks[0] = (b0 > 0 ? b0 : 1) * sms;
+    g_flow_blocks[1] = (b1 > 0 ? b1 : 1) * sms;
 }
+
+bool sweep_uses_flow() { return g_sweep_mode == 3; }
 
 void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g, double dt,
                   bool backward) {
     if (ncell_g <= 0) return;
     const int b = backward ? 1 : 0;
-    if (g_sweep_mode == 2) {
+    if (g_sweep_mode >= 2) {
         if (D.split)
             k_sweep_pipe<true><<<div_up(ncell_g, 128), 128, 0, st>>>(D, gcells, ncell_g, dt, b);
         else

@@ -39,6 +39,7 @@ struct sld_ctx {
     Dev D{};
     std::vector<void*> allocs;
     int* d_gcells = nullptr;
+    SweepFlow flow{};                  // data-flow schedule of the spin sweeps
     int* d_te_gcells = nullptr;
     int* d_te_gstart = nullptr;
     unsigned char* d_te_color = nullptr;
@@ -99,6 +100,7 @@ int check_flags(sld_ctx* c) {
     if (err & SLD_FLAG_CAPACITY) return SLD_ERR_CAPACITY;
     if (err & SLD_FLAG_TABLE) return SLD_ERR_TABLE;
     if (err & SLD_FLAG_NAN) return SLD_ERR_NAN;
+    if (err & SLD_FLAG_WAIT) return SLD_ERR_TIMEOUT;
     return SLD_OK;
 }
 
@@ -116,6 +118,11 @@ void enqueue_ds(sld_ctx* c, const Dev& D, double dt, int& eoff) {
     const auto& G = c->G;
     double dt_half = dt / 2e0;
     if (c->P.spinlang) launch_spin_noise(D, c->st, eoff, dt_half);
+    if (sweep_uses_flow()) {
+        launch_sweep_flow(D, c->st, c->flow, dt_half);
+        if (c->P.spinlang) eoff += 2;
+        return;
+    }
     for (int g = 0; g < G.ngroups; ++g)
         launch_sweep(D, c->st, c->d_gcells + G.gstart[g], G.gstart[g + 1] - G.gstart[g],
                      dt_half, false);
@@ -210,6 +217,7 @@ const char* sld_error_string(int code) {
     case SLD_ERR_IO: return "file could not be read";
     case SLD_ERR_STATE: return "call out of order";
     case SLD_ERR_NOMEM: return "device allocation failed";
+    case SLD_ERR_TIMEOUT: return "a bounded device-side wait ran out (spin-sweep schedule)";
     default: return "unknown error";
     }
 }
@@ -389,6 +397,31 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
                 col[G.te_gcells[m]] = (unsigned char)g;
         cudaMemcpy(c->d_te_color, col.data(), nte, cudaMemcpyHostToDevice);
         D.te_color = c->d_te_color;
+    }
+    {
+        // spin-sweep tasks: at most 32 cells of one colour group each, forward
+        // groups 0..G-1 then backward G-1..0 (core_ds_CPU.cpp:35-83)
+        std::vector<int4> tasks;
+        for (int pass = 0; pass < 2; ++pass)
+            for (int k = 0; k < G.ngroups; ++k) {
+                const int g = pass == 0 ? k : G.ngroups - 1 - k;
+                for (int m = G.gstart[g]; m < G.gstart[g + 1]; m += 32)
+                    tasks.push_back(make_int4(pass, m, std::min(32, G.gstart[g + 1] - m), g));
+            }
+        std::vector<unsigned char> grp(G.ncells, 0);
+        for (int g = 0; g < G.ngroups; ++g)
+            for (int m = G.gstart[g]; m < G.gstart[g + 1]; ++m) grp[G.gcells[m]] = (unsigned char)g;
+        int4* d_tasks = nullptr;
+        unsigned char* d_grp = nullptr;
+        ok = c->alloc(&d_tasks, tasks.size()) == 0 && c->alloc(&d_grp, (size_t)G.ncells) == 0 &&
+             c->alloc(&c->flow.cell_flag, (size_t)G.ncells) == 0 && c->alloc(&c->flow.sync, 2) == 0;
+        if (!ok) { sld_destroy(c); return SLD_ERR_NOMEM; }
+        cudaMemcpy(d_tasks, tasks.data(), sizeof(int4) * tasks.size(), cudaMemcpyHostToDevice);
+        cudaMemcpy(d_grp, grp.data(), (size_t)G.ncells, cudaMemcpyHostToDevice);
+        c->flow.tasks = d_tasks;
+        c->flow.ntasks = (int)tasks.size();
+        c->flow.gcells = c->d_gcells;
+        c->flow.cell_group = d_grp;
     }
     D.te_gcells = c->d_te_gcells;
     D.te_gstart = c->d_te_gstart;

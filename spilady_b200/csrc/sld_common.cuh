@@ -26,6 +26,7 @@
 #define SLD_FLAG_CAPACITY 1u
 #define SLD_FLAG_TABLE 2u
 #define SLD_FLAG_NAN 4u
+#define SLD_FLAG_WAIT 8u         // a bounded device-side wait ran out
 
 struct Ctl {
     unsigned long long epoch;     // Philox counter: one per noise-drawing sweep
@@ -261,6 +262,31 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 
 static inline int div_up(long a, long b) { return (int)((a + b - 1) / b); }
 
+// One exchange term of H = sum_j J s_j and sum_j J |s_j|, with every product
+// and sum rounded on its own (no fused multiply-add): the FP64 form then adds
+// exactly as the reference's separate multiply and add do, and every kernel
+// that sums the same list gets the same bits whatever its control flow (the
+// compiler fuses a multiply into an add only within one basic block).
+__device__ __forceinline__ void exch_add64(double& hx, double& hy, double& hz, double& hj,
+                                           double J, const double4& s) {
+    hx = __dadd_rn(hx, __dmul_rn(J, s.x));
+    hy = __dadd_rn(hy, __dmul_rn(J, s.y));
+    hz = __dadd_rn(hz, __dmul_rn(J, s.z));
+    hj = __dadd_rn(hj, __dmul_rn(J, s.w));
+}
+// the same in FP32 with Kahan compensation (split form)
+__device__ __forceinline__ void exch_add32(float ks[4], float kc[4], float J, const float4& s) {
+    const float w[4] = {__fmul_rn(J, s.x), __fmul_rn(J, s.y), __fmul_rn(J, s.z),
+                        __fmul_rn(J, s.w)};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        float y = __fsub_rn(w[q], kc[q]);
+        float t = __fadd_rn(ks[q], y);
+        kc[q] = __fsub_rn(__fsub_rn(t, ks[q]), y);
+        ks[q] = t;
+    }
+}
+
 // Exchange field of atom i from its J list: H = sum J_ij s_j and
 // sumJ = sum J_ij |s_j| in list order.  The list is read in batches of 8
 // (indices and J first, then the 8 spins) so that a batch costs two memory
@@ -299,19 +325,11 @@ __device__ __forceinline__ void exchange_field(const Dev& D, int i, double3& H, 
             }
             if (!D.split) {
                 double J = Jv[u];
-                hx += J * sj[u].x; hy += J * sj[u].y; hz += J * sj[u].z;
-                hj += J * sj[u].w;
+                exch_add64(hx, hy, hz, hj, J, sj[u]);
             } else {
-                float J = (float)Jv[u];
-                float v[4] = {J * (float)sj[u].x, J * (float)sj[u].y, J * (float)sj[u].z,
-                              J * (float)sj[u].w};
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    float y = v[q] - kc[q];
-                    float t = ks[q] + y;
-                    kc[q] = (t - ks[q]) - y;
-                    ks[q] = t;
-                }
+                exch_add32(ks, kc, (float)Jv[u],
+                           make_float4((float)sj[u].x, (float)sj[u].y, (float)sj[u].z,
+                                       (float)sj[u].w));
             }
         }
     }
@@ -338,6 +356,17 @@ void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g,
                   bool backward);
 void launch_spin_noise(const Dev& D, cudaStream_t st, int epoch_off, double dt);
 void launch_spin32(const Dev& D, cudaStream_t st);
+// data-flow schedule of both sweeps of one core_ds call (k_spin.cu)
+struct SweepFlow {
+    const int4* tasks;                // (backward, first, count, group), sweep order
+    int ntasks;
+    const int* gcells;                // cells by colour group
+    const unsigned char* cell_group;  // colour group of each link cell
+    int* cell_flag;                   // tag of each cell's last finished sweep
+    int* sync;                        // [0] tag base of the next call, [1] next task
+};
+bool sweep_uses_flow();
+void launch_sweep_flow(const Dev& D, cudaStream_t st, const SweepFlow& F, double dt);
 void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off);
 void launch_dr(const Dev& D, cudaStream_t st, double dt);
 void launch_temperature(const Dev& D, cudaStream_t st);

@@ -238,3 +238,62 @@ def test_split_form_electron_mesh_runs_and_tracks_fp64():
     for n in ("s", "p", "Te"):
         err = relerr(b.get(n), a.get(n))
         assert err <= SPLIT_TOL, f"{n}: {err:.3e}"
+
+
+# ------------------------------------------------------ sweep schedules
+def _run_with_sweep_mode(mode, monkeypatch, precision):
+    monkeypatch.setenv("SLD_SWEEP_MODE", str(mode))
+    eng = engine_mod()
+    params, r, p, s = initial_state(8, seed=15, tilt=0.3, temperature=600.0)
+    e = eng.Engine(params, r, p, s, spinlang=True, lattlang=True, localcolmot=True,
+                   precision=precision)
+    e.run(3)
+    e.core_ds(params["step"] / 2)
+    e.sync()
+    out = {n: e.get(n) for n in ("s", "H", "HL", "sumJ", "p", "r")}
+    e.close()
+    return out
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_sweep_schedules_give_identical_bits(monkeypatch, precision):
+    # one launch per colour group with the pipelined walk (2) and the
+    # data-flow schedule of the same walk (3) visit the cells in orders the
+    # reference's dependencies cannot tell apart: bit for bit the same.  The
+    # plain walk (1) is separate code: the same bits in the split form, whose
+    # sums are rounded step by step; in FP64 the compiler may fuse a
+    # different product of a two-product sum in its integrator (last bit).
+    ref = _run_with_sweep_mode(3, monkeypatch, precision)
+    got = _run_with_sweep_mode(2, monkeypatch, precision)
+    for n, a in ref.items():
+        assert np.array_equal(got[n], a), f"mode 2 {n}"
+    got = _run_with_sweep_mode(1, monkeypatch, precision)
+    for n, a in ref.items():
+        if precision == 1:
+            assert np.array_equal(got[n], a), f"mode 1 {n}"
+        else:
+            assert relerr(got[n], a) <= 1e-14, f"mode 1 {n}: {relerr(got[n], a):.2e}"
+
+
+# ------------------------------------------------------ core_dTe kernels
+@pytest.mark.parametrize("mode", [2, 1, 0])
+@pytest.mark.parametrize("precision", [0, 2])
+def test_core_dte_kernels_and_forms(monkeypatch, mode, precision):
+    # hub (2), cluster (1) and one-CTA (0) kernels, with the reference's
+    # heat-capacity expressions (FP64 form) and with the fitted ones (the
+    # split form's, here in its FP64 twin): one core_dTe and one full step
+    monkeypatch.setenv("SLD_DTE_MODE", str(mode))
+    from spilady_b200.lattice import hot_spot_te
+    sw = dict(spinlang=True, lattlang=True, eltemp=True, localcolmot=True, renormalize=True,
+              te_mesh=4)
+    params, r, p, s = initial_state(8, seed=16, tilt=0.35)
+    te = hot_spot_te(4, params["box"][0], peak=3000.0, background=300.0, sigma=6.0)
+    o = orc.System(params, r, p, s, te=te, rng=orc.RNG_PHILOX, **sw)
+    e = engine_mod().Engine(params, r, p, s, te=te, precision=precision, **sw)
+    o.core_dTe(5e-16)
+    e.core_dTe(5e-16)
+    compare(o, e, ["Te", "Ee"], TOL1, f"core_dTe mode {mode}")
+    if precision == 0:
+        o.run(1)
+        e.run(1)
+        compare(o, e, ATOM + ["Te", "Tl"], 1e-10, f"step, dTe mode {mode}")
