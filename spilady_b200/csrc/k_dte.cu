@@ -5,7 +5,7 @@
 //   C  C dTe/dt = kappa Laplacian Te    (colour sweep forward and back over
 //      the cells, then the total Ee rescaled to its value before the sweep)
 // Three kernels, by mesh size:
-//   k_dte_hub      meshes up to kHubMaxCells: a 4-CTA cluster, the sweep on
+//   k_dte_hub      meshes up to kHubMaxCells: an 8-CTA cluster, the sweep on
 //                  one CTA's shared memory, with the colour lists and a
 //                  neighbour table there too (the default);
 //   k_dte_cluster  any mesh: the cells spread over a cluster, Te in global
@@ -237,8 +237,8 @@ __global__ void __launch_bounds__(256) k_dte_cluster(Dev D, double dt) {
 }
 
 // ---------------------------------------------------------------------
-#define HUB_CL 4
-// Cluster "hub" form: every CTA of a 4-CTA cluster does the cell-local A and
+#define HUB_CL 8
+// Cluster "hub" form: every CTA of an 8-CTA cluster does the cell-local A and
 // B parts for its share of the cells in parallel; CTA 0 holds all Te and
 // Te_to_Ee(Te) in its shared memory (the others read and write them through
 // distributed shared memory) and runs C's colour phases with block barriers.
@@ -246,13 +246,19 @@ __global__ void __launch_bounds__(256) k_dte_cluster(Dev D, double dt) {
 //   - Each CTA keeps its cells' coupling source Gel Tl + Ges Ts_L and rate
 //     (Gel + Ges) h/2/boltz in its own shared memory: they do not change
 //     during core_dTe, so the substeps read no global memory.
-//   - In a colour phase, half of the hub's threads update the Te of the
-//     phase's cells (the chain the next phase waits for) while the other
-//     half evaluate Te_to_Ee for the cells of the previous phase, which no
-//     cell of this phase reads.  The one exception is the last forward
-//     colour, updated again right away by the backward pass: its Te_to_Ee is
-//     evaluated in place.  Every value is the one of the plain sequence.
-static const int kHubMaxCells = 6400;    // 8 (2 n + 2 + 2 n / 4) + 16 n bytes of shared memory
+//   - The hub also keeps the colour lists and a table of each cell's six
+//     neighbours in its shared memory.
+//   - Reference expressions: in a colour phase, half of the hub's threads
+//     update the Te of the phase's cells (the chain the next phase waits for)
+//     while the other half evaluate Te_to_Ee for the cells of the previous
+//     phase, which no cell of this phase reads.  The one exception is the
+//     last forward colour, updated again right away by the backward pass:
+//     its Te_to_Ee is evaluated in place.  Every value is the one of the
+//     plain sequence.
+//   - Fitted expressions: an update keeps the energy it converts to Te (what
+//     Te_to_Ee would return, up to rounding), so the sweep evaluates no
+//     Te_to_Ee at all.
+static const int kHubMaxCells = 6400;    // 8 (2 n + 2 + 2 n / 8) + 16 n bytes of shared memory
 
 template <bool FAST>
 __global__ void __launch_bounds__(1024) k_dte_hub(Dev D, double dt, int per) {
@@ -306,37 +312,60 @@ __global__ void __launch_bounds__(1024) k_dte_hub(Dev D, double dt, int per) {
             if (threadIdx.x == 0) tot = t;
             __syncthreads();
             double start = tot;
-            const int G = D.te_ngroups, half = blockDim.x / 2;
-            const bool worker = threadIdx.x < half;
-            const int lane = worker ? threadIdx.x : threadIdx.x - half;
-            int pb = 0, pe = 0;   // cells of the previous phase whose Te_to_Ee is due
-            for (int p = 0; p < 2 * G; ++p) {
-                const int g = p < G ? p : 2 * G - 1 - p;
-                const int b = D.te_gstart[g], e = D.te_gstart[g + 1];
-                if (worker) {
-                    for (int m = b + lane; m < e; m += half) {
+            const int G = D.te_ngroups;
+            if constexpr (FAST) {
+                // the fitted form keeps the energy each update converts, the
+                // value Te_to_Ee(Te) returns up to rounding, so no thread
+                // evaluates Te_to_Ee during the sweep
+                for (int p = 0; p < 2 * G; ++p) {
+                    const int g = p < G ? p : 2 * G - 1 - p;
+                    const int b = D.te_gstart[g], e = D.te_gstart[g + 1];
+                    for (int m = b + threadIdx.x; m < e; m += blockDim.x) {
                         int k = sGc[m];
                         const unsigned short* q = sNb + 6 * k;
                         const double* sT = hsm;
                         double T = sT[k];
-                        T = te_T<FAST>(hsm[n + k] + te_lap<FAST>(gm, T, sT[q[0]], sT[q[1]], sT[q[2]],
-                                                                 sT[q[3]], sT[q[4]], sT[q[5]]));
-                        hsm[k] = T;
-                        if (p == G - 1) hsm[n + k] = te_E<FAST>(T);
+                        double x = hsm[n + k] + te_lap<FAST>(gm, T, sT[q[0]], sT[q[1]], sT[q[2]],
+                                                             sT[q[3]], sT[q[4]], sT[q[5]]);
+                        hsm[k] = te_T<FAST>(x);
+                        hsm[n + k] = x;
                     }
-                } else {
-                    for (int m = pb + lane; m < pe; m += half) {
-                        int k = sGc[m];
-                        hsm[n + k] = te_E<FAST>(hsm[k]);
-                    }
+                    __syncthreads();
                 }
-                __syncthreads();
-                pb = p == G - 1 ? 0 : b;
-                pe = p == G - 1 ? 0 : e;
-            }
-            for (int m = pb + threadIdx.x; m < pe; m += blockDim.x) {
-                int k = sGc[m];
-                hsm[n + k] = te_E<FAST>(hsm[k]);
+            } else {
+                const int half = blockDim.x / 2;
+                const bool worker = threadIdx.x < half;
+                const int lane = worker ? threadIdx.x : threadIdx.x - half;
+                int pb = 0, pe = 0;   // cells of the previous phase whose Te_to_Ee is due
+                for (int p = 0; p < 2 * G; ++p) {
+                    const int g = p < G ? p : 2 * G - 1 - p;
+                    const int b = D.te_gstart[g], e = D.te_gstart[g + 1];
+                    if (worker) {
+                        for (int m = b + lane; m < e; m += half) {
+                            int k = sGc[m];
+                            const unsigned short* q = sNb + 6 * k;
+                            const double* sT = hsm;
+                            double T = sT[k];
+                            T = te_T<FAST>(hsm[n + k] + te_lap<FAST>(gm, T, sT[q[0]], sT[q[1]],
+                                                                     sT[q[2]], sT[q[3]], sT[q[4]],
+                                                                     sT[q[5]]));
+                            hsm[k] = T;
+                            if (p == G - 1) hsm[n + k] = te_E<FAST>(T);
+                        }
+                    } else {
+                        for (int m = pb + lane; m < pe; m += half) {
+                            int k = sGc[m];
+                            hsm[n + k] = te_E<FAST>(hsm[k]);
+                        }
+                    }
+                    __syncthreads();
+                    pb = p == G - 1 ? 0 : b;
+                    pe = p == G - 1 ? 0 : e;
+                }
+                for (int m = pb + threadIdx.x; m < pe; m += blockDim.x) {
+                    int k = sGc[m];
+                    hsm[n + k] = te_E<FAST>(hsm[k]);
+                }
             }
             __syncthreads();
             acc = 0.0;
