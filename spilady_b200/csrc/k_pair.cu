@@ -27,83 +27,106 @@ __device__ __forceinline__ double3 pair_d(const Dev& D, double4 ri, int pk) {
 }
 
 // MODE 0: FP64 tables (the reference's arithmetic); 1: split form (FP32
-// analytic); 2: the analytic forms in FP64
+// analytic); 2: the analytic forms in FP64.
+//
+// Two passes per atom.  The first walks the 27 cells and only tests the
+// cutoff, writing the accepted neighbours to the atom's list in traversal
+// order; the second walks that list and does the per-pair work (density,
+// exchange list).  In one pass, some lane of a warp accepts almost every
+// candidate (about 26 of 162 pass), so the whole per-pair body would run,
+// divergent, for nearly every candidate of every lane.  The second pass
+// recomputes each accepted pair vector with the same arithmetic, so the
+// results are those of a single pass.
+template <int MODE>
+__device__ __forceinline__ bool pair_accept(const Dev& D, double3 d) {
+    if constexpr (MODE == 1) {
+        float dx = (float)d.x, dy = (float)d.y, dz = (float)d.z;
+        return dx * dx + dy * dy + dz * dz < (float)D.rcut_max_sq;
+    } else {
+        return d.x * d.x + d.y * d.y + d.z * d.z < D.rcut_max_sq;
+    }
+}
+
 template <int MODE>
 __device__ void pairs_one(const Dev& D, int i, int write_rho) {
     constexpr bool SPLIT = MODE == 1;
     unsigned* err = &D.ctl->err;
     const int N = D.natom;
-    double4 ri = D.r[i];
+    const double4 ri = D.r[i];
     int c0 = D.cell_of[i], cx, cy, cz;
     cell_xyz(D, c0, cx, cy, cz);
-    double rho = 0.0;
-    Kahan rho32;
-    const float rmax2f = (float)D.rcut_max_sq, rmag2f = (float)D.rcut_mag_sq;
-    const float rpotf = (float)D.rcut_pot;
-    int nn = 0, nj = 0;
+    // pass 1: the cutoff test in the reference's traversal order
+    int nn = 0;
     for (int k = 0; k < 27; ++k) {
         bool wrap = false;
         int c = k == 26 ? c0 : nbr_cell_w(D, cx, cy, cz, k, wrap);
         int st = D.cell_start[c], n = D.cell_count[c];
         for (int m = 0; m < n; ++m) {
-          {
             int j = D.cell_atoms[st + m];
             if (j == i) continue;
             double4 rj = D.r[j];
             double3 d = make_double3(ri.x - rj.x, ri.y - rj.y, ri.z - rj.z);
             if (wrap) d = find_image(D, d);
-            if constexpr (!SPLIT) {
-                double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
-                if (rsq >= D.rcut_max_sq) continue;
-                if (nn < SLD_MAXNB) D.nbr[(size_t)nn * N + i] = j | (wrap ? SLD_WRAP : 0);
-                ++nn;
-                double r0 = sqrt(rsq);
-                if (r0 < D.rcut_pot) {
-                    if constexpr (MODE == 0) {
-                        rho += interp(D.tf, r0, D.inv_r, err);
-                    } else {
-                        double f, df;
-                        dens64(D, r0, f, df);
-                        rho += f;
-                    }
-                }
-                if (rsq < D.rcut_mag_sq) {
-                    if (nj < SLD_MAXJ) {
-                        D.jl[(size_t)i * SLD_MAXJ + nj] = j;
-                        double J, dJ;
-                        if constexpr (MODE == 0) J = interp(D.tJ, r0, D.inv_r, err);
-                        else exch64(r0, J, dJ);
-                        D.jv[(size_t)i * SLD_MAXJ + nj] = J;
-                    }
-                    ++nj;
-                }
-            } else {
-                float dx = (float)d.x, dy = (float)d.y, dz = (float)d.z;
-                float rsq = dx * dx + dy * dy + dz * dz;
-                if (rsq >= rmax2f) continue;
-                if (nn < SLD_MAXNB) D.nbr[(size_t)nn * N + i] = j | (wrap ? SLD_WRAP : 0);
-                ++nn;
-                double r64 = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
-                float f, df;
-                if ((float)r64 < rpotf) {
-                    dens32r(D, r64, f, df);
-                    rho32.add(f);
-                }
-                if (rsq < rmag2f) {
-                    if (nj < SLD_MAXJ) {
-                        float J, dJ;
-                        exch32r(r64, J, dJ);
-                        D.jl[(size_t)i * SLD_MAXJ + nj] = j;
-                        D.jvf[(size_t)i * SLD_MAXJ + nj] = J;
-                    }
-                    ++nj;
+            if (!pair_accept<MODE>(D, d)) continue;
+            if (nn < SLD_MAXNB) D.nbr[(size_t)nn * N + i] = j | (wrap ? SLD_WRAP : 0);
+            ++nn;
+        }
+    }
+    const int nl = nn < SLD_MAXNB ? nn : SLD_MAXNB;
+    // pass 2: density and exchange list over the accepted pairs
+    double rho = 0.0;
+    Kahan rho32;
+    const float rmag2f = (float)D.rcut_mag_sq;
+    const float rpotf = (float)D.rcut_pot;
+    int nj = 0;
+    for (int e = 0; e < nl; ++e) {
+        const int pk = D.nbr[(size_t)e * N + i];
+        const int j = pk & SLD_JMASK;
+        double3 d = pair_d(D, ri, pk);
+        if constexpr (!SPLIT) {
+            double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
+            double r0 = sqrt(rsq);
+            if (r0 < D.rcut_pot) {
+                if constexpr (MODE == 0) {
+                    rho += interp(D.tf, r0, D.inv_r, err);
+                } else {
+                    double f, df;
+                    dens64(D, r0, f, df);
+                    rho += f;
                 }
             }
-          }
+            if (rsq < D.rcut_mag_sq) {
+                if (nj < SLD_MAXJ) {
+                    D.jl[(size_t)i * SLD_MAXJ + nj] = j;
+                    double J, dJ;
+                    if constexpr (MODE == 0) J = interp(D.tJ, r0, D.inv_r, err);
+                    else exch64(r0, J, dJ);
+                    D.jv[(size_t)i * SLD_MAXJ + nj] = J;
+                }
+                ++nj;
+            }
+        } else {
+            float dx = (float)d.x, dy = (float)d.y, dz = (float)d.z;
+            float rsq = dx * dx + dy * dy + dz * dz;
+            double r64 = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
+            float f, df;
+            if ((float)r64 < rpotf) {
+                dens32r(D, r64, f, df);
+                rho32.add(f);
+            }
+            if (rsq < rmag2f) {
+                if (nj < SLD_MAXJ) {
+                    float J, dJ;
+                    exch32r(r64, J, dJ);
+                    D.jl[(size_t)i * SLD_MAXJ + nj] = j;
+                    D.jvf[(size_t)i * SLD_MAXJ + nj] = J;
+                }
+                ++nj;
+            }
         }
     }
     if (nn > SLD_MAXNB || nj > SLD_MAXJ) atomicOr(err, SLD_FLAG_CAPACITY);
-    D.nbr_n[i] = nn < SLD_MAXNB ? nn : SLD_MAXNB;
+    D.nbr_n[i] = nl;
     D.jl_n[i] = nj < SLD_MAXJ ? nj : SLD_MAXJ;
     if (write_rho) D.rho[i] = SPLIT ? rho32.value() : rho;
 }
