@@ -179,6 +179,7 @@ __global__ void __launch_bounds__(256) k_dr(Dev D, double dt) {
     double3 x = periodic(D, make_double3(r.x + k * p.x, r.y + k * p.y, r.z + k * p.z));
     if (!isfinite(x.x + x.y + x.z)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
     D.r[i] = make_double4(x.x, x.y, x.z, 0.0);
+    D.r32s[D.cell_slot[i]] = make_float4((float)x.x, (float)x.y, (float)x.z, 0.f);
 }
 
 void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off) {

@@ -117,7 +117,8 @@ __global__ void k_scatter(Dev D) {
     D.cell_atoms[pos] = i;
 }
 
-// Order each cell's members by descending stamp (head first).
+// Order each cell's members by descending stamp (head first), then record
+// each member's slot and its FP32 position in slot order.
 __global__ void k_cellsort(Dev D) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= D.ncells) return;
@@ -133,6 +134,12 @@ __global__ void k_cellsort(Dev D) {
             --m;
         }
         a[m + 1] = v;
+    }
+    for (int k = 0; k < n; ++k) {
+        int i = a[k];
+        D.cell_slot[i] = st + k;
+        double4 r = D.r[i];
+        D.r32s[st + k] = make_float4((float)r.x, (float)r.y, (float)r.z, 0.f);
     }
 }
 

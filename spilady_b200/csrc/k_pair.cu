@@ -29,14 +29,25 @@ __device__ __forceinline__ double3 pair_d(const Dev& D, double4 ri, int pk) {
 // MODE 0: FP64 tables (the reference's arithmetic); 1: split form (FP32
 // analytic); 2: the analytic forms in FP64.
 //
-// Two passes per atom.  The first walks the 27 cells and only tests the
-// cutoff, writing the accepted neighbours to the atom's list in traversal
-// order; the second walks that list and does the per-pair work (density,
-// exchange list).  In one pass, some lane of a warp accepts almost every
-// candidate (about 26 of 162 pass), so the whole per-pair body would run,
-// divergent, for nearly every candidate of every lane.  The second pass
-// recomputes each accepted pair vector with the same arithmetic, so the
-// results are those of a single pass.
+// Two passes per atom.  The first walks the 27 cells with a loose cutoff
+// test in FP32 on the cell-ordered FP32 positions (one contiguous 16-byte
+// load and a few FP32 operations per candidate; a neighbour cell across the
+// box is shifted by its box vector), writing the slots that pass to the
+// atom's list in traversal order.  The second walks that list, applies the
+// reference's exact test (FP64 pair vector with find_image), compacts the
+// list in place to the atom indices that pass, and does the per-pair work
+// (density, exchange list).  The lists and sums are those of one exact pass.
+// In one pass, some lane of a warp accepts almost every candidate (about 26
+// of 162 pass), so the per-pair body would run, divergent, for nearly every
+// candidate of every lane.
+//
+// The loose test keeps every pair the exact one keeps: with coordinates
+// below B in magnitude, each FP32 rounding moves a coordinate by at most
+// e = ulp(B)/2; a pair-vector component collects four of them (two
+// positions, the difference, the box shift), so r^2 near the cutoff moves by
+// at most 2 r_max (4 sqrt(3) e) + (4 sqrt(3) e)^2 plus the FP32 rounding of
+// the sum.  D.pair_loose, set on the host from the box, is twice that.
+
 template <int MODE>
 __device__ __forceinline__ bool pair_accept(const Dev& D, double3 d) {
     if constexpr (MODE == 1) {
@@ -55,20 +66,40 @@ __device__ void pairs_one(const Dev& D, int i, int write_rho) {
     const double4 ri = D.r[i];
     int c0 = D.cell_of[i], cx, cy, cz;
     cell_xyz(D, c0, cx, cy, cz);
-    // pass 1: the cutoff test in the reference's traversal order
+    // pass 1: loose cutoff test in the reference's traversal order
     int nn = 0;
+    const int myslot = D.cell_slot[i];
+    const float rx = (float)ri.x, ry = (float)ri.y, rz = (float)ri.z;
+    const float cut = (float)D.rcut_max_sq + D.pair_loose;
+    const float ax = (float)D.d[0];
+    const float bx = (float)D.d[1], by = (float)D.d[2];
+    const float qx = (float)D.d[3], qy = (float)D.d[4], qz = (float)D.d[5];
     for (int k = 0; k < 27; ++k) {
-        bool wrap = false;
-        int c = k == 26 ? c0 : nbr_cell_w(D, cx, cy, cz, k, wrap);
-        int st = D.cell_start[c], n = D.cell_count[c];
+        int sx = 0, sy = 0, sz = 0;
+        const int c = k == 26 ? c0 : nbr_cell_s(D, cx, cy, cz, k, sx, sy, sz);
+        const bool wrap = D.small_grid || (sx | sy | sz) != 0;
+        // image of the neighbour cell: its atoms + sx a + sy b + sz c
+        const float hx = sx * ax + sy * bx + sz * qx;
+        const float hy = sy * by + sz * qy;
+        const float hz = sz * qz;
+        const int st = D.cell_start[c], n = D.cell_count[c];
         for (int m = 0; m < n; ++m) {
-            int j = D.cell_atoms[st + m];
-            if (j == i) continue;
-            double4 rj = D.r[j];
-            double3 d = make_double3(ri.x - rj.x, ri.y - rj.y, ri.z - rj.z);
-            if (wrap) d = find_image(D, d);
-            if (!pair_accept<MODE>(D, d)) continue;
-            if (nn < SLD_MAXNB) D.nbr[(size_t)nn * N + i] = j | (wrap ? SLD_WRAP : 0);
+            const int slot = st + m;
+            if (slot == myslot) continue;
+            bool take;
+            if (!D.small_grid) {
+                const float4 q = __ldg(D.r32s + slot);
+                const float dx = (rx - q.x) - hx, dy = (ry - q.y) - hy, dz = (rz - q.z) - hz;
+                take = dx * dx + dy * dy + dz * dz < cut;
+            } else {
+                // three cells along an axis: the image is the reference's
+                // minimum image of each pair
+                const double4 rj = D.r[D.cell_atoms[slot]];
+                take = pair_accept<MODE>(
+                    D, find_image(D, make_double3(ri.x - rj.x, ri.y - rj.y, ri.z - rj.z)));
+            }
+            if (!take) continue;
+            if (nn < SLD_MAXNB) D.nbr[(size_t)nn * N + i] = slot | (wrap ? SLD_WRAP : 0);
             ++nn;
         }
     }
@@ -78,11 +109,15 @@ __device__ void pairs_one(const Dev& D, int i, int write_rho) {
     Kahan rho32;
     const float rmag2f = (float)D.rcut_mag_sq;
     const float rpotf = (float)D.rcut_pot;
-    int nj = 0;
+    int nj = 0, w = 0;
     for (int e = 0; e < nl; ++e) {
-        const int pk = D.nbr[(size_t)e * N + i];
-        const int j = pk & SLD_JMASK;
+        const int ps = D.nbr[(size_t)e * N + i];
+        const int j = D.cell_atoms[ps & SLD_JMASK];
+        const int pk = j | (ps & SLD_WRAP);
         double3 d = pair_d(D, ri, pk);
+        if (!pair_accept<MODE>(D, d)) continue;
+        D.nbr[(size_t)w * N + i] = pk;
+        ++w;
         if constexpr (!SPLIT) {
             double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
             double r0 = sqrt(rsq);
@@ -126,7 +161,7 @@ __device__ void pairs_one(const Dev& D, int i, int write_rho) {
         }
     }
     if (nn > SLD_MAXNB || nj > SLD_MAXJ) atomicOr(err, SLD_FLAG_CAPACITY);
-    D.nbr_n[i] = nl;
+    D.nbr_n[i] = w;
     D.jl_n[i] = nj < SLD_MAXJ ? nj : SLD_MAXJ;
     if (write_rho) D.rho[i] = SPLIT ? rho32.value() : rho;
 }

@@ -292,6 +292,17 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     D.rcut_pot_sq = prm->rcut_pot * prm->rcut_pot;
     D.rcut_mag_sq = prm->rcut_mag * prm->rcut_mag;
     D.rcut_max_sq = G.rcut_max * G.rcut_max;
+    {
+        // FP32 pair pre-test margin (k_pair.cu): coordinates stay below B
+        double B = 0.0;
+        for (int k = 0; k < 6; ++k) B += std::fabs(G.d[k]);
+        B *= 2.0;
+        const double e = std::ldexp(1.0, std::ilogb(B) - 23);   // ulp(B) / 2 in FP32
+        const double dl = 4.0 * std::sqrt(3.0) * e;
+        const double rm = G.rcut_max + dl;
+        const double bound = 2.0 * rm * dl + dl * dl + 4.0 * std::ldexp(rm * rm, -23);
+        D.pair_loose = (float)(2.0 * bound);
+    }
     D.atmass = prm->atmass * kUtoeV * (1e-10 * 1e-10);
     D.temperature = prm->temperature * kBoltz;
     D.gamma_L = prm->gamma_L_over_mass * D.atmass;
@@ -350,6 +361,7 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
          c->alloc(&D.dF, n) == 0;
     if (prm->spinlang) ok = ok && c->alloc(&D.xi, 6 * n) == 0;
     if (prm->precision == SLD_SPLIT) ok = ok && c->alloc(&D.s32, n) == 0;
+    ok = ok && c->alloc(&D.r32s, n) == 0 && c->alloc(&D.cell_slot, n) == 0;
     {
         float* cub = nullptr;
         double* cub64 = nullptr;

@@ -75,6 +75,10 @@ struct Dev {
     double4 *r, *p, *f, *s, *H, *HL;
     float4* s32;                  // split form: s rounded to FP32, written with s by every
                                   // spin writer; the FP32 exchange sums gather it
+    float4* r32s;                 // positions rounded to FP32 in cell-list order (slot
+                                  // order), written by links and by every drift
+    int* cell_slot;               // index of each atom in cell_atoms (its slot)
+    float pair_loose;             // margin of the FP32 pair pre-test (A^2), k_pair.cu
     double *rho, *pe, *ke, *me, *me0, *vir, *sumJ, *stress;
     int *cell_of, *id, *node;
     long long* stamp;
@@ -160,6 +164,19 @@ __device__ __forceinline__ int nbr_cell_w(const Dev& D, int cx, int cy, int cz, 
     x = x < 0 ? x + D.nx : (x >= D.nx ? x - D.nx : x);
     y = y < 0 ? y + D.ny : (y >= D.ny ? y - D.ny : y);
     z = z < 0 ? z + D.nz : (z >= D.nz ? z - D.nz : z);
+    return x + (y + z * D.ny) * D.nx;
+}
+// the same, with the periodic image of the neighbour cell: s* = -1 / +1 when
+// it lies across the low / high face of the box along that axis
+__device__ __forceinline__ int nbr_cell_s(const Dev& D, int cx, int cy, int cz, int k, int& sx,
+                                          int& sy, int& sz) {
+    int x = cx + kNbr[k][0], y = cy + kNbr[k][1], z = cz + kNbr[k][2];
+    sx = x < 0 ? -1 : (x >= D.nx ? 1 : 0);
+    sy = y < 0 ? -1 : (y >= D.ny ? 1 : 0);
+    sz = z < 0 ? -1 : (z >= D.nz ? 1 : 0);
+    x -= sx * D.nx;
+    y -= sy * D.ny;
+    z -= sz * D.nz;
     return x + (y + z * D.ny) * D.nx;
 }
 __device__ __forceinline__ void cell_xyz(const Dev& D, int c, int& cx, int& cy, int& cz) {
