@@ -186,6 +186,23 @@ void enqueue_step(sld_ctx* c) {
     launch_advance(Dn, M, eoff, 1);
 }
 
+// The cells of a colour group are independent, so their order within the
+// group is free.  A thread walks one cell, and a warp takes as long as its
+// fullest cell: ordering each group by atom count (taken now, after the
+// initial links) gives the 32 cells of a warp about the same walk.
+int order_groups_by_count(sld_ctx* c) {
+    auto& G = c->G;
+    std::vector<int> cnt(G.ncells);
+    if (cudaMemcpy(cnt.data(), c->D.cell_count, sizeof(int) * G.ncells, cudaMemcpyDeviceToHost))
+        return SLD_ERR_CUDA;
+    for (int g = 0; g < G.ngroups; ++g)
+        std::stable_sort(G.gcells.begin() + G.gstart[g], G.gcells.begin() + G.gstart[g + 1],
+                         [&](int a, int b) { return cnt[a] > cnt[b]; });
+    if (cudaMemcpy(c->d_gcells, G.gcells.data(), sizeof(int) * G.ncells, cudaMemcpyHostToDevice))
+        return SLD_ERR_CUDA;
+    return SLD_OK;
+}
+
 int validate(const sld_params* p) {
     if (!p) return SLD_ERR_ARG;
     if (!(p->box[0] > 0 && p->box[2] > 0 && p->box[5] > 0)) return SLD_ERR_ARG;
@@ -491,7 +508,9 @@ int sld_set_state(sld_ctx* c, const double* r, const double* p, const double* s)
     }
     int rc = launch_status();
     if (rc) return rc;
-    return check_flags(c);
+    rc = check_flags(c);
+    if (rc) return rc;
+    return order_groups_by_count(c);
 }
 
 void sld_destroy(sld_ctx* c) {
