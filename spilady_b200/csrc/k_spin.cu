@@ -55,22 +55,21 @@ __device__ __forceinline__ void visit_store(const Dev& D, int i, double3 s, doub
     }
 }
 
-// The noise increments of both sweeps of one core_ds call, drawn for every
-// atom in one parallel pass before the sweeps (the draw is counter-based, so
-// it does not depend on when it is made, and the temperature does not change
-// during core_ds); the sweeps' serial chains only read them.  Stored atom
-// major: [natom][sweep][3], dS = sqrt(2 T gamma_S_HL / dt) xi.
+// The visit records of both sweeps of one core_ds call, made for every atom
+// in one parallel pass before the sweeps: rho (which the sweeps do not
+// change) and the noise increment dS = sqrt(2 T gamma_S_HL / dt) xi (the
+// draw is counter-based, so it does not depend on when it is made, and the
+// temperature does not change during core_ds).  A visit then reads one
+// 32-byte record; the sweeps' serial chains only read them.
 __global__ void __launch_bounds__(256) k_spin_noise(Dev D, int epoch_off, double dt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= D.natom) return;
     unsigned long long e0 = D.ctl->epoch + (unsigned long long)epoch_off;
     double T = D.eltemp ? D.Te[D.node[i]] : D.temperature;
+    const double rho = D.rho[i];
     for (int v = 0; v < 2; ++v) {
         double3 x = spin_noise_dS(D, T, normals3(D.seed, 0u, (unsigned)D.id[i], e0 + v), dt);
-        double* o = D.xi + 6 * (size_t)i + 3 * v;
-        o[0] = x.x;
-        o[1] = x.y;
-        o[2] = x.z;
+        D.vrec[2 * (size_t)i + v] = make_double4(rho, x.x, x.y, x.z);
     }
 }
 
@@ -90,9 +89,8 @@ void launch_spin32(const Dev& D, cudaStream_t st) {
     k_spin32<<<div_up(D.natom, 256), 256, 0, st>>>(D);
 }
 
-__device__ __forceinline__ double3 spin_noise_at(const Dev& D, int i, int sweep) {
-    const double* x = D.xi + 6 * (size_t)i + 3 * sweep;
-    return make_double3(x[0], x[1], x[2]);
+__device__ __forceinline__ double4 visit_record(const Dev& D, int i, int sweep) {
+    return D.vrec[2 * (size_t)i + sweep];
 }
 
 // one visit entirely from global memory (the fallback path)
@@ -104,8 +102,9 @@ __device__ void visit_global(const Dev& D, int i, double dt, bool fields) {
     double rho = 0.0;
     double3 dS = make_double3(0.0, 0.0, 0.0);
     if (D.spinlang) {
-        rho = D.rho[i];
-        dS = spin_noise_at(D, i, fields ? 1 : 0);
+        const double4 q = visit_record(D, i, fields ? 1 : 0);
+        rho = q.x;
+        dS = make_double3(q.y, q.z, q.w);
     }
     double3 HL;
     double3 s = spin_integrate_dS(D, make_double3(s4.x, s4.y, s4.z), H, sumJ, rho, dS, dt, HL);
@@ -175,9 +174,9 @@ __global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restri
             S.inn[a] = (unsigned char)(nin < SW_MAXIN ? nin : SW_MAXIN);
             if (nin > SW_MAXIN) S.overflow = 1;
             if (D.spinlang) {
-                double3 dS = spin_noise_at(D, i, fields ? 1 : 0);
-                S.aux[a][0] = D.rho[i];
-                S.aux[a][1] = dS.x; S.aux[a][2] = dS.y; S.aux[a][3] = dS.z;
+                const double4 q = visit_record(D, i, fields ? 1 : 0);
+                S.aux[a][0] = q.x;
+                S.aux[a][1] = q.y; S.aux[a][2] = q.z; S.aux[a][3] = q.w;
             }
         }
         __syncthreads();
@@ -362,9 +361,10 @@ __device__ __forceinline__ void visit_fetch(const Dev& D, const RowIdx& r, int s
     }
     v.si = ld_spin<CG>(D.s + i);
     if (D.spinlang) {
-        v.rho = __ldg(D.rho + i);
-        const double* x = D.xi + 6 * (size_t)i + 3 * sweep;
-        v.dS = make_double3(__ldg(x), __ldg(x + 1), __ldg(x + 2));
+        const double2* q = reinterpret_cast<const double2*>(D.vrec + 2 * (size_t)i + sweep);
+        const double2 q0 = __ldg(q), q1 = __ldg(q + 1);
+        v.rho = q0.x;
+        v.dS = make_double3(q0.y, q1.x, q1.y);
     } else {
         v.rho = 0.0;
         v.dS = make_double3(0.0, 0.0, 0.0);
@@ -382,10 +382,8 @@ __device__ __forceinline__ void visit_field(const Dev& D, const VisitRegs<SPLIT>
     auto add64 = [&](double J, double4 s) { exch_add64(hx, hy, hz, hj, J, s); };
 #pragma unroll
     for (int u = 0; u < SC_PJ; ++u) {
-        if (u < v.nj) {
-            if constexpr (SPLIT) add32(v.J[u], v.sj[u]);
-            else add64(v.J[u], v.sj[u]);
-        }
+        if constexpr (SPLIT) exch_add32_if(u < v.nj, ks, kc, v.J[u], v.sj[u]);
+        else exch_add64_if(u < v.nj, hx, hy, hz, hj, v.J[u], v.sj[u]);
     }
     for (int e = SC_PJ; e < v.nj; ++e) {
         const size_t at = (size_t)v.i * SLD_MAXJ + e;

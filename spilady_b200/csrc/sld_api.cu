@@ -376,7 +376,7 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
          c->alloc(&c->jl_set[1], (size_t)SLD_MAXJ * n) == 0 &&
          c->alloc(&c->jln_set[0], n) == 0 && c->alloc(&c->jln_set[1], n) == 0 &&
          c->alloc(&D.dF, n) == 0;
-    if (prm->spinlang) ok = ok && c->alloc(&D.xi, 6 * n) == 0;
+    if (prm->spinlang) ok = ok && c->alloc(&D.vrec, 2 * n) == 0;
     if (prm->precision == SLD_SPLIT) ok = ok && c->alloc(&D.s32, n) == 0;
     ok = ok && c->alloc(&D.r32s, n) == 0 && c->alloc(&D.cell_slot, n) == 0;
     {

@@ -101,7 +101,8 @@ struct Dev {
     double* jv;                   // FP64 form
     float* jvf;                   // split form
     double* dF;                   // F'(rho) per atom, refreshed after each rho pass
-    double* xi;                   // [natom][2 sweeps][3] spin-noise normals of one core_ds
+    double4* vrec;                // [natom][2 sweeps] visit records of one core_ds: rho and
+                                  // the noise increment dS of the atom's visit in that sweep
     // control and reduction scratch
     Ctl* ctl;
     double* red;                  // partial sums
@@ -312,6 +313,34 @@ __device__ __forceinline__ void exch_add32(float ks[4], float kc[4], float J, co
 // on_skip(j, J)).  FP64 form: FP64 products and sums; split form: FP32
 // products with compensated FP32 sums.
 #define SLD_GB 8
+// The same terms taken only when `on`: computed unconditionally and kept by
+// selects, so an unrolled sum over a fixed number of slots needs no branch
+// per slot (the kept values are those of the plain sum).
+__device__ __forceinline__ void exch_add64_if(bool on, double& hx, double& hy, double& hz,
+                                              double& hj, double J, const double4& s) {
+    const double ax = __dadd_rn(hx, __dmul_rn(J, s.x));
+    const double ay = __dadd_rn(hy, __dmul_rn(J, s.y));
+    const double az = __dadd_rn(hz, __dmul_rn(J, s.z));
+    const double aj = __dadd_rn(hj, __dmul_rn(J, s.w));
+    hx = on ? ax : hx;
+    hy = on ? ay : hy;
+    hz = on ? az : hz;
+    hj = on ? aj : hj;
+}
+__device__ __forceinline__ void exch_add32_if(bool on, float ks[4], float kc[4], float J,
+                                              const float4& s) {
+    const float w[4] = {__fmul_rn(J, s.x), __fmul_rn(J, s.y), __fmul_rn(J, s.z),
+                        __fmul_rn(J, s.w)};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float y = __fsub_rn(w[q], kc[q]);
+        const float t = __fadd_rn(ks[q], y);
+        const float c = __fsub_rn(__fsub_rn(t, ks[q]), y);
+        ks[q] = on ? t : ks[q];
+        kc[q] = on ? c : kc[q];
+    }
+}
+
 template <class Skip, class OnSkip>
 __device__ __forceinline__ void exchange_field(const Dev& D, int i, double3& H, double& sumJ,
                                                Skip skip, OnSkip on_skip) {
