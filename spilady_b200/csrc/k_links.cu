@@ -17,34 +17,52 @@ __global__ void k_zero_counts(Dev D) {
     if (D.te_mesh > 0 && c < D.nte) D.te_count[c] = 0;
 }
 
+// atomicAdd(&a[key], 1) for every lane with key >= 0, one atomic per
+// distinct key of the warp (the leader adds the count of its peers): the
+// atoms of a warp mostly share a few link cells and one Te node.  Returns
+// this lane's rank among its peers.  All 32 lanes must call it.
+__device__ __forceinline__ int warp_count_add(int* a, int key, int* base_out) {
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (key >= 0 && lane == leader) base = atomicAdd(a + key, __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (base_out) *base_out = base;
+    return __popc(peers & ((1u << lane) - 1u));
+}
+
 __global__ void k_bin(Dev D, int initial) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= D.natom) return;
-    double4 r = D.r[i];
-    double3 q = to_frac(D, r.x, r.y, r.z);
-    int lx = (int)(q.x * D.nx), ly = (int)(q.y * D.ny), lz = (int)(q.z * D.nz);
-    lx = lx < 0 ? 0 : (lx >= D.nx ? D.nx - 1 : lx);
-    ly = ly < 0 ? 0 : (ly >= D.ny ? D.ny - 1 : ly);
-    lz = lz < 0 ? 0 : (lz >= D.nz ? D.nz - 1 : lz);
-    int c = lx + (ly + lz * D.ny) * D.nx;
-    int id = D.id[i];
-    if (initial) {
-        D.stamp[i] = (long long)id;
-    } else if (c != D.cell_of[i]) {
-        long long L = D.ctl->links_calls + 1;
-        D.stamp[i] = (L << 32) | (long long)id;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < D.natom;
+    int c = -1, k = -1;
+    if (valid) {
+        double4 r = D.r[i];
+        double3 q = to_frac(D, r.x, r.y, r.z);
+        int lx = (int)(q.x * D.nx), ly = (int)(q.y * D.ny), lz = (int)(q.z * D.nz);
+        lx = lx < 0 ? 0 : (lx >= D.nx ? D.nx - 1 : lx);
+        ly = ly < 0 ? 0 : (ly >= D.ny ? D.ny - 1 : ly);
+        lz = lz < 0 ? 0 : (lz >= D.nz ? D.nz - 1 : lz);
+        c = lx + (ly + lz * D.ny) * D.nx;
+        int id = D.id[i];
+        if (initial) {
+            D.stamp[i] = (long long)id;
+        } else if (c != D.cell_of[i]) {
+            long long L = D.ctl->links_calls + 1;
+            D.stamp[i] = (L << 32) | (long long)id;
+        }
+        D.cell_of[i] = c;
+        if (D.te_mesh > 0) {
+            int a = (int)(q.x * D.tx), b = (int)(q.y * D.ty), e = (int)(q.z * D.tz);
+            a = a < 0 ? 0 : (a >= D.tx ? D.tx - 1 : a);
+            b = b < 0 ? 0 : (b >= D.ty ? D.ty - 1 : b);
+            e = e < 0 ? 0 : (e >= D.tz ? D.tz - 1 : e);
+            k = a + (b + e * D.ty) * D.tx;
+            D.node[i] = k;
+        }
     }
-    D.cell_of[i] = c;
-    atomicAdd(&D.cell_count[c], 1);
-    if (D.te_mesh > 0) {
-        int a = (int)(q.x * D.tx), b = (int)(q.y * D.ty), e = (int)(q.z * D.tz);
-        a = a < 0 ? 0 : (a >= D.tx ? D.tx - 1 : a);
-        b = b < 0 ? 0 : (b >= D.ty ? D.ty - 1 : b);
-        e = e < 0 ? 0 : (e >= D.tz ? D.tz - 1 : e);
-        int k = a + (b + e * D.ty) * D.tx;
-        D.node[i] = k;
-        atomicAdd(&D.te_count[k], 1);
-    }
+    warp_count_add(D.cell_count, c, nullptr);
+    if (D.te_mesh > 0) warp_count_add(D.te_count, k, nullptr);
 }
 
 // inclusive warp scan
@@ -110,11 +128,11 @@ __global__ void __launch_bounds__(1024) k_scan3(Dev D) {
 }
 
 __global__ void k_scatter(Dev D) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= D.natom) return;
-    int c = D.cell_of[i];
-    int pos = D.cell_start[c] + atomicAdd(&D.cell_fill[c], 1);
-    D.cell_atoms[pos] = i;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = i < D.natom ? D.cell_of[i] : -1;
+    int base = 0;
+    const int rank = warp_count_add(D.cell_fill, c, &base);
+    if (c >= 0) D.cell_atoms[D.cell_start[c] + base + rank] = i;
 }
 
 // Order each cell's members by descending stamp (head first), then record

@@ -506,8 +506,8 @@ __global__ void __launch_bounds__(128) k_force32(Dev D) {
             pe.add(0.5f * phi);
         }
         if ((PART & PART_MAG) && r0 < rmag) {
-            double4 sj4 = D.s[j];
-            float tx = (float)sj4.x, ty = (float)sj4.y, tz = (float)sj4.z;
+            const float4 sj4 = D.s32[j];   // (float) of the spin
+            float tx = sj4.x, ty = sj4.y, tz = sj4.z;
             float sj_sq = tx * tx + ty * ty + tz * tz;
             float dot = sx * tx + sy * ty + sz * tz;
             float times = sqrtf(si_sqf * sj_sq);

@@ -358,24 +358,34 @@ __device__ __forceinline__ void exchange_field(const Dev& D, int i, double3& H, 
             Jv[u] = e < nj ? (D.split ? (double)D.jvf[at] : D.jv[at])
                            : 0.0;
         }
-        double4 sj[SLD_GB];
+        if (!D.split) {
+            double4 sj[SLD_GB];
 #pragma unroll
-        for (int u = 0; u < SLD_GB; ++u)
-            sj[u] = jj[u] >= 0 ? D.s[jj[u]] : make_double4(0, 0, 0, 0);
+            for (int u = 0; u < SLD_GB; ++u)
+                sj[u] = jj[u] >= 0 ? D.s[jj[u]] : make_double4(0, 0, 0, 0);
 #pragma unroll
-        for (int u = 0; u < SLD_GB; ++u) {
-            if (jj[u] < 0) continue;
-            if (skip(jj[u])) {
-                on_skip(jj[u], Jv[u]);
-                continue;
+            for (int u = 0; u < SLD_GB; ++u) {
+                if (jj[u] < 0) continue;
+                if (skip(jj[u])) {
+                    on_skip(jj[u], Jv[u]);
+                    continue;
+                }
+                exch_add64(hx, hy, hz, hj, Jv[u], sj[u]);
             }
-            if (!D.split) {
-                double J = Jv[u];
-                exch_add64(hx, hy, hz, hj, J, sj[u]);
-            } else {
-                exch_add32(ks, kc, (float)Jv[u],
-                           make_float4((float)sj[u].x, (float)sj[u].y, (float)sj[u].z,
-                                       (float)sj[u].w));
+        } else {
+            // the FP32 copy of the spins: the values the FP32 sums use
+            float4 sj[SLD_GB];
+#pragma unroll
+            for (int u = 0; u < SLD_GB; ++u)
+                sj[u] = jj[u] >= 0 ? D.s32[jj[u]] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int u = 0; u < SLD_GB; ++u) {
+                if (jj[u] < 0) continue;
+                if (skip(jj[u])) {
+                    on_skip(jj[u], Jv[u]);
+                    continue;
+                }
+                exch_add32(ks, kc, (float)Jv[u], sj[u]);
             }
         }
     }
