@@ -35,14 +35,23 @@ sys.path.insert(0, ROOT)
 
 METRIC = "atom-steps/s, 4.19M-atom bcc Fe SLD: split-FP32 vs plain FP64 on one B200"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
-# compulsory HBM bytes per atom for each phase of one step (FP64 form):
-# each atom's own state read/written once per pass, neighbour data reused on
-# chip.  links 28, core_ds (4 visits of r, s, rho in and s out) 320,
-# core_dp (2 kicks incl. rescale) 240, core_dr 72, rho 32, force 80.
-ALGO_BYTES = {"links": 28, "core_ds": 320, "core_dp": 240, "core_dr": 72,
-              "calculate_rho": 32, "calculate_force_energy": 80,
-              "calculate_temperature": 80, "check_energy": 32, "core_dTe": 0,
+# Algorithmic HBM bytes per atom and step for each phase: each atom's own data
+# and list rows read or written once, neighbour data (spins, positions) reused
+# on chip or in L2.  core_ds: a visit reads its spin (32 B) and writes it
+# (32 B + the 16 B FP32 copy), reads its exchange row (14 pairs x 8 B) and its
+# visit record (32 B) = 224 B; backward visits also write H, HL, sum J (72 B);
+# 4 visits per step, 2 backward, plus the visit records (64 B, twice) = 1168.
+ALGO_BYTES = {"links": 70, "calculate_rho": 264, "calculate_force_energy": 290,
+              "core_ds": 1168, "core_dp": 340, "core_dr": 112,
+              "calculate_temperature": 290, "check_energy": 32, "core_dTe": 0,
               "bookkeeping": 0}
+# DRAM bytes per atom and step of core_ds from an ncu capture (bcc Fe 64^3
+# cells, split form, cold caches as ncu replays them): one sweep launch of
+# 10,648 cells (65,536 visits) read 33.32 MB and wrote 0.03 MB (508 B per
+# visit); the visit-record pass read 8.41 MB for 524,288 atoms (16 B per atom).
+CORE_DS_TRAFFIC_PER_ATOM = 4 * 508.4 + 2 * 16.0
+ROOFLINE_KERNEL = {"core_ds": "k_sweep_pipe + k_spin_noise (core_ds: 72 sweep launches "
+                              "and 2 visit-record passes per step)"}
 
 
 def parse():
@@ -238,17 +247,26 @@ def main():
 
     # per-phase device time (CUDA events on the engine's stream), a few steps
     prof = {}
-    nprof = 1 if args.small else 3
+    nprof = 1 if args.small else 5
     for _ in range(nprof):
         for k, v in e.profile_step().items():
             prof[k] = prof.get(k, 0.0) + v / nprof
     dom = max(prof, key=prof.get)
     peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
     hbm = peaks.get("hbm_gbs", 6650.0)
-    achieved = ALGO_BYTES.get(dom, 0) * natom / (prof[dom] / 1e3) / 1e9 if prof[dom] > 0 else 0.0
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
-                "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
-                "peak_source": "measured" if peaks else "fallback",
+    step_s = prof[dom] / 1e3
+    achieved = ALGO_BYTES.get(dom, 0) * natom / step_s / 1e9 if prof[dom] > 0 else 0.0
+    traffic = CORE_DS_TRAFFIC_PER_ATOM * natom if dom == "core_ds" else None
+    roofline = {"bound": "hbm", "kernel": ROOFLINE_KERNEL.get(dom, dom), "achieved": achieved,
+                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": traffic,
+                "per": "one step of the phase (algorithmic bytes and traffic per step)",
+                "algorithmic_bytes": ALGO_BYTES.get(dom, 0) * natom,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at 64^3, "
+                                  "scaled per visit" if traffic else None,
+                "peak_source": "measured (burst copy)" if peaks else "fallback",
+                "timing": f"CUDA events around each phase on the engine stream, {nprof} "
+                          "sequential steps after the timed region",
                 "phase_ms": {k: round(v, 4) for k, v in prof.items()}}
 
     # end to end through the public API with host buffers: upload the state,
