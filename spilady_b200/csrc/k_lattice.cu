@@ -201,3 +201,48 @@ void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off) {
 void launch_dr(const Dev& D, cudaStream_t st, double dt) {
     k_dr<<<div_up(D.natom, 256), 256, 0, st>>>(D, dt);
 }
+
+// sld_set_state on the device: the caller's r, p, s ([atom][3], caller order)
+// to slot order, with the periodic wrap (periodic_CPU.cpp:31-50), |s| and the
+// kinetic energy.  Products and sums are rounded one by one in the order the
+// host expressions evaluate them, so the values are those of a plain C++ loop.
+__device__ __forceinline__ double add3_rn(double a, double b, double c) {
+    return __dadd_rn(__dadd_rn(a, b), c);
+}
+
+__global__ void __launch_bounds__(256) k_load_state(Dev D, const double* __restrict__ r,
+                                                    const double* __restrict__ p,
+                                                    const double* __restrict__ s) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= D.natom) return;
+    const size_t i = (size_t)D.id[k];
+    double x = r[3 * i], y = r[3 * i + 1], z = r[3 * i + 2];
+    const double* I = D.inv;
+    const double* d = D.d;
+    double qx = add3_rn(__dmul_rn(I[0], x), __dmul_rn(I[1], y), __dmul_rn(I[3], z));
+    double qy = __dadd_rn(__dmul_rn(I[2], y), __dmul_rn(I[4], z));
+    double qz = __dmul_rn(I[5], z);
+    int idx = 0;
+    if (qx < 0.0 || qx >= 1.0) { qx = __dsub_rn(qx, (double)(int)qx); ++idx; }
+    if (qy < 0.0 || qy >= 1.0) { qy = __dsub_rn(qy, (double)(int)qy); ++idx; }
+    if (qz < 0.0 || qz >= 1.0) { qz = __dsub_rn(qz, (double)(int)qz); ++idx; }
+    if (idx > 0) {
+        x = add3_rn(__dmul_rn(d[0], qx), __dmul_rn(d[1], qy), __dmul_rn(d[3], qz));
+        y = __dadd_rn(__dmul_rn(d[2], qy), __dmul_rn(d[4], qz));
+        z = __dmul_rn(d[5], qz);
+    }
+    D.r[k] = make_double4(x, y, z, 0.0);
+    const double px = p[3 * i], py = p[3 * i + 1], pz = p[3 * i + 2];
+    D.p[k] = make_double4(px, py, pz, 0.0);
+    const double sx = s[3 * i], sy = s[3 * i + 1], sz = s[3 * i + 2];
+    const double s0 = sqrt(add3_rn(__dmul_rn(sx, sx), __dmul_rn(sy, sy), __dmul_rn(sz, sz)));
+    D.s[k] = make_double4(sx, sy, sz, s0);
+    if (D.split) D.s32[k] = make_float4((float)sx, (float)sy, (float)sz, (float)s0);
+    D.ke[k] = __ddiv_rn(__ddiv_rn(add3_rn(__dmul_rn(px, px), __dmul_rn(py, py),
+                                          __dmul_rn(pz, pz)), 2.0), D.atmass);
+}
+
+void launch_load_state(const Dev& D, cudaStream_t st, const double* r, const double* p,
+                       const double* s) {
+    k_load_state<<<div_up(D.natom, 256), 256, 0, st>>>(D, r, p, s);
+}

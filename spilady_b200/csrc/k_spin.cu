@@ -77,18 +77,6 @@ void launch_spin_noise(const Dev& D, cudaStream_t st, int epoch_off, double dt) 
     k_spin_noise<<<div_up(D.natom, 256), 256, 0, st>>>(D, epoch_off, dt);
 }
 
-// s32 = (float)s for every atom, after the spins are loaded from the host
-__global__ void __launch_bounds__(256) k_spin32(Dev D) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= D.natom) return;
-    double4 s = D.s[i];
-    D.s32[i] = make_float4((float)s.x, (float)s.y, (float)s.z, (float)s.w);
-}
-
-void launch_spin32(const Dev& D, cudaStream_t st) {
-    k_spin32<<<div_up(D.natom, 256), 256, 0, st>>>(D);
-}
-
 __device__ __forceinline__ double4 visit_record(const Dev& D, int i, int sweep) {
     return D.vrec[2 * (size_t)i + sweep];
 }

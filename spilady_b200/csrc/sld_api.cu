@@ -62,6 +62,7 @@ struct sld_ctx {
     int scan_blocks = 1;
     int red_cap = 0;
     bool lists_stale = false;   // positions moved since the neighbour lists were built
+    bool groups_ordered = false;   // colour groups ordered by cell counts (first set_state)
 
     template <class T>
     int alloc(T** p, size_t n) {
@@ -188,8 +189,9 @@ void enqueue_step(sld_ctx* c) {
 
 // The cells of a colour group are independent, so their order within the
 // group is free.  A thread walks one cell, and a warp takes as long as its
-// fullest cell: ordering each group by atom count (taken now, after the
-// initial links) gives the 32 cells of a warp about the same walk.
+// fullest cell: ordering each group by atom count (taken after the links of
+// the context's first set_state) gives the 32 cells of a warp about the same
+// walk.  Counts change little over a run, and the order affects only speed.
 int order_groups_by_count(sld_ctx* c) {
     auto& G = c->G;
     std::vector<int> cnt(G.ncells);
@@ -475,26 +477,16 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
 int sld_set_state(sld_ctx* c, const double* r, const double* p, const double* s) {
     if (!c || !r || !p || !s) return SLD_ERR_ARG;
     Dev& D = c->D;
-    size_t n = (size_t)D.natom;
-    std::vector<double4> hr(n), hp(n), hs(n);
-    std::vector<double> hke(n);
-    double m = D.atmass;
-    for (size_t k = 0; k < n; ++k) {
-        int i = c->id_of_slot[k];
-        double x = r[3 * i], y = r[3 * i + 1], z = r[3 * i + 2];
-        sld::host_periodic(c->G, x, y, z);
-        hr[k] = make_double4(x, y, z, 0.0);
-        hp[k] = make_double4(p[3 * i], p[3 * i + 1], p[3 * i + 2], 0.0);
-        double sx = s[3 * i], sy = s[3 * i + 1], sz = s[3 * i + 2];
-        hs[k] = make_double4(sx, sy, sz, std::sqrt(sx * sx + sy * sy + sz * sz));
-        double px = p[3 * i], py = p[3 * i + 1], pz = p[3 * i + 2];
-        hke[k] = (px * px + py * py + pz * pz) / 2e0 / m;
-    }
-    CK(cudaMemcpyAsync(D.r, hr.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(D.p, hp.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(D.s, hs.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, c->st));
-    if (D.split) launch_spin32(D, c->st);
-    CK(cudaMemcpyAsync(D.ke, hke.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+    const size_t n = (size_t)D.natom;
+    // The caller's arrays go to the device as they are, into the neighbour
+    // list's memory (192 bytes per atom; the pair pass below rebuilds the
+    // list), and one kernel puts them in slot order with the periodic wrap,
+    // |s| and the kinetic energy.
+    double* raw = reinterpret_cast<double*>(D.nbr);
+    CK(cudaMemcpyAsync(raw, r, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(raw + 3 * n, p, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(raw + 6 * n, s, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->st));
+    launch_load_state(D, c->st, raw, raw + 3 * n, raw + 6 * n);
     Ctl z{};
     CK(cudaMemcpyAsync(D.ctl, &z, sizeof(Ctl), cudaMemcpyHostToDevice, c->st));
     // initialize(): links, rho, forces, cell temperatures, reference energy
@@ -510,6 +502,8 @@ int sld_set_state(sld_ctx* c, const double* r, const double* p, const double* s)
     if (rc) return rc;
     rc = check_flags(c);
     if (rc) return rc;
+    if (c->groups_ordered) return SLD_OK;
+    c->groups_ordered = true;
     return order_groups_by_count(c);
 }
 

@@ -411,7 +411,8 @@ void launch_force_mag(const Dev& D, cudaStream_t st);   // adds the magnetic ter
 void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g, double dt,
                   bool backward);
 void launch_spin_noise(const Dev& D, cudaStream_t st, int epoch_off, double dt);
-void launch_spin32(const Dev& D, cudaStream_t st);
+void launch_load_state(const Dev& D, cudaStream_t st, const double* r, const double* p,
+                       const double* s);
 // data-flow schedule of both sweeps of one core_ds call (k_spin.cu)
 struct SweepFlow {
     const int4* tasks;                // (backward, first, count, group), sweep order
