@@ -610,8 +610,12 @@ void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g,
     if (ncell_g <= 0) return;
     const int b = backward ? 1 : 0;
     if (g_sweep_mode >= 2) {
+        // Block sizes that fill the register file: the split form's kernel takes
+        // 212 registers a thread, 9 warps an SM, so blocks of 3 warps (128-thread
+        // blocks would leave one warp's registers idle); the FP64 form's 255
+        // registers allow 8 warps, 2 blocks of 4.
         if (D.split)
-            k_sweep_pipe<true><<<div_up(ncell_g, 128), 128, 0, st>>>(D, gcells, ncell_g, dt, b);
+            k_sweep_pipe<true><<<div_up(ncell_g, 96), 96, 0, st>>>(D, gcells, ncell_g, dt, b);
         else
             k_sweep_pipe<false><<<div_up(ncell_g, 128), 128, 0, st>>>(D, gcells, ncell_g, dt, b);
         return;
