@@ -253,12 +253,17 @@ __global__ void __launch_bounds__(128) k_sweep_cell(Dev D, const int* __restrict
 // field is summed in exchange-list order with exchange_field's arithmetic,
 // so the result is the one of k_sweep_cell.  The split form gathers the FP32
 // copy of the spins (16 bytes per neighbour, the values its FP32 sums use).
-#define SC_PJ 16
+// Exchange entries prefetched per visit.  In bcc Fe the exchange cutoff
+// (3.75 A) takes the 14 atoms of the first two shells (the third is at
+// 4.05 A); rare longer rows read their extra entries when used.  The row
+// indices are loaded 16 at a time (four 16-byte loads).
+#define SC_PJ 14
+#define SC_ROW 16
 
 // the exchange-list indices of one atom, as loaded (not yet masked by nj)
 struct RowIdx {
     int i, nj;
-    int4 w[SC_PJ / 4];
+    int4 w[SC_ROW / 4];
 };
 
 __device__ __forceinline__ void row_load(const Dev& D, int i, RowIdx& r) {
@@ -266,7 +271,7 @@ __device__ __forceinline__ void row_load(const Dev& D, int i, RowIdx& r) {
     r.nj = __ldg(D.jl_n + i);
     const int4* jl4 = reinterpret_cast<const int4*>(D.jl + (size_t)i * SLD_MAXJ);
 #pragma unroll
-    for (int q = 0; q < SC_PJ / 4; ++q) r.w[q] = __ldg(jl4 + q);
+    for (int q = 0; q < SC_ROW / 4; ++q) r.w[q] = __ldg(jl4 + q);
 }
 
 template <bool SPLIT>
@@ -319,19 +324,21 @@ __device__ __forceinline__ void visit_fetch(const Dev& D, const RowIdx& r, int s
     v.i = i;
     v.nj = nj;
 #pragma unroll
-    for (int q = 0; q < SC_PJ / 4; ++q) {
-        v.jj[4 * q + 0] = 4 * q + 0 < nj ? r.w[q].x : -1;
-        v.jj[4 * q + 1] = 4 * q + 1 < nj ? r.w[q].y : -1;
-        v.jj[4 * q + 2] = 4 * q + 2 < nj ? r.w[q].z : -1;
-        v.jj[4 * q + 3] = 4 * q + 3 < nj ? r.w[q].w : -1;
+    for (int u = 0; u < SC_PJ; ++u) {
+        const int4 w = r.w[u / 4];
+        const int x = (u & 3) == 0 ? w.x : (u & 3) == 1 ? w.y : (u & 3) == 2 ? w.z : w.w;
+        v.jj[u] = u < nj ? x : -1;
     }
     const size_t row = (size_t)i * SLD_MAXJ;
     if constexpr (SPLIT) {
         const float4* j4 = reinterpret_cast<const float4*>(D.jvf + row);
+        float4 jw[SC_ROW / 4];
 #pragma unroll
-        for (int q = 0; q < SC_PJ / 4; ++q) {
-            float4 w = __ldg(j4 + q);
-            v.J[4 * q + 0] = w.x; v.J[4 * q + 1] = w.y; v.J[4 * q + 2] = w.z; v.J[4 * q + 3] = w.w;
+        for (int q = 0; q < SC_ROW / 4; ++q) jw[q] = __ldg(j4 + q);
+#pragma unroll
+        for (int u = 0; u < SC_PJ; ++u) {
+            const float4 w = jw[u / 4];
+            v.J[u] = (u & 3) == 0 ? w.x : (u & 3) == 1 ? w.y : (u & 3) == 2 ? w.z : w.w;
         }
 #pragma unroll
         for (int u = 0; u < SC_PJ; ++u)
@@ -611,9 +618,10 @@ void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g,
     const int b = backward ? 1 : 0;
     if (g_sweep_mode >= 2) {
         // Block sizes that fill the register file: the split form's kernel takes
-        // 212 registers a thread, 9 warps an SM, so blocks of 3 warps (128-thread
-        // blocks would leave one warp's registers idle); the FP64 form's 255
-        // registers allow 8 warps, 2 blocks of 4.
+        // about 200 registers a thread, 9 warps an SM, so blocks of 3 warps
+        // (128-thread blocks would leave one warp's registers idle; holding it
+        // to 200 registers for a tenth warp measured slower); the FP64 form's
+        // 255 registers allow 8 warps, 2 blocks of 4.
         if (D.split)
             k_sweep_pipe<true><<<div_up(ncell_g, 96), 96, 0, st>>>(D, gcells, ncell_g, dt, b);
         else

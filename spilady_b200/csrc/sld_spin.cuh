@@ -41,22 +41,43 @@ __device__ __forceinline__ void sin_1mcos(double x, double& sn, double& omc) {
 // (w = -H/hbar is formed with one reciprocal and |w| with one reciprocal
 // square root: the reference divides each component, which differs in the
 // last bit at most)
-__device__ __forceinline__ double3 spin_rotation(double3 H, double3 s, double dt) {
+//
+// The rotation about -H/hbar by |w| dt depends only on H and dt, so its
+// coefficients are formed once (RotCoef) and applied to any spin (rot_apply);
+// the Langevin scheme's first and last parts share them.
+struct RotCoef {
+    double3 w;                      // unit axis
+    double A, B;                    // sin, 1 - cos of the angle
+    double w12, w23, w13, w1s, w2s, w3s;
+};
+
+__device__ __forceinline__ RotCoef rot_coef(double3 H, double dt) {
     const double k = -1.0 / SLD_HBAR;
+    RotCoef c;
     double3 w = make_double3(H.x * k, H.y * k, H.z * k);
     double w2 = w.x * w.x + w.y * w.y + w.z * w.z;
     double iw = w2 > 0.0 ? rsqrt(w2) : 0.0;
     double w0 = w2 * iw;
     w = make_double3(w.x * iw, w.y * iw, w.z * iw);
-    double w12 = w.x * w.y, w23 = w.y * w.z, w13 = w.x * w.z;
-    double w1s = w.x * w.x, w2s = w.y * w.y, w3s = w.z * w.z;
-    double A, B;
-    sin_1mcos(w0 * dt, A, B);
+    c.w = w;
+    c.w12 = w.x * w.y; c.w23 = w.y * w.z; c.w13 = w.x * w.z;
+    c.w1s = w.x * w.x; c.w2s = w.y * w.y; c.w3s = w.z * w.z;
+    sin_1mcos(w0 * dt, c.A, c.B);
+    return c;
+}
+
+__device__ __forceinline__ double3 rot_apply(const RotCoef& c, double3 s) {
+    const double3 w = c.w;
+    const double A = c.A, B = c.B;
     double3 o;
-    o.x = s.x + (s.x * B * (-w2s - w3s) + s.y * (B * w12 - A * w.z) + s.z * (A * w.y + B * w13));
-    o.y = s.y + (s.y * B * (-w1s - w3s) + s.z * (B * w23 - A * w.x) + s.x * (A * w.z + B * w12));
-    o.z = s.z + (s.z * B * (-w1s - w2s) + s.x * (B * w13 - A * w.y) + s.y * (A * w.x + B * w23));
+    o.x = s.x + (s.x * B * (-c.w2s - c.w3s) + s.y * (B * c.w12 - A * w.z) + s.z * (A * w.y + B * c.w13));
+    o.y = s.y + (s.y * B * (-c.w1s - c.w3s) + s.z * (B * c.w23 - A * w.x) + s.x * (A * w.z + B * c.w12));
+    o.z = s.z + (s.z * B * (-c.w1s - c.w2s) + s.x * (B * c.w13 - A * w.y) + s.y * (A * w.x + B * c.w23));
     return o;
+}
+
+__device__ __forceinline__ double3 spin_rotation(double3 H, double3 s, double dt) {
+    return rot_apply(rot_coef(H, dt), s);
 }
 
 // Landau field plus the exchange correction (calculate_spin_CPU.cpp:127-136)
@@ -84,7 +105,8 @@ __device__ __forceinline__ double3 spin_integrate_dS(const Dev& D, double3 s, do
     double dt_half = dt / 2.0, dt_quad = dt / 4.0, g = D.gamma_S_HL;
     double L[4];
     for (int k = 0; k < 4; ++k) L[k] = interp_const(D.landau[k], rho, D.inv_rho);
-    s = spin_rotation(H, s, dt_half);                                   // part 1
+    const RotCoef rc = rot_coef(H, dt_half);
+    s = rot_apply(rc, s);                                               // part 1
     HL = landau_field(L, sumJ, s);                                      // part 2
     double a = g * dt_quad;
     double3 t = make_double3(s.x + a * (H.x + HL.x), s.y + a * (H.y + HL.y), s.z + a * (H.z + HL.z));
@@ -98,7 +120,7 @@ __device__ __forceinline__ double3 spin_integrate_dS(const Dev& D, double3 s, do
     HL = landau_field(L, sumJ, t);
     a = g * dt_half;
     s = make_double3(s.x + a * (H.x + HL.x), s.y + a * (H.y + HL.y), s.z + a * (H.z + HL.z));
-    return spin_rotation(H, s, dt_half);                                // part 5
+    return rot_apply(rc, s);                                            // part 5
 }
 
 // The noise increment of one visit at temperature T (eV): the normals xi
