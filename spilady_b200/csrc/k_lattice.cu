@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(128) k_dp_lang(Dev D, double dt, int epoch_off
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     double px = 0, py = 0, pz = 0;
     if (c < D.ncells) {
-        int n = D.cell_count[c];
+        int n = cell_n(D, c);
         const int* a = D.cell_atoms + D.cell_start[c];
         if (n > 0) {
             unsigned long long epoch = D.ctl->epoch + (unsigned long long)epoch_off;

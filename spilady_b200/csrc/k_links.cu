@@ -140,8 +140,9 @@ __global__ void k_scatter(Dev D) {
 __global__ void k_cellsort(Dev D) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= D.ncells) return;
-    int st = D.cell_start[c], n = D.cell_count[c];
-    if (n > SLD_MAXC) atomicOr(&D.ctl->err, SLD_FLAG_CAPACITY);
+    int st = D.cell_start[c];
+    if (D.cell_count[c] > SLD_MAXC) atomicOr(&D.ctl->err, SLD_FLAG_CAPACITY);
+    const int n = cell_n(D, c);
     int* a = D.cell_atoms + st;
     for (int k = 1; k < n; ++k) {
         int v = a[k];

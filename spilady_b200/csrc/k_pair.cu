@@ -82,7 +82,7 @@ __device__ void pairs_one(const Dev& D, int i, int write_rho) {
         const float hx = sx * ax + sy * bx + sz * qx;
         const float hy = sy * by + sz * qy;
         const float hz = sz * qz;
-        const int st = D.cell_start[c], n = D.cell_count[c];
+        const int st = D.cell_start[c], n = cell_n(D, c);
         for (int m = 0; m < n; ++m) {
             const int slot = st + m;
             if (slot == myslot) continue;
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(PW_WARPS * 32) k_pairs_warp(Dev D, int write_r
     bool wr = false;
     if (lane < 27) {
         nc = lane == 26 ? c : nbr_cell_w(D, cx, cy, cz, lane, wr);
-        cnt = D.cell_count[nc];
+        cnt = cell_n(D, nc);
         st = D.cell_start[nc];
     }
     int inc = cnt;

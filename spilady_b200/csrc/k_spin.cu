@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restri
         int lane = threadIdx.x, n = 0, st = 0, c = -1;
         if (lane < ncb) {
             c = gcells[cbeg + lane];
-            n = D.cell_count[c];
+            n = cell_n(D, c);
             st = D.cell_start[c];
         }
         int inc = n;
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(128) k_sweep_cell(Dev D, const int* __restrict
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ncell_g) return;
     int c = gcells[t];
-    int st = D.cell_start[c], n = D.cell_count[c];
+    int st = D.cell_start[c], n = cell_n(D, c);
     bool fields = backward != 0;
     for (int m = 0; m < n; ++m) {
         int i = D.cell_atoms[st + (backward ? n - 1 - m : m)];
@@ -400,7 +400,7 @@ __device__ __forceinline__ void visit_field(const Dev& D, const VisitRegs<SPLIT>
 template <bool SPLIT, bool CG>
 __device__ __forceinline__ void cell_walk(const Dev& D, int c, double dt, int backward) {
     constexpr bool kDeep = SPLIT;   // indices two visits ahead
-    const int n = D.cell_count[c];
+    const int n = cell_n(D, c);
     if (n <= 0) return;
     const int* ca = D.cell_atoms + D.cell_start[c];
     const bool fields = backward != 0;   // the backward sweep is each atom's last visit

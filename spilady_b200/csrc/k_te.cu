@@ -71,7 +71,7 @@ __device__ __forceinline__ void temp_finish(const Dev& D, int k, double n, doubl
 __global__ void __launch_bounds__(128) k_temp_cell(Dev D) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= D.ncells) return;
-    int st = D.cell_start[c], n = D.cell_count[c];
+    int st = D.cell_start[c], n = cell_n(D, c);
     double ke = 0, ax = 0, ay = 0, az = 0, Rup = 0, Rdn = 0, Lup = 0, Ldn = 0;
     for (int m = 0; m < n; ++m) {
         int i = D.cell_atoms[st + m];

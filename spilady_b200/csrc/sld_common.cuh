@@ -180,6 +180,16 @@ __device__ __forceinline__ int nbr_cell_s(const Dev& D, int cx, int cy, int cz, 
     z -= sz * D.nz;
     return x + (y + z * D.ny) * D.nx;
 }
+// The atoms of link cell c that a kernel walks: at most SLD_MAXC.  A fuller
+// cell (a system that has blown up, or an input far outside the reference's
+// densities) has set SLD_FLAG_CAPACITY in links, so the step is reported as
+// failed; the bound keeps every per-cell walk short in the meantime instead of
+// letting one thread walk millions of atoms.
+__device__ __forceinline__ int cell_n(const Dev& D, int c) {
+    const int n = D.cell_count[c];
+    return n < SLD_MAXC ? n : SLD_MAXC;
+}
+
 __device__ __forceinline__ void cell_xyz(const Dev& D, int c, int& cx, int& cy, int& cz) {
     cx = c % D.nx;
     int t = c / D.nx;

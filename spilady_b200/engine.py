@@ -23,6 +23,7 @@ ERRORS = {
     -1: "SLD_ERR_ARG", -2: "SLD_ERR_CUDA", -3: "SLD_ERR_GEOMETRY",
     -4: "SLD_ERR_CAPACITY", -5: "SLD_ERR_TABLE", -6: "SLD_ERR_NAN",
     -7: "SLD_ERR_IO", -8: "SLD_ERR_STATE", -9: "SLD_ERR_NOMEM",
+    -10: "SLD_ERR_TIMEOUT",
 }
 
 

@@ -64,3 +64,13 @@ def test_error_strings():
     L = engine.lib()
     for code in range(0, -10, -1):
         assert L.sld_error_string(code)
+
+
+def test_error_strings_cover_every_code():
+    L = engine.lib()
+    L.sld_error_string.restype = C.c_char_p
+    for code in range(0, -11, -1):
+        msg = L.sld_error_string(code).decode()
+        assert msg and msg != "unknown error", code
+        if code < 0:
+            assert code in engine.ERRORS, code
