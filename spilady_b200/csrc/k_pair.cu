@@ -44,7 +44,7 @@ __device__ __forceinline__ double3 pair_d(const Dev& D, double4 ri, int pk) {
 // The loose test keeps every pair the exact one keeps: with coordinates
 // below B in magnitude, each FP32 rounding moves a coordinate by at most
 // e = ulp(B)/2; a pair-vector component collects four of them (two
-// positions, the difference, the box shift), so r^2 near the cutoff moves by
+// positions, the box shift, the difference), so r^2 near the cutoff moves by
 // at most 2 r_max (4 sqrt(3) e) + (4 sqrt(3) e)^2 plus the FP32 rounding of
 // the sum.  D.pair_loose, set on the host from the box, is twice that.
 
@@ -69,38 +69,54 @@ __device__ void pairs_one(const Dev& D, int i, int write_rho) {
     // pass 1: loose cutoff test in the reference's traversal order
     int nn = 0;
     const int myslot = D.cell_slot[i];
-    const float rx = (float)ri.x, ry = (float)ri.y, rz = (float)ri.z;
-    const float cut = (float)D.rcut_max_sq + D.pair_loose;
-    const float ax = (float)D.d[0];
-    const float bx = (float)D.d[1], by = (float)D.d[2];
-    const float qx = (float)D.d[3], qy = (float)D.d[4], qz = (float)D.d[5];
-    for (int k = 0; k < 27; ++k) {
-        int sx = 0, sy = 0, sz = 0;
-        const int c = k == 26 ? c0 : nbr_cell_s(D, cx, cy, cz, k, sx, sy, sz);
-        const bool wrap = D.small_grid || (sx | sy | sz) != 0;
-        // image of the neighbour cell: its atoms + sx a + sy b + sz c
-        const float hx = sx * ax + sy * bx + sz * qx;
-        const float hy = sy * by + sz * qy;
-        const float hz = sz * qz;
-        const int st = D.cell_start[c], n = cell_n(D, c);
-        for (int m = 0; m < n; ++m) {
-            const int slot = st + m;
-            if (slot == myslot) continue;
-            bool take;
-            if (!D.small_grid) {
-                const float4 q = __ldg(D.r32s + slot);
-                const float dx = (rx - q.x) - hx, dy = (ry - q.y) - hy, dz = (rz - q.z) - hz;
-                take = dx * dx + dy * dy + dz * dz < cut;
-            } else {
-                // three cells along an axis: the image is the reference's
-                // minimum image of each pair
-                const double4 rj = D.r[D.cell_atoms[slot]];
-                take = pair_accept<MODE>(
-                    D, find_image(D, make_double3(ri.x - rj.x, ri.y - rj.y, ri.z - rj.z)));
+    auto keep = [&](int slot, bool wrap) {
+        if (nn < SLD_MAXNB) D.nbr[(size_t)nn * N + i] = slot | (wrap ? SLD_WRAP : 0);
+        ++nn;
+    };
+    if (!D.small_grid) {
+        const float rx = (float)ri.x, ry = (float)ri.y, rz = (float)ri.z;
+        const float cut = (float)D.rcut_max_sq + D.pair_loose;
+        const float ax = (float)D.d[0];
+        const float bx = (float)D.d[1], by = (float)D.d[2];
+        const float qx = (float)D.d[3], qy = (float)D.d[4], qz = (float)D.d[5];
+        for (int k = 0; k < 27; ++k) {
+            int sx = 0, sy = 0, sz = 0;
+            const int c = k == 26 ? c0 : nbr_cell_s(D, cx, cy, cz, k, sx, sy, sz);
+            const bool wrap = (sx | sy | sz) != 0;
+            // this atom seen from the neighbour cell's image (its atoms
+            // + sx a + sy b + sz c)
+            const float ex = rx - (sx * ax + sy * bx + sz * qx);
+            const float ey = ry - (sy * by + sz * qy);
+            const float ez = rz - sz * qz;
+            const int st = __ldg(D.cell_start + c), n = min(__ldg(D.cell_count + c), SLD_MAXC);
+            for (int m0 = 0; m0 < n; m0 += 4) {
+                float4 q[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    q[u] = m0 + u < n ? __ldg(D.r32s + st + m0 + u) : make_float4(1e30f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int slot = st + m0 + u;
+                    const float dx = ex - q[u].x, dy = ey - q[u].y, dz = ez - q[u].z;
+                    if (dx * dx + dy * dy + dz * dz < cut && slot != myslot) keep(slot, wrap);
+                }
             }
-            if (!take) continue;
-            if (nn < SLD_MAXNB) D.nbr[(size_t)nn * N + i] = slot | (wrap ? SLD_WRAP : 0);
-            ++nn;
+        }
+    } else {
+        // three cells along an axis: the image is the reference's minimum
+        // image of each pair
+        for (int k = 0; k < 27; ++k) {
+            bool wrap = false;
+            const int c = k == 26 ? c0 : nbr_cell_w(D, cx, cy, cz, k, wrap);
+            const int st = D.cell_start[c], n = cell_n(D, c);
+            for (int m = 0; m < n; ++m) {
+                const int slot = st + m;
+                if (slot == myslot) continue;
+                const double4 rj = D.r[D.cell_atoms[slot]];
+                if (pair_accept<MODE>(
+                        D, find_image(D, make_double3(ri.x - rj.x, ri.y - rj.y, ri.z - rj.z))))
+                    keep(slot, true);
+            }
         }
     }
     const int nl = nn < SLD_MAXNB ? nn : SLD_MAXNB;
