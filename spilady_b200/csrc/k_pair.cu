@@ -188,147 +188,6 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, int write_rho) {
     if (i < D.natom) pairs_one<MODE>(D, i, write_rho);
 }
 
-// One warp per link cell: the cell's 27-cell candidate set (positions, atom
-// indices, a flag for pairs across the box) is staged once in shared memory
-// in the reference's traversal order, then every atom of the cell is tested
-// against it 32 candidates at a time.  List entries are placed with a warp
-// ballot, so each list keeps the traversal order.  A cell whose candidate
-// set does not fit falls back to one thread per atom.
-#define PW_WARPS 4
-#define PW_CAP 384
-template <int MODE>
-__global__ void __launch_bounds__(PW_WARPS * 32) k_pairs_warp(Dev D, int write_rho) {
-    constexpr bool SPLIT = MODE == 1;
-    __shared__ double s_rx[PW_WARPS][PW_CAP], s_ry[PW_WARPS][PW_CAP], s_rz[PW_WARPS][PW_CAP];
-    __shared__ int s_j[PW_WARPS][PW_CAP];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c = blockIdx.x * PW_WARPS + warp;
-    if (c >= D.ncells) return;
-    unsigned* err = &D.ctl->err;
-    const int N = D.natom;
-    int cx, cy, cz;
-    cell_xyz(D, c, cx, cy, cz);
-    int nc = c, cnt = 0, st = 0;
-    bool wr = false;
-    if (lane < 27) {
-        nc = lane == 26 ? c : nbr_cell_w(D, cx, cy, cz, lane, wr);
-        cnt = cell_n(D, nc);
-        st = D.cell_start[nc];
-    }
-    int inc = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int t = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += t;
-    }
-    const int off = inc - cnt;
-    const int T = __shfl_sync(0xffffffffu, inc, 31);
-    const int own_off = __shfl_sync(0xffffffffu, off, 26);
-    const int own_n = __shfl_sync(0xffffffffu, cnt, 26);
-    if (T > PW_CAP) {   // too dense for the staging area
-        int own_st = __shfl_sync(0xffffffffu, st, 26);
-        for (int h = lane; h < own_n; h += 32) pairs_one<MODE>(D, D.cell_atoms[own_st + h], write_rho);
-        return;
-    }
-    const unsigned wrap_lanes = __ballot_sync(0xffffffffu, wr);
-    for (int k = 0; k < 27; ++k) {
-        int stk = __shfl_sync(0xffffffffu, st, k), ck = __shfl_sync(0xffffffffu, cnt, k);
-        int ok = __shfl_sync(0xffffffffu, off, k);
-        for (int m = lane; m < ck; m += 32) {
-            int j = D.cell_atoms[stk + m];
-            double4 r = D.r[j];
-            s_j[warp][ok + m] = j | (((wrap_lanes >> k) & 1u) ? SLD_WRAP : 0);
-            s_rx[warp][ok + m] = r.x;
-            s_ry[warp][ok + m] = r.y;
-            s_rz[warp][ok + m] = r.z;
-        }
-    }
-    __syncwarp();
-    const float rmax2f = (float)D.rcut_max_sq, rmag2f = (float)D.rcut_mag_sq;
-    const float rpotf = (float)D.rcut_pot;
-    const unsigned lt = (1u << lane) - 1u;
-    for (int h = 0; h < own_n; ++h) {
-        const int ci = own_off + h;
-        const int i = s_j[warp][ci] & SLD_JMASK;
-        const double rix = s_rx[warp][ci], riy = s_ry[warp][ci], riz = s_rz[warp][ci];
-        int nn = 0, nj = 0;
-        double rho = 0.0;
-        Kahan rho32;
-        for (int base = 0; base < T; base += 32) {
-            const int idx = base + lane;
-            int pk = idx < T ? s_j[warp][idx] : -1;
-            int j = pk & SLD_JMASK;
-            bool in_max = false, in_mag = false;
-            double r64 = 0.0;
-            if (pk >= 0 && j != i) {
-                double3 d = make_double3(rix - s_rx[warp][idx], riy - s_ry[warp][idx],
-                                         riz - s_rz[warp][idx]);
-                if (pk & SLD_WRAP) d = find_image(D, d);
-                if constexpr (!SPLIT) {
-                    double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
-                    in_max = rsq < D.rcut_max_sq;
-                    in_mag = rsq < D.rcut_mag_sq;
-                    r64 = sqrt(rsq);
-                } else {
-                    float dx = (float)d.x, dy = (float)d.y, dz = (float)d.z;
-                    float rsq = dx * dx + dy * dy + dz * dz;
-                    in_max = rsq < rmax2f;
-                    in_mag = rsq < rmag2f;
-                    if (in_max) r64 = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
-                }
-            }
-            unsigned bm = __ballot_sync(0xffffffffu, in_max);
-            if (in_max) {
-                int pos = nn + __popc(bm & lt);
-                if (pos < SLD_MAXNB) D.nbr[(size_t)pos * N + i] = pk;
-                if constexpr (MODE == 0) {
-                    if (r64 < D.rcut_pot) rho += interp(D.tf, r64, D.inv_r, err);
-                } else if constexpr (MODE == 2) {
-                    if (r64 < D.rcut_pot) {
-                        double f, df;
-                        dens64(D, r64, f, df);
-                        rho += f;
-                    }
-                } else {
-                    if ((float)r64 < rpotf) {
-                        float f, df;
-                        dens32r(D, r64, f, df);
-                        rho32.add(f);
-                    }
-                }
-            }
-            nn += __popc(bm);
-            unsigned bj = __ballot_sync(0xffffffffu, in_mag && in_max);
-            if (in_mag && in_max) {
-                int pj = nj + __popc(bj & lt);
-                if (pj < SLD_MAXJ) {
-                    D.jl[(size_t)i * SLD_MAXJ + pj] = j;
-                    if constexpr (MODE == 0) {
-                        D.jv[(size_t)i * SLD_MAXJ + pj] = interp(D.tJ, r64, D.inv_r, err);
-                    } else if constexpr (MODE == 2) {
-                        double J, dJ;
-                        exch64(r64, J, dJ);
-                        D.jv[(size_t)i * SLD_MAXJ + pj] = J;
-                    } else {
-                        float J, dJ;
-                        exch32r(r64, J, dJ);
-                        D.jvf[(size_t)i * SLD_MAXJ + pj] = J;
-                    }
-                }
-            }
-            nj += __popc(bj);
-        }
-        double rsum = SPLIT ? rho32.value() : rho;
-        rsum = warp_sum(rsum);
-        if (lane == 0) {
-            if (nn > SLD_MAXNB || nj > SLD_MAXJ) atomicOr(err, SLD_FLAG_CAPACITY);
-            D.nbr_n[i] = nn < SLD_MAXNB ? nn : SLD_MAXNB;
-            D.jl_n[i] = nj < SLD_MAXJ ? nj : SLD_MAXJ;
-            if (write_rho) D.rho[i] = rsum;
-        }
-    }
-}
-
 // F'(rho) per atom (the force pass needs it for both atoms of every pair)
 template <int MODE>
 __global__ void __launch_bounds__(256) k_embed(Dev D) {
@@ -558,21 +417,8 @@ static void launch_force_part(const Dev& D, cudaStream_t st) {
     else k_force64<false, PART><<<nb, 128, 0, st>>>(D);
 }
 
-static int g_pairs_mode = -1;   // 0: one thread per atom (default), 1: one warp per cell
-
 void launch_pairs(const Dev& D, cudaStream_t st, bool write_rho) {
-    if (g_pairs_mode < 0) {
-        const char* v = getenv("SLD_PAIRS_MODE");
-        g_pairs_mode = (v && v[0] == '1') ? 1 : 0;
-    }
     int w = write_rho ? 1 : 0;
-    if (g_pairs_mode == 1) {
-        int nb = div_up(D.ncells, PW_WARPS);
-        if (D.split) k_pairs_warp<1><<<nb, PW_WARPS * 32, 0, st>>>(D, w);
-        else if (D.analytic) k_pairs_warp<2><<<nb, PW_WARPS * 32, 0, st>>>(D, w);
-        else k_pairs_warp<0><<<nb, PW_WARPS * 32, 0, st>>>(D, w);
-        return;
-    }
     int nb = div_up(D.natom, 128);
     if (D.split) k_pairs<1><<<nb, 128, 0, st>>>(D, w);
     else if (D.analytic) k_pairs<2><<<nb, 128, 0, st>>>(D, w);
