@@ -39,77 +39,130 @@ __device__ __forceinline__ void add3(double4& a, double k, double x, double y, d
     a.x = a.x + k * x; a.y = a.y + k * y; a.z = a.z + k * z;
 }
 
+// The momenta of one cell's atoms, m = 0..n-1 in list order: in the block's
+// shared memory (cells of up to KDP_MAXA atoms: the kick's six passes then
+// read and write shared memory, and global memory once each way) or in
+// global memory.  The arithmetic is the same code for both.
+#define KDP_BLOCK 128
+#define KDP_MAXA 12
+struct PGlobal {
+    const Dev& D;
+    const int* a;
+    __device__ double3 get(int m) const {
+        const double4 p = D.p[a[m]];
+        return make_double3(p.x, p.y, p.z);
+    }
+    __device__ void set(int m, double3 v) const { D.p[a[m]] = make_double4(v.x, v.y, v.z, 0.0); }
+};
+struct PShared {
+    double* s;   // s[(3 m + k) KDP_BLOCK]: component k of atom m of this thread's cell
+    __device__ double3 get(int m) const {
+        return make_double3(s[(3 * m) * KDP_BLOCK], s[(3 * m + 1) * KDP_BLOCK],
+                            s[(3 * m + 2) * KDP_BLOCK]);
+    }
+    __device__ void set(int m, double3 v) const {
+        s[(3 * m) * KDP_BLOCK] = v.x;
+        s[(3 * m + 1) * KDP_BLOCK] = v.y;
+        s[(3 * m + 2) * KDP_BLOCK] = v.z;
+    }
+};
+
 // C1 / C2: p_i += gamma/m dt / n (sum_cell p - p_i), Gauss-Seidel in list
 // order.  The reference re-adds the cell's momenta for every atom; here the
 // cell sum is carried along and corrected by each update (the same sum up to
 // rounding), so the pass is linear in the cell's size.
-__device__ __forceinline__ void cell_mix(const Dev& D, const int* a, int n, double dt, bool backward) {
+template <class P>
+__device__ __forceinline__ void cell_mix(const Dev& D, const P& P_, int n, double dt, bool backward) {
     double factor = D.gamma_L / D.atmass * dt / n;
     double sx = 0.0, sy = 0.0, sz = 0.0;
     for (int m = 0; m < n; ++m) {
-        double4 pm = D.p[a[m]];
+        double3 pm = P_.get(m);
         sx = sx + pm.x; sy = sy + pm.y; sz = sz + pm.z;
     }
     for (int q = 0; q < n; ++q) {
-        int i = a[backward ? n - 1 - q : q];
-        double4 p = D.p[i];
+        const int m = backward ? n - 1 - q : q;
+        double3 p = P_.get(m);
         double nx = p.x + factor * (sx - p.x);
         double ny = p.y + factor * (sy - p.y);
         double nz = p.z + factor * (sz - p.z);
         sx += nx - p.x; sy += ny - p.y; sz += nz - p.z;
-        D.p[i] = make_double4(nx, ny, nz, 0.0);
+        P_.set(m, make_double3(nx, ny, nz));
     }
 }
 
-__device__ __forceinline__ void friction(const Dev& D, const int* a, int n, double dt) {
+template <class P>
+__device__ __forceinline__ void friction(const Dev& D, const P& P_, int n, double dt) {
     double e = D.localcolmot ? exp(-D.gamma_L / D.atmass * dt * (1.0 - 1.0 / n))
                              : exp(-D.gamma_L / D.atmass * dt);
     for (int m = 0; m < n; ++m) {
-        double4 p = D.p[a[m]];
+        double3 p = P_.get(m);
         p.x = e * p.x; p.y = e * p.y; p.z = e * p.z;
-        D.p[a[m]] = p;
+        P_.set(m, p);
     }
 }
 
-__global__ void __launch_bounds__(128) k_dp_lang(Dev D, double dt, int epoch_off) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    double px = 0, py = 0, pz = 0;
-    if (c < D.ncells) {
-        int n = cell_n(D, c);
-        const int* a = D.cell_atoms + D.cell_start[c];
-        if (n > 0) {
-            unsigned long long epoch = D.ctl->epoch + (unsigned long long)epoch_off;
-            if (D.localcolmot) cell_mix(D, a, n, dt / 2.0, false);
-            friction(D, a, n, dt / 2.0);
-            double ax = 0.0, ay = 0.0, az = 0.0;
-            for (int m = 0; m < n; ++m) {            // A: force + noise
-                int i = a[m];
-                double T = D.eltemp ? D.Te[D.node[i]] : D.temperature;
-                double amp = sqrt(2.0 * T * D.gamma_L / dt);
-                double3 xi = normals3(D.seed, 0u, (unsigned)D.id[i], epoch);
-                double fx = amp * xi.x, fy = amp * xi.y, fz = amp * xi.z;
-                double4 f = D.f[i], p = D.p[i];
-                p.x = p.x + dt * (f.x + fx); p.y = p.y + dt * (f.y + fy); p.z = p.z + dt * (f.z + fz);
-                D.p[i] = p;
-                ax = ax + fx; ay = ay + fy; az = az + fz;
-            }
-            if (D.localcolmot) {
-                ax = ax / n; ay = ay / n; az = az / n;
-                for (int m = 0; m < n; ++m) {
-                    double4 p = D.p[a[m]];
-                    p.x = p.x - dt * ax; p.y = p.y - dt * ay; p.z = p.z - dt * az;
-                    D.p[a[m]] = p;
-                }
-            }
-            friction(D, a, n, dt / 2.0);
-            if (D.localcolmot) cell_mix(D, a, n, dt / 2.0, true);
-            for (int m = 0; m < n; ++m) {
-                double4 p = D.p[a[m]];
-                px += p.x; py += p.y; pz += p.z;
-            }
+// core_dp_CPU.cpp:51-85 for one cell: C1(dt/2) B(dt/2) A(dt) B(dt/2) C2(dt/2);
+// returns the cell's momentum sum for rescale_momentum
+template <class P>
+__device__ __forceinline__ double3 dp_cell(const Dev& D, const P& P_, const int* a, int n, double dt,
+                                           unsigned long long epoch) {
+    if (D.localcolmot) cell_mix(D, P_, n, dt / 2.0, false);
+    friction(D, P_, n, dt / 2.0);
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    for (int m = 0; m < n; ++m) {            // A: force + noise
+        int i = a[m];
+        double T = D.eltemp ? D.Te[D.node[i]] : D.temperature;
+        double amp = sqrt(2.0 * T * D.gamma_L / dt);
+        double3 xi = normals3(D.seed, 0u, (unsigned)D.id[i], epoch);
+        double fx = amp * xi.x, fy = amp * xi.y, fz = amp * xi.z;
+        double4 f = D.f[i];
+        double3 p = P_.get(m);
+        p.x = p.x + dt * (f.x + fx); p.y = p.y + dt * (f.y + fy); p.z = p.z + dt * (f.z + fz);
+        P_.set(m, p);
+        ax = ax + fx; ay = ay + fy; az = az + fz;
+    }
+    if (D.localcolmot) {
+        ax = ax / n; ay = ay / n; az = az / n;
+        for (int m = 0; m < n; ++m) {
+            double3 p = P_.get(m);
+            p.x = p.x - dt * ax; p.y = p.y - dt * ay; p.z = p.z - dt * az;
+            P_.set(m, p);
         }
     }
-    block_partials3(D, px, py, pz);
+    friction(D, P_, n, dt / 2.0);
+    if (D.localcolmot) cell_mix(D, P_, n, dt / 2.0, true);
+    double px = 0, py = 0, pz = 0;
+    for (int m = 0; m < n; ++m) {
+        double3 p = P_.get(m);
+        px += p.x; py += p.y; pz += p.z;
+    }
+    return make_double3(px, py, pz);
+}
+
+__global__ void __launch_bounds__(KDP_BLOCK) k_dp_lang(Dev D, double dt, int epoch_off) {
+    __shared__ double sp[3 * KDP_MAXA * KDP_BLOCK];
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double3 ps = make_double3(0.0, 0.0, 0.0);
+    if (c < D.ncells) {
+        const int n = cell_n(D, c);
+        const int* a = D.cell_atoms + D.cell_start[c];
+        const unsigned long long epoch = D.ctl->epoch + (unsigned long long)epoch_off;
+        if (n > 0 && n <= KDP_MAXA) {
+            const PShared P_{sp + threadIdx.x};
+            for (int m = 0; m < n; ++m) {
+                const double4 p = D.p[a[m]];
+                P_.set(m, make_double3(p.x, p.y, p.z));
+            }
+            ps = dp_cell(D, P_, a, n, dt, epoch);
+            for (int m = 0; m < n; ++m) {
+                const double3 p = P_.get(m);
+                D.p[a[m]] = make_double4(p.x, p.y, p.z, 0.0);
+            }
+        } else if (n > 0) {
+            ps = dp_cell(D, PGlobal{D, a}, a, n, dt, epoch);
+        }
+    }
+    block_partials3(D, ps.x, ps.y, ps.z);
 }
 
 __global__ void __launch_bounds__(1024) k_avep(Dev D, int nb) {
@@ -185,8 +238,8 @@ __global__ void __launch_bounds__(256) k_dr(Dev D, double dt) {
 void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off) {
     int nb;
     if (D.lattlang) {
-        nb = div_up(D.ncells, 128);
-        k_dp_lang<<<nb, 128, 0, st>>>(D, dt, epoch_off);
+        nb = div_up(D.ncells, KDP_BLOCK);
+        k_dp_lang<<<nb, KDP_BLOCK, 0, st>>>(D, dt, epoch_off);
     } else {
         nb = div_up(D.natom, 256);
         k_dp_nve<<<nb, 256, 0, st>>>(D, dt);
