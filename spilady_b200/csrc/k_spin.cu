@@ -29,6 +29,11 @@
 #define SW_THREADS 256
 #define SW_MAXA 256
 #define SW_MAXIN 12
+// the sweep kernels' `backward` argument: bit 0 the backward sweep (tail ->
+// head, the second visit record); bit 1 no H, HL, sum J stores (the step
+// graph overwrites them later in the same step)
+#define SW_BACKWARD 1
+#define SW_NO_FIELDS 2
 
 struct SweepShared {
     double s[SW_MAXA][4];           // current spin, |s|
@@ -82,7 +87,7 @@ __device__ __forceinline__ double4 visit_record(const Dev& D, int i, int sweep) 
 }
 
 // one visit entirely from global memory (the fallback path)
-__device__ void visit_global(const Dev& D, int i, double dt, bool fields) {
+__device__ void visit_global(const Dev& D, int i, double dt, int sweep, bool fields) {
     double3 H;
     double sumJ;
     exchange_field(D, i, H, sumJ, [](int) { return false; }, [](int, double) {});
@@ -90,7 +95,7 @@ __device__ void visit_global(const Dev& D, int i, double dt, bool fields) {
     double rho = 0.0;
     double3 dS = make_double3(0.0, 0.0, 0.0);
     if (D.spinlang) {
-        const double4 q = visit_record(D, i, fields ? 1 : 0);
+        const double4 q = visit_record(D, i, sweep);
         rho = q.x;
         dS = make_double3(q.y, q.z, q.w);
     }
@@ -105,7 +110,8 @@ __global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restri
     SweepShared& S = *reinterpret_cast<SweepShared*>(smem_raw);
     const int cbeg = blockIdx.x * SW_CPB;
     const int ncb = min(SW_CPB, ncell_g - cbeg);
-    const bool fields = backward != 0;   // the backward sweep is each atom's last visit
+    const bool bwd = (backward & SW_BACKWARD) != 0;
+    const bool fields = bwd && !(backward & SW_NO_FIELDS);   // the backward sweep is each atom's last visit
     if (threadIdx.x < 32) {
         int lane = threadIdx.x, n = 0, st = 0, c = -1;
         if (lane < ncb) {
@@ -162,7 +168,7 @@ __global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restri
             S.inn[a] = (unsigned char)(nin < SW_MAXIN ? nin : SW_MAXIN);
             if (nin > SW_MAXIN) S.overflow = 1;
             if (D.spinlang) {
-                const double4 q = visit_record(D, i, fields ? 1 : 0);
+                const double4 q = visit_record(D, i, bwd ? 1 : 0);
                 S.aux[a][0] = q.x;
                 S.aux[a][1] = q.y; S.aux[a][2] = q.z; S.aux[a][3] = q.w;
             }
@@ -173,7 +179,7 @@ __global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restri
             if (threadIdx.x < ncb) {
                 int q = threadIdx.x, n = S.cell_n[q], b = S.cell_base[q];
                 for (int t = 0; t < n; ++t) {
-                    int a = b + (backward ? n - 1 - t : t);
+                    int a = b + (bwd ? n - 1 - t : t);
                     double3 H = make_double3(S.h[a][0], S.h[a][1], S.h[a][2]);
                     double sumJ = S.h[a][3];
                     for (int e = 0; e < S.inn[a]; ++e) {
@@ -213,8 +219,8 @@ __global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restri
     if (threadIdx.x < ncb) {
         int q = threadIdx.x, n = S.cell_n[q], st = S.cell_start[q];
         for (int t = 0; t < n; ++t) {
-            int i = D.cell_atoms[st + (backward ? n - 1 - t : t)];
-            visit_global(D, i, dt, fields);
+            int i = D.cell_atoms[st + (bwd ? n - 1 - t : t)];
+            visit_global(D, i, dt, bwd ? 1 : 0, fields);
         }
     }
 }
@@ -227,10 +233,11 @@ __global__ void __launch_bounds__(128) k_sweep_cell(Dev D, const int* __restrict
     if (t >= ncell_g) return;
     int c = gcells[t];
     int st = D.cell_start[c], n = cell_n(D, c);
-    bool fields = backward != 0;
+    const bool bwd = (backward & SW_BACKWARD) != 0;
+    const bool fields = bwd && !(backward & SW_NO_FIELDS);
     for (int m = 0; m < n; ++m) {
-        int i = D.cell_atoms[st + (backward ? n - 1 - m : m)];
-        visit_global(D, i, dt, fields);
+        int i = D.cell_atoms[st + (bwd ? n - 1 - m : m)];
+        visit_global(D, i, dt, bwd ? 1 : 0, fields);
     }
 }
 
@@ -403,9 +410,11 @@ __device__ __forceinline__ void cell_walk(const Dev& D, int c, double dt, int ba
     const int n = cell_n(D, c);
     if (n <= 0) return;
     const int* ca = D.cell_atoms + D.cell_start[c];
-    const bool fields = backward != 0;   // the backward sweep is each atom's last visit
-    const int sweep = fields ? 1 : 0;
-    auto atom_at = [&](int m) { return __ldg(ca + (backward ? n - 1 - m : m)); };
+    const bool bwd = (backward & SW_BACKWARD) != 0;
+    // the backward sweep is each atom's last visit of the call
+    const bool fields = bwd && !(backward & SW_NO_FIELDS);
+    const int sweep = bwd ? 1 : 0;
+    auto atom_at = [&](int m) { return __ldg(ca + (bwd ? n - 1 - m : m)); };
     VisitRegs<SPLIT> v;
     RowIdx r;
     row_load(D, atom_at(0), r);
@@ -540,7 +549,7 @@ __device__ bool flow_wait(const Dev& D, const SweepFlow& F, int c, int g, bool b
 }
 
 template <bool SPLIT>
-__global__ void __launch_bounds__(128) k_sweep_flow(Dev D, SweepFlow F, double dt) {
+__global__ void __launch_bounds__(128) k_sweep_flow(Dev D, SweepFlow F, double dt, int flags) {
     const int lane = threadIdx.x & 31;
     const int tagF = F.sync[0] + 1, tagB = tagF + 1;
     int task = 0;
@@ -565,7 +574,7 @@ __global__ void __launch_bounds__(128) k_sweep_flow(Dev D, SweepFlow F, double d
         }
         if (c >= 0) {
             __threadfence();                  // the flags above before the spins below
-            cell_walk<SPLIT, true>(D, c, dt, bwd ? 1 : 0);
+            cell_walk<SPLIT, true>(D, c, dt, (bwd ? SW_BACKWARD : 0) | flags);
             __threadfence();                  // this cell's spins before its flag
             atomicExch(F.cell_flag + c, bwd ? tagB : tagF);
         }
@@ -583,12 +592,13 @@ __global__ void k_flow_next(SweepFlow F) {
 
 static int g_flow_blocks[2] = {0, 0};
 
-void launch_sweep_flow(const Dev& D, cudaStream_t st, const SweepFlow& F, double dt) {
+void launch_sweep_flow(const Dev& D, cudaStream_t st, const SweepFlow& F, double dt, bool fields) {
+    const int flags = fields ? 0 : SW_NO_FIELDS;
     const int k = D.split ? 1 : 0;
     if (D.split)
-        k_sweep_flow<true><<<g_flow_blocks[k], 128, 0, st>>>(D, F, dt);
+        k_sweep_flow<true><<<g_flow_blocks[k], 128, 0, st>>>(D, F, dt, flags);
     else
-        k_sweep_flow<false><<<g_flow_blocks[k], 128, 0, st>>>(D, F, dt);
+        k_sweep_flow<false><<<g_flow_blocks[k], 128, 0, st>>>(D, F, dt, flags);
     k_flow_next<<<1, 32, 0, st>>>(F);
 }
 
@@ -613,9 +623,9 @@ void sweep_init() {
 bool sweep_uses_flow() { return g_sweep_mode == 3; }
 
 void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g, double dt,
-                  bool backward) {
+                  bool backward, bool fields) {
     if (ncell_g <= 0) return;
-    const int b = backward ? 1 : 0;
+    const int b = (backward ? SW_BACKWARD : 0) | (fields ? 0 : SW_NO_FIELDS);
     if (g_sweep_mode >= 2) {
         // Block sizes that fill the register file: the split form's kernel takes
         // about 200 registers a thread, 9 warps an SM, so blocks of 3 warps

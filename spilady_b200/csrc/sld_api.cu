@@ -115,22 +115,27 @@ int launch_status() {
 }
 
 // One core_ds call: forward sweep, backward sweep.
-void enqueue_ds(sld_ctx* c, const Dev& D, double dt, int& eoff) {
+// core_ds (core_ds_CPU.cpp:35-83).  fields: store H, HL and sum J at each
+// atom's last visit, as the reference's calculate_spin does; the step graph
+// passes false where the same step overwrites them before anything reads
+// them (the first core_ds of a step; with eltemp, calculate_temperature
+// recomputes all three).
+void enqueue_ds(sld_ctx* c, const Dev& D, double dt, int& eoff, bool fields = true) {
     const auto& G = c->G;
     double dt_half = dt / 2e0;
     if (c->P.spinlang) launch_spin_noise(D, c->st, eoff, dt_half);
     if (sweep_uses_flow()) {
-        launch_sweep_flow(D, c->st, c->flow, dt_half);
+        launch_sweep_flow(D, c->st, c->flow, dt_half, fields);
         if (c->P.spinlang) eoff += 2;
         return;
     }
     for (int g = 0; g < G.ngroups; ++g)
         launch_sweep(D, c->st, c->d_gcells + G.gstart[g], G.gstart[g + 1] - G.gstart[g],
-                     dt_half, false);
+                     dt_half, false, fields);
     if (c->P.spinlang) ++eoff;
     for (int g = G.ngroups - 1; g >= 0; --g)
         launch_sweep(D, c->st, c->d_gcells + G.gstart[g], G.gstart[g + 1] - G.gstart[g],
-                     dt_half, true);
+                     dt_half, true, fields);
     if (c->P.spinlang) ++eoff;
 }
 void enqueue_ds(sld_ctx* c, double dt, int& eoff) { enqueue_ds(c, c->D, dt, eoff); }
@@ -173,9 +178,9 @@ void enqueue_step(sld_ctx* c) {
     cudaEventRecord(ev[2], A);
     launch_force_eam(Dn, A);
     cudaEventRecord(ev[3], A);
-    enqueue_ds(c, Dc, dt / 2e0, eoff);
+    enqueue_ds(c, Dc, dt / 2e0, eoff, false);
     cudaStreamWaitEvent(M, ev[2], 0);
-    enqueue_ds(c, Dn, dt / 2e0, eoff);
+    enqueue_ds(c, Dn, dt / 2e0, eoff, !c->P.eltemp);
     cudaStreamWaitEvent(M, ev[3], 0);
     launch_force_mag(Dn, M);
     enqueue_dp(c, Dn, dt / 2e0, eoff);
@@ -636,10 +641,10 @@ int sld_profile_step(sld_ctx* c, double* ms) {
     timed(0, [&] { launch_links(Dc, c->st, false, c->scan_blocks); });
     if (c->P.eltemp) timed(1, [&] { launch_dte(Dc, c->st, dt / 2e0); });
     timed(2, [&] { enqueue_dp(c, Dc, dt / 2e0, eoff); });
-    timed(3, [&] { enqueue_ds(c, Dc, dt / 2e0, eoff); });
+    timed(3, [&] { enqueue_ds(c, Dc, dt / 2e0, eoff, false); });
     timed(4, [&] { launch_dr(Dc, c->st, dt); });
     timed(5, [&] { launch_pairs(Dn, c->st, true); });
-    timed(3, [&] { enqueue_ds(c, Dn, dt / 2e0, eoff); });
+    timed(3, [&] { enqueue_ds(c, Dn, dt / 2e0, eoff, !c->P.eltemp); });
     timed(6, [&] { launch_force(Dn, c->st); });
     timed(2, [&] { enqueue_dp(c, Dn, dt / 2e0, eoff); });
     if (c->P.eltemp) {

@@ -419,7 +419,7 @@ void launch_embed(const Dev& D, cudaStream_t st);
 void launch_force_eam(const Dev& D, cudaStream_t st);   // lattice terms (no spins)
 void launch_force_mag(const Dev& D, cudaStream_t st);   // adds the magnetic terms
 void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g, double dt,
-                  bool backward);
+                  bool backward, bool fields);
 void launch_spin_noise(const Dev& D, cudaStream_t st, int epoch_off, double dt);
 void launch_load_state(const Dev& D, cudaStream_t st, const double* r, const double* p,
                        const double* s);
@@ -433,7 +433,8 @@ struct SweepFlow {
     int* sync;                        // [0] tag base of the next call, [1] next task
 };
 bool sweep_uses_flow();
-void launch_sweep_flow(const Dev& D, cudaStream_t st, const SweepFlow& F, double dt);
+void launch_sweep_flow(const Dev& D, cudaStream_t st, const SweepFlow& F, double dt,
+                       bool fields);
 void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off);
 void launch_dr(const Dev& D, cudaStream_t st, double dt);
 void launch_temperature(const Dev& D, cudaStream_t st);
