@@ -88,6 +88,10 @@ typedef struct {
                                     (check.cpp:33)                default.h:64 */
     int precision;               /* sld_precision */
     int device;                  /* CUDA device ordinal */
+    int replica;                 /* key of this system's noise stream: the
+                                    Philox key is (random_seed, replica), so
+                                    replicas of one seed draw independent
+                                    noise (0 for a single system) */
 } sld_params;
 
 typedef struct sld_ctx sld_ctx;
@@ -187,6 +191,22 @@ int sld_profile_step(sld_ctx* ctx, double* ms_out);
 int sld_step_kernel_count(sld_ctx* ctx, int* out);
 
 const char* sld_error_string(int code);
+
+/* Batched replicas: several independent systems (contexts created on one
+   device, each with its own size, parameters and noise stream, see
+   sld_params.replica) advanced together.  Each step is one CUDA graph with
+   every context's main-loop step (sld_run's sequence) as an independent
+   branch, so the launches of small systems overlap on the GPU.  Every
+   context ends in the state that sld_run on it alone would give.  A context
+   may still be used on its own between batch runs; destroy the batch before
+   its contexts.  No reference counterpart: the reference runs one system per
+   process. */
+typedef struct sld_batch sld_batch;
+int sld_batch_create(sld_batch** out, sld_ctx* const* ctxs, int n);
+int sld_batch_run(sld_batch* batch, int nsteps);
+/* Milliseconds of device time of the last sld_batch_run (CUDA events). */
+int sld_batch_last_run_ms(sld_batch* batch, double* out);
+void sld_batch_destroy(sld_batch* batch);
 
 /* Allocation-free averages.  This entry point has no counterpart in the
    reference; it exists for callers that cannot let a library allocate

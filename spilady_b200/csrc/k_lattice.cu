@@ -113,7 +113,7 @@ __device__ __forceinline__ double3 dp_cell(const Dev& D, const P& P_, const int*
         int i = a[m];
         double T = D.eltemp ? D.Te[D.node[i]] : D.temperature;
         double amp = sqrt(2.0 * T * D.gamma_L / dt);
-        double3 xi = normals3(D.seed, 0u, (unsigned)D.id[i], epoch);
+        double3 xi = normals3(D.seed, D.replica, (unsigned)D.id[i], epoch);
         double fx = amp * xi.x, fy = amp * xi.y, fz = amp * xi.z;
         double4 f = D.f[i];
         double3 p = P_.get(m);

@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(256) k_spin_noise(Dev D, int epoch_off, double
     double T = D.eltemp ? D.Te[D.node[i]] : D.temperature;
     const double rho = D.rho[i];
     for (int v = 0; v < 2; ++v) {
-        double3 x = spin_noise_dS(D, T, normals3(D.seed, 0u, (unsigned)D.id[i], e0 + v), dt);
+        double3 x = spin_noise_dS(D, T, normals3(D.seed, D.replica, (unsigned)D.id[i], e0 + v), dt);
         D.vrec[2 * (size_t)i + v] = make_double4(rho, x.x, x.y, x.z);
     }
 }

@@ -5,6 +5,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -246,6 +248,49 @@ const char* sld_error_string(int code) {
     }
 }
 
+// Potential tables on the device, shared by every context on that device
+// with the same table range (they depend only on rcut_max): 8 tables of 10^6
+// doubles, built once (about a second on the host) and kept until the
+// process exits.  Replicas of one system then share one copy.
+struct DevTables {
+    double* t[sld::kTabCount];
+    double inv_r, inv_rho;
+    double landau[4];
+};
+static std::mutex g_tab_mu;
+static std::map<std::pair<int, uint64_t>, DevTables> g_tabs;
+
+static int device_tables(int dev, double rmax, DevTables* out) {
+    std::lock_guard<std::mutex> lock(g_tab_mu);
+    uint64_t bits;
+    std::memcpy(&bits, &rmax, sizeof(bits));
+    auto it = g_tabs.find({dev, bits});
+    if (it != g_tabs.end()) {
+        *out = it->second;
+        return SLD_OK;
+    }
+    sld::Tables T;
+    sld::build_tables(T, rmax);
+    DevTables d{};
+    d.inv_r = T.inv_r;
+    d.inv_rho = T.inv_rho;
+    for (int k = 0; k < 4; ++k) d.landau[k] = T.landau[k];
+    for (int k = 0; k < sld::kTabCount; ++k) {
+        if (cudaMalloc(&d.t[k], sizeof(double) * sld::kNInput) != cudaSuccess) {
+            for (int q = 0; q < k; ++q) cudaFree(d.t[q]);
+            return SLD_ERR_NOMEM;
+        }
+        if (cudaMemcpy(d.t[k], T.t[k].data(), sizeof(double) * sld::kNInput,
+                       cudaMemcpyHostToDevice) != cudaSuccess) {
+            for (int q = 0; q <= k; ++q) cudaFree(d.t[q]);
+            return SLD_ERR_CUDA;
+        }
+    }
+    g_tabs[{dev, bits}] = d;
+    *out = d;
+    return SLD_OK;
+}
+
 int sld_params_default(sld_params* o) {
     if (!o) return SLD_ERR_ARG;
     std::memset(o, 0, sizeof(*o));
@@ -303,8 +348,9 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     }
     for (int k = 0; k < 4; ++k) cudaEventCreateWithFlags(&c->fork_ev[k], cudaEventDisableTiming);
 
-    sld::Tables T;
-    sld::build_tables(T, G.rcut_max);
+    DevTables T;
+    rc = device_tables(prm->device, G.rcut_max, &T);
+    if (rc) { sld_destroy(c); return rc; }
 
     Dev& D = c->D;
     for (int k = 0; k < 6; ++k) { D.d[k] = G.d[k]; D.inv[k] = G.inv[k]; }
@@ -340,6 +386,7 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     D.nx = G.nx; D.ny = G.ny; D.nz = G.nz; D.ncells = G.ncells;
     D.tx = G.tx; D.ty = G.ty; D.tz = G.tz; D.nte = G.nte; D.te_mesh = prm->te_mesh;
     D.seed = (unsigned)prm->random_seed;
+    D.replica = (unsigned)prm->replica;
     D.spinlang = prm->spinlang; D.lattlang = prm->lattlang; D.eltemp = prm->eltemp;
     D.localcolmot = prm->localcolmot; D.renormalize = prm->renormalize_energy;
     D.print_every = c->P.interval_of_print_out;
@@ -358,13 +405,8 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     sld::pot_cubic_tables(cubic_h, cubic64_h);
 
     size_t n = (size_t)natom;
-    double* tabs[sld::kTabCount];
     bool ok = true;
-    for (int k = 0; k < sld::kTabCount; ++k) {
-        ok = ok && c->alloc(&tabs[k], sld::kNInput) == SLD_OK;
-        if (ok) cudaMemcpy(tabs[k], T.t[k].data(), sizeof(double) * sld::kNInput, cudaMemcpyHostToDevice);
-    }
-    if (!ok) { sld_destroy(c); return SLD_ERR_NOMEM; }
+    double* const* tabs = T.t;
     D.tF = tabs[sld::kF]; D.tdF = tabs[sld::kdF]; D.tf = tabs[sld::kf]; D.tdf = tabs[sld::kdf];
     D.tphi = tabs[sld::kPhi]; D.tdphi = tabs[sld::kdPhi]; D.tJ = tabs[sld::kJ]; D.tdJ = tabs[sld::kdJ];
 
@@ -617,6 +659,143 @@ int sld_run(sld_ctx* c, int nsteps) {
     }
     CK(cudaEventRecord(c->ev1, c->st));
     return SLD_OK;
+}
+
+// ---------------------------------------------------------------------
+// batched replicas
+
+struct sld_batch {
+    std::vector<sld_ctx*> ctx;
+    std::vector<int> base;             // each context's buffer set when graph 0 was made
+    cudaStream_t st = nullptr;
+    cudaEvent_t root = nullptr, done = nullptr, ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> join;     // one per context
+    cudaGraphExec_t graphs[2] = {nullptr, nullptr};
+    int device = 0;
+};
+
+static void batch_drop_graphs(sld_batch* b) {
+    for (int k = 0; k < 2; ++k)
+        if (b->graphs[k]) {
+            cudaGraphExecDestroy(b->graphs[k]);
+            b->graphs[k] = nullptr;
+        }
+}
+
+// graph k: every context at buffer set base ^ k
+static int batch_capture(sld_batch* b, int k) {
+    std::vector<int> saved(b->ctx.size());
+    for (size_t q = 0; q < b->ctx.size(); ++q) {
+        saved[q] = b->ctx[q]->cur;
+        use_set(b->ctx[q], b->base[q] ^ k);
+    }
+    cudaGraph_t g = nullptr;
+    int rc = SLD_OK;
+    if (cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = SLD_ERR_CUDA;
+    if (rc == SLD_OK) {
+        cudaEventRecord(b->root, b->st);
+        for (size_t q = 0; q < b->ctx.size(); ++q) {
+            sld_ctx* c = b->ctx[q];
+            cudaStreamWaitEvent(c->st, b->root, 0);
+            enqueue_step(c);
+            cudaEventRecord(b->join[q], c->st);
+            cudaStreamWaitEvent(b->st, b->join[q], 0);
+        }
+        if (cudaStreamEndCapture(b->st, &g) != cudaSuccess) rc = SLD_ERR_CUDA;
+    }
+    if (rc == SLD_OK && cudaGraphInstantiate(&b->graphs[k], g, 0) != cudaSuccess) rc = SLD_ERR_CUDA;
+    if (g) cudaGraphDestroy(g);
+    for (size_t q = 0; q < b->ctx.size(); ++q) use_set(b->ctx[q], saved[q]);
+    return rc;
+}
+
+int sld_batch_create(sld_batch** out, sld_ctx* const* ctxs, int n) {
+    if (!out || !ctxs || n <= 0) return SLD_ERR_ARG;
+    *out = nullptr;
+    std::vector<sld_ctx*> v(ctxs, ctxs + n);
+    for (int q = 0; q < n; ++q) {
+        if (!v[q] || v[q]->P.device != v[0]->P.device) return SLD_ERR_ARG;
+        for (int r = 0; r < q; ++r)
+            if (v[r] == v[q]) return SLD_ERR_ARG;
+    }
+    sld_batch* b = new (std::nothrow) sld_batch;
+    if (!b) return SLD_ERR_NOMEM;
+    b->ctx = v;
+    b->device = v[0]->P.device;
+    b->join.assign(n, nullptr);
+    bool ok = cudaSetDevice(b->device) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->root, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreate(&b->ev0) == cudaSuccess && cudaEventCreate(&b->ev1) == cudaSuccess;
+    for (int q = 0; q < n && ok; ++q)
+        ok = cudaEventCreateWithFlags(&b->join[q], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        sld_batch_destroy(b);
+        return SLD_ERR_CUDA;
+    }
+    *out = b;
+    return SLD_OK;
+}
+
+int sld_batch_run(sld_batch* b, int nsteps) {
+    if (!b || nsteps < 0) return SLD_ERR_ARG;
+    CK(cudaSetDevice(b->device));
+    // the batch stream follows whatever is queued on each context's stream
+    for (size_t q = 0; q < b->ctx.size(); ++q) {
+        sld_ctx* c = b->ctx[q];
+        fresh_lists(c);
+        CK(cudaEventRecord(b->join[q], c->st));
+        CK(cudaStreamWaitEvent(b->st, b->join[q], 0));
+    }
+    // graphs are made for the contexts' buffer sets relative to each other;
+    // a context stepped on its own since then has shifted, so remake them
+    bool same = b->base.size() == b->ctx.size();
+    for (size_t q = 0; same && q < b->ctx.size(); ++q)
+        same = (b->ctx[q]->cur ^ b->base[q]) == (b->ctx[0]->cur ^ b->base[0]);
+    if (!same) {
+        batch_drop_graphs(b);
+        b->base.resize(b->ctx.size());
+        for (size_t q = 0; q < b->ctx.size(); ++q) b->base[q] = b->ctx[q]->cur;
+    }
+    for (int k = 0; k < 2; ++k)
+        if (!b->graphs[k]) {
+            int rc = batch_capture(b, k);
+            if (rc) return rc;
+        }
+    int k = b->ctx[0]->cur ^ b->base[0];
+    CK(cudaEventRecord(b->ev0, b->st));
+    for (int s = 0; s < nsteps; ++s) {
+        CK(cudaGraphLaunch(b->graphs[k], b->st));
+        for (sld_ctx* c : b->ctx) use_set(c, 1 - c->cur);
+        k ^= 1;
+    }
+    CK(cudaEventRecord(b->ev1, b->st));
+    // later work on each context follows the batch
+    CK(cudaEventRecord(b->done, b->st));
+    for (sld_ctx* c : b->ctx) CK(cudaStreamWaitEvent(c->st, b->done, 0));
+    return launch_status();
+}
+
+int sld_batch_last_run_ms(sld_batch* b, double* out) {
+    if (!b || !out) return SLD_ERR_ARG;
+    CK(cudaEventSynchronize(b->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    *out = ms;
+    return SLD_OK;
+}
+
+void sld_batch_destroy(sld_batch* b) {
+    if (!b) return;
+    if (b->st) cudaStreamSynchronize(b->st);
+    batch_drop_graphs(b);
+    for (cudaEvent_t e : b->join)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : {b->root, b->done, b->ev0, b->ev1})
+        if (e) cudaEventDestroy(e);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
 }
 
 int sld_profile_step(sld_ctx* c, double* ms) {

@@ -61,6 +61,7 @@ struct Dev {
     int natom, nx, ny, nz, ncells;
     int tx, ty, tz, nte, te_mesh;
     unsigned seed;
+    unsigned replica;             // second word of the Philox key
     int spinlang, lattlang, eltemp, localcolmot, renormalize, print_every;
     int te_nloop;
     int small_grid;               // a link-cell axis of 3: every pair gets the minimum image

@@ -44,6 +44,7 @@ extern "C" int sld_read_variables(const char* path, sld_params* P) {
         else if (key == "te_nloop") P->te_nloop = iv;
         else if (key == "precision") P->precision = (val == "split" || iv == 1) ? SLD_SPLIT : SLD_FP64;
         else if (key == "current_device") P->device = iv;
+        else if (key == "replica") P->replica = iv;
     }
     return SLD_OK;
 }

@@ -45,7 +45,7 @@ class Params(C.Structure):
         ("localcolmot", C.c_int), ("renormalize_energy", C.c_int),
         ("te_mesh", C.c_int), ("te_nloop", C.c_int),
         ("interval_of_print_out", C.c_int), ("precision", C.c_int),
-        ("device", C.c_int),
+        ("device", C.c_int), ("replica", C.c_int),
     ]
 
 
@@ -85,6 +85,11 @@ def lib():
         L.sld_last_run_ms.argtypes = [vp, P]
         L.sld_profile_step.argtypes = [vp, P]
         L.sld_step_kernel_count.argtypes = [vp, C.POINTER(C.c_int)]
+        L.sld_batch_create.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int]
+        L.sld_batch_run.argtypes = [vp, C.c_int]
+        L.sld_batch_last_run_ms.argtypes = [vp, P]
+        L.sld_batch_destroy.argtypes = [vp]
+        L.sld_batch_destroy.restype = None
         L.sld_error_string.argtypes = [C.c_int]
         L.sld_error_string.restype = C.c_char_p
         _lib = L
@@ -102,7 +107,7 @@ def _check(rc, where):
 
 def make_params(params, *, spinlang=False, lattlang=False, eltemp=False,
                 localcolmot=False, renormalize=False, te_mesh=0, te_nloop=50,
-                precision=FP64, device=0, interval_of_print_out=1):
+                precision=FP64, device=0, interval_of_print_out=1, replica=0):
     """sld_params from a variables.in-style dict plus the control switches."""
     P = Params()
     lib().sld_params_default(C.byref(P))
@@ -118,6 +123,7 @@ def make_params(params, *, spinlang=False, lattlang=False, eltemp=False,
     P.te_mesh, P.te_nloop = int(te_mesh), int(te_nloop)
     P.precision, P.device = int(precision), int(device)
     P.interval_of_print_out = int(interval_of_print_out)
+    P.replica = int(replica)
     return P
 
 
@@ -229,6 +235,36 @@ class Engine:
         out = np.empty(1, np.float64)
         _check(self.L.sld_last_run_ms(self.h, _dp(out)), "last_run_ms")
         return float(out[0])
+
+
+class Batch:
+    """Several engines (independent replicas on one device) advanced
+    together: each step is one CUDA graph holding every engine's step.  Each
+    engine ends as if it had run alone; destroy the batch before its engines."""
+
+    def __init__(self, engines):
+        self.L = lib()
+        self.engines = list(engines)
+        arr = (C.c_void_p * len(self.engines))(*[e.h for e in self.engines])
+        h = C.c_void_p()
+        _check(self.L.sld_batch_create(C.byref(h), arr, len(self.engines)), "batch_create")
+        self.h = h
+
+    def run(self, nsteps):
+        _check(self.L.sld_batch_run(self.h, int(nsteps)), "batch_run")
+
+    def last_run_ms(self):
+        out = np.empty(1, np.float64)
+        _check(self.L.sld_batch_last_run_ms(self.h, _dp(out)), "batch_last_run_ms")
+        return float(out[0])
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.sld_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 def header_symbols(path=HEADER):
