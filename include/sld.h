@@ -92,6 +92,8 @@ typedef struct {
                                     Philox key is (random_seed, replica), so
                                     replicas of one seed draw independent
                                     noise (0 for a single system) */
+    int interval_of_config_out;  /* con-/cel- file interval (write_config.cpp:33)
+                                                                  default.h:65 */
 } sld_params;
 
 typedef struct sld_ctx sld_ctx;
@@ -160,6 +162,37 @@ int sld_get_cell_lists(sld_ctx* ctx, int* out);
    out[0..9] = <pe>, <ke>, <me>, <me0>, <Ee>, Tl (K), <Te> (K), <sx>,
    <sy>, <sz>. */
 int sld_averages(sld_ctx* ctx, double* out10);
+
+/* Print-out of check(int current_step) (check.cpp:31-47): when
+   (current_step + 1) % interval_of_print_out == 0, appends one line each to
+   enr-<out_body>.dat (step, time, <pe>, <ke>, <me>, <me0>[, <Ee>]),
+   tmp- (step, time, Tl, Ts_R, Ts_L[, <Te>]), str- (step, time, box, density,
+   mean and six components of the stress in GPa), prs- (step, time, box,
+   density, pressure in GPa) and spn- (step, time, <s>, |<s>|, <m>, |<m>|),
+   in the directory dir (NULL or "": the working directory), as
+   check_energy/temperature/stress/pressure/spin_CPU.cpp:35-79 do.  Call it
+   after sld_run with the index of the last step run (-1 before the first).
+   The energy renormalisation that check_energy performs runs inside the step
+   (sld_run); with it, enr- holds the averages formed before that step's
+   renormalisation, as the reference prints.  Without eltemp, Ts_R and Ts_L
+   come from freshly computed fields, which, as in the reference, overwrite
+   Heff_H, Heff_L and sum_Jij_sj (check_temperature_CPU.cpp:58-116). */
+int sld_check(sld_ctx* ctx, const char* dir, const char* out_body, int current_step);
+
+/* write_config(int current_step) (write_config.cpp:31-169): when
+   current_step is -1 (file 0000), -2 (file 9999) or
+   (current_step + 1) % interval_of_config_out == 0 (file
+   current_step / interval_of_config_out + 1), writes
+   con-<out_body>_NNNN.dat (natom, time, "SLDHL"; box; per atom: index,
+   element, r, p, f, stress (6), rho, ke, pe, s, |s|, Heff_H, Heff_L, me,
+   me0, local volume) and, with eltemp, cel-<out_body>_NNNN.dat (per cell,
+   x-major: centre, Te, Tl, Ts_R, Ts_L; the Te mesh's nodes when te_mesh >
+   0).  The reference prints the x component of Heff_H and Heff_L in their y
+   columns (write_config.cpp:120,123); this writes the y component unless
+   flags holds SLD_WRITE_HEFF_AS_REFERENCE. */
+#define SLD_WRITE_HEFF_AS_REFERENCE 1
+int sld_write_config(sld_ctx* ctx, const char* dir, const char* out_body, int current_step,
+                     int flags);
 
 /* out[0..5] = natom, ncells, ngroups, n_te_cells, nx, ny (link cells). */
 int sld_info(sld_ctx* ctx, int* out6);

@@ -19,6 +19,13 @@
  * and one "core" op is the body of the reference main loop
  * (spilady.cpp:50-57): core(step); total_time += step; and, because it
  * changes Te, the check_energy() call of check() when renormalizeEnergy is on.
+ * The "step" op is the whole body with the reference's output: core(step);
+ * total_time += step; check(step); write_config(step) (scale() is a no-op
+ * without its barostat/thermostat switches).  check() appends to
+ * enr-/tmp-/str-/prs-/spn-ref.dat and write_config() writes
+ * con-ref_NNNN.dat (and cel-ref_NNNN.dat with eltemp) in the working
+ * directory, with interval_of_print_out 1 and interval_of_config_out as set
+ * by the config-interval op (default 1).
  *
  * Job file (little endian):
  *   int32  magic 0x534c4431, natom, omp_threads, n_te, n_ops
@@ -41,7 +48,8 @@
 enum {
     OP_DUMP = 0, OP_LINKS = 1, OP_RHO = 2, OP_FORCE = 3, OP_DS = 4,
     OP_DP = 5, OP_DR = 6, OP_DTE = 7, OP_TEMP = 8, OP_CORE = 9,
-    OP_CHECK_ENERGY = 10
+    OP_CHECK_ENERGY = 10, OP_STEP = 11, OP_CONFIG_INTERVAL = 12, OP_WRITE_CONFIG = 13,
+    OP_CHECK = 14
 };
 
 static double g_last_wall = 0.0;
@@ -138,6 +146,7 @@ int main(int argc, char** argv) {
     out_body = (char*)malloc(8);
     strcpy(out_body, "ref");
     interval_of_print_out = 1;
+    interval_of_config_out = 1;
 
     d.xx = pr[0]; d.yx = pr[1]; d.yy = pr[2]; d.zx = pr[3]; d.zy = pr[4]; d.zz = pr[5];
     step = pr[6];
@@ -251,6 +260,21 @@ int main(int argc, char** argv) {
             break;
         }
         case OP_CHECK_ENERGY: check_energy((int)arg); break;
+        case OP_STEP: {
+            long nsteps = (long)arg;
+            for (long j = 0; j < nsteps; ++j) {
+                int cur = (int)g_steps_done;
+                core(cur);
+                total_time += step;
+                check(cur);
+                write_config(cur);
+                ++g_steps_done;
+            }
+            break;
+        }
+        case OP_CONFIG_INTERVAL: interval_of_config_out = (int)arg; break;
+        case OP_WRITE_CONFIG: write_config((int)arg); break;
+        case OP_CHECK: check((int)arg); break;
         default: die("unknown op");
         }
     }

@@ -19,7 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
 OP_DUMP, OP_LINKS, OP_RHO, OP_FORCE, OP_DS, OP_DP, OP_DR, OP_DTE, OP_TEMP, \
-    OP_CORE, OP_CHECK_ENERGY = range(11)
+    OP_CORE, OP_CHECK_ENERGY, OP_STEP, OP_CONFIG_INTERVAL, OP_WRITE_CONFIG, \
+    OP_CHECK = range(15)
 
 ATOM_FIELDS = [
     "rx", "ry", "rz", "px", "py", "pz", "fx", "fy", "fz", "sx", "sy", "sz",
@@ -121,8 +122,11 @@ def read_dumps(path):
     return out
 
 
-def run(mode, params, r, p, s, te=None, ops=(), threads=1, timeout=3600):
-    """Run the reference harness in a scratch directory; return the dumps."""
+def run(mode, params, r, p, s, te=None, ops=(), threads=1, timeout=3600,
+        files=False):
+    """Run the reference harness in a scratch directory; return the dumps,
+    and with ``files`` also a dict of the ``.dat`` files the reference wrote
+    there (name -> text: its enr-/tmp-/.../con-/cel- output)."""
     exe = binary(mode)
     if not os.access(exe, os.X_OK):
         raise FileNotFoundError(f"{exe} missing: run sh oracle/ref/build.sh")
@@ -137,4 +141,12 @@ def run(mode, params, r, p, s, te=None, ops=(), threads=1, timeout=3600):
         if res.returncode != 0:
             raise RuntimeError(f"reference harness failed ({res.returncode}):"
                                f" {res.stderr.decode()[-2000:]}")
-        return read_dumps(out)
+        dumps = read_dumps(out)
+        if not files:
+            return dumps
+        texts = {}
+        for name in sorted(os.listdir(tmp)):
+            if name.endswith(".dat"):
+                with open(os.path.join(tmp, name)) as fh:
+                    texts[name] = fh.read()
+        return dumps, texts

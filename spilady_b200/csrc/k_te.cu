@@ -63,6 +63,9 @@ __device__ __forceinline__ void temp_finish(const Dev& D, int k, double n, doubl
     }
     D.TsR[k] = Rup / Rdn / 2.0 / SLD_BOLTZ;
     D.TsL[k] = Lup / Ldn / SLD_BOLTZ;
+    // the cell sums check_temperature adds up (check_temperature_CPU.cpp:49-55,86-92)
+    double* q = D.trl + 4 * (size_t)k;
+    q[0] = Rup; q[1] = Rdn; q[2] = Lup; q[3] = Ldn;
     D.Ges[k] = SLD_BOLTZ * D.gamma_S_HL * Ldn / per;
 }
 
@@ -198,6 +201,10 @@ __global__ void __launch_bounds__(1024) k_renorm(Dev D, int nb, int mode) {
             err = t - D.ctl->initial_ave_energy;
         }
         err_s = err;
+        // what check_energy prints for this step (check_energy_CPU.cpp:113-130)
+        D.ctl->chk[0] = pe; D.ctl->chk[1] = ke; D.ctl->chk[2] = me; D.ctl->chk[3] = me0;
+        D.ctl->chk[4] = Ee;
+        D.ctl->chk_tag = mode == 0 ? 1 : cur + 2;
     }
     __syncthreads();
     double err = err_s;
@@ -296,4 +303,81 @@ void launch_virial(const Dev& D, cudaStream_t st) {
     int nb = div_up(D.natom, 256);
     k_vir_partials<<<nb, 256, 0, st>>>(D);
     k_vir_final<<<1, 1024, 0, st>>>(D, nb);
+}
+
+// ---------------------------------------------------------------------
+// Sums behind the print-out lines of check() (check.cpp:31-47): per-atom
+// energies (check_energy_CPU.cpp:35-60), spins (check_spin_CPU.cpp:35-50),
+// virial and stresses (check_pressure_CPU.cpp:35-38,
+// check_stress_CPU.cpp:35-50), and the spin-temperature sums
+// (check_temperature_CPU.cpp:43-130).  Without eltemp the reference forms the
+// latter from freshly computed fields, overwriting Heff_H, Heff_L and
+// sum_Jij_sj of every atom; ATOM_TEMP does the same through temp_atom.  With
+// eltemp it adds up the cell sums of the last calculate_temperature.
+// Fixed-order block sums, so a check is bit-reproducible.
+
+template <bool ATOM_TEMP>
+__global__ void __launch_bounds__(256) k_check_partials(Dev D, double* part) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[SLD_CHK_ATOM];
+#pragma unroll
+    for (int k = 0; k < SLD_CHK_ATOM; ++k) v[k] = 0.0;
+    if (i < D.natom) {
+        v[SLD_CHK_PE] = D.pe[i]; v[SLD_CHK_KE] = D.ke[i];
+        v[SLD_CHK_ME] = D.me[i]; v[SLD_CHK_ME0] = D.me0[i];
+        double4 s = D.s[i];
+        v[SLD_CHK_SX] = s.x; v[SLD_CHK_SY] = s.y; v[SLD_CHK_SZ] = s.z;
+        v[SLD_CHK_VIR] = D.vir[i];
+        const double* st = D.stress + 6 * (size_t)i;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) v[SLD_CHK_STRESS + k] = st[k];
+        if (ATOM_TEMP)
+            temp_atom(D, i, v[SLD_CHK_RUP], v[SLD_CHK_RDN], v[SLD_CHK_LUP], v[SLD_CHK_LDN]);
+    }
+    __shared__ double sh[32];
+    for (int k = 0; k < SLD_CHK_ATOM; ++k) {
+        double t = block_sum(v[k], sh);
+        if (threadIdx.x == 0) part[SLD_CHK_ATOM * (size_t)blockIdx.x + k] = t;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_check_final(Dev D, const double* part, int nb,
+                                                      bool atom_temp, double* out) {
+    __shared__ double sh[32];
+    for (int k = 0; k < SLD_CHK_ATOM; ++k) {
+        double a = 0;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) a += part[SLD_CHK_ATOM * (size_t)b + k];
+        a = block_sum(a, sh);
+        if (threadIdx.x == 0) out[k] = a;
+    }
+    if (!D.eltemp) return;
+    double per = (double)D.natom / (double)D.nte;
+    double r[4] = {0, 0, 0, 0}, te = 0, ee = 0;
+    for (int k = threadIdx.x; k < D.nte; k += blockDim.x) {
+        const double* q = D.trl + 4 * (size_t)k;
+        r[0] += q[0]; r[1] += q[1]; r[2] += q[2]; r[3] += q[3];
+        double t = D.Te[k];
+        te += t;
+        ee += per * te_to_Ee(t);
+    }
+    for (int k = 0; k < 4; ++k) r[k] = block_sum(r[k], sh);
+    te = block_sum(te, sh);
+    ee = block_sum(ee, sh);
+    if (threadIdx.x == 0) {
+        if (!atom_temp)
+            for (int k = 0; k < 4; ++k) out[SLD_CHK_RUP + k] = r[k];
+        out[SLD_CHK_TE] = te;
+        out[SLD_CHK_EE] = ee;
+    }
+}
+
+// part: SLD_CHK_ATOM doubles per 256 atoms; out: SLD_CHK_N doubles
+void launch_check_sums(const Dev& D, cudaStream_t st, double* part, double* out) {
+    int nb = div_up(D.natom, 256);
+    bool atom_temp = !D.eltemp;
+    if (atom_temp)
+        k_check_partials<true><<<nb, 256, 0, st>>>(D, part);
+    else
+        k_check_partials<false><<<nb, 256, 0, st>>>(D, part);
+    k_check_final<<<1, 1024, 0, st>>>(D, part, nb, atom_temp, out);
 }

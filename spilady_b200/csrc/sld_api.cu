@@ -46,6 +46,7 @@ struct sld_ctx {
     int* d_te_gstart = nullptr;
     unsigned char* d_te_color = nullptr;
     double* d_avg = nullptr;
+    double* d_chk = nullptr;           // check() sums: per-block partials, then totals
     cudaStream_t st = nullptr;
     cudaStream_t st2 = nullptr;        // second branch of the step graph
     cudaEvent_t fork_ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -307,6 +308,7 @@ int sld_params_default(sld_params* o) {
     o->random_seed = 1234;
     o->te_nloop = 50;
     o->interval_of_print_out = 1;
+    o->interval_of_config_out = 1000;
     o->precision = SLD_FP64;
     return SLD_OK;
 }
@@ -322,6 +324,7 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     c->P = *prm;
     if (c->P.te_nloop <= 0) c->P.te_nloop = 50;
     if (c->P.interval_of_print_out <= 0) c->P.interval_of_print_out = 1;
+    if (c->P.interval_of_config_out <= 0) c->P.interval_of_config_out = 1000;
 
     // geometry, link cells, colour groups, initial order (host)
     std::vector<double> r0(r, r + 3 * (size_t)natom);
@@ -455,10 +458,12 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     int nte = G.nte;
     ok = ok && c->alloc(&D.Te, nte) == 0 && c->alloc(&D.Ee, nte) == 0 && c->alloc(&D.Tl, nte) == 0 &&
          c->alloc(&D.TsR, nte) == 0 && c->alloc(&D.TsL, nte) == 0 && c->alloc(&D.Gel, nte) == 0 &&
-         c->alloc(&D.Ges, nte) == 0 && c->alloc(&D.acc, 9 * (size_t)nte) == 0;
+         c->alloc(&D.Ges, nte) == 0 && c->alloc(&D.acc, 9 * (size_t)nte) == 0 &&
+         c->alloc(&D.trl, 4 * (size_t)nte) == 0;
     c->red_cap = std::max(div_up(natom, 128), div_up(G.ncells, 128)) + 8;
     ok = ok && c->alloc(&D.red, 8 * (size_t)c->red_cap) == 0;
     ok = ok && c->alloc(&D.ctl, 1) == 0 && c->alloc(&c->d_avg, 16) == 0;
+    ok = ok && c->alloc(&c->d_chk, SLD_CHK_ATOM * (size_t)div_up(natom, 256) + SLD_CHK_N) == 0;
     ok = ok && c->alloc(&c->d_gcells, (size_t)G.ncells) == 0;
     ok = ok && c->alloc(&c->d_te_gcells, (size_t)nte) == 0 &&
          c->alloc(&c->d_te_gstart, G.te_gstart.size()) == 0 &&
@@ -992,6 +997,163 @@ int sld_total_time(sld_ctx* c, double* out) {
     CK(cudaMemcpyAsync(out, &c->D.ctl->total_time, sizeof(double), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     return SLD_OK;
+}
+
+// check() (check.cpp:31-47) without its renormalisation, which the step
+// itself runs: one line each appended to enr-, tmp-, str-, prs- and spn-,
+// in that order, with the reference's expressions (check_energy_CPU.cpp:35-138,
+// check_temperature_CPU.cpp:35-157, check_stress_CPU.cpp:35-79,
+// check_pressure_CPU.cpp:35-59, check_spin_CPU.cpp:35-76).
+int sld_check(sld_ctx* c, const char* dir, const char* out_body, int current_step) {
+    if (!c || !out_body) return SLD_ERR_ARG;
+    if ((current_step + 1) % c->P.interval_of_print_out != 0) return SLD_OK;
+    const Dev& D = c->D;
+    double* part = c->d_chk;
+    double* tot = c->d_chk + SLD_CHK_ATOM * (size_t)div_up(D.natom, 256);
+    launch_check_sums(D, c->st, part, tot);
+    int rc = launch_status();
+    if (rc) return rc;
+    double S[SLD_CHK_N];
+    Ctl ctl;
+    CK(cudaMemcpyAsync(S, tot, sizeof S, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(&ctl, D.ctl, sizeof ctl, cudaMemcpyDeviceToHost, c->st));
+    rc = check_flags(c);
+    if (rc) return rc;
+
+    const double n = (double)D.natom, t = ctl.total_time;
+    const double* d = c->G.d;
+    const bool el = c->P.eltemp != 0;
+    const double density = n / c->G.box_volume;
+    double v[16];
+    int k = 0;
+
+    // check_energy: with renormalizeEnergy the averages it formed before
+    // moving the error into the electrons at this step
+    double pe = S[SLD_CHK_PE] / n, ke = S[SLD_CHK_KE] / n;
+    double me = S[SLD_CHK_ME] / n, me0 = S[SLD_CHK_ME0] / n, Ee = S[SLD_CHK_EE] / n;
+    if (el && c->P.renormalize_energy && ctl.chk_tag == (long long)current_step + 2) {
+        pe = ctl.chk[0]; ke = ctl.chk[1]; me = ctl.chk[2]; me0 = ctl.chk[3]; Ee = ctl.chk[4];
+    }
+    v[k++] = t; v[k++] = pe; v[k++] = ke; v[k++] = me; v[k++] = me0;
+    if (el) v[k++] = Ee;
+    rc = sld::append_line(sld::out_path(dir, "enr-", out_body, -1), current_step, v, k);
+    if (rc) return rc;
+
+    // check_temperature
+    k = 0;
+    v[k++] = t;
+    v[k++] = S[SLD_CHK_KE] * 2e0 / 3e0 / n / kBoltz;
+    v[k++] = S[SLD_CHK_RUP] / S[SLD_CHK_RDN] / 2e0 / kBoltz;
+    v[k++] = S[SLD_CHK_LUP] / S[SLD_CHK_LDN] / kBoltz;
+    if (el) v[k++] = S[SLD_CHK_TE] / (double)D.nte / kBoltz;
+    rc = sld::append_line(sld::out_path(dir, "tmp-", out_body, -1), current_step, v, k);
+    if (rc) return rc;
+
+    // check_stress: per-atom stresses in eV/A^3, averaged and converted to GPa
+    double st[6];
+    for (int q = 0; q < 6; ++q) st[q] = S[SLD_CHK_STRESS + q] * (160.217653e0 / n);
+    k = 0;
+    v[k++] = t;
+    for (int q = 0; q < 6; ++q) v[k++] = d[q];
+    v[k++] = density;
+    v[k++] = (st[0] + st[1] + st[2]) / 3e0;
+    for (int q = 0; q < 6; ++q) v[k++] = st[q];
+    rc = sld::append_line(sld::out_path(dir, "str-", out_body, -1), current_step, v, k);
+    if (rc) return rc;
+
+    // check_pressure
+    double tmp = 2e0 / 3e0 * S[SLD_CHK_KE] / n;
+    double pressure0 = density * (tmp - S[SLD_CHK_VIR] / (3e0 * n));
+    pressure0 *= 160.217653e0;
+    k = 0;
+    v[k++] = t;
+    for (int q = 0; q < 6; ++q) v[k++] = d[q];
+    v[k++] = density;
+    v[k++] = pressure0;
+    rc = sld::append_line(sld::out_path(dir, "prs-", out_body, -1), current_step, v, k);
+    if (rc) return rc;
+
+    // check_spin: magnetisation m = -g s (spilady.h:60)
+    const double el_g = 2.0023193043622e0;
+    double ax = S[SLD_CHK_SX] / n, ay = S[SLD_CHK_SY] / n, az = S[SLD_CHK_SZ] / n;
+    double mx = -el_g * ax, my = -el_g * ay, mz = -el_g * az;
+    k = 0;
+    v[k++] = t;
+    v[k++] = ax; v[k++] = ay; v[k++] = az;
+    v[k++] = std::sqrt(ax * ax + ay * ay + az * az);
+    v[k++] = mx; v[k++] = my; v[k++] = mz;
+    v[k++] = std::sqrt(mx * mx + my * my + mz * mz);
+    return sld::append_line(sld::out_path(dir, "spn-", out_body, -1), current_step, v, k);
+}
+
+// write_config (write_config.cpp:31-169): con-<out_body>_NNNN.dat and, with
+// eltemp, cel-<out_body>_NNNN.dat.
+int sld_write_config(sld_ctx* c, const char* dir, const char* out_body, int current_step,
+                     int flags) {
+    if (!c || !out_body) return SLD_ERR_ARG;
+    const int every = c->P.interval_of_config_out;
+    if (!(current_step == -1 || current_step == -2 || (current_step + 1) % every == 0))
+        return SLD_OK;
+    int n_output = current_step == -1 ? 0 : current_step == -2 ? 9999 : current_step / every + 1;
+    double t = 0;
+    int rc = sld_total_time(c, &t);
+    if (rc) return rc;
+    const long n = c->D.natom;
+
+    // columns: r p f stress(6) rho ke pe s s0 Heff_H Heff_L me me0 local_volume
+    enum { NCOL = 31 };
+    struct Col { const char* field; int width; int at; };
+    const Col cols[] = {{"r", 3, 0},    {"p", 3, 3},    {"f", 3, 6},   {"stress", 6, 9},
+                        {"rho", 1, 15}, {"ke", 1, 16},  {"pe", 1, 17}, {"s", 3, 18},
+                        {"s0", 1, 21},  {"H", 3, 22},   {"HL", 3, 25}, {"me", 1, 28},
+                        {"me0", 1, 29}, {"local_volume", 1, 30}};
+    std::vector<double> table((size_t)n * NCOL), tmp((size_t)n * 6);
+    for (const Col& col : cols) {
+        long got = sld_get(c, col.field, tmp.data(), (long)tmp.size());
+        if (got < 0) return (int)got;
+        for (long i = 0; i < n; ++i)
+            for (int w = 0; w < col.width; ++w)
+                table[(size_t)i * NCOL + col.at + w] = tmp[(size_t)i * col.width + w];
+    }
+    if (flags & SLD_WRITE_HEFF_AS_REFERENCE) {
+        // write_config.cpp:120,123 print the x component in the y column
+        for (long i = 0; i < n; ++i) {
+            double* row = &table[(size_t)i * NCOL];
+            row[23] = row[22];
+            row[26] = row[25];
+        }
+    }
+    rc = sld::write_con_file(sld::out_path(dir, "con-", out_body, n_output), n, t, c->G.d, "SLDHL",
+                             "Fe", NCOL, table.data());
+    if (rc || !c->P.eltemp) return rc;
+
+    // cel-: cells x-major (ix outermost), centre, Te (K), Tl, Ts_R, Ts_L
+    const auto& G = c->G;
+    const bool mesh = c->P.te_mesh > 0;
+    const int ax = mesh ? G.tx : G.nx, ay = mesh ? G.ty : G.ny, az = mesh ? G.tz : G.nz;
+    const long m = G.nte;
+    std::vector<double> Te(m), Tl(m), TsR(m), TsL(m);
+    const char* names[4] = {"Te", "Tl", "Ts_R", "Ts_L"};
+    double* dst[4] = {Te.data(), Tl.data(), TsR.data(), TsL.data()};
+    for (int q = 0; q < 4; ++q) {
+        long got = sld_get(c, names[q], dst[q], m);
+        if (got < 0) return (int)got;
+    }
+    const double* d = G.d;
+    std::vector<double> cel((size_t)m * 7);
+    size_t row = 0;
+    for (int ix = 0; ix < ax; ++ix)
+        for (int iy = 0; iy < ay; ++iy)
+            for (int iz = 0; iz < az; ++iz) {
+                long i = ix + (long)iy * ax + (long)iz * ax * ay;
+                double qx = (ix + 0.5) / ax, qy = (iy + 0.5) / ay, qz = (iz + 0.5) / az;
+                double* o = &cel[row++ * 7];
+                o[0] = d[0] * qx + d[1] * qy + d[3] * qz;
+                o[1] = d[2] * qy + d[4] * qz;
+                o[2] = d[5] * qz;
+                o[3] = Te[i]; o[4] = Tl[i]; o[5] = TsR[i]; o[6] = TsL[i];
+            }
+    return sld::write_cel_file(sld::out_path(dir, "cel-", out_body, n_output), m, t, d, 7, cel.data());
 }
 
 int sld_info(sld_ctx* c, int* o) {

@@ -40,6 +40,10 @@ struct Ctl {
     double ke_factor;
     double virial;
     double avg[8];                // last energy averages
+    // averages check_energy formed before its last renormalisation (pe, ke,
+    // me, me0, Ee per atom) and the step it ran at, as step + 2 (0: none)
+    double chk[5];
+    long long chk_tag;
 };
 
 // data of the quintic that joins the ZBL core to the cubic knots of the
@@ -87,6 +91,7 @@ struct Dev {
     int *cell_start, *cell_count, *cell_atoms, *cell_fill, *scan_tmp;
     // Te cells
     double *Te, *Ee, *Tl, *TsR, *TsL, *Gel, *Ges, *acc;   // acc: 9 per Te cell
+    double* trl;   // per Te cell: sum_R_up, sum_R_dn, sum_L_up, sum_L_dn
     int* te_count;
     const int *te_gcells, *te_gstart;
     const unsigned char* te_color;   // colour group of each Te cell
@@ -445,3 +450,12 @@ void launch_energy_check(const Dev& D, cudaStream_t st, int mode);
 void launch_advance(const Dev& D, cudaStream_t st, int epochs, int steps);
 void launch_averages(const Dev& D, cudaStream_t st, double* out_dev);
 void launch_virial(const Dev& D, cudaStream_t st);
+// slots of the check() sums (launch_check_sums): per-atom sums first
+enum {
+    SLD_CHK_PE, SLD_CHK_KE, SLD_CHK_ME, SLD_CHK_ME0, SLD_CHK_SX, SLD_CHK_SY, SLD_CHK_SZ,
+    SLD_CHK_VIR, SLD_CHK_STRESS,                       // 6: 11 22 33 12 23 31
+    SLD_CHK_RUP = SLD_CHK_STRESS + 6, SLD_CHK_RDN, SLD_CHK_LUP, SLD_CHK_LDN,
+    SLD_CHK_ATOM,                                      // per-atom sums end here
+    SLD_CHK_TE = SLD_CHK_ATOM, SLD_CHK_EE, SLD_CHK_N
+};
+void launch_check_sums(const Dev& D, cudaStream_t st, double* part, double* out);

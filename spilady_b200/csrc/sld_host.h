@@ -1,5 +1,6 @@
 // Host-side geometry: box, link cells, colour groups, the initial atom order.
 #pragma once
+#include <string>
 #include <vector>
 
 #include "../../include/sld.h"
@@ -28,5 +29,17 @@ void host_periodic(const HostGeom& G, double& x, double& y, double& z);
 // allocate_cells_CPU.cpp:33-125: greedy colouring of an nx*ny*nz periodic
 // grid with the 26-neighbour stencil, cells scanned in index order
 int colour_grid(int nx, int ny, int nz, std::vector<int>& gstart, std::vector<int>& gcells);
+
+// Output files in the reference's formats (sld_io.cpp).  out_path forms
+// <dir>/<prefix><body>[_NNNN].dat (n_output < 0: no number); append_line adds
+// "<step> v0 ... v(n-1)"; write_con_file writes a con- file (header, box,
+// one row "<i> <element> ..." per atom of the natom x ncols table);
+// write_cel_file a cel- file (one row per cell).
+std::string out_path(const char* dir, const char* prefix, const char* body, int n_output);
+int append_line(const std::string& path, int step, const double* v, int n);
+int write_con_file(const std::string& path, long natom, double total_time, const double* box,
+                   const char* type, const char* element, int ncols, const double* table);
+int write_cel_file(const std::string& path, long ncells, double total_time, const double* box,
+                   int ncols, const double* table);
 
 }  // namespace sld

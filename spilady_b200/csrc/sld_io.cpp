@@ -3,6 +3,10 @@
 //                  ignored), plus this engine's runtime switches
 //   con- files     read_config.cpp:39-116 (atoms configuration)
 //   readTe files   map_cells.cpp:33-39,136-150 (electron temperature per cell)
+// and the output files (written by sld_check / sld_write_config):
+//   enr- tmp- str- prs- spn- lines   check.cpp:31-47 and check_*_CPU.cpp
+//   con- cel- files                  write_config.cpp:31-169
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -10,9 +14,11 @@
 #include <fstream>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/sld.h"
+#include "sld_host.h"
 
 extern "C" int sld_read_variables(const char* path, sld_params* P) {
     if (!path || !P) return SLD_ERR_ARG;
@@ -34,6 +40,7 @@ extern "C" int sld_read_variables(const char* path, sld_params* P) {
         else if (key == "min_length_link_cell") P->min_length_link_cell = v;
         else if (key == "kappa_e") P->kappa_e = v;
         else if (key == "interval_of_print_out") P->interval_of_print_out = iv;
+        else if (key == "interval_of_config_out") P->interval_of_config_out = iv;
         // control.h switches, which the reference fixes at compile time
         else if (key == "spinlang") P->spinlang = iv;
         else if (key == "lattlang") P->lattlang = iv;
@@ -125,3 +132,114 @@ extern "C" int sld_create_from_config(sld_ctx** out, const sld_params* prm, cons
     return sld_create(out, &P, (int)natom, r.data(), p.data(), s.data(),
                       te.empty() ? nullptr : te.data());
 }
+
+// ---------------------------------------------------------------------
+// Output files (check.cpp, write_config.cpp).  Numbers are written as the
+// reference's streams write them, setiosflags(ios::scientific) with
+// setprecision(15): printf's "%.15e".
+
+namespace sld {
+
+std::string out_path(const char* dir, const char* prefix, const char* body, int n_output) {
+    std::string p;
+    if (dir && *dir) {
+        p = dir;
+        if (p.back() != '/') p += '/';
+    }
+    p += prefix;
+    p += body;
+    if (n_output >= 0) {
+        // write_config.cpp:48-58 forms the four digits by character
+        // arithmetic (n_output 9999 is the final write, write(-2))
+        char s[6] = {'_', (char)(n_output / 1000 + '0'), (char)((n_output % 1000) / 100 + '0'),
+                     (char)((n_output % 100) / 10 + '0'), (char)(n_output % 10 + '0'), '\0'};
+        p += s;
+    }
+    p += ".dat";
+    return p;
+}
+
+int append_line(const std::string& path, int step, const double* v, int n) {
+    FILE* f = std::fopen(path.c_str(), "a");
+    if (!f) return SLD_ERR_IO;
+    std::fprintf(f, "%d", step);
+    for (int k = 0; k < n; ++k) std::fprintf(f, " %.15e", v[k]);
+    std::fputc('\n', f);
+    return std::fclose(f) == 0 ? SLD_OK : SLD_ERR_IO;
+}
+
+namespace {
+
+// rows [r0, r1) of a table, formatted by up to T threads into one buffer per
+// thread, written in order; a row is "<i> <element> v0 ... v(n-1)\n" (con-)
+// or "v0 ... v(n-1) \n" (cel-, every value followed by a space)
+int write_rows(FILE* f, long nrows, int ncols, const double* table, const char* element) {
+    const long kBatch = 1L << 14;
+    unsigned T = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::string> buf(T);
+    for (long b0 = 0; b0 < nrows; b0 += kBatch * (long)T) {
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < T; ++t) {
+            th.emplace_back([&, t] {
+                std::string& o = buf[t];
+                o.clear();
+                long r0 = b0 + (long)t * kBatch, r1 = std::min(nrows, r0 + kBatch);
+                char num[40];
+                for (long r = r0; r < r1; ++r) {
+                    const double* v = table + (size_t)r * ncols;
+                    if (element) {
+                        int m = std::snprintf(num, sizeof num, "%ld ", r);
+                        o.append(num, m);
+                        o += element;
+                        for (int k = 0; k < ncols; ++k) {
+                            m = std::snprintf(num, sizeof num, " %.15e", v[k]);
+                            o.append(num, m);
+                        }
+                    } else {
+                        for (int k = 0; k < ncols; ++k) {
+                            int m = std::snprintf(num, sizeof num, "%.15e ", v[k]);
+                            o.append(num, m);
+                        }
+                    }
+                    o += '\n';
+                }
+            });
+        }
+        for (auto& x : th) x.join();
+        for (unsigned t = 0; t < T; ++t)
+            if (!buf[t].empty() && std::fwrite(buf[t].data(), 1, buf[t].size(), f) != buf[t].size())
+                return SLD_ERR_IO;
+    }
+    return SLD_OK;
+}
+
+void box_lines(FILE* f, const double* d) {
+    std::fprintf(f, "%.15e %.15e %.15e\n", d[0], d[1], d[2]);
+    std::fprintf(f, "%.15e %.15e %.15e\n", d[3], d[4], d[5]);
+}
+
+}  // namespace
+
+int write_con_file(const std::string& path, long natom, double total_time, const double* box,
+                   const char* type, const char* element, int ncols, const double* table) {
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) return SLD_ERR_IO;
+    std::fprintf(f, "%ld %.15e %s\n", natom, total_time, type);
+    box_lines(f, box);
+    int rc = write_rows(f, natom, ncols, table, element);
+    if (std::fclose(f) != 0 && rc == SLD_OK) rc = SLD_ERR_IO;
+    return rc;
+}
+
+int write_cel_file(const std::string& path, long ncells, double total_time, const double* box,
+                   int ncols, const double* table) {
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) return SLD_ERR_IO;
+    std::fprintf(f, "%ld %.15e\n", ncells, total_time);
+    box_lines(f, box);
+    int rc = write_rows(f, ncells, ncols, table, nullptr);
+    if (std::fclose(f) != 0 && rc == SLD_OK) rc = SLD_ERR_IO;
+    return rc;
+}
+
+}  // namespace sld

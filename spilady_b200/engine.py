@@ -46,6 +46,7 @@ class Params(C.Structure):
         ("te_mesh", C.c_int), ("te_nloop", C.c_int),
         ("interval_of_print_out", C.c_int), ("precision", C.c_int),
         ("device", C.c_int), ("replica", C.c_int),
+        ("interval_of_config_out", C.c_int),
     ]
 
 
@@ -90,6 +91,8 @@ def lib():
         L.sld_batch_last_run_ms.argtypes = [vp, P]
         L.sld_batch_destroy.argtypes = [vp]
         L.sld_batch_destroy.restype = None
+        L.sld_check.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int]
+        L.sld_write_config.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int, C.c_int]
         L.sld_error_string.argtypes = [C.c_int]
         L.sld_error_string.restype = C.c_char_p
         _lib = L
@@ -107,7 +110,8 @@ def _check(rc, where):
 
 def make_params(params, *, spinlang=False, lattlang=False, eltemp=False,
                 localcolmot=False, renormalize=False, te_mesh=0, te_nloop=50,
-                precision=FP64, device=0, interval_of_print_out=1, replica=0):
+                precision=FP64, device=0, interval_of_print_out=1, replica=0,
+                interval_of_config_out=1000):
     """sld_params from a variables.in-style dict plus the control switches."""
     P = Params()
     lib().sld_params_default(C.byref(P))
@@ -124,6 +128,7 @@ def make_params(params, *, spinlang=False, lattlang=False, eltemp=False,
     P.precision, P.device = int(precision), int(device)
     P.interval_of_print_out = int(interval_of_print_out)
     P.replica = int(replica)
+    P.interval_of_config_out = int(interval_of_config_out)
     return P
 
 
@@ -141,16 +146,33 @@ class Engine:
         r = np.ascontiguousarray(r, np.float64).reshape(-1, 3)
         p = np.ascontiguousarray(p, np.float64).reshape(-1, 3)
         s = np.ascontiguousarray(s, np.float64).reshape(-1, 3)
-        self.natom = r.shape[0]
         te_arr = None if te is None else np.ascontiguousarray(te, np.float64)
         h = C.c_void_p()
-        _check(L.sld_create(C.byref(h), C.byref(self.P), self.natom, _dp(r),
+        _check(L.sld_create(C.byref(h), C.byref(self.P), r.shape[0], _dp(r),
                             _dp(p), _dp(s), None if te_arr is None else _dp(te_arr)),
                "sld_create")
+        self._attach(h)
+
+    def _attach(self, h):
         self.h = h
         info = (C.c_int * 6)()
-        _check(L.sld_info(self.h, info), "sld_info")
+        _check(self.L.sld_info(self.h, info), "sld_info")
+        self.natom = info[0]
         self.ncells, self.ngroups, self.nte = info[1], info[2], info[3]
+
+    @classmethod
+    def from_config(cls, params, con_path, te_path=None, **switches):
+        """A system read from a con- file (read_config.cpp format) and,
+        optionally, a readTe file; box and natom come from the file."""
+        self = cls.__new__(cls)
+        self.L = lib()
+        self.P = make_params(params, **switches)
+        h = C.c_void_p()
+        _check(self.L.sld_create_from_config(
+            C.byref(h), C.byref(self.P), str(con_path).encode(),
+            None if te_path is None else str(te_path).encode()), "sld_create_from_config")
+        self._attach(h)
+        return self
 
     def close(self):
         if getattr(self, "h", None):
@@ -231,6 +253,17 @@ class Engine:
         _check(self.L.sld_step_kernel_count(self.h, C.byref(n)), "step_kernel_count")
         return n.value
 
+    def check(self, out_dir, out_body, current_step):
+        """check(current_step): append the enr-/tmp-/str-/prs-/spn- lines."""
+        _check(self.L.sld_check(self.h, str(out_dir).encode(), out_body.encode(),
+                                int(current_step)), "check")
+
+    def write_config(self, out_dir, out_body, current_step, heff_as_reference=False):
+        """write_config(current_step): con- (and cel-) files."""
+        _check(self.L.sld_write_config(self.h, str(out_dir).encode(), out_body.encode(),
+                                       int(current_step), 1 if heff_as_reference else 0),
+               "write_config")
+
     def last_run_ms(self):
         out = np.empty(1, np.float64)
         _check(self.L.sld_last_run_ms(self.h, _dp(out)), "last_run_ms")
@@ -252,6 +285,17 @@ class Batch:
 
     def run(self, nsteps):
         _check(self.L.sld_batch_run(self.h, int(nsteps)), "batch_run")
+
+    def check(self, out_dir, out_body, current_step):
+        """check(current_step): append the enr-/tmp-/str-/prs-/spn- lines."""
+        _check(self.L.sld_check(self.h, str(out_dir).encode(), out_body.encode(),
+                                int(current_step)), "check")
+
+    def write_config(self, out_dir, out_body, current_step, heff_as_reference=False):
+        """write_config(current_step): con- (and cel-) files."""
+        _check(self.L.sld_write_config(self.h, str(out_dir).encode(), out_body.encode(),
+                                       int(current_step), 1 if heff_as_reference else 0),
+               "write_config")
 
     def last_run_ms(self):
         out = np.empty(1, np.float64)
