@@ -94,6 +94,21 @@ typedef struct {
                                     noise (0 for a single system) */
     int interval_of_config_out;  /* con-/cel- file interval (write_config.cpp:33)
                                                                   default.h:65 */
+    /* sld_scale (scale.cpp:31-44): control.h's PRESSURE, STRESS and
+       changestep switches and their variables */
+    int pressure_control;        /* Berendsen barostat on the pressure
+                                    (scale_pressure_CPU.cpp:35-60) */
+    int stress_control;          /* Berendsen barostat on the stress tensor
+                                    (scale_stress_CPU.cpp:35-85) */
+    int change_step;             /* adaptive time step (scale_step_CPU.cpp:35-100) */
+    int interval_of_scale_pressure;  /*                           default.h:188 */
+    int interval_of_scale_stress;    /*                           default.h:179 */
+    double pressure;             /* target pressure, GPa          default.h:189 */
+    double stress[6];            /* target stresses, GPa: stress_xx yx yy zx zy zz
+                                                                  default.h:180-185 */
+    double baro_damping_time;    /* s                             default.h:192 */
+    double displace_limit;       /* Angstrom per step             default.h:218 */
+    double phi_limit;            /* rad per step                  default.h:219 */
 } sld_params;
 
 typedef struct sld_ctx sld_ctx;
@@ -193,6 +208,27 @@ int sld_check(sld_ctx* ctx, const char* dir, const char* out_body, int current_s
 #define SLD_WRITE_HEFF_AS_REFERENCE 1
 int sld_write_config(sld_ctx* ctx, const char* dir, const char* out_body, int current_step,
                      int flags);
+
+/* scale(int current_step) (scale.cpp:31-44), called after sld_check:
+   - stress_control, when (current_step + 1) % interval_of_scale_stress == 0:
+     the box and positions follow the stresses of the last sld_check
+     (scale_stress_CPU.cpp:35-85);
+   - pressure_control, when (current_step + 1) % interval_of_scale_pressure
+     == 0: the box and positions are scaled by the cube root of
+     1 + dt_since_last/baro_damping_time (P_last_check - pressure)/100 GPa
+     (scale_pressure_CPU.cpp:35-60);
+   - change_step: the time step becomes 0.8 of itself when an atom moved
+     more than displace_limit or a spin turned more than phi_limit in one
+     step, else 1.05 of itself (scale_step_CPU.cpp:35-100).
+   After a box change the next step uses exchange couplings of the new
+   positions and the densities of the old ones, as the reference does.
+   out3 (may be NULL) receives displace_max (Angstrom), phi_max (rad) and
+   the new time step (s), which the reference prints; without change_step
+   they are 0, 0 and the unchanged step.  With any of the three switches
+   set, sld_run launches each step's kernels directly instead of replaying
+   a graph, because the box and step change between steps; such contexts
+   cannot join a batch. */
+int sld_scale(sld_ctx* ctx, int current_step, double* out3);
 
 /* out[0..5] = natom, ncells, ngroups, n_te_cells, nx, ny (link cells). */
 int sld_info(sld_ctx* ctx, int* out6);

@@ -13,6 +13,8 @@
 #   nve     NVE spin-lattice (no thermostat)
 #   lang    + spinlang + lattlang        (Langevin spin and lattice)
 #   langte  + eltemp + localcolmot + renormalizeEnergy
+#   baro    NVE + PRESSURE + STRESS  (Berendsen barostats, scale.cpp)
+#   dtstep  NVE + changestep          (adaptive time step, scale_step_CPU.cpp)
 #
 # usage: sh oracle/ref/build.sh [reference_dir]
 set -e
@@ -28,7 +30,7 @@ mkdir -p "$OUT"
 CXX=${ORACLE_CXX:-g++}
 FLAGS="-O3 -fopenmp -U_FORTIFY_SOURCE -D_FORTIFY_SOURCE=0 -DCPU -DOMP -DSLDHL -w"
 
-for mode in nve lang langte; do
+for mode in nve lang langte baro dtstep; do
     src="$OUT/src_$mode"
     obj="$OUT/obj_$mode"
     mkdir -p "$src" "$obj"
@@ -48,6 +50,8 @@ for mode in nve lang langte; do
             echo "#define spinlang"; echo "#define lattlang"
             echo "#define eltemp"; echo "#define localcolmot"
             echo "#define renormalizeEnergy" ;;
+        baro) echo "#define PRESSURE"; echo "#define STRESS" ;;
+        dtstep) echo "#define changestep" ;;
         esac
     } > "$src/control.h.new"
     if ! cmp -s "$src/control.h.new" "$src/control.h"; then
@@ -67,4 +71,4 @@ for mode in nve lang langte; do
     for p in $pids; do wait "$p"; done
     $CXX -fopenmp "$obj"/*.o -o "$OUT/spilady_ref_$mode" -lm
 done
-echo "built: $OUT/spilady_ref_nve $OUT/spilady_ref_lang $OUT/spilady_ref_langte"
+echo "built: $(ls "$OUT"/spilady_ref_* | tr '\n' ' ')"

@@ -20,8 +20,9 @@
  * (spilady.cpp:50-57): core(step); total_time += step; and, because it
  * changes Te, the check_energy() call of check() when renormalizeEnergy is on.
  * The "step" op is the whole body with the reference's output: core(step);
- * total_time += step; check(step); write_config(step) (scale() is a no-op
- * without its barostat/thermostat switches).  check() appends to
+ * total_time += step; check(step); scale(step); write_config(step) (scale()
+ * does nothing without the PRESSURE, STRESS or changestep switches of the
+ * baro and dtstep builds).  check() appends to
  * enr-/tmp-/str-/prs-/spn-ref.dat and write_config() writes
  * con-ref_NNNN.dat (and cel-ref_NNNN.dat with eltemp) in the working
  * directory, with interval_of_print_out 1 and interval_of_config_out as set
@@ -49,7 +50,12 @@ enum {
     OP_DUMP = 0, OP_LINKS = 1, OP_RHO = 2, OP_FORCE = 3, OP_DS = 4,
     OP_DP = 5, OP_DR = 6, OP_DTE = 7, OP_TEMP = 8, OP_CORE = 9,
     OP_CHECK_ENERGY = 10, OP_STEP = 11, OP_CONFIG_INTERVAL = 12, OP_WRITE_CONFIG = 13,
-    OP_CHECK = 14
+    OP_CHECK = 14,
+    /* OP_SET + k sets input variable k (read_variables.cpp:197-241):
+       0 pressure, 1 baro_damping_time, 2-7 stress_xx yx yy zx zy zz,
+       8 interval_of_scale_pressure, 9 interval_of_scale_stress,
+       10 displace_limit, 11 phi_limit */
+    OP_SET = 100
 };
 
 static double g_last_wall = 0.0;
@@ -218,6 +224,12 @@ int main(int argc, char** argv) {
     calculate_temperature();
 #endif
     total_time = 0e0;
+#ifdef PRESSURE
+    last_total_time_pressure = total_time;   /* initial.cpp:92-97 */
+#endif
+#ifdef STRESS
+    last_total_time_stress = total_time;
+#endif
     initialize_random_number();
 #if defined eltemp && defined renormalizeEnergy
     check_energy(-1);
@@ -267,6 +279,7 @@ int main(int argc, char** argv) {
                 core(cur);
                 total_time += step;
                 check(cur);
+                scale(cur);
                 write_config(cur);
                 ++g_steps_done;
             }
@@ -275,6 +288,26 @@ int main(int argc, char** argv) {
         case OP_CONFIG_INTERVAL: interval_of_config_out = (int)arg; break;
         case OP_WRITE_CONFIG: write_config((int)arg); break;
         case OP_CHECK: check((int)arg); break;
+#ifdef PRESSURE
+        case OP_SET + 0: pressure = arg; break;
+        case OP_SET + 8: interval_of_scale_pressure = (int)arg; break;
+#endif
+#if defined STRESS || defined PRESSURE
+        case OP_SET + 1: baro_damping_time = arg; break;
+#endif
+#ifdef STRESS
+        case OP_SET + 2: stress_xx = arg; break;
+        case OP_SET + 3: stress_yx = arg; break;
+        case OP_SET + 4: stress_yy = arg; break;
+        case OP_SET + 5: stress_zx = arg; break;
+        case OP_SET + 6: stress_zy = arg; break;
+        case OP_SET + 7: stress_zz = arg; break;
+        case OP_SET + 9: interval_of_scale_stress = (int)arg; break;
+#endif
+#ifdef changestep
+        case OP_SET + 10: displace_limit = arg; break;
+        case OP_SET + 11: phi_limit = arg; break;
+#endif
         default: die("unknown op");
         }
     }

@@ -21,6 +21,17 @@ REF_DIR = os.path.join(HERE, "_ref")
 OP_DUMP, OP_LINKS, OP_RHO, OP_FORCE, OP_DS, OP_DP, OP_DR, OP_DTE, OP_TEMP, \
     OP_CORE, OP_CHECK_ENERGY, OP_STEP, OP_CONFIG_INTERVAL, OP_WRITE_CONFIG, \
     OP_CHECK = range(15)
+# OP_SET + k sets an input variable of the baro / dtstep builds (harness.cpp)
+OP_SET = 100
+SET_VARS = {"pressure": 0, "baro_damping_time": 1, "stress_xx": 2, "stress_yx": 3,
+            "stress_yy": 4, "stress_zx": 5, "stress_zy": 6, "stress_zz": 7,
+            "interval_of_scale_pressure": 8, "interval_of_scale_stress": 9,
+            "displace_limit": 10, "phi_limit": 11}
+
+
+def set_ops(**values):
+    """Ops that set the given input variables (names as in variables.in)."""
+    return [(OP_SET + SET_VARS[k], float(v)) for k, v in values.items()]
 
 ATOM_FIELDS = [
     "rx", "ry", "rz", "px", "py", "pz", "fx", "fy", "fz", "sx", "sy", "sz",

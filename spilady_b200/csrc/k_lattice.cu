@@ -299,3 +299,98 @@ void launch_load_state(const Dev& D, cudaStream_t st, const double* r, const dou
                        const double* s) {
     k_load_state<<<div_up(D.natom, 256), 256, 0, st>>>(D, r, p, s);
 }
+
+// ---------------------------------------------------------------------
+// Box rescaling of the barostats (scale.cpp:31-44).  D carries the new box.
+// Products and sums are rounded one by one, as the reference's expressions.
+
+// scale_pressure_CPU.cpp:57-59: r = factor r
+__global__ void __launch_bounds__(256) k_scale_positions(Dev D, double factor) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.natom) return;
+    double4 r = D.r[i];
+    double x = __dmul_rn(factor, r.x), y = __dmul_rn(factor, r.y), z = __dmul_rn(factor, r.z);
+    D.r[i] = make_double4(x, y, z, 0.0);
+    D.r32s[D.cell_slot[i]] = make_float4((float)x, (float)y, (float)z, 0.f);
+}
+
+// scale_stress_CPU.cpp:66-80: fractional coordinates from the old inverse
+// box, back to positions with the new box
+struct InvBox { double v[6]; };
+__global__ void __launch_bounds__(256) k_reshape_positions(Dev D, InvBox old) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.natom) return;
+    double4 r = D.r[i];
+    const double* I = old.v;
+    const double* d = D.d;
+    double qx = add3_rn(__dmul_rn(I[0], r.x), __dmul_rn(I[1], r.y), __dmul_rn(I[3], r.z));
+    double qy = __dadd_rn(__dmul_rn(I[2], r.y), __dmul_rn(I[4], r.z));
+    double qz = __dmul_rn(I[5], r.z);
+    double x = add3_rn(__dmul_rn(d[0], qx), __dmul_rn(d[1], qy), __dmul_rn(d[3], qz));
+    double y = __dadd_rn(__dmul_rn(d[2], qy), __dmul_rn(d[4], qz));
+    double z = __dmul_rn(d[5], qz);
+    D.r[i] = make_double4(x, y, z, 0.0);
+    D.r32s[D.cell_slot[i]] = make_float4((float)x, (float)y, (float)z, 0.f);
+}
+
+void launch_scale_positions(const Dev& D, cudaStream_t st, double factor) {
+    k_scale_positions<<<div_up(D.natom, 256), 256, 0, st>>>(D, factor);
+}
+
+void launch_reshape_positions(const Dev& D, cudaStream_t st, const double old_inv[6]) {
+    InvBox b;
+    for (int k = 0; k < 6; ++k) b.v[k] = old_inv[k];
+    k_reshape_positions<<<div_up(D.natom, 256), 256, 0, st>>>(D, b);
+}
+
+// scale_step_CPU.cpp:39-73: the largest |p|^2 and |Heff_H|^2 over the atoms
+__global__ void __launch_bounds__(256) k_max_partials(Dev D, double* part) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double a = 0.0, b = 0.0;
+    if (i < D.natom) {
+        double4 p = D.p[i], h = D.H[i];
+        a = add3_rn(__dmul_rn(p.x, p.x), __dmul_rn(p.y, p.y), __dmul_rn(p.z, p.z));
+        b = add3_rn(__dmul_rn(h.x, h.x), __dmul_rn(h.y, h.y), __dmul_rn(h.z, h.z));
+    }
+    __shared__ double sa[8], sb[8];
+    for (int o = 16; o > 0; o >>= 1) {
+        a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+        b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+    }
+    int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { sa[w] = a; sb[w] = b; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) { a = fmax(a, sa[k]); b = fmax(b, sb[k]); }
+        part[2 * (size_t)blockIdx.x] = a;
+        part[2 * (size_t)blockIdx.x + 1] = b;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_max_final(const double* part, int nb, double* out) {
+    double a = 0.0, b = 0.0;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+        a = fmax(a, part[2 * (size_t)k]);
+        b = fmax(b, part[2 * (size_t)k + 1]);
+    }
+    __shared__ double sa[32], sb[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+        b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+    }
+    int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { sa[w] = a; sb[w] = b; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) { a = fmax(a, sa[k]); b = fmax(b, sb[k]); }
+        out[0] = a;
+        out[1] = b;
+    }
+}
+
+// part: 2 doubles per 256 atoms; out: 2 doubles (max |p|^2, max |Heff_H|^2)
+void launch_max_p_h(const Dev& D, cudaStream_t st, double* part, double* out) {
+    int nb = div_up(D.natom, 256);
+    k_max_partials<<<nb, 256, 0, st>>>(D, part);
+    k_max_final<<<1, 1024, 0, st>>>(part, nb, out);
+}

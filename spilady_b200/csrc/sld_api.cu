@@ -47,6 +47,13 @@ struct sld_ctx {
     unsigned char* d_te_color = nullptr;
     double* d_avg = nullptr;
     double* d_chk = nullptr;           // check() sums: per-block partials, then totals
+    // what the last sld_check printed and the barostats read (check_pressure,
+    // check_stress), and the barostats' clocks (initial.cpp:92-97)
+    double pressure0 = 0.0, ave_stress[6] = {0, 0, 0, 0, 0, 0};
+    double last_t_pressure = 0.0, last_t_stress = 0.0;
+    // box volume of the last force pass: its local volume V/N per atom
+    // (calculate_force_energy_CPU.cpp:276) stays until the next force pass
+    double force_volume = 0.0;
     cudaStream_t st = nullptr;
     cudaStream_t st2 = nullptr;        // second branch of the step graph
     cudaEvent_t fork_ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -186,6 +193,7 @@ void enqueue_step(sld_ctx* c) {
     enqueue_ds(c, Dn, dt / 2e0, eoff, !c->P.eltemp);
     cudaStreamWaitEvent(M, ev[3], 0);
     launch_force_mag(Dn, M);
+    c->force_volume = Dn.box_volume;
     enqueue_dp(c, Dn, dt / 2e0, eoff);
     if (c->P.eltemp) {
         launch_temperature(Dn, M);
@@ -211,6 +219,24 @@ int order_groups_by_count(sld_ctx* c) {
     if (cudaMemcpy(c->d_gcells, G.gcells.data(), sizeof(int) * G.ncells, cudaMemcpyHostToDevice))
         return SLD_ERR_CUDA;
     return SLD_OK;
+}
+
+// FP32 pair pre-test margin (k_pair.cu) for the box of G: coordinates stay
+// below B, each rounding is at most ulp(B) / 2
+float pair_margin(const sld::HostGeom& G) {
+    double B = 0.0;
+    for (int k = 0; k < 6; ++k) B += std::fabs(G.d[k]);
+    B *= 2.0;
+    const double e = std::ldexp(1.0, std::ilogb(B) - 23);   // ulp(B) / 2 in FP32
+    const double dl = 4.0 * std::sqrt(3.0) * e;
+    const double rm = G.rcut_max + dl;
+    const double bound = 2.0 * rm * dl + dl * dl + 4.0 * std::ldexp(rm * rm, -23);
+    return (float)(2.0 * bound);
+}
+
+// the box or the time step changes between steps (sld_scale)
+bool dynamic_step(const sld_ctx* c) {
+    return c->P.change_step || c->P.pressure_control || c->P.stress_control;
 }
 
 int validate(const sld_params* p) {
@@ -309,6 +335,11 @@ int sld_params_default(sld_params* o) {
     o->te_nloop = 50;
     o->interval_of_print_out = 1;
     o->interval_of_config_out = 1000;
+    o->interval_of_scale_pressure = 1;
+    o->interval_of_scale_stress = 1;
+    o->baro_damping_time = 1e-13;
+    o->displace_limit = 0.01;
+    o->phi_limit = 2e0 * 3.141592653589793238462e0 / 10e0;
     o->precision = SLD_FP64;
     return SLD_OK;
 }
@@ -325,6 +356,8 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     if (c->P.te_nloop <= 0) c->P.te_nloop = 50;
     if (c->P.interval_of_print_out <= 0) c->P.interval_of_print_out = 1;
     if (c->P.interval_of_config_out <= 0) c->P.interval_of_config_out = 1000;
+    if (c->P.interval_of_scale_pressure <= 0) c->P.interval_of_scale_pressure = 1;
+    if (c->P.interval_of_scale_stress <= 0) c->P.interval_of_scale_stress = 1;
 
     // geometry, link cells, colour groups, initial order (host)
     std::vector<double> r0(r, r + 3 * (size_t)natom);
@@ -365,17 +398,7 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     D.rcut_pot_sq = prm->rcut_pot * prm->rcut_pot;
     D.rcut_mag_sq = prm->rcut_mag * prm->rcut_mag;
     D.rcut_max_sq = G.rcut_max * G.rcut_max;
-    {
-        // FP32 pair pre-test margin (k_pair.cu): coordinates stay below B
-        double B = 0.0;
-        for (int k = 0; k < 6; ++k) B += std::fabs(G.d[k]);
-        B *= 2.0;
-        const double e = std::ldexp(1.0, std::ilogb(B) - 23);   // ulp(B) / 2 in FP32
-        const double dl = 4.0 * std::sqrt(3.0) * e;
-        const double rm = G.rcut_max + dl;
-        const double bound = 2.0 * rm * dl + dl * dl + 4.0 * std::ldexp(rm * rm, -23);
-        D.pair_loose = (float)(2.0 * bound);
-    }
+    D.pair_loose = pair_margin(G);
     D.atmass = prm->atmass * kUtoeV * (1e-10 * 1e-10);
     D.temperature = prm->temperature * kBoltz;
     D.gamma_L = prm->gamma_L_over_mass * D.atmass;
@@ -541,11 +564,16 @@ int sld_set_state(sld_ctx* c, const double* r, const double* p, const double* s)
     launch_load_state(D, c->st, raw, raw + 3 * n, raw + 6 * n);
     Ctl z{};
     CK(cudaMemcpyAsync(D.ctl, &z, sizeof(Ctl), cudaMemcpyHostToDevice, c->st));
+    // a fresh start: the barostats' clocks at total_time 0 (initial.cpp:92-97)
+    c->last_t_pressure = c->last_t_stress = 0.0;
+    c->pressure0 = 0.0;
+    for (int q = 0; q < 6; ++q) c->ave_stress[q] = 0.0;
     // initialize(): links, rho, forces, cell temperatures, reference energy
     launch_links(D, c->st, true, c->scan_blocks);
     launch_pairs(D, c->st, true);
     c->lists_stale = false;
     launch_force(D, c->st);
+    c->force_volume = D.box_volume;
     if (c->P.eltemp) {
         launch_temperature(D, c->st);
         if (c->P.renormalize_energy) launch_energy_check(D, c->st, 0);
@@ -600,6 +628,7 @@ int sld_calculate_force_energy(sld_ctx* c) {
     if (!c) return SLD_ERR_ARG;
     fresh_lists(c);
     launch_force(c->D, c->st);
+    c->force_volume = c->D.box_volume;
     return launch_status();
 }
 
@@ -645,6 +674,16 @@ int sld_calculate_temperature(sld_ctx* c) {
 int sld_run(sld_ctx* c, int nsteps) {
     if (!c || nsteps < 0) return SLD_ERR_ARG;
     fresh_lists(c);
+    if (dynamic_step(c)) {
+        // box or time step set by sld_scale between steps: launch directly
+        CK(cudaEventRecord(c->ev0, c->st));
+        for (int k = 0; k < nsteps; ++k) {
+            enqueue_step(c);
+            use_set(c, 1 - c->cur);
+        }
+        CK(cudaEventRecord(c->ev1, c->st));
+        return launch_status();
+    }
     for (int k = 0; k < 2; ++k) {
         if (c->step_graphs[k]) continue;
         int saved = c->cur;
@@ -719,7 +758,7 @@ int sld_batch_create(sld_batch** out, sld_ctx* const* ctxs, int n) {
     *out = nullptr;
     std::vector<sld_ctx*> v(ctxs, ctxs + n);
     for (int q = 0; q < n; ++q) {
-        if (!v[q] || v[q]->P.device != v[0]->P.device) return SLD_ERR_ARG;
+        if (!v[q] || v[q]->P.device != v[0]->P.device || dynamic_step(v[q])) return SLD_ERR_ARG;
         for (int r = 0; r < q; ++r)
             if (v[r] == v[q]) return SLD_ERR_ARG;
     }
@@ -830,6 +869,7 @@ int sld_profile_step(sld_ctx* c, double* ms) {
     timed(5, [&] { launch_pairs(Dn, c->st, true); });
     timed(3, [&] { enqueue_ds(c, Dn, dt / 2e0, eoff, !c->P.eltemp); });
     timed(6, [&] { launch_force(Dn, c->st); });
+    c->force_volume = Dn.box_volume;
     timed(2, [&] { enqueue_dp(c, Dn, dt / 2e0, eoff); });
     if (c->P.eltemp) {
         timed(7, [&] { launch_temperature(Dn, c->st); });
@@ -937,7 +977,7 @@ long sld_get(sld_ctx* c, const char* field, double* out, long cap) {
     if (f == "stress") return scal(D.stress, 6);
     if (f == "local_volume") {
         if (cap < (long)n) return SLD_ERR_ARG;
-        for (size_t k = 0; k < n; ++k) out[k] = D.box_volume / D.natom;
+        for (size_t k = 0; k < n; ++k) out[k] = c->force_volume / D.natom;
         return (long)n;
     }
     if (f == "cell" || f == "node") {
@@ -1065,6 +1105,8 @@ int sld_check(sld_ctx* c, const char* dir, const char* out_body, int current_ste
     double tmp = 2e0 / 3e0 * S[SLD_CHK_KE] / n;
     double pressure0 = density * (tmp - S[SLD_CHK_VIR] / (3e0 * n));
     pressure0 *= 160.217653e0;
+    c->pressure0 = pressure0;
+    for (int q = 0; q < 6; ++q) c->ave_stress[q] = st[q];
     k = 0;
     v[k++] = t;
     for (int q = 0; q < 6; ++q) v[k++] = d[q];
@@ -1154,6 +1196,96 @@ int sld_write_config(sld_ctx* c, const char* dir, const char* out_body, int curr
                 o[3] = Te[i]; o[4] = Tl[i]; o[5] = TsR[i]; o[6] = TsL[i];
             }
     return sld::write_cel_file(sld::out_path(dir, "cel-", out_body, n_output), m, t, d, 7, cel.data());
+}
+
+// A new box (upper-triangular d): the host geometry, the device copy of the
+// box and the FP32 pre-test margin follow it; the exchange lists are rebuilt
+// from the moved positions before the next step, keeping the densities
+// (calculate_spin walks the pairs of the current positions while rho is the
+// last calculate_rho's, calculate_spin_CPU.cpp).
+static void apply_box(sld_ctx* c, const double* d) {
+    auto& G = c->G;
+    for (int k = 0; k < 6; ++k) G.d[k] = d[k];
+    sld::box_derived(G);
+    for (int k = 0; k < 6; ++k) { c->D.d[k] = G.d[k]; c->D.inv[k] = G.inv[k]; }
+    for (int k = 0; k < 3; ++k) c->D.box_len[k] = G.box_len[k];
+    c->D.box_volume = G.box_volume;
+    c->D.pair_loose = pair_margin(G);
+    for (int k = 0; k < 6; ++k) c->P.box[k] = d[k];
+    c->lists_stale = true;
+}
+
+int sld_scale(sld_ctx* c, int current_step, double* out3) {
+    if (!c) return SLD_ERR_ARG;
+    const sld_params& P = c->P;
+    double t = 0.0;
+    int rc = sld_total_time(c, &t);
+    if (rc) return rc;
+    const double ftmass = 100e0;   // the piston's fictitious mass, GPa
+    if (P.stress_control && (current_step + 1) % P.interval_of_scale_stress == 0) {
+        // scale_stress_CPU.cpp:35-85; the statements run in this order, so
+        // later ones read the components updated before them
+        double delta_time = t - c->last_t_stress;
+        c->last_t_stress = t;
+        double pre = delta_time / P.baro_damping_time / ftmass;
+        const double* a = c->ave_stress;   // 11 22 33 12 23 31
+        const double* w = P.stress;        // xx yx yy zx zy zz
+        double fxx = pre * (a[0] - w[0]), fyx = pre * (a[3] - w[1]);
+        double fyy = pre * (a[1] - w[2]), fzx = pre * (a[5] - w[3]);
+        double fzy = pre * (a[4] - w[4]), fzz = pre * (a[2] - w[5]);
+        double xx = c->G.d[0], yx = c->G.d[1], yy = c->G.d[2];
+        double zx = c->G.d[3], zy = c->G.d[4], zz = c->G.d[5];
+        xx = (1e0 + fxx) * xx;
+        yx = (1e0 + fxx) * yx + fyx * (yy + xx) / 2e0;
+        yy = (1e0 + fyy) * yy;
+        zx = (1e0 + fxx) * zx + fzx * (zz + xx) / 2e0;
+        zy = (1e0 + fyy) * zy + fzy * (zz + yy) / 2e0;
+        zz = (1e0 + fzz) * zz;
+        double old_inv[6], nd[6] = {xx, yx, yy, zx, zy, zz};
+        for (int k = 0; k < 6; ++k) old_inv[k] = c->G.inv[k];
+        apply_box(c, nd);
+        launch_reshape_positions(c->D, c->st, old_inv);
+        rc = launch_status();
+        if (rc) return rc;
+    }
+    if (P.pressure_control && (current_step + 1) % P.interval_of_scale_pressure == 0) {
+        // scale_pressure_CPU.cpp:35-60
+        double delta_time = t - c->last_t_pressure;
+        c->last_t_pressure = t;
+        double factor = std::pow(
+            1e0 + delta_time / P.baro_damping_time * (c->pressure0 - P.pressure) / ftmass, 1e0 / 3e0);
+        double nd[6];
+        for (int k = 0; k < 6; ++k) nd[k] = c->G.d[k] * factor;
+        apply_box(c, nd);
+        launch_scale_positions(c->D, c->st, factor);
+        rc = launch_status();
+        if (rc) return rc;
+    }
+    double res[3] = {0.0, 0.0, P.step};
+    if (P.change_step) {
+        // scale_step_CPU.cpp:35-100
+        double* part = c->d_chk;
+        double* m = c->d_chk + 2 * (size_t)div_up(c->D.natom, 256);
+        launch_max_p_h(c->D, c->st, part, m);
+        double h[2];
+        CK(cudaMemcpyAsync(h, m, sizeof h, cudaMemcpyDeviceToHost, c->st));
+        rc = check_flags(c);
+        if (rc) return rc;
+        const double hbar = 6.58211899e-16;   // eV s (spilady.h:58)
+        double step = P.step;
+        double displace_max = std::sqrt(h[0]) / c->D.atmass * step;
+        double phi_max = std::sqrt(h[1]) / hbar * step;
+        if (displace_max > P.displace_limit || phi_max > P.phi_limit)
+            step *= 0.80;
+        else
+            step *= 1.05;
+        c->P.step = step;
+        c->D.step = step;
+        res[0] = displace_max; res[1] = phi_max; res[2] = step;
+    }
+    if (out3)
+        for (int k = 0; k < 3; ++k) out3[k] = res[k];
+    return SLD_OK;
 }
 
 int sld_info(sld_ctx* c, int* o) {

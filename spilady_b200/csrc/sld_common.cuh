@@ -443,6 +443,11 @@ void launch_sweep_flow(const Dev& D, cudaStream_t st, const SweepFlow& F, double
                        bool fields);
 void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off);
 void launch_dr(const Dev& D, cudaStream_t st, double dt);
+// barostat position rescaling (D holds the new box) and the adaptive time
+// step's maxima (k_lattice.cu)
+void launch_scale_positions(const Dev& D, cudaStream_t st, double factor);
+void launch_reshape_positions(const Dev& D, cudaStream_t st, const double old_inv[6]);
+void launch_max_p_h(const Dev& D, cudaStream_t st, double* part, double* out);
 void launch_temperature(const Dev& D, cudaStream_t st);
 void launch_dte(const Dev& D, cudaStream_t st, double dt);
 int dte_init(int device);

@@ -59,10 +59,8 @@ int colour_grid(int nx, int ny, int nz, std::vector<int>& gstart, std::vector<in
     return (int)gstart.size() - 1;
 }
 
-int setup_geometry(const sld_params& P, int natom, const std::vector<double>& r, HostGeom& G,
-                   std::vector<int>& id_of_slot, std::vector<int>& slot_of_id) {
-    const double* d = P.box;
-    for (int k = 0; k < 6; ++k) G.d[k] = d[k];
+void box_derived(HostGeom& G) {
+    const double* d = G.d;
     // vec_utils_CPU.cpp:135-148
     G.inv[0] = 1e0 / d[0];
     G.inv[1] = -d[1] / (d[0] * d[2]);
@@ -74,6 +72,13 @@ int setup_geometry(const sld_params& P, int natom, const std::vector<double>& r,
     G.box_len[1] = std::sqrt(d[1] * d[1] + d[2] * d[2]);
     G.box_len[2] = std::sqrt(d[3] * d[3] + d[4] * d[4] + d[5] * d[5]);
     G.box_volume = d[0] * d[2] * d[5];
+}
+
+int setup_geometry(const sld_params& P, int natom, const std::vector<double>& r, HostGeom& G,
+                   std::vector<int>& id_of_slot, std::vector<int>& slot_of_id) {
+    const double* d = P.box;
+    for (int k = 0; k < 6; ++k) G.d[k] = d[k];
+    box_derived(G);
     G.rcut_max = P.rcut_max;
     G.min_len = P.min_length_link_cell;
     if (G.rcut_max > G.min_len) G.min_len = G.rcut_max + 0.001;   // read_variables.cpp:262

@@ -17,6 +17,10 @@ struct HostGeom {
     std::vector<int> te_gstart, te_gcells;  // Te-cell colour groups
 };
 
+// inverse box, edge lengths and volume from G.d (vec_utils_CPU.cpp:135-148,
+// initial.cpp's box_length and box_volume)
+void box_derived(HostGeom& G);
+
 // Fills G from the parameters; id_of_slot / slot_of_id give the storage
 // order (atoms sorted by initial link cell, each cell in the reference's
 // initial list order).  r is not modified.

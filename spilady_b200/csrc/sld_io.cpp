@@ -41,12 +41,27 @@ extern "C" int sld_read_variables(const char* path, sld_params* P) {
         else if (key == "kappa_e") P->kappa_e = v;
         else if (key == "interval_of_print_out") P->interval_of_print_out = iv;
         else if (key == "interval_of_config_out") P->interval_of_config_out = iv;
+        else if (key == "interval_of_scale_pressure") P->interval_of_scale_pressure = iv;
+        else if (key == "interval_of_scale_stress") P->interval_of_scale_stress = iv;
+        else if (key == "pressure") P->pressure = v;
+        else if (key == "stress_xx") P->stress[0] = v;
+        else if (key == "stress_yx") P->stress[1] = v;
+        else if (key == "stress_yy") P->stress[2] = v;
+        else if (key == "stress_zx") P->stress[3] = v;
+        else if (key == "stress_zy") P->stress[4] = v;
+        else if (key == "stress_zz") P->stress[5] = v;
+        else if (key == "baro_damping_time") P->baro_damping_time = v;
+        else if (key == "displace_limit") P->displace_limit = v;
+        else if (key == "phi_limit") P->phi_limit = v;
         // control.h switches, which the reference fixes at compile time
         else if (key == "spinlang") P->spinlang = iv;
         else if (key == "lattlang") P->lattlang = iv;
         else if (key == "eltemp") P->eltemp = iv;
         else if (key == "localcolmot") P->localcolmot = iv;
         else if (key == "renormalizeEnergy") P->renormalize_energy = iv;
+        else if (key == "PRESSURE") P->pressure_control = iv;
+        else if (key == "STRESS") P->stress_control = iv;
+        else if (key == "changestep") P->change_step = iv;
         else if (key == "te_mesh") P->te_mesh = iv;
         else if (key == "te_nloop") P->te_nloop = iv;
         else if (key == "precision") P->precision = (val == "split" || iv == 1) ? SLD_SPLIT : SLD_FP64;

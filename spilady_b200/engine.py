@@ -47,6 +47,11 @@ class Params(C.Structure):
         ("interval_of_print_out", C.c_int), ("precision", C.c_int),
         ("device", C.c_int), ("replica", C.c_int),
         ("interval_of_config_out", C.c_int),
+        ("pressure_control", C.c_int), ("stress_control", C.c_int),
+        ("change_step", C.c_int), ("interval_of_scale_pressure", C.c_int),
+        ("interval_of_scale_stress", C.c_int), ("pressure", C.c_double),
+        ("stress", C.c_double * 6), ("baro_damping_time", C.c_double),
+        ("displace_limit", C.c_double), ("phi_limit", C.c_double),
     ]
 
 
@@ -92,6 +97,7 @@ def lib():
         L.sld_batch_destroy.argtypes = [vp]
         L.sld_batch_destroy.restype = None
         L.sld_check.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int]
+        L.sld_scale.argtypes = [vp, C.c_int, P]
         L.sld_write_config.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int, C.c_int]
         L.sld_error_string.argtypes = [C.c_int]
         L.sld_error_string.restype = C.c_char_p
@@ -111,7 +117,8 @@ def _check(rc, where):
 def make_params(params, *, spinlang=False, lattlang=False, eltemp=False,
                 localcolmot=False, renormalize=False, te_mesh=0, te_nloop=50,
                 precision=FP64, device=0, interval_of_print_out=1, replica=0,
-                interval_of_config_out=1000):
+                interval_of_config_out=1000, pressure_control=False,
+                stress_control=False, change_step=False):
     """sld_params from a variables.in-style dict plus the control switches."""
     P = Params()
     lib().sld_params_default(C.byref(P))
@@ -129,6 +136,19 @@ def make_params(params, *, spinlang=False, lattlang=False, eltemp=False,
     P.interval_of_print_out = int(interval_of_print_out)
     P.replica = int(replica)
     P.interval_of_config_out = int(interval_of_config_out)
+    P.pressure_control, P.stress_control = int(pressure_control), int(stress_control)
+    P.change_step = int(change_step)
+    # barostat / time-step variables, variables.in names (read_variables.cpp:197-241)
+    for k in ("pressure", "baro_damping_time", "displace_limit", "phi_limit"):
+        if k in params:
+            setattr(P, k, float(params[k]))
+    for k in ("interval_of_scale_pressure", "interval_of_scale_stress"):
+        if k in params:
+            setattr(P, k, int(params[k]))
+    for j, k in enumerate(("stress_xx", "stress_yx", "stress_yy", "stress_zx",
+                           "stress_zy", "stress_zz")):
+        if k in params:
+            P.stress[j] = float(params[k])
     return P
 
 
@@ -264,6 +284,13 @@ class Engine:
                                        int(current_step), 1 if heff_as_reference else 0),
                "write_config")
 
+    def scale(self, current_step):
+        """scale(current_step): barostats and adaptive time step; returns
+        (displace_max, phi_max, new step)."""
+        out = np.zeros(3, np.float64)
+        _check(self.L.sld_scale(self.h, int(current_step), _dp(out)), "scale")
+        return tuple(float(x) for x in out)
+
     def last_run_ms(self):
         out = np.empty(1, np.float64)
         _check(self.L.sld_last_run_ms(self.h, _dp(out)), "last_run_ms")
@@ -296,6 +323,13 @@ class Batch:
         _check(self.L.sld_write_config(self.h, str(out_dir).encode(), out_body.encode(),
                                        int(current_step), 1 if heff_as_reference else 0),
                "write_config")
+
+    def scale(self, current_step):
+        """scale(current_step): barostats and adaptive time step; returns
+        (displace_max, phi_max, new step)."""
+        out = np.zeros(3, np.float64)
+        _check(self.L.sld_scale(self.h, int(current_step), _dp(out)), "scale")
+        return tuple(float(x) for x in out)
 
     def last_run_ms(self):
         out = np.empty(1, np.float64)

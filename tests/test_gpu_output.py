@@ -216,3 +216,57 @@ def test_output_intervals_and_file_numbers(tmp_path):
     for pre, ncol in [("enr-", 6), ("tmp-", 5), ("str-", 16), ("prs-", 10), ("spn-", 10)]:
         rows = [l.split() for l in open(tmp_path / f"{pre}i.dat")]
         assert all(len(x) == ncol for x in rows), pre
+
+
+# Barostats and the adaptive time step (scale.cpp): the reference's baro
+# build has PRESSURE and STRESS, its dtstep build changestep; a barostat is
+# switched off in the baro build by an interval that is never reached.
+NEVER = 10**9
+SCALE_CASES = {
+    # name: (reference mode, engine switches, variables)
+    "pressure": ("baro", dict(pressure_control=True),
+                 dict(pressure=5.0, interval_of_scale_stress=NEVER,
+                      baro_damping_time=2e-14)),
+    # shear and normal targets: the box becomes triclinic
+    "stress": ("baro", dict(stress_control=True),
+               dict(stress_xx=2.0, stress_yx=0.5, stress_zy=-0.4, stress_zz=-1.0,
+                    interval_of_scale_pressure=NEVER, baro_damping_time=2e-14)),
+    # limits at which the step first shrinks (x0.8), then grows (x1.05)
+    "dtstep": ("dtstep", dict(change_step=True), dict(displace_limit=0.006, phi_limit=100.0)),
+}
+
+
+@pytest.mark.parametrize("case", sorted(SCALE_CASES))
+def test_barostats_and_adaptive_step_match_reference(case, tmp_path):
+    mode, sw, var = SCALE_CASES[case]
+    if not rj.available(mode):
+        pytest.skip("reference build missing")
+    nsteps = 6
+    params, r, p, s = initial_state(6, seed=11, tilt=0.2, temperature=600.0)
+    params = dict(params, **var)
+    ops = rj.set_ops(**var) + [(rj.OP_STEP, nsteps)]
+    _, ref = rj.run(mode, params, r, p, s, ops=ops, files=True)
+    e = engine_mod().Engine(params, r, p, s, interval_of_config_out=1, **sw)
+    d = tmp_path / "out"
+    d.mkdir()
+    steps = []
+    for k in range(nsteps):
+        e.run(1)
+        e.check(d, "b200", k)
+        steps.append(e.scale(k)[2])
+        e.write_config(d, "b200", k, heff_as_reference=True)
+    ours = read_all(d)
+    assert sorted(ours) == sorted(n.replace("-ref", "-b200") for n in ref)
+    worst = {n: compare_text(ours[n], ref[n.replace("-b200", "-ref")], TOL_FILE, n)
+             for n in sorted(ours)}
+    print(case, " ".join(f"{n}:{w:.1e}" for n, w in worst.items()))
+    box = [float(x) for x in ours["prs-b200.dat"].splitlines()[-1].split()[2:8]]
+    if case == "pressure":
+        assert box[0] != params["box"][0] and box[1] == 0.0
+    if case == "stress":
+        assert box[1] != 0.0 and box[4] != 0.0          # d.yx, d.zy sheared
+    if case == "dtstep":
+        ratio = np.array(steps[1:]) / np.array(steps[:-1])
+        assert np.any(np.isclose(ratio, 0.8)) and np.any(np.isclose(ratio, 1.05))
+        times = [float(l.split()[1]) for l in ours["enr-b200.dat"].splitlines()]
+        assert np.allclose(np.diff(times), steps[:-1], rtol=1e-12)
