@@ -230,6 +230,38 @@ int sld_write_config(sld_ctx* ctx, const char* dir, const char* out_body, int cu
    cannot join a batch. */
 int sld_scale(sld_ctx* ctx, int current_step, double* out3);
 
+/* Gradients with respect to the potential's parameters.  No reference
+   counterpart: the reference's potential is fixed code (DD05.cpp,
+   JijFe.cpp).  theta holds the 36 constants of its forms, in this order:
+     [0, 2)   F(rho): a, b                       DD05.cpp:6-20
+     [2, 8)   f(r): coefficients a_k, [8, 14) knots r_k    DD05.cpp:22-44
+     [14, 22) phi(r): coefficients V_k, [22, 30) knots     DD05.cpp:64-84
+     [30, 32) J(r) = A (1 - r/rc)^3: A, rc        JijFe.cpp:5-12
+     [32, 36) Landau A, B, C, D                   JijFe.cpp:15-43
+   The ZBL core and the 1.8-2.0 A join keep their form; the join's end at
+   2.0 A follows the parameters.  The energy is E = sum_i (pe + me + me0)
+   (calculate_force_energy_CPU.cpp:33-216); the loss is L = sum_i |f_i|^2 +
+   |Heff_H,i|^2, forces and exchange fields of the configuration.  The
+   context must be NVE (no thermostats, no electron temperature, no sld_scale
+   switches) in an FP64 form; its state is unchanged afterwards. */
+#define SLD_ADJ_NTHETA 36
+int sld_adjoint_theta_default(double* theta36);
+
+/* One configuration (the context's current state): out4 = E, L, sum |f|^2,
+   sum |H|^2; dE and dL (36 each, may be NULL) = their gradients in theta,
+   evaluated in FP64 by reverse-mode differentiation. */
+int sld_adjoint_config(sld_ctx* ctx, const double* theta36, double* out4, double* dE36,
+                       double* dL36);
+
+/* Through a trajectory: nsteps NVE main-loop steps (core.cpp:55-63) from
+   the context's current state with the parameters theta; *L = the loss of
+   the final configuration and dL36 (may be NULL: forward only) its gradient
+   in theta, by reverse-mode differentiation through every step with the
+   state kept every checkpoint_every steps and each segment recomputed once
+   in the reverse pass. */
+int sld_adjoint_trajectory(sld_ctx* ctx, const double* theta36, int nsteps,
+                           int checkpoint_every, double* L, double* dL36);
+
 /* out[0..5] = natom, ncells, ngroups, n_te_cells, nx, ny (link cells). */
 int sld_info(sld_ctx* ctx, int* out6);
 

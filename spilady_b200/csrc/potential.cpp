@@ -17,16 +17,21 @@
 
 namespace sld {
 
+static const double kEmbA = 4.100199340884814, kEmbB = 1.565647547483517;
+static const double kDensA[6] = {0.9332056681088162, -1.162558782567700, -0.3502026949249225,
+                                 0.4287820835430028, 4.907925057809273,  -5.307049068415304};
+static const double kDensK[6] = {3.0, 2.8666666666666666, 2.7333333333333333, 2.6, 2.4, 2.3};
+static const double kJA = 0.870, kJRC = 3.75;
+
 static double emb_F(double rho) {
-    const double a = 4.100199340884814, b = 1.565647547483517;
+    const double a = kEmbA, b = kEmbB;
     if (rho >= 1e0) return -a * std::sqrt(rho);
     return -a * std::sqrt(rho) - b / std::log(2e0) * (1e0 - std::sqrt(rho)) * std::log(2e0 - rho);
 }
 
 static double dens_f(double r) {
-    static const double a[6] = {0.9332056681088162, -1.162558782567700, -0.3502026949249225,
-                                0.4287820835430028, 4.907925057809273, -5.307049068415304};
-    static const double k[6] = {3.0, 2.8666666666666666, 2.7333333333333333, 2.6, 2.4, 2.3};
+    const double* a = kDensA;
+    const double* k = kDensK;
     double f = 0e0;
     for (int i = 0; i < 6; ++i)
         if (r < k[i]) f += a[i] * std::pow(k[i] - r, 3);
@@ -81,7 +86,7 @@ static double pair_phi(double r) {
 }
 
 static double exch_J(double r) {
-    const double A = 0.870, rc = 3.75;
+    const double A = kJA, rc = kJRC;
     double J = 0e0;
     if (r < rc) J = A * std::pow(1.0 - r / rc, 3);
     return J;
@@ -135,6 +140,16 @@ double pot_F(double rho) { return emb_F(rho); }
 double pot_f(double r) { return dens_f(r); }
 double pot_phi(double r) { return pair_phi(r); }
 double pot_J(double r) { return exch_J(r); }
+
+void pot_theta(double o[36]) {
+    o[0] = kEmbA;
+    o[1] = kEmbB;
+    for (int i = 0; i < 6; ++i) { o[2 + i] = kDensA[i]; o[8 + i] = kDensK[i]; }
+    for (int i = 0; i < 8; ++i) { o[14 + i] = kPV[i]; o[22 + i] = kPK[i]; }
+    o[30] = kJA;
+    o[31] = kJRC;
+    for (int i = 0; i < 4; ++i) o[32 + i] = kLandau[i];
+}
 
 void pot_join_data(double o[7]) {
     const double x1 = 1.8, x2 = 2.0, h = 1e-7;

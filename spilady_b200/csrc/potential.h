@@ -18,6 +18,10 @@ double pot_F(double rho);
 double pot_f(double r);
 double pot_phi(double r);
 double pot_J(double r);
+// The 36 parameters of the forms above, in the order of the adjoint's
+// parameter vector: F's a, b; f's 6 coefficients, 6 knots; phi's 8
+// coefficients, 8 knots; J's amplitude and range; Landau A, B, C, D
+void pot_theta(double out[36]);
 // Hermite data of the pair term's 1.8-2.0 A join: y, y', y'' of the ZBL core
 // at 1.8 A and of the cubic knots at 2.0 A, then the ZBL screening length
 void pot_join_data(double out[7]);

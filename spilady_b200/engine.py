@@ -99,6 +99,9 @@ def lib():
         L.sld_check.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int]
         L.sld_scale.argtypes = [vp, C.c_int, P]
         L.sld_write_config.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int, C.c_int]
+        L.sld_adjoint_theta_default.argtypes = [P]
+        L.sld_adjoint_config.argtypes = [vp, P, P, P, P]
+        L.sld_adjoint_trajectory.argtypes = [vp, P, C.c_int, C.c_int, P, P]
         L.sld_error_string.argtypes = [C.c_int]
         L.sld_error_string.restype = C.c_char_p
         _lib = L
@@ -154,6 +157,17 @@ def make_params(params, *, spinlang=False, lattlang=False, eltemp=False,
 
 VEC_FIELDS = {"r": 3, "p": 3, "f": 3, "s": 3, "H": 3, "HL": 3, "stress": 6}
 CELL_FIELDS = ("Te", "Ee", "Tl", "Ts_R", "Ts_L", "Gel", "Ges", "count")
+
+
+ADJ_NTHETA = 36
+
+
+def adjoint_theta_default():
+    """The potential's 36 parameters (DD05 embedding, density and pair
+    terms, J(r), Landau), in sld_adjoint_*'s order."""
+    th = np.zeros(ADJ_NTHETA)
+    _check(lib().sld_adjoint_theta_default(_dp(th)), "adjoint_theta_default")
+    return th
 
 
 class Engine:
@@ -291,6 +305,24 @@ class Engine:
         _check(self.L.sld_scale(self.h, int(current_step), _dp(out)), "scale")
         return tuple(float(x) for x in out)
 
+    def adjoint_config(self, theta):
+        """(E, L, sum|f|^2, sum|H|^2), dE/dtheta, dL/dtheta at the current
+        configuration."""
+        th = np.ascontiguousarray(theta, np.float64)
+        out, dE, dL = np.zeros(4), np.zeros(ADJ_NTHETA), np.zeros(ADJ_NTHETA)
+        _check(self.L.sld_adjoint_config(self.h, _dp(th), _dp(out), _dp(dE), _dp(dL)),
+               "adjoint_config")
+        return out, dE, dL
+
+    def adjoint_trajectory(self, theta, nsteps, checkpoint_every=20, grad=True):
+        """Loss after nsteps NVE steps and (grad) its gradient in theta."""
+        th = np.ascontiguousarray(theta, np.float64)
+        Lv, dL = np.zeros(1), np.zeros(ADJ_NTHETA)
+        _check(self.L.sld_adjoint_trajectory(self.h, _dp(th), int(nsteps), int(checkpoint_every),
+                                             _dp(Lv), _dp(dL) if grad else None),
+               "adjoint_trajectory")
+        return (float(Lv[0]), dL) if grad else float(Lv[0])
+
     def last_run_ms(self):
         out = np.empty(1, np.float64)
         _check(self.L.sld_last_run_ms(self.h, _dp(out)), "last_run_ms")
@@ -330,6 +362,24 @@ class Batch:
         out = np.zeros(3, np.float64)
         _check(self.L.sld_scale(self.h, int(current_step), _dp(out)), "scale")
         return tuple(float(x) for x in out)
+
+    def adjoint_config(self, theta):
+        """(E, L, sum|f|^2, sum|H|^2), dE/dtheta, dL/dtheta at the current
+        configuration."""
+        th = np.ascontiguousarray(theta, np.float64)
+        out, dE, dL = np.zeros(4), np.zeros(ADJ_NTHETA), np.zeros(ADJ_NTHETA)
+        _check(self.L.sld_adjoint_config(self.h, _dp(th), _dp(out), _dp(dE), _dp(dL)),
+               "adjoint_config")
+        return out, dE, dL
+
+    def adjoint_trajectory(self, theta, nsteps, checkpoint_every=20, grad=True):
+        """Loss after nsteps NVE steps and (grad) its gradient in theta."""
+        th = np.ascontiguousarray(theta, np.float64)
+        Lv, dL = np.zeros(1), np.zeros(ADJ_NTHETA)
+        _check(self.L.sld_adjoint_trajectory(self.h, _dp(th), int(nsteps), int(checkpoint_every),
+                                             _dp(Lv), _dp(dL) if grad else None),
+               "adjoint_trajectory")
+        return (float(Lv[0]), dL) if grad else float(Lv[0])
 
     def last_run_ms(self):
         out = np.empty(1, np.float64)

@@ -1,0 +1,123 @@
+"""Gradients in the potential's parameters (sld_adjoint_*), checked against
+FP64 central finite differences of the same functions (h = 1e-6 of each
+parameter, 1e-6 absolute for a zero one), and the adjoint's forward
+dynamics against the engine's own NVE step.
+
+Tolerances: each component within 1e-6 of the finite difference plus 1e-8
+of the largest component (the finite differences themselves carry about
+1e-9 relative rounding error from L / h).
+"""
+import numpy as np
+import pytest
+
+from conftest import relerr
+from spilady_b200.lattice import initial_state
+
+pytestmark = pytest.mark.gpu
+
+
+def E():
+    from spilady_b200 import engine
+    return engine
+
+
+def system(ncell=8, seed=21, **kw):
+    params, r, p, s = initial_state(ncell, seed=seed, tilt=0.2, temperature=300.0,
+                                    pos_sigma=0.05)
+    return params, r, p, s, E().Engine(params, r, p, s, precision=E().FP64_ANALYTIC, **kw)
+
+
+def steps(theta):
+    return np.where(theta != 0.0, 1e-6 * np.abs(theta), 1e-6)
+
+
+def check_grad(g, fd, name):
+    scale = np.max(np.abs(fd))
+    bad = np.abs(g - fd) > 1e-6 * np.abs(fd) + 1e-8 * scale
+    worst = np.max(np.abs(g - fd) / (np.abs(fd) + 1e-8 * scale))
+    assert not bad.any(), (f"{name}: components {np.nonzero(bad)[0].tolist()} differ; "
+                           f"worst scaled error {worst:.2e}\n{g}\n{fd}")
+    return worst
+
+
+def test_adjoint_forward_matches_engine():
+    params, r, p, s, e = system()
+    th = E().adjoint_theta_default()
+    out, _, _ = e.adjoint_config(th)
+    e_engine = (e.get("pe") + e.get("me") + e.get("me0")).sum()
+    assert abs(out[0] - e_engine) <= 1e-12 * abs(e_engine)
+    assert abs(out[2] - (e.get("f") ** 2).sum()) <= 1e-10 * out[2]
+    assert abs(out[1] - out[2] - out[3]) <= 1e-12 * out[1]
+
+
+def test_config_gradients_against_finite_differences():
+    params, r, p, s, e = system()
+    th = E().adjoint_theta_default()
+    out, dE, dL = e.adjoint_config(th)
+    h = steps(th)
+    fdE, fdL = np.zeros(36), np.zeros(36)
+    for k in range(36):
+        tp, tm = th.copy(), th.copy()
+        tp[k] += h[k]
+        tm[k] -= h[k]
+        op, om = e.adjoint_config(tp)[0], e.adjoint_config(tm)[0]
+        fdE[k] = (op[0] - om[0]) / (2 * h[k])
+        fdL[k] = (op[1] - om[1]) / (2 * h[k])
+    we = check_grad(dE, fdE, "dE/dtheta")
+    wl = check_grad(dL, fdL, "dL/dtheta")
+    print(f"config: dE worst {we:.1e}, dL worst {wl:.1e}")
+    # the Landau constants move the energy but not the forces or fields
+    assert np.all(dL[32:] == 0.0) and np.all(dE[32:] != 0.0)
+
+
+def test_trajectory_gradient_against_finite_differences():
+    params, r, p, s, e = system()
+    th = E().adjoint_theta_default()
+    K = 10
+    L, dL = e.adjoint_trajectory(th, K, checkpoint_every=4)
+    h = steps(th)
+    fd = np.zeros(36)
+    for k in range(36):
+        tp, tm = th.copy(), th.copy()
+        tp[k] += h[k]
+        tm[k] -= h[k]
+        fd[k] = (e.adjoint_trajectory(tp, K, 4, grad=False) -
+                 e.adjoint_trajectory(tm, K, 4, grad=False)) / (2 * h[k])
+    w = check_grad(dL, fd, "trajectory dL/dtheta")
+    print(f"trajectory ({K} steps): worst {w:.1e}")
+    # the checkpoint spacing changes only the recomputation
+    L1, dL1 = e.adjoint_trajectory(th, K, checkpoint_every=1)
+    L2, dL2 = e.adjoint_trajectory(th, K, checkpoint_every=K)
+    assert L1 == L and L2 == L
+    assert relerr(dL1, dL) <= 1e-12 and relerr(dL2, dL) <= 1e-12
+
+
+def test_trajectory_of_zero_steps_is_the_configuration():
+    params, r, p, s, e = system()
+    th = E().adjoint_theta_default()
+    out, _, dLc = e.adjoint_config(th)
+    L0, dL0 = e.adjoint_trajectory(th, 0)
+    assert abs(L0 - out[1]) <= 1e-13 * out[1]
+    assert relerr(dL0, dLc) <= 1e-12
+
+
+def test_adjoint_dynamics_are_the_engine_step_and_leave_the_state():
+    params, r, p, s, e = system()
+    th = E().adjoint_theta_default()
+    before = {k: e.get(k).copy() for k in ("r", "p", "s", "f")}
+    K = 12
+    L = e.adjoint_trajectory(th, K, 5, grad=False)
+    for k, v in before.items():
+        assert np.array_equal(e.get(k), v), k
+    # the engine's own NVE steps reach the configuration whose loss the
+    # adjoint's forward run reported
+    ref = E().Engine(params, r, p, s, precision=E().FP64_ANALYTIC)
+    ref.run(K)
+    out, _, _ = ref.adjoint_config(th)
+    assert abs(out[1] - L) <= 1e-9 * L
+    # the context steps on exactly as an untouched one
+    e.run(3)
+    fresh = E().Engine(params, r, p, s, precision=E().FP64_ANALYTIC)
+    fresh.run(3)
+    for k in ("r", "p", "s"):
+        assert np.array_equal(e.get(k), fresh.get(k)), k
