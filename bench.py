@@ -67,9 +67,13 @@ def parse():
     ap.add_argument("--small", action="store_true",
                     help="short run for profiler captures: no CPU baseline, no e2e leg, "
                          "one phase-profile step")
-    ap.add_argument("--workload", default="single", choices=["single", "replicas"],
+    ap.add_argument("--workload", default="single", choices=["single", "replicas", "adjoint"],
                     help="single: the 128^3 spin-lattice-electron system; replicas: many "
-                         "independent small systems advanced as one batch")
+                         "independent small systems advanced as one batch; adjoint: gradients "
+                         "in the potential's parameters (20^3 cells, NVE)")
+    ap.add_argument("--adj-steps", type=int, default=200,
+                    help="adjoint workload: trajectory length (steps of 1 fs)")
+    ap.add_argument("--adj-checkpoint", type=int, default=20)
     ap.add_argument("--replicas", type=int, default=96)
     ap.add_argument("--out", default=None,
                     help="replicas workload: write per-replica magnetisation vs T here (JSON)")
@@ -300,6 +304,81 @@ def run_replicas(args, world, rank, local):
     print(json.dumps(line))
 
 
+def run_adjoint(args, world, rank, local):
+    """Gradients of E and of L = sum |f|^2 + |H|^2 in the 36 potential
+    parameters: bcc Fe 20^3 cells (16,000 atoms), positions displaced by a
+    Gaussian of 0.05 A, spins tilted by 0.2 rad, NVE, dt 1 fs; one
+    configuration, then through args.adj_steps steps with a checkpoint every
+    args.adj_checkpoint steps; each gradient against FP64 central finite
+    differences (h = 1e-6 of each parameter)."""
+    from spilady_b200 import engine
+    from spilady_b200.lattice import initial_state
+    import torch
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return
+    prec = {"fp64": engine.FP64, "split": engine.SPLIT,
+            "fp64-analytic": engine.FP64_ANALYTIC}[args.precision]
+    params, r, p, s = initial_state(20, seed=2029, tilt=0.2, temperature=300.0, pos_sigma=0.05)
+    params["step"] = 1e-15
+    e = engine.Engine(params, r, p, s, device=local, precision=prec)
+    th = engine.adjoint_theta_default()
+    h = np.where(th != 0.0, 1e-6 * np.abs(th), 1e-6)
+    K, C = args.adj_steps, args.adj_checkpoint
+
+    def timed(fn, reps):
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            out = fn()
+        return out, (time.perf_counter() - t0) / reps * 1e3
+
+    (cfg, ms_cfg) = timed(lambda: e.adjoint_config(th), 3)
+    out, dE, dL = cfg
+    ((Lk, dLk), ms_traj) = timed(lambda: e.adjoint_trajectory(th, K, C), 1)
+    (_, ms_fwd) = timed(lambda: e.adjoint_trajectory(th, K, C, grad=False), 1)
+
+    def fd(fn):
+        g = np.zeros(len(th))
+        for k in range(len(th)):
+            tp, tm = th.copy(), th.copy()
+            tp[k] += h[k]
+            tm[k] -= h[k]
+            g[k] = (fn(tp) - fn(tm)) / (2 * h[k])
+        return g
+
+    def err(g, f):
+        scale = np.max(np.abs(f))
+        return float(np.max(np.abs(g - f)) / scale)
+
+    # finite differences of the FP64 model (the split forward's FP32 rounding
+    # would swamp differences of 1e-6 in the parameters)
+    e64 = engine.Engine(params, r, p, s, device=local, precision=engine.FP64_ANALYTIC)
+    fdE = fd(lambda t: e64.adjoint_config(t)[0][0])
+    fdL = fd(lambda t: e64.adjoint_config(t)[0][1])
+    fdT = fd(lambda t: e64.adjoint_trajectory(t, K, C, grad=False))
+    _, dLk64 = e64.adjoint_trajectory(th, K, C)
+    line = {
+        "metric": f"ms per gradient of L in 36 potential parameters through {K} NVE steps, "
+                  f"{e.natom}-atom bcc Fe",
+        "value": ms_traj, "unit": "ms", "n_gpus": 1, "steps": K, "warmup": 1,
+        "ms_per_step": ms_traj / max(K, 1), "higher_is_better": False, "scaling": None,
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"bcc Fe 20^3 cells ({e.natom} atoms), positions +N(0, 0.05 A), "
+                               f"spin tilt 0.2 rad, NVE dt 1 fs, {K} steps, checkpoint every {C}",
+                   "forward_precision": args.precision},
+        "forward_ms": ms_fwd, "config_gradient_ms": ms_cfg,
+        "E": out[0], "L": out[1], "L_final": Lk,
+        "vs_finite_differences": {"dE_config": err(dE, fdE), "dL_config": err(dL, fdL),
+                                  f"dL_{K}_steps": err(dLk, fdT),
+                                  f"dL_{K}_steps_fp64_forward": err(dLk64, fdT),
+                                  "how": "max |adjoint - FD| / max |FD| over the 36 parameters; "
+                                         "FD: FP64 central differences, h = 1e-6 relative"},
+        "roofline": None, "cpu_baseline": None, "e2e": None,
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     if args.small:
@@ -311,6 +390,9 @@ def main():
         return
     if args.workload == "replicas":
         run_replicas(args, world, rank, local)
+        return
+    if args.workload == "adjoint":
+        run_adjoint(args, world, rank, local)
         return
     from spilady_b200 import engine
     params, r, p, s, te, sw = workload(args.size)

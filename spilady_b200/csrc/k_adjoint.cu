@@ -17,6 +17,7 @@
 // by visit, colour group by colour group, in the opposite order.
 #include "sld_adjpot.cuh"
 #include "sld_adjoint.cuh"
+#include "sld_pot32.cuh"
 
 namespace {
 
@@ -28,7 +29,8 @@ __device__ __forceinline__ double3 adj_pair_vec(const Dev& D, double4 ri, int pk
     return d;
 }
 
-__device__ __forceinline__ double warp_sum(double v) {
+// warp sum of v on every lane
+__device__ __forceinline__ double warp_allsum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
@@ -60,24 +62,33 @@ __device__ void block_theta(const double* loc, int lo, int hi, double* row, doub
 // forward
 
 // rho_i = sum_j f(r_ij) over r_ij < rcut_pot (calculate_rho_CPU.cpp:33-69);
-// dF_i = F'(rho_i)
+// dF_i = F'(rho_i).  SPLIT: the pair terms in FP32, summed with compensation.
+template <bool SPLIT>
 __global__ void __launch_bounds__(128) k_adj_rho(Dev D, AdjDev A, AdjConst K) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= D.natom) return;
     ThPlain th{K.th};
     double4 ri = D.r[i];
     double rho = 0.0;
+    Kahan acc;
     int nn = D.nbr_n[i];
     for (int e = 0; e < nn; ++e) {
         double4 rj;
         double3 d = adj_pair_vec(D, ri, D.nbr[(size_t)e * D.natom + i], rj);
         double r0 = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
         if (r0 < D.rcut_pot) {
-            double f, df;
-            adj_dens(r0, th, f, df);
-            rho += f;
+            if constexpr (SPLIT) {
+                float f, df;
+                adj_dens32(K, (float)r0, f, df);
+                acc.add(f);
+            } else {
+                double f, df;
+                adj_dens(r0, th, f, df);
+                rho += f;
+            }
         }
     }
+    if constexpr (SPLIT) rho = acc.value();
     double F, dF;
     adj_emb(rho, th, F, dF);
     A.rho[i] = rho;
@@ -88,6 +99,7 @@ __global__ void __launch_bounds__(128) k_adj_rho(Dev D, AdjDev A, AdjConst K) {
 // 33-216 with the Landau slopes zero, inner_spin calculate_spin_CPU.cpp:
 // 201-235); per atom: f, e = pe + me + me0, H, and |f|^2 + |H|^2 into the
 // block partials [E, L]
+template <bool SPLIT>
 __global__ void __launch_bounds__(128) k_adj_force(Dev D, AdjDev A, AdjConst K) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     ThPlain th{K.th};
@@ -97,6 +109,9 @@ __global__ void __launch_bounds__(128) k_adj_force(Dev D, AdjDev A, AdjConst K) 
         double si_sq = si.x * si.x + si.y * si.y + si.z * si.z;
         double rho_i = A.rho[i], dF_i = A.dF[i];
         double fx = 0, fy = 0, fz = 0, pe = 0, me = 0, me0 = 0, hx = 0, hy = 0, hz = 0;
+        Kahan kfx, kfy, kfz, kpe, kme, kme0, khx, khy, khz;
+        const float six = (float)si.x, siy = (float)si.y, siz = (float)si.z;
+        const float si_sq32 = six * six + siy * siy + siz * siz;
         int nn = D.nbr_n[i];
         for (int e = 0; e < nn; ++e) {
             int pk = D.nbr[(size_t)e * D.natom + i];
@@ -105,6 +120,35 @@ __global__ void __launch_bounds__(128) k_adj_force(Dev D, AdjDev A, AdjConst K) 
             double3 d = adj_pair_vec(D, ri, pk, rj);
             double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
             double r0 = sqrt(rsq);
+            if constexpr (SPLIT) {
+                float rf = (float)r0, dudr = 0.f;
+                if (r0 < D.rcut_pot) {
+                    float f, df, phi, dphi;
+                    adj_dens32(K, rf, f, df);
+                    adj_pair32(K, r0, phi, dphi);
+                    dudr = ((float)dF_i + (float)A.dF[j]) * df + dphi;
+                    kpe.add(0.5f * phi);
+                }
+                if (r0 < D.rcut_mag || rsq < D.rcut_mag_sq) {
+                    double4 sj = D.s[j];
+                    float sjx = (float)sj.x, sjy = (float)sj.y, sjz = (float)sj.z;
+                    float J, dJ;
+                    adj_exch32(K, rf, J, dJ);
+                    if (r0 < D.rcut_mag) {
+                        float sdot = six * sjx + siy * sjy + siz * sjz;
+                        float stimes = sqrtf(si_sq32 * (sjx * sjx + sjy * sjy + sjz * sjz));
+                        dudr += -dJ * (sdot - stimes);
+                        kme.add(-0.5f * J * sdot);
+                        kme0.add(0.5f * J * stimes);
+                    }
+                    if (rsq < D.rcut_mag_sq) {
+                        khx.add(J * sjx); khy.add(J * sjy); khz.add(J * sjz);
+                    }
+                }
+                float force = -dudr / rf;
+                kfx.add(force * (float)d.x); kfy.add(force * (float)d.y); kfz.add(force * (float)d.z);
+                continue;
+            }
             double dudr = 0.0;
             if (r0 < D.rcut_pot) {
                 double f, df, phi, dphi;
@@ -131,6 +175,11 @@ __global__ void __launch_bounds__(128) k_adj_force(Dev D, AdjDev A, AdjConst K) 
             }
             double force = -dudr / r0;
             fx += force * d.x; fy += force * d.y; fz += force * d.z;
+        }
+        if constexpr (SPLIT) {
+            fx = kfx.value(); fy = kfy.value(); fz = kfz.value();
+            pe = kpe.value(); me = kme.value(); me0 = kme0.value();
+            hx = khx.value(); hy = khy.value(); hz = khz.value();
         }
         double F, dF;
         adj_emb(rho_i, th, F, dF);
@@ -175,36 +224,51 @@ __device__ __forceinline__ void adj_rot(const T H[3], const T s[3], double dt, T
 }
 
 // One colour group of an NVE spin sweep (core_ds_CPU.cpp:35-83 with
-// calculate_spin_CPU.cpp:43-46): a thread walks one cell, head to tail
+// calculate_spin_CPU.cpp:43-46): a warp walks one cell, head to tail
 // (forward) or tail to head (backward), rotating each spin about its
-// exchange field of the current neighbour spins.
+// exchange field of the current neighbour spins; the lanes share the
+// neighbours of the visit.
+template <bool SPLIT>
 __global__ void __launch_bounds__(128) k_adj_sweep(Dev D, AdjConst K, const int* cells, int n,
                                                    double dt, int backward) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
+    int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= n) return;
     ThPlain th{K.th};
-    int c = cells[t];
+    int c = cells[w];
     int st = D.cell_start[c], cnt = cell_n(D, c);
     for (int m = 0; m < cnt; ++m) {
         int i = D.cell_atoms[st + (backward ? cnt - 1 - m : m)];
-        double4 ri = D.r[i], si = D.s[i];
+        double4 ri = D.r[i];
         double hx = 0, hy = 0, hz = 0;
         int nn = D.nbr_n[i];
-        for (int e = 0; e < nn; ++e) {
+        for (int e = lane; e < nn; e += 32) {
             int pk = D.nbr[(size_t)e * D.natom + i];
             double4 rj;
             double3 d = adj_pair_vec(D, ri, pk, rj);
             double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
             if (rsq < D.rcut_mag_sq) {
-                double J, dJ;
-                adj_exch(sqrt(rsq), th, J, dJ);
                 double4 sj = D.s[pk & SLD_JMASK];
-                hx += J * sj.x; hy += J * sj.y; hz += J * sj.z;
+                if constexpr (SPLIT) {
+                    float J, dJ;
+                    adj_exch32(K, (float)sqrt(rsq), J, dJ);
+                    hx += (double)(J * (float)sj.x);
+                    hy += (double)(J * (float)sj.y);
+                    hz += (double)(J * (float)sj.z);
+                } else {
+                    double J, dJ;
+                    adj_exch(sqrt(rsq), th, J, dJ);
+                    hx += J * sj.x; hy += J * sj.y; hz += J * sj.z;
+                }
             }
         }
-        double H[3] = {hx, hy, hz}, s[3] = {si.x, si.y, si.z}, o[3];
-        adj_rot(H, s, dt, o);
-        D.s[i] = make_double4(o[0], o[1], o[2], sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]));
+        hx = warp_allsum(hx); hy = warp_allsum(hy); hz = warp_allsum(hz);
+        if (lane == 0) {
+            double4 si = D.s[i];
+            double H[3] = {hx, hy, hz}, s[3] = {si.x, si.y, si.z}, o[3];
+            adj_rot(H, s, dt, o);
+            D.s[i] = make_double4(o[0], o[1], o[2], sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]));
+        }
+        __syncwarp();
     }
 }
 
@@ -298,7 +362,7 @@ __global__ void __launch_bounds__(128) k_adj_energy_grad(Dev D, AdjDev A, AdjCon
 #define ADJ_NF (7 + TH_LANDAU)
 __global__ void __launch_bounds__(128) k_adj_force_rev(Dev D, AdjDev A, AdjConst K) {
     typedef Dual<ADJ_NF> T;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     double loc[ADJ_NTHETA];
     for (int k = 0; k < ADJ_NTHETA; ++k) loc[k] = 0.0;
     if (i < D.natom) {
@@ -310,10 +374,9 @@ __global__ void __launch_bounds__(128) k_adj_force_rev(Dev D, AdjDev A, AdjConst
         T si_sq = six * six + siy * siy + siz * siz;
         T F_i, dF_i;
         adj_emb(rho_i, th, F_i, dF_i);
-        double g[ADJ_NF];
-        for (int k = 0; k < ADJ_NF; ++k) g[k] = 0.0;
+        double g[7] = {0, 0, 0, 0, 0, 0, 0};
         int nn = D.nbr_n[i];
-        for (int m = 0; m < nn; ++m) {
+        for (int m = lane; m < nn; m += 32) {
             int pk = D.nbr[(size_t)m * D.natom + i];
             int j = pk & SLD_JMASK;
             double4 rj;
@@ -342,14 +405,17 @@ __global__ void __launch_bounds__(128) k_adj_force_rev(Dev D, AdjDev A, AdjConst
             double4 fbj = A.fb[j];
             double ux = fbi.x - fbj.x, uy = fbi.y - fbj.y, uz = fbi.z - fbj.z;
             T gij = force * (dx * ux + dy * uy + dz * uz);
-            for (int k = 0; k < ADJ_NF; ++k) g[k] += gij.d[k];
+            for (int k = 0; k < 7; ++k) g[k] += gij.d[k];
+            for (int k = 0; k < TH_LANDAU; ++k) loc[k] += 0.5 * gij.d[7 + k];
         }
-        double4 rb = A.rb[i];
-        A.rb[i] = make_double4(rb.x + g[0], rb.y + g[1], rb.z + g[2], 0.0);
-        A.rhob[i] += g[3];
-        double4 sb = A.sb[i];
-        A.sb[i] = make_double4(sb.x + g[4], sb.y + g[5], sb.z + g[6], 0.0);
-        for (int k = 0; k < TH_LANDAU; ++k) loc[k] = 0.5 * g[7 + k];
+        for (int k = 0; k < 7; ++k) g[k] = warp_sum(g[k]);
+        if (lane == 0) {
+            double4 rb = A.rb[i];
+            A.rb[i] = make_double4(rb.x + g[0], rb.y + g[1], rb.z + g[2], 0.0);
+            A.rhob[i] += g[3];
+            double4 sb = A.sb[i];
+            A.sb[i] = make_double4(sb.x + g[4], sb.y + g[5], sb.z + g[6], 0.0);
+        }
     }
     __shared__ double sh[32];
     block_theta(loc, 0, TH_LANDAU, A.thb + (size_t)blockIdx.x * ADJ_NTHETA, sh);
@@ -446,16 +512,25 @@ __global__ void k_adj_clear_rhob(AdjDev A, int n) {
 // s1 if the forward sweep visited it earlier, else its s0.  sbar holds the
 // adjoint of each spin's latest version in reverse order: a visit turns its
 // atom's entry from the rotated spin's adjoint into the input spin's and
-// adds the field's adjoint to the neighbours' entries.
+// adds the field's adjoint to the neighbours' entries.  A warp takes one
+// cell, its lanes the neighbours of a visit.
+__device__ __forceinline__ bool adj_visited_before(const Dev& D, const AdjDev& A, int c, int i,
+                                                   int j, int backward, int group, bool& same) {
+    int cj = D.cell_of[j];
+    same = cj == c;
+    if (same) return backward ? D.cell_slot[j] > D.cell_slot[i] : D.cell_slot[j] < D.cell_slot[i];
+    return backward ? A.cell_group[cj] > group : A.cell_group[cj] < group;
+}
+
 __global__ void __launch_bounds__(128) k_adj_sweep_rev(Dev D, AdjDev A, AdjConst K,
                                                        const int* cells, int n, double dt,
                                                        int backward, int group,
                                                        const double4* __restrict__ s0,
                                                        const double4* __restrict__ s1) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     double lj[2] = {0.0, 0.0};
-    if (t < n) {
-        int c = cells[t];
+    if (w < n) {
+        int c = cells[w];
         int st = D.cell_start[c], cnt = cell_n(D, c);
         const double A0 = K.th[TH_JA], rc = K.th[TH_JRC];
         for (int m = cnt - 1; m >= 0; --m) {
@@ -465,7 +540,7 @@ __global__ void __launch_bounds__(128) k_adj_sweep_rev(Dev D, AdjDev A, AdjConst
             int nn = D.nbr_n[i];
             // the field of the visit
             double hx = 0, hy = 0, hz = 0;
-            for (int e = 0; e < nn; ++e) {
+            for (int e = lane; e < nn; e += 32) {
                 int pk = D.nbr[(size_t)e * D.natom + i];
                 int j = pk & SLD_JMASK;
                 double4 rj;
@@ -474,17 +549,14 @@ __global__ void __launch_bounds__(128) k_adj_sweep_rev(Dev D, AdjDev A, AdjConst
                 if (rsq >= D.rcut_mag_sq) continue;
                 double r = sqrt(rsq);
                 if (r >= rc) continue;
-                int cj = D.cell_of[j];
-                bool before = cj == c ? (backward ? D.cell_slot[j] > D.cell_slot[i]
-                                                  : D.cell_slot[j] < D.cell_slot[i])
-                                      : (backward ? A.cell_group[cj] > group
-                                                  : A.cell_group[cj] < group);
-                double4 sj = before ? s1[j] : s0[j];
+                bool same;
+                double4 sj = adj_visited_before(D, A, c, i, j, backward, group, same) ? s1[j] : s0[j];
                 double u = 1.0 - r / rc;
                 double J = A0 * u * u * u;
                 hx += J * sj.x; hy += J * sj.y; hz += J * sj.z;
             }
-            // Jacobian of the rotation in (H, s)
+            hx = warp_allsum(hx); hy = warp_allsum(hy); hz = warp_allsum(hz);
+            // Jacobian of the rotation in (H, s), on every lane
             typedef Dual<6> T;
             double4 sp = s0[i];
             T H[3] = {dseed<6>(hx, 0), dseed<6>(hy, 1), dseed<6>(hz, 2)};
@@ -498,10 +570,11 @@ __global__ void __launch_bounds__(128) k_adj_sweep_rev(Dev D, AdjDev A, AdjConst
                 hb[k] = ob[0] * o[0].d[k] + ob[1] * o[1].d[k] + ob[2] * o[2].d[k];
                 sin_[k] = ob[0] * o[0].d[3 + k] + ob[1] * o[1].d[3 + k] + ob[2] * o[2].d[3 + k];
             }
-            A.sb[i] = make_double4(sin_[0], sin_[1], sin_[2], 0.0);
+            __syncwarp();
+            if (lane == 0) A.sb[i] = make_double4(sin_[0], sin_[1], sin_[2], 0.0);
             // the field's adjoint to the neighbours' spins, the positions and J
             double rbx = 0, rby = 0, rbz = 0;
-            for (int e = 0; e < nn; ++e) {
+            for (int e = lane; e < nn; e += 32) {
                 int pk = D.nbr[(size_t)e * D.natom + i];
                 int j = pk & SLD_JMASK;
                 double4 rj;
@@ -510,13 +583,8 @@ __global__ void __launch_bounds__(128) k_adj_sweep_rev(Dev D, AdjDev A, AdjConst
                 if (rsq >= D.rcut_mag_sq) continue;
                 double r = sqrt(rsq);
                 if (r >= rc) continue;
-                int cj = D.cell_of[j];
-                bool same = cj == c;
-                bool before = same ? (backward ? D.cell_slot[j] > D.cell_slot[i]
-                                               : D.cell_slot[j] < D.cell_slot[i])
-                                   : (backward ? A.cell_group[cj] > group
-                                               : A.cell_group[cj] < group);
-                double4 sj = before ? s1[j] : s0[j];
+                bool same;
+                double4 sj = adj_visited_before(D, A, c, i, j, backward, group, same) ? s1[j] : s0[j];
                 double u = 1.0 - r / rc;
                 double J = A0 * u * u * u;
                 double dJ = -3.0 * A0 * u * u / rc;
@@ -528,6 +596,7 @@ __global__ void __launch_bounds__(128) k_adj_sweep_rev(Dev D, AdjDev A, AdjConst
                 double* sbj = reinterpret_cast<double*>(A.sb + j);
                 double* rbj = reinterpret_cast<double*>(A.rb + j);
                 if (same) {
+                    // only this warp touches the atoms of its cell
                     sbj[0] += J * hb[0]; sbj[1] += J * hb[1]; sbj[2] += J * hb[2];
                     rbj[0] -= gx; rbj[1] -= gy; rbj[2] -= gz;
                 } else {
@@ -536,8 +605,12 @@ __global__ void __launch_bounds__(128) k_adj_sweep_rev(Dev D, AdjDev A, AdjConst
                     atomicAdd(rbj, -gx); atomicAdd(rbj + 1, -gy); atomicAdd(rbj + 2, -gz);
                 }
             }
-            double4 rb = A.rb[i];
-            A.rb[i] = make_double4(rb.x + rbx, rb.y + rby, rb.z + rbz, 0.0);
+            rbx = warp_sum(rbx); rby = warp_sum(rby); rbz = warp_sum(rbz);
+            if (lane == 0) {
+                double4 rb = A.rb[i];
+                A.rb[i] = make_double4(rb.x + rbx, rb.y + rby, rb.z + rbz, 0.0);
+            }
+            __syncwarp();
         }
     }
     double loc[ADJ_NTHETA];
@@ -641,16 +714,27 @@ __global__ void k_adj_seed_loss(Dev D, AdjDev A) {
 static int adj_blocks(int n, int b) { return (n + b - 1) / b; }
 
 void adj_rho(const Dev& D, const AdjDev& A, const AdjConst& K, cudaStream_t st) {
-    k_adj_rho<<<adj_blocks(D.natom, 128), 128, 0, st>>>(D, A, K);
+    if (D.split)
+        k_adj_rho<true><<<adj_blocks(D.natom, 128), 128, 0, st>>>(D, A, K);
+    else
+        k_adj_rho<false><<<adj_blocks(D.natom, 128), 128, 0, st>>>(D, A, K);
 }
 void adj_force(const Dev& D, const AdjDev& A, const AdjConst& K, cudaStream_t st, double* el2) {
     int nb = adj_blocks(D.natom, 128);
-    k_adj_force<<<nb, 128, 0, st>>>(D, A, K);
+    if (D.split)
+        k_adj_force<true><<<nb, 128, 0, st>>>(D, A, K);
+    else
+        k_adj_force<false><<<nb, 128, 0, st>>>(D, A, K);
     if (el2) k_adj_el<<<1, 32, 0, st>>>(A, nb, el2);
 }
 void adj_sweep(const Dev& D, const AdjConst& K, cudaStream_t st, const int* cells, int n, double dt,
                bool backward) {
-    if (n > 0) k_adj_sweep<<<adj_blocks(n, 128), 128, 0, st>>>(D, K, cells, n, dt, backward);
+    if (n <= 0) return;
+    int nb = adj_blocks(n, 4);   // a warp per cell
+    if (D.split)
+        k_adj_sweep<true><<<nb, 128, 0, st>>>(D, K, cells, n, dt, backward);
+    else
+        k_adj_sweep<false><<<nb, 128, 0, st>>>(D, K, cells, n, dt, backward);
 }
 void adj_kick(const Dev& D, cudaStream_t st, double h, double4* ppre) {
     k_adj_kick<<<1, 1024, 0, st>>>(D, h, ppre);
@@ -661,7 +745,7 @@ void adj_energy_grad(const Dev& D, const AdjDev& A, const AdjConst& K, cudaStrea
     k_adj_theta_acc<<<1, 64, 0, st>>>(A, nb);
 }
 void adj_force_rev(const Dev& D, const AdjDev& A, const AdjConst& K, cudaStream_t st) {
-    int nb = adj_blocks(D.natom, 128);
+    int nb = adj_blocks(D.natom, 4);   // a warp per atom
     k_adj_force_rev<<<nb, 128, 0, st>>>(D, A, K);
     k_adj_theta_acc<<<1, 64, 0, st>>>(A, nb);
 }
@@ -676,12 +760,16 @@ void adj_rho_rev(const Dev& D, const AdjDev& A, const AdjConst& K, cudaStream_t 
     k_adj_theta_acc<<<1, 64, 0, st>>>(A, nb);
     k_adj_clear_rhob<<<adj_blocks(D.natom, 256), 256, 0, st>>>(A, D.natom);
 }
+// the block partials of theta's adjoint stay in A.thb (rows < nb) until
+// adj_theta_flush
 void adj_sweep_rev(const Dev& D, const AdjDev& A, const AdjConst& K, cudaStream_t st,
                    const int* cells, int n, double dt, bool backward, int group, const double4* s0,
                    const double4* s1) {
     if (n <= 0) return;
-    int nb = adj_blocks(n, 128);
+    int nb = adj_blocks(n, 4);   // a warp per cell
     k_adj_sweep_rev<<<nb, 128, 0, st>>>(D, A, K, cells, n, dt, backward, group, s0, s1);
+}
+void adj_theta_flush(const AdjDev& A, cudaStream_t st, int nb) {
     k_adj_theta_acc<<<1, 64, 0, st>>>(A, nb);
 }
 void adj_kick_rev(const Dev& D, const AdjDev& A, cudaStream_t st, double h, const double4* ppre) {

@@ -99,7 +99,8 @@ int alloc_adj(Adj& a, sld_ctx* c, const double* theta) {
     A.fb = a.pool.get<double4>(n);
     A.hb = a.pool.get<double4>(n);
     A.rhob = a.pool.get<double>(n);
-    size_t nblk = std::max<size_t>((size_t)a.nb, (a.nc + 127) / 128);
+    // block rows: a thread per atom, or a warp per atom or cell
+    size_t nblk = std::max<size_t>((a.n + 3) / 4, (a.nc + 3) / 4) + 1;
     A.thb = a.pool.get<double>(nblk * ADJ_NTHETA);
     A.theta_bar = a.pool.get<double>(ADJ_NTHETA);
     a.el2 = a.pool.get<double>(2);
@@ -268,6 +269,9 @@ void sweeps_rev(const Adj& a, const Dev& D, double dt, const double4* s0, const 
     for (int g = G.ngroups - 1; g >= 0; --g)
         adj_sweep_rev(D, a.A, a.K, c->st, c->d_gcells + G.gstart[g], G.gstart[g + 1] - G.gstart[g], h,
                       false, g, s0, mid);
+    int rows = 0;
+    for (int g = 0; g < G.ngroups; ++g) rows = std::max(rows, (G.gstart[g + 1] - G.gstart[g] + 3) / 4);
+    adj_theta_flush(a.A, c->st, rows);
 }
 
 // One step reversed.  In: the adjoints of the step's end state (rb, pb, sb)
@@ -297,7 +301,7 @@ int check_ctx(sld_ctx* c) {
     const sld_params& P = c->P;
     // the NVE spin-lattice step of the reference: no thermostats, no electrons
     if (P.spinlang || P.lattlang || P.eltemp || P.change_step || P.pressure_control ||
-        P.stress_control || P.precision == SLD_SPLIT)
+        P.stress_control)
         return SLD_ERR_ARG;
     return SLD_OK;
 }

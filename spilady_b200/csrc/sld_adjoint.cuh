@@ -29,6 +29,7 @@ void adj_rho_rev(const Dev& D, const AdjDev& A, const AdjConst& K, cudaStream_t 
 void adj_sweep_rev(const Dev& D, const AdjDev& A, const AdjConst& K, cudaStream_t st,
                    const int* cells, int n, double dt, bool backward, int group, const double4* s0,
                    const double4* s1);
+void adj_theta_flush(const AdjDev& A, cudaStream_t st, int nb);
 void adj_kick_rev(const Dev& D, const AdjDev& A, cudaStream_t st, double h, const double4* ppre);
 void adj_drift_rev(const Dev& D, const AdjDev& A, cudaStream_t st, double dt);
 void adj_seed_loss(const Dev& D, const AdjDev& A, cudaStream_t st);

@@ -174,3 +174,54 @@ __device__ __forceinline__ void adj_exch(const T& r, const P& th, T& J, T& dJ) {
         dJ = -3.0 * A * u * u / rc;
     }
 }
+
+// FP32 twins of the pair forms for the split-precision forward pass (the
+// parameters rounded to FP32; the 1.8-2.0 A join and the ZBL core, reached
+// only in close collisions, in FP64)
+__device__ __forceinline__ void adj_dens32(const AdjConst& K, float r, float& f, float& df) {
+    f = 0.f;
+    df = 0.f;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        float kk = (float)K.th[TH_DK + k];
+        if (r < kk) {
+            float u = kk - r, a = (float)K.th[TH_DA + k];
+            f = fmaf(a * u * u, u, f);
+            df = fmaf(-3.f * a, u * u, df);
+        }
+    }
+}
+
+__device__ __forceinline__ void adj_pair32(const AdjConst& K, double r64, float& v, float& dv) {
+    float r = (float)r64;
+    if (r64 > 2.0) {
+        v = 0.f;
+        dv = 0.f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            float kk = (float)K.th[TH_PK + k];
+            if (r < kk) {
+                float u = kk - r, V = (float)K.th[TH_PV + k];
+                v = fmaf(V * u * u, u, v);
+                dv = fmaf(-3.f * V, u * u, dv);
+            }
+        }
+    } else {
+        double v64, dv64;
+        adj_pair(K, r64, ThPlain{K.th}, v64, dv64);
+        v = (float)v64;
+        dv = (float)dv64;
+    }
+}
+
+__device__ __forceinline__ void adj_exch32(const AdjConst& K, float r, float& J, float& dJ) {
+    float A = (float)K.th[TH_JA], rc = (float)K.th[TH_JRC];
+    J = 0.f;
+    dJ = 0.f;
+    if (r < rc) {
+        float u = 1.f - r / rc;
+        J = A * u * u * u;
+        dJ = -3.f * A * u * u / rc;
+    }
+}
+

@@ -121,3 +121,19 @@ def test_adjoint_dynamics_are_the_engine_step_and_leave_the_state():
     fresh.run(3)
     for k in ("r", "p", "s"):
         assert np.array_equal(e.get(k), fresh.get(k)), k
+
+
+def test_split_forward_gradient_tracks_fp64():
+    # forward in split FP32 (pair terms in FP32 with compensated sums),
+    # adjoint in FP64: the gradient of the FP64 model along the split
+    # trajectory, against the FP64 finite differences
+    params, r, p, s, e64 = system()
+    es = E().Engine(params, r, p, s, precision=E().SPLIT)
+    th = E().adjoint_theta_default()
+    K = 10
+    L64, g64 = e64.adjoint_trajectory(th, K, 5)
+    Ls, gs = es.adjoint_trajectory(th, K, 5)
+    assert abs(Ls - L64) <= 1e-5 * L64
+    err = np.max(np.abs(gs - g64)) / np.max(np.abs(g64))
+    print(f"split forward: L rel {abs(Ls - L64) / L64:.1e}, gradient rel {err:.1e}")
+    assert err <= 1e-4
