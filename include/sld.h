@@ -59,6 +59,13 @@ extern "C" {
    SLD_SPLIT). */
 typedef enum { SLD_FP64 = 0, SLD_SPLIT = 1, SLD_FP64_ANALYTIC = 2 } sld_precision;
 
+/* The Hamiltonian, control.h's mode switch (control.h:8-12; core.cpp:31-76):
+   SLDHL spin-lattice, Heisenberg-Landau (the default); SLDH spin-lattice,
+   Heisenberg; MD lattice only; SDH and SDHL spins only, on a fixed lattice. */
+typedef enum {
+    SLD_HAM_SLDHL = 0, SLD_HAM_SLDH = 1, SLD_HAM_MD = 2, SLD_HAM_SDH = 3, SLD_HAM_SDHL = 4
+} sld_hamiltonian;
+
 typedef struct {
     double box[6];               /* d.xx d.yx d.yy d.zx d.zy d.zz (Angstrom);
                                     struct.h box_vector, upper-triangular */
@@ -109,6 +116,9 @@ typedef struct {
     double baro_damping_time;    /* s                             default.h:192 */
     double displace_limit;       /* Angstrom per step             default.h:218 */
     double phi_limit;            /* rad per step                  default.h:219 */
+    int hamiltonian;             /* sld_hamiltonian */
+    double gamma_S_H;            /* spin Langevin, Heisenberg (SDH, SLDH), unitless
+                                                                  default.h:172 */
 } sld_params;
 
 typedef struct sld_ctx sld_ctx;
@@ -284,7 +294,8 @@ int sld_last_run_ms(sld_ctx* ctx, double* out);
    device milliseconds of: links, core_dTe (both calls), core_dp (both),
    core_ds (both), core_dr, calculate_rho, calculate_force_energy,
    calculate_temperature, energy check, bookkeeping.  The step advances the
-   state exactly as sld_run(ctx, 1) does. */
+   state exactly as sld_run(ctx, 1) does.  Spin-lattice Hamiltonians (SLDHL,
+   SLDH) only. */
 #define SLD_PHASES 10
 int sld_profile_step(sld_ctx* ctx, double* ms_out);
 

@@ -15,6 +15,10 @@
 #   langte  + eltemp + localcolmot + renormalizeEnergy
 #   baro    NVE + PRESSURE + STRESS  (Berendsen barostats, scale.cpp)
 #   dtstep  NVE + changestep          (adaptive time step, scale_step_CPU.cpp)
+# and the other Hamiltonians (-DMD, -DSDH, -DSDHL, -DSLDH in place of -DSLDHL),
+# each without thermostats and with the Langevin thermostats of its degrees
+# of freedom:
+#   md md_lang  sdh sdh_lang  sdhl sdhl_lang  sldh sldh_lang
 #
 # usage: sh oracle/ref/build.sh [reference_dir]
 set -e
@@ -28,9 +32,17 @@ fi
 mkdir -p "$OUT"
 # the system g++ (an inherited CXX may point at a compiler without libgomp)
 CXX=${ORACLE_CXX:-g++}
-FLAGS="-O3 -fopenmp -U_FORTIFY_SOURCE -D_FORTIFY_SOURCE=0 -DCPU -DOMP -DSLDHL -w"
+BASE="-O3 -fopenmp -U_FORTIFY_SOURCE -D_FORTIFY_SOURCE=0 -DCPU -DOMP -w"
 
-for mode in nve lang langte baro dtstep; do
+for mode in nve lang langte baro dtstep md md_lang sdh sdh_lang sdhl sdhl_lang sldh sldh_lang; do
+    case "$mode" in
+    md*) ham=MD ;;
+    sdhl*) ham=SDHL ;;
+    sdh*) ham=SDH ;;
+    sldh*) ham=SLDH ;;
+    *) ham=SLDHL ;;
+    esac
+    FLAGS="$BASE -D$ham"
     src="$OUT/src_$mode"
     obj="$OUT/obj_$mode"
     mkdir -p "$src" "$obj"
@@ -52,6 +64,9 @@ for mode in nve lang langte baro dtstep; do
             echo "#define renormalizeEnergy" ;;
         baro) echo "#define PRESSURE"; echo "#define STRESS" ;;
         dtstep) echo "#define changestep" ;;
+        md_lang) echo "#define lattlang" ;;
+        sdh_lang|sdhl_lang) echo "#define spinlang" ;;
+        sldh_lang) echo "#define spinlang"; echo "#define lattlang" ;;
         esac
     } > "$src/control.h.new"
     if ! cmp -s "$src/control.h.new" "$src/control.h"; then

@@ -42,6 +42,17 @@
 #define MAIN
 #include "spilady.h"
 
+/* what the compiled Hamiltonian has (struct.h:44-118 declares the fields) */
+#if defined MD || defined SLDH || defined SLDHL
+#define H_LATT 1
+#endif
+#if defined SDH || defined SDHL || defined SLDH || defined SLDHL
+#define H_SPIN 1
+#endif
+#if defined SDHL || defined SLDHL
+#define H_HL 1
+#endif
+
 #include <stdio.h>
 #include <stdint.h>
 #include <vector>
@@ -82,18 +93,50 @@ static void dump(FILE* out) {
         atom_struct* p = first_atom_ptr + i;
         double* o = &a[(size_t)i * ATOM_FIELDS];
         int k = 0;
+        /* fields the compiled Hamiltonian lacks are written as 0 */
+        for (int q = 0; q < ATOM_FIELDS; ++q) o[q] = 0.0;
         o[k++] = p->r.x; o[k++] = p->r.y; o[k++] = p->r.z;
+#ifdef H_LATT
         o[k++] = p->p.x; o[k++] = p->p.y; o[k++] = p->p.z;
         o[k++] = p->f.x; o[k++] = p->f.y; o[k++] = p->f.z;
+#else
+        k += 6;
+#endif
+#ifdef H_SPIN
         o[k++] = p->s.x; o[k++] = p->s.y; o[k++] = p->s.z;
         o[k++] = p->s0;
         o[k++] = p->Heff_H.x; o[k++] = p->Heff_H.y; o[k++] = p->Heff_H.z;
+#else
+        k += 7;
+#endif
+#ifdef H_HL
         o[k++] = p->Heff_L.x; o[k++] = p->Heff_L.y; o[k++] = p->Heff_L.z;
+#else
+        k += 3;
+#endif
+#ifdef H_LATT
         o[k++] = p->rho; o[k++] = p->pe; o[k++] = p->ke;
-        o[k++] = p->me; o[k++] = p->me0; o[k++] = p->vir;
+#else
+        k += 3;
+#endif
+#ifdef H_SPIN
+        o[k++] = p->me; o[k++] = p->me0;
+#else
+        k += 2;
+#endif
+#ifdef H_LATT
+        o[k++] = p->vir;
         o[k++] = p->stress11; o[k++] = p->stress22; o[k++] = p->stress33;
         o[k++] = p->stress12; o[k++] = p->stress23; o[k++] = p->stress31;
-        o[k++] = p->sum_Jij_sj; o[k++] = p->local_volume;
+#else
+        k += 7;
+#endif
+#ifdef SLDHL
+        o[k++] = p->sum_Jij_sj;
+#else
+        k += 1;
+#endif
+        o[k++] = p->local_volume;
         o[k++] = (double)p->new_cell_index;
         if (k != ATOM_FIELDS) die("field count");
     }
@@ -106,8 +149,16 @@ static void dump(FILE* out) {
         double* o = &c[(size_t)i * 8];
         o[0] = q->no_of_atoms_in_cell;
 #ifdef eltemp
-        o[1] = q->Te / boltz; o[2] = q->Ee; o[3] = q->Tl;
-        o[4] = q->Ts_R; o[5] = q->Ts_L; o[6] = q->Gel; o[7] = q->Ges;
+        o[1] = q->Te / boltz; o[2] = q->Ee;
+#ifdef H_LATT
+        o[3] = q->Tl; o[6] = q->Gel;
+#endif
+#ifdef H_SPIN
+        o[4] = q->Ts_R; o[7] = q->Ges;
+#endif
+#ifdef H_HL
+        o[5] = q->Ts_L;
+#endif
 #endif
     }
     wr(out, c.data(), c.size());
@@ -163,9 +214,19 @@ int main(int argc, char** argv) {
     gamma_L = gamma_L_over_mass * atmass;
 #endif
 #ifdef spinlang
+#if defined SDH || defined SLDH
+    gamma_S_H = pr[10];
+#else
     gamma_S_HL = pr[10];
 #endif
-    rcut_pot = pr[11]; rcut_mag = pr[12]; rcut_max = pr[13];
+#endif
+#ifdef H_LATT
+    rcut_pot = pr[11];
+#endif
+#ifdef H_SPIN
+    rcut_mag = pr[12];
+#endif
+    rcut_max = pr[13];
     min_length_link_cell = pr[14];
 #ifdef eltemp
     kappa_e = pr[15];
@@ -173,8 +234,12 @@ int main(int argc, char** argv) {
     random_seed = seed;
     /* read_variables.cpp:256-276 */
     if (rcut_max > min_length_link_cell) min_length_link_cell = rcut_max + 0.001;
+#ifdef H_LATT
     rcut_pot_sq = pow(rcut_pot, 2);
+#endif
+#ifdef H_SPIN
     rcut_mag_sq = pow(rcut_mag, 2);
+#endif
     rcut_max_sq = pow(rcut_max, 2);
 
     potential_table();
@@ -189,12 +254,16 @@ int main(int argc, char** argv) {
     for (int i = 0; i < n; ++i) {
         atom_struct* a = first_atom_ptr + i;
         a->r = vec_init(r[3 * i], r[3 * i + 1], r[3 * i + 2]);
+#ifdef H_LATT
         a->p = vec_init(p[3 * i], p[3 * i + 1], p[3 * i + 2]);
+        a->ke = vec_sq(a->p) / 2e0 / atmass;
+#endif
+#ifdef H_SPIN
         a->s = vec_init(s[3 * i], s[3 * i + 1], s[3 * i + 2]);
         a->s0 = vec_length(a->s);
         a->m = vec_times(-el_g, a->s);
         a->m0 = vec_length(a->m);
-        a->ke = vec_sq(a->p) / 2e0 / atmass;
+#endif
         a->element[0] = 'F'; a->element[1] = 'e';
     }
     box_length.x = fabs(d.xx);
@@ -218,7 +287,9 @@ int main(int argc, char** argv) {
 #endif
     initial_links();
     allocate_cells();
+#ifdef H_LATT
     calculate_rho();
+#endif
     calculate_force_energy();
 #ifdef eltemp
     calculate_temperature();
@@ -245,11 +316,15 @@ int main(int argc, char** argv) {
         switch (code) {
         case OP_DUMP: dump(out); break;
         case OP_LINKS: links(); break;
-        case OP_RHO: calculate_rho(); break;
         case OP_FORCE: calculate_force_energy(); break;
-        case OP_DS: core_ds(arg); break;
+#ifdef H_LATT
+        case OP_RHO: calculate_rho(); break;
         case OP_DP: core_dp(arg); break;
         case OP_DR: core_dr(arg); break;
+#endif
+#ifdef H_SPIN
+        case OP_DS: core_ds(arg); break;
+#endif
 #ifdef eltemp
         case OP_DTE: core_dTe(arg); break;
         case OP_TEMP: calculate_temperature(); break;

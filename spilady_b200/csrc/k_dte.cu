@@ -69,16 +69,18 @@ __device__ __forceinline__ double te_lap(const DteGeom& g, double T, double xp, 
 }
 
 // Gel Tl + Ges Ts_L and (Gel + Ges) hh / boltz of cell k
+// (core_dTe_CPU.cpp:66-122: the lattice's and the spins' coupling, by what
+// the Hamiltonian has; Ts_R for the Heisenberg Hamiltonians)
 __device__ __forceinline__ double te_src(const Dev& D, int k) {
     double dE = 0.0;
-    dE += D.Gel[k] * D.Tl[k];
-    dE += D.Ges[k] * D.TsL[k];
+    if (D.latt) dE += D.Gel[k] * D.Tl[k];
+    if (D.spin) dE += D.Ges[k] * (D.landau_on ? D.TsL[k] : D.TsR[k]);
     return dE;
 }
 __device__ __forceinline__ double te_rate(const Dev& D, int k, double hh) {
     double g = 0.0;
-    g += D.Gel[k];
-    g += D.Ges[k];
+    if (D.latt) g += D.Gel[k];
+    if (D.spin) g += D.Ges[k];
     g *= hh / SLD_BOLTZ;
     return g;
 }

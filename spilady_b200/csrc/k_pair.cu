@@ -224,12 +224,14 @@ __device__ __forceinline__ void force_finish(const Dev& D, int i, double si_sq, 
         D.pe[i] = pe;
     }
     if (PART & PART_MAG) {
-        double A = interp_const(D.landau[0], rho_i, D.inv_rho);
-        double B = interp_const(D.landau[1], rho_i, D.inv_rho);
-        double C = interp_const(D.landau[2], rho_i, D.inv_rho);
-        double Dd = interp_const(D.landau[3], rho_i, D.inv_rho);
-        double s4 = si_sq * si_sq;
-        me += A * si_sq + B * s4 + C * (s4 * si_sq) + Dd * (s4 * s4);
+        if (D.landau_on) {   // the Heisenberg-Landau Hamiltonians
+            double A = interp_const(D.landau[0], rho_i, D.inv_rho);
+            double B = interp_const(D.landau[1], rho_i, D.inv_rho);
+            double C = interp_const(D.landau[2], rho_i, D.inv_rho);
+            double Dd = interp_const(D.landau[3], rho_i, D.inv_rho);
+            double s4 = si_sq * si_sq;
+            me += A * si_sq + B * s4 + C * (s4 * si_sq) + Dd * (s4 * s4);
+        }
         D.me[i] = me;
         D.me0[i] = me0;
     }
@@ -430,9 +432,13 @@ void launch_embed(const Dev& D, cudaStream_t st) {
     else if (D.analytic) k_embed<2><<<nb, 256, 0, st>>>(D);
     else k_embed<0><<<nb, 256, 0, st>>>(D);
 }
+// all terms of the Hamiltonian: MD has no spins
 void launch_force(const Dev& D, cudaStream_t st) {
     launch_embed(D, st);
-    launch_force_part<PART_ALL>(D, st);
+    if (D.spin)
+        launch_force_part<PART_ALL>(D, st);
+    else
+        launch_force_part<PART_EAM>(D, st);
 }
 void launch_force_eam(const Dev& D, cudaStream_t st) {
     launch_embed(D, st);

@@ -403,8 +403,9 @@ __device__ __forceinline__ void visit_field(const Dev& D, const VisitRegs<SPLIT>
     sumJ = hj;
 }
 
-// the walk of one cell c in the reference's order (backward: tail -> head)
-template <bool SPLIT, bool CG>
+// the walk of one cell c in the reference's order (backward: tail -> head);
+// INTEG 0: the Heisenberg-Landau visit, 1: the Heisenberg one (SDH, SLDH)
+template <bool SPLIT, bool CG, int INTEG = 0>
 __device__ __forceinline__ void cell_walk(const Dev& D, int c, double dt, int backward) {
     constexpr bool kDeep = SPLIT;   // indices two visits ahead
     const int n = cell_n(D, c);
@@ -432,6 +433,7 @@ __device__ __forceinline__ void cell_walk(const Dev& D, int c, double dt, int ba
         double sumJ;
         visit_field<SPLIT, CG>(D, v, H, sumJ);
         const double3 s_old = make_double3(v.si.x, v.si.y, v.si.z);
+        const double s0_old = v.si.w;
         const double rho = v.rho;
         const double3 dS = v.dS;
         const bool more = m + 1 < n;
@@ -446,8 +448,12 @@ __device__ __forceinline__ void cell_walk(const Dev& D, int c, double dt, int ba
                 i_after = m + 2 < n ? atom_at(m + 2) : -1;
             }
         }
-        double3 HL;
-        double3 s = spin_integrate_dS(D, s_old, H, sumJ, rho, dS, dt, HL);
+        double3 HL = make_double3(0.0, 0.0, 0.0);
+        double3 s;
+        if constexpr (INTEG == 1)
+            s = spin_integrate_H(D, s_old, s0_old, H, dS, dt);
+        else
+            s = spin_integrate_dS(D, s_old, H, sumJ, rho, dS, dt, HL);
         double s0 = sqrt(s.x * s.x + s.y * s.y + s.z * s.z);
         if (!isfinite(s0)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
         const double4 s4 = make_double4(s.x, s.y, s.z, s0);
@@ -456,7 +462,7 @@ __device__ __forceinline__ void cell_walk(const Dev& D, int c, double dt, int ba
         if constexpr (SPLIT) D.s32[i] = sr;
         if (fields) {
             D.H[i] = make_double4(H.x, H.y, H.z, 0.0);
-            D.HL[i] = make_double4(HL.x, HL.y, HL.z, 0.0);
+            if constexpr (INTEG == 0) D.HL[i] = make_double4(HL.x, HL.y, HL.z, 0.0);
             if (D.spinlang) D.sumJ[i] = sumJ;
         }
         if (more) {
@@ -467,12 +473,12 @@ __device__ __forceinline__ void cell_walk(const Dev& D, int c, double dt, int ba
     }
 }
 
-template <bool SPLIT>
+template <bool SPLIT, int INTEG>
 __global__ void __launch_bounds__(128) k_sweep_pipe(Dev D, const int* __restrict__ gcells,
                                                     int ncell_g, double dt, int backward) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ncell_g) return;
-    cell_walk<SPLIT, false>(D, gcells[t], dt, backward);
+    cell_walk<SPLIT, false, INTEG>(D, gcells[t], dt, backward);
 }
 
 // ---------------------------------------------------------------------
@@ -626,16 +632,25 @@ void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g,
                   bool backward, bool fields) {
     if (ncell_g <= 0) return;
     const int b = (backward ? SW_BACKWARD : 0) | (fields ? 0 : SW_NO_FIELDS);
-    if (g_sweep_mode >= 2) {
+    if (g_sweep_mode >= 2 || D.hint) {
         // Block sizes that fill the register file: the split form's kernel takes
         // about 200 registers a thread, 9 warps an SM, so blocks of 3 warps
         // (128-thread blocks would leave one warp's registers idle; holding it
         // to 200 registers for a tenth warp measured slower); the FP64 form's
-        // 255 registers allow 8 warps, 2 blocks of 4.
-        if (D.split)
-            k_sweep_pipe<true><<<div_up(ncell_g, 96), 96, 0, st>>>(D, gcells, ncell_g, dt, b);
-        else
-            k_sweep_pipe<false><<<div_up(ncell_g, 128), 128, 0, st>>>(D, gcells, ncell_g, dt, b);
+        // 255 registers allow 8 warps, 2 blocks of 4.  The Heisenberg
+        // Hamiltonians' visit has its own instance (the other sweep variants
+        // have only the Heisenberg-Landau visit).
+        if (D.split) {
+            if (D.hint)
+                k_sweep_pipe<true, 1><<<div_up(ncell_g, 96), 96, 0, st>>>(D, gcells, ncell_g, dt, b);
+            else
+                k_sweep_pipe<true, 0><<<div_up(ncell_g, 96), 96, 0, st>>>(D, gcells, ncell_g, dt, b);
+        } else {
+            if (D.hint)
+                k_sweep_pipe<false, 1><<<div_up(ncell_g, 128), 128, 0, st>>>(D, gcells, ncell_g, dt, b);
+            else
+                k_sweep_pipe<false, 0><<<div_up(ncell_g, 128), 128, 0, st>>>(D, gcells, ncell_g, dt, b);
+        }
         return;
     }
     if (g_sweep_mode == 1) {

@@ -20,6 +20,8 @@ __device__ __forceinline__ void gather_field_t(const Dev& D, int i, double3& H, 
 // the five sums (R_up, R_dn, L_up, L_dn) it contributes
 __device__ __forceinline__ void temp_atom(const Dev& D, int i, double& Rup, double& Rdn, double& Lup,
                                           double& Ldn) {
+    Rup = Rdn = Lup = Ldn = 0.0;
+    if (!D.spin) return;
     double3 H;
     double sumJ;
     gather_field_t(D, i, H, sumJ);
@@ -28,6 +30,9 @@ __device__ __forceinline__ void temp_atom(const Dev& D, int i, double& Rup, doub
     double cx_ = s.y * H.z - H.y * s.z, cy_ = s.z * H.x - H.z * s.x, cz_ = s.x * H.y - H.x * s.y;
     Rup = cx_ * cx_ + cy_ * cy_ + cz_ * cz_;
     Rdn = s.x * H.x + s.y * H.y + s.z * H.z;
+    D.H[i] = make_double4(H.x, H.y, H.z, 0.0);
+    if (!D.landau_on) return;   // the Heisenberg Hamiltonians: no Landau field
+    if (!D.hc) sumJ = 0.0;      // the exchange correction is SLDHL's
     double rho = D.rho[i];
     double A = interp_const(D.landau[0], rho, D.inv_rho);
     double B = interp_const(D.landau[1], rho, D.inv_rho);
@@ -42,9 +47,8 @@ __device__ __forceinline__ void temp_atom(const Dev& D, int i, double& Rup, doub
     Lup = hx * hx + hy * hy + hz * hz;
     Ldn = 6.0 * A + 20.0 * B * s_sq + 42.0 * C * (s_sq * s_sq) + 72.0 * Dd * (s_sq * s_sq * s_sq);
     Ldn += 2.0 * sumJ / s0;
-    D.H[i] = make_double4(H.x, H.y, H.z, 0.0);
     D.HL[i] = make_double4(HL.x, HL.y, HL.z, 0.0);
-    D.sumJ[i] = sumJ;
+    if (D.hc) D.sumJ[i] = sumJ;
 }
 
 // per-Te-cell results from the sums (calculate_temperature_CPU.cpp:118-142)
@@ -52,7 +56,8 @@ __device__ __forceinline__ void temp_finish(const Dev& D, int k, double n, doubl
                                             double apy, double apz, double Rup, double Rdn, double Lup,
                                             double Ldn) {
     double per = (double)D.natom / (double)D.nte;
-    if (D.localcolmot) {
+    if (!D.latt) {
+    } else if (D.localcolmot) {
         apx = apx / n; apy = apy / n; apz = apz / n;
         sum_ke -= n * (apx * apx + apy * apy + apz * apz) / 2.0 / D.atmass;
         D.Tl[k] = 2.0 / 3.0 * sum_ke / (n - 1.0) / SLD_BOLTZ;
@@ -61,12 +66,17 @@ __device__ __forceinline__ void temp_finish(const Dev& D, int k, double n, doubl
         D.Tl[k] = sum_ke * 2.0 / 3.0 / n / SLD_BOLTZ;
         D.Gel[k] = 3.0 * n * SLD_BOLTZ * D.gamma_L / D.atmass / per;
     }
-    D.TsR[k] = Rup / Rdn / 2.0 / SLD_BOLTZ;
-    D.TsL[k] = Lup / Ldn / SLD_BOLTZ;
+    if (D.spin) D.TsR[k] = Rup / Rdn / 2.0 / SLD_BOLTZ;
+    if (D.landau_on) {
+        D.TsL[k] = Lup / Ldn / SLD_BOLTZ;
+        D.Ges[k] = SLD_BOLTZ * D.gamma_S_HL * Ldn / per;
+    } else if (D.spin) {
+        // the Heisenberg Hamiltonians (calculate_temperature_CPU.cpp:128-131)
+        D.Ges[k] = 2e0 * SLD_BOLTZ * D.gamma_S_H * Rdn / SLD_HBAR / per;
+    }
     // the cell sums check_temperature adds up (check_temperature_CPU.cpp:49-55,86-92)
     double* q = D.trl + 4 * (size_t)k;
     q[0] = Rup; q[1] = Rdn; q[2] = Lup; q[3] = Ldn;
-    D.Ges[k] = SLD_BOLTZ * D.gamma_S_HL * Ldn / per;
 }
 
 // Te on link cells: one thread per cell, atoms in list order (the
@@ -191,15 +201,15 @@ __global__ void __launch_bounds__(1024) k_renorm(Dev D, int nb, int mode) {
         double n = (double)D.natom;
         double pe = a / n, ke = b / n, me = c / n, me0 = d / n, Ee = e / n;
         double err = 0.0;
-        if (mode == 0) {
-            double t = 0.0;
-            t += pe; t += ke; t += me; t += me0; t += Ee;
+        // the terms of the Hamiltonian's energy (check_energy_CPU.cpp:86-108)
+        double t = 0.0;
+        if (D.latt) { t += pe; t += ke; }
+        if (D.spin) { t += me; t += me0; }
+        t += Ee;
+        if (mode == 0)
             D.ctl->initial_ave_energy = t;
-        } else {
-            double t = 0.0;
-            t += pe; t += ke; t += me; t += me0; t += Ee;
+        else
             err = t - D.ctl->initial_ave_energy;
-        }
         err_s = err;
         // what check_energy prints for this step (check_energy_CPU.cpp:113-130)
         D.ctl->chk[0] = pe; D.ctl->chk[1] = ke; D.ctl->chk[2] = me; D.ctl->chk[3] = me0;

@@ -73,7 +73,7 @@ void enqueue_ds(sld_ctx* c, const Dev& D, double dt, int& eoff, bool fields = tr
     const auto& G = c->G;
     double dt_half = dt / 2e0;
     if (c->P.spinlang) launch_spin_noise(D, c->st, eoff, dt_half);
-    if (sweep_uses_flow()) {
+    if (sweep_uses_flow() && !D.hint) {
         launch_sweep_flow(D, c->st, c->flow, dt_half, fields);
         if (c->P.spinlang) eoff += 2;
         return;
@@ -102,7 +102,52 @@ void enqueue_dp(sld_ctx* c, double dt, int& eoff) { enqueue_dp(c, c->D, dt, eoff
 //   second:  core_dTe(dt/2) |  dr | rho + lists | force(EAM)
 // The lists and rho of this step go to the other buffer set, so the first
 // sweep still reads the previous ones; the step ends with that set current.
+// MD (core.cpp:38-56 without spins): links | dp | dr | rho | forces | dp
+void enqueue_step_md(sld_ctx* c) {
+    double dt = c->P.step;
+    int eoff = 0;
+    const Dev Dc = dev_set(c, c->cur), Dn = dev_set(c, 1 - c->cur);
+    cudaStream_t M = c->st;
+    launch_links(Dc, M, false, c->scan_blocks);
+    if (c->P.eltemp) launch_dte(Dc, M, dt / 2e0);
+    enqueue_dp(c, Dc, dt / 2e0, eoff);
+    launch_dr(Dc, M, dt);
+    launch_pairs(Dn, M, true);
+    launch_force(Dn, M);
+    c->force_volume = Dn.box_volume;
+    enqueue_dp(c, Dn, dt / 2e0, eoff);
+    if (c->P.eltemp) {
+        launch_temperature(Dn, M);
+        launch_dte(Dn, M, dt / 2e0);
+        if (c->P.renormalize_energy) launch_energy_check(Dn, M, 1);
+    }
+    launch_advance(Dn, M, eoff, 1);
+}
+
+// SDH, SDHL (core.cpp:41-48): the spins on a fixed lattice, core_ds(step);
+// the energies of the force pass every step (the reference forms them at
+// print-out steps only; nothing else reads them).  Both buffer sets hold the
+// same lists and rho (sld_set_state), so the alternation of the step graphs
+// changes nothing.
+void enqueue_step_spin(sld_ctx* c) {
+    double dt = c->P.step;
+    int eoff = 0;
+    const Dev Dc = dev_set(c, c->cur);
+    cudaStream_t M = c->st;
+    if (c->P.eltemp) launch_dte(Dc, M, dt / 2e0);
+    enqueue_ds(c, Dc, dt, eoff, !c->P.eltemp);
+    launch_force(Dc, M);
+    if (c->P.eltemp) {
+        launch_temperature(Dc, M);
+        launch_dte(Dc, M, dt / 2e0);
+        if (c->P.renormalize_energy) launch_energy_check(Dc, M, 1);
+    }
+    launch_advance(Dc, M, eoff, 1);
+}
+
 void enqueue_step(sld_ctx* c) {
+    if (!c->D.spin) return enqueue_step_md(c);
+    if (!c->D.latt) return enqueue_step_spin(c);
     double dt = c->P.step;
     int eoff = 0;
     const Dev Dc = dev_set(c, c->cur), Dn = dev_set(c, 1 - c->cur);
@@ -184,8 +229,14 @@ int validate(const sld_params* p) {
     if (!(p->step > 0) || !(p->atmass > 0) || !(p->temperature >= 0)) return SLD_ERR_ARG;
     if (!(p->rcut_pot > 0 && p->rcut_mag > 0 && p->rcut_max > 0)) return SLD_ERR_ARG;
     if (p->rcut_pot > p->rcut_max || p->rcut_mag > p->rcut_max) return SLD_ERR_ARG;
-    if (p->eltemp && !(p->spinlang && p->lattlang)) return SLD_ERR_ARG;
+    if (p->hamiltonian < SLD_HAM_SLDHL || p->hamiltonian > SLD_HAM_SDHL) return SLD_ERR_ARG;
+    const bool latt = p->hamiltonian <= SLD_HAM_MD, spin = p->hamiltonian != SLD_HAM_MD;
+    // thermostats of degrees of freedom the Hamiltonian has; with eltemp the
+    // thermostats of all of them (the reference would not compile the rest)
+    if ((p->spinlang && !spin) || (p->lattlang && !latt)) return SLD_ERR_ARG;
+    if (p->eltemp && !((p->spinlang || !spin) && (p->lattlang || !latt))) return SLD_ERR_ARG;
     if (p->localcolmot && !p->lattlang) return SLD_ERR_ARG;
+    if ((p->pressure_control || p->stress_control) && !latt) return SLD_ERR_ARG;
     if (p->precision != SLD_FP64 && p->precision != SLD_SPLIT &&
         p->precision != SLD_FP64_ANALYTIC)
         return SLD_ERR_ARG;
@@ -265,6 +316,8 @@ int sld_params_default(sld_params* o) {
     o->atmass = 55.847e0;
     o->gamma_L_over_mass = 6e11;
     o->gamma_S_HL = 5.88e13;
+    o->gamma_S_H = 8e-3;
+    o->hamiltonian = SLD_HAM_SLDHL;
     o->rcut_pot = 4.1001;
     o->rcut_mag = 3.7501;
     o->rcut_max = 4.1001;
@@ -342,6 +395,13 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     D.temperature = prm->temperature * kBoltz;
     D.gamma_L = prm->gamma_L_over_mass * D.atmass;
     D.gamma_S_HL = prm->gamma_S_HL;
+    D.gamma_S_H = prm->gamma_S_H;
+    D.ham = prm->hamiltonian;
+    D.latt = (D.ham == SLD_HAM_SLDHL || D.ham == SLD_HAM_SLDH || D.ham == SLD_HAM_MD) ? 1 : 0;
+    D.spin = D.ham != SLD_HAM_MD ? 1 : 0;
+    D.landau_on = (D.ham == SLD_HAM_SLDHL || D.ham == SLD_HAM_SDHL) ? 1 : 0;
+    D.hc = D.ham == SLD_HAM_SLDHL ? 1 : 0;
+    D.hint = (D.ham == SLD_HAM_SDH || D.ham == SLD_HAM_SLDH) ? 1 : 0;
     D.step = prm->step;
     D.inv_r = T.inv_r;
     D.inv_rho = T.inv_rho;
@@ -510,6 +570,8 @@ int sld_set_state(sld_ctx* c, const double* r, const double* p, const double* s)
     // initialize(): links, rho, forces, cell temperatures, reference energy
     launch_links(D, c->st, true, c->scan_blocks);
     launch_pairs(D, c->st, true);
+    // a fixed lattice: both buffer sets get the (only) lists and densities
+    if (!D.latt) launch_pairs(dev_set(c, 1 - c->cur), c->st, true);
     c->lists_stale = false;
     launch_force(D, c->st);
     c->force_volume = D.box_volume;
@@ -783,6 +845,7 @@ void sld_batch_destroy(sld_batch* b) {
 
 int sld_profile_step(sld_ctx* c, double* ms) {
     if (!c || !ms) return SLD_ERR_ARG;
+    if (!c->D.latt || !c->D.spin) return SLD_ERR_ARG;   // the spin-lattice step's phases
     fresh_lists(c);
     cudaEvent_t ev[2];
     CK(cudaEventCreate(&ev[0]));
@@ -1013,7 +1076,10 @@ int sld_check(sld_ctx* c, const char* dir, const char* out_body, int current_ste
     if (el && c->P.renormalize_energy && ctl.chk_tag == (long long)current_step + 2) {
         pe = ctl.chk[0]; ke = ctl.chk[1]; me = ctl.chk[2]; me0 = ctl.chk[3]; Ee = ctl.chk[4];
     }
-    v[k++] = t; v[k++] = pe; v[k++] = ke; v[k++] = me; v[k++] = me0;
+    // the columns of the Hamiltonian's degrees of freedom
+    v[k++] = t;
+    if (D.latt) { v[k++] = pe; v[k++] = ke; }
+    if (D.spin) { v[k++] = me; v[k++] = me0; }
     if (el) v[k++] = Ee;
     rc = sld::append_line(sld::out_path(dir, "enr-", out_body, -1), current_step, v, k);
     if (rc) return rc;
@@ -1021,38 +1087,40 @@ int sld_check(sld_ctx* c, const char* dir, const char* out_body, int current_ste
     // check_temperature
     k = 0;
     v[k++] = t;
-    v[k++] = S[SLD_CHK_KE] * 2e0 / 3e0 / n / kBoltz;
-    v[k++] = S[SLD_CHK_RUP] / S[SLD_CHK_RDN] / 2e0 / kBoltz;
-    v[k++] = S[SLD_CHK_LUP] / S[SLD_CHK_LDN] / kBoltz;
+    if (D.latt) v[k++] = S[SLD_CHK_KE] * 2e0 / 3e0 / n / kBoltz;
+    if (D.spin) v[k++] = S[SLD_CHK_RUP] / S[SLD_CHK_RDN] / 2e0 / kBoltz;
+    if (D.landau_on) v[k++] = S[SLD_CHK_LUP] / S[SLD_CHK_LDN] / kBoltz;
     if (el) v[k++] = S[SLD_CHK_TE] / (double)D.nte / kBoltz;
     rc = sld::append_line(sld::out_path(dir, "tmp-", out_body, -1), current_step, v, k);
     if (rc) return rc;
+    if (D.latt) {
+        // check_stress: per-atom stresses in eV/A^3, averaged and converted to GPa
+        double st[6];
+        for (int q = 0; q < 6; ++q) st[q] = S[SLD_CHK_STRESS + q] * (160.217653e0 / n);
+        k = 0;
+        v[k++] = t;
+        for (int q = 0; q < 6; ++q) v[k++] = d[q];
+        v[k++] = density;
+        v[k++] = (st[0] + st[1] + st[2]) / 3e0;
+        for (int q = 0; q < 6; ++q) v[k++] = st[q];
+        rc = sld::append_line(sld::out_path(dir, "str-", out_body, -1), current_step, v, k);
+        if (rc) return rc;
 
-    // check_stress: per-atom stresses in eV/A^3, averaged and converted to GPa
-    double st[6];
-    for (int q = 0; q < 6; ++q) st[q] = S[SLD_CHK_STRESS + q] * (160.217653e0 / n);
-    k = 0;
-    v[k++] = t;
-    for (int q = 0; q < 6; ++q) v[k++] = d[q];
-    v[k++] = density;
-    v[k++] = (st[0] + st[1] + st[2]) / 3e0;
-    for (int q = 0; q < 6; ++q) v[k++] = st[q];
-    rc = sld::append_line(sld::out_path(dir, "str-", out_body, -1), current_step, v, k);
-    if (rc) return rc;
-
-    // check_pressure
-    double tmp = 2e0 / 3e0 * S[SLD_CHK_KE] / n;
-    double pressure0 = density * (tmp - S[SLD_CHK_VIR] / (3e0 * n));
-    pressure0 *= 160.217653e0;
-    c->pressure0 = pressure0;
-    for (int q = 0; q < 6; ++q) c->ave_stress[q] = st[q];
-    k = 0;
-    v[k++] = t;
-    for (int q = 0; q < 6; ++q) v[k++] = d[q];
-    v[k++] = density;
-    v[k++] = pressure0;
-    rc = sld::append_line(sld::out_path(dir, "prs-", out_body, -1), current_step, v, k);
-    if (rc) return rc;
+        // check_pressure
+        double tmp = 2e0 / 3e0 * S[SLD_CHK_KE] / n;
+        double pressure0 = density * (tmp - S[SLD_CHK_VIR] / (3e0 * n));
+        pressure0 *= 160.217653e0;
+        c->pressure0 = pressure0;
+        for (int q = 0; q < 6; ++q) c->ave_stress[q] = st[q];
+        k = 0;
+        v[k++] = t;
+        for (int q = 0; q < 6; ++q) v[k++] = d[q];
+        v[k++] = density;
+        v[k++] = pressure0;
+        rc = sld::append_line(sld::out_path(dir, "prs-", out_body, -1), current_step, v, k);
+        if (rc) return rc;
+    }
+    if (!D.spin) return SLD_OK;
 
     // check_spin: magnetisation m = -g s (spilady.h:60)
     const double el_g = 2.0023193043622e0;
@@ -1081,60 +1149,78 @@ int sld_write_config(sld_ctx* c, const char* dir, const char* out_body, int curr
     if (rc) return rc;
     const long n = c->D.natom;
 
-    // columns: r p f stress(6) rho ke pe s s0 Heff_H Heff_L me me0 local_volume
-    enum { NCOL = 31 };
-    struct Col { const char* field; int width; int at; };
-    const Col cols[] = {{"r", 3, 0},    {"p", 3, 3},    {"f", 3, 6},   {"stress", 6, 9},
-                        {"rho", 1, 15}, {"ke", 1, 16},  {"pe", 1, 17}, {"s", 3, 18},
-                        {"s0", 1, 21},  {"H", 3, 22},   {"HL", 3, 25}, {"me", 1, 28},
-                        {"me0", 1, 29}, {"local_volume", 1, 30}};
-    std::vector<double> table((size_t)n * NCOL), tmp((size_t)n * 6);
+    // columns (write_config.cpp:100-127), by what the Hamiltonian has:
+    // r [p f stress(6) rho ke pe] [s s0 Heff_H [Heff_L] me me0] local_volume
+    const Dev& D = c->D;
+    struct Col { const char* field; int width; };
+    std::vector<Col> cols = {{"r", 3}};
+    if (D.latt)
+        for (Col k : {Col{"p", 3}, Col{"f", 3}, Col{"stress", 6}, Col{"rho", 1}, Col{"ke", 1},
+                      Col{"pe", 1}})
+            cols.push_back(k);
+    int hcol = -1, lcol = -1, ncol = 0;
+    for (const Col& k : cols) ncol += k.width;
+    if (D.spin) {
+        cols.push_back({"s", 3}); cols.push_back({"s0", 1}); ncol += 4;
+        hcol = ncol; cols.push_back({"H", 3}); ncol += 3;
+        if (D.landau_on) { lcol = ncol; cols.push_back({"HL", 3}); ncol += 3; }
+        cols.push_back({"me", 1}); cols.push_back({"me0", 1}); ncol += 2;
+    }
+    cols.push_back({"local_volume", 1});
+    ncol += 1;
+    std::vector<double> table((size_t)n * ncol), tmp((size_t)n * 6);
+    int at = 0;
     for (const Col& col : cols) {
         long got = sld_get(c, col.field, tmp.data(), (long)tmp.size());
         if (got < 0) return (int)got;
         for (long i = 0; i < n; ++i)
             for (int w = 0; w < col.width; ++w)
-                table[(size_t)i * NCOL + col.at + w] = tmp[(size_t)i * col.width + w];
+                table[(size_t)i * ncol + at + w] = tmp[(size_t)i * col.width + w];
+        at += col.width;
     }
     if (flags & SLD_WRITE_HEFF_AS_REFERENCE) {
         // write_config.cpp:120,123 print the x component in the y column
         for (long i = 0; i < n; ++i) {
-            double* row = &table[(size_t)i * NCOL];
-            row[23] = row[22];
-            row[26] = row[25];
+            double* row = &table[(size_t)i * ncol];
+            if (hcol >= 0) row[hcol + 1] = row[hcol];
+            if (lcol >= 0) row[lcol + 1] = row[lcol];
         }
     }
-    rc = sld::write_con_file(sld::out_path(dir, "con-", out_body, n_output), n, t, c->G.d, "SLDHL",
-                             "Fe", NCOL, table.data());
+    static const char* kType[] = {"SLDHL", "SLDH", "MD", "SDH", "SDHL"};
+    rc = sld::write_con_file(sld::out_path(dir, "con-", out_body, n_output), n, t, c->G.d,
+                             kType[D.ham], "Fe", ncol, table.data());
     if (rc || !c->P.eltemp) return rc;
 
-    // cel-: cells x-major (ix outermost), centre, Te (K), Tl, Ts_R, Ts_L
+    // cel-: cells x-major (ix outermost), centre, Te (K) [Tl] [Ts_R] [Ts_L]
     const auto& G = c->G;
     const bool mesh = c->P.te_mesh > 0;
     const int ax = mesh ? G.tx : G.nx, ay = mesh ? G.ty : G.ny, az = mesh ? G.tz : G.nz;
     const long m = G.nte;
-    std::vector<double> Te(m), Tl(m), TsR(m), TsL(m);
-    const char* names[4] = {"Te", "Tl", "Ts_R", "Ts_L"};
-    double* dst[4] = {Te.data(), Tl.data(), TsR.data(), TsL.data()};
-    for (int q = 0; q < 4; ++q) {
-        long got = sld_get(c, names[q], dst[q], m);
+    std::vector<const char*> names = {"Te"};
+    if (D.latt) names.push_back("Tl");
+    if (D.spin) names.push_back("Ts_R");
+    if (D.landau_on) names.push_back("Ts_L");
+    const int nv = (int)names.size(), w = 3 + nv;
+    std::vector<double> vals((size_t)m * nv);
+    for (int q = 0; q < nv; ++q) {
+        long got = sld_get(c, names[q], vals.data() + (size_t)q * m, m);
         if (got < 0) return (int)got;
     }
     const double* d = G.d;
-    std::vector<double> cel((size_t)m * 7);
+    std::vector<double> cel((size_t)m * w);
     size_t row = 0;
     for (int ix = 0; ix < ax; ++ix)
         for (int iy = 0; iy < ay; ++iy)
             for (int iz = 0; iz < az; ++iz) {
                 long i = ix + (long)iy * ax + (long)iz * ax * ay;
                 double qx = (ix + 0.5) / ax, qy = (iy + 0.5) / ay, qz = (iz + 0.5) / az;
-                double* o = &cel[row++ * 7];
+                double* o = &cel[row++ * w];
                 o[0] = d[0] * qx + d[1] * qy + d[3] * qz;
                 o[1] = d[2] * qy + d[4] * qz;
                 o[2] = d[5] * qz;
-                o[3] = Te[i]; o[4] = Tl[i]; o[5] = TsR[i]; o[6] = TsL[i];
+                for (int q = 0; q < nv; ++q) o[3 + q] = vals[(size_t)q * m + i];
             }
-    return sld::write_cel_file(sld::out_path(dir, "cel-", out_body, n_output), m, t, d, 7, cel.data());
+    return sld::write_cel_file(sld::out_path(dir, "cel-", out_body, n_output), m, t, d, w, cel.data());
 }
 
 // A new box (upper-triangular d): the host geometry, the device copy of the
@@ -1212,9 +1298,10 @@ int sld_scale(sld_ctx* c, int current_step, double* out3) {
         if (rc) return rc;
         const double hbar = 6.58211899e-16;   // eV s (spilady.h:58)
         double step = P.step;
-        double displace_max = std::sqrt(h[0]) / c->D.atmass * step;
-        double phi_max = std::sqrt(h[1]) / hbar * step;
-        if (displace_max > P.displace_limit || phi_max > P.phi_limit)
+        // the lattice's and the spins' limits, by what the Hamiltonian has
+        double displace_max = c->D.latt ? std::sqrt(h[0]) / c->D.atmass * step : 0.0;
+        double phi_max = c->D.spin ? std::sqrt(h[1]) / hbar * step : 0.0;
+        if ((c->D.latt && displace_max > P.displace_limit) || (c->D.spin && phi_max > P.phi_limit))
             step *= 0.80;
         else
             step *= 1.05;

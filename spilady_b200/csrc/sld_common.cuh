@@ -67,6 +67,11 @@ struct Dev {
     unsigned seed;
     unsigned replica;             // second word of the Philox key
     int spinlang, lattlang, eltemp, localcolmot, renormalize, print_every;
+    // the Hamiltonian (sld_hamiltonian) and what it has: lattice degrees of
+    // freedom, spins, the Landau terms, the exchange correction of the Landau
+    // field (SLDHL only), the Heisenberg Langevin scheme (SDH, SLDH)
+    int ham, latt, spin, landau_on, hc, hint;
+    double gamma_S_H;
     int te_nloop;
     int small_grid;               // a link-cell axis of 3: every pair gets the minimum image
     int split;                    // 1: split-precision form (FP32 pair terms)

@@ -33,6 +33,16 @@ extern "C" int sld_read_variables(const char* path, sld_params* P) {
         else if (key == "atmass") P->atmass = v;
         else if (key == "gamma_L_over_mass") P->gamma_L_over_mass = v;
         else if (key == "gamma_S_HL") P->gamma_S_HL = v;
+        else if (key == "gamma_S_H") P->gamma_S_H = v;
+        else if (key == "hamiltonian") {
+            // the name of control.h's switch, or its number
+            if (val == "SLDHL") P->hamiltonian = SLD_HAM_SLDHL;
+            else if (val == "SLDH") P->hamiltonian = SLD_HAM_SLDH;
+            else if (val == "MD") P->hamiltonian = SLD_HAM_MD;
+            else if (val == "SDH") P->hamiltonian = SLD_HAM_SDH;
+            else if (val == "SDHL") P->hamiltonian = SLD_HAM_SDHL;
+            else P->hamiltonian = iv;
+        }
         else if (key == "random_seed") P->random_seed = iv;
         else if (key == "rcut_pot") P->rcut_pot = v;
         else if (key == "rcut_mag") P->rcut_mag = v;
@@ -100,7 +110,15 @@ extern "C" int sld_create_from_config(sld_ctx** out, const sld_params* prm, cons
     std::string type;
     sld_params P = *prm;
     if (!(in >> natom >> total_time >> type)) return SLD_ERR_IO;
-    if (type != "SLDHL") return SLD_ERR_IO;   // read_config.cpp:60-65
+    // the file's Hamiltonian (read_config.cpp:60-65) selects the context's
+    if (type == "SLDHL") P.hamiltonian = SLD_HAM_SLDHL;
+    else if (type == "SLDH") P.hamiltonian = SLD_HAM_SLDH;
+    else if (type == "MD") P.hamiltonian = SLD_HAM_MD;
+    else if (type == "SDH") P.hamiltonian = SLD_HAM_SDH;
+    else if (type == "SDHL") P.hamiltonian = SLD_HAM_SDHL;
+    else return SLD_ERR_IO;
+    const bool latt = P.hamiltonian <= SLD_HAM_MD, spin = P.hamiltonian != SLD_HAM_MD;
+    const bool hl = P.hamiltonian == SLD_HAM_SLDHL || P.hamiltonian == SLD_HAM_SDHL;
     if (!(in >> P.box[0] >> P.box[1] >> P.box[2] >> P.box[3] >> P.box[4] >> P.box[5]))
         return SLD_ERR_IO;
     if (natom <= 0) return SLD_ERR_IO;
@@ -112,15 +130,18 @@ extern "C" int sld_create_from_config(sld_ctx** out, const sld_params* prm, cons
         std::istringstream ls(line);
         long idx;
         std::string el;
-        double v[30];
+        double v[32];
         if (!(ls >> idx >> el)) return SLD_ERR_IO;
-        // r(3) p(3) f(3) stress(6) rho ke pe s(3) s0 Heff_H(3) Heff_L(3) me me0 local_volume
-        for (int k = 0; k < 27; ++k)
+        // r(3) [p(3) f(3) stress(6) rho ke pe] [s(3) s0 Heff_H(3) [Heff_L(3)] me me0]
+        // local_volume (write_config.cpp:100-127)
+        const int nv = 3 + (latt ? 15 : 0) + (spin ? 9 + (hl ? 3 : 0) : 0) + 1;
+        for (int k = 0; k < nv; ++k)
             if (!(ls >> v[k])) return SLD_ERR_IO;
+        const int sat = latt ? 18 : 3;
         for (int k = 0; k < 3; ++k) {
             r[3 * i + k] = v[k];
-            p[3 * i + k] = v[3 + k];
-            s[3 * i + k] = v[18 + k];
+            p[3 * i + k] = latt ? v[3 + k] : 0.0;
+            s[3 * i + k] = spin ? v[sat + k] : 0.0;
         }
     }
     std::vector<double> te;
@@ -139,8 +160,12 @@ extern "C" int sld_create_from_config(sld_ctx** out, const sld_params* prm, cons
         for (int ix = 0; ix < nx; ++ix)
             for (int iy = 0; iy < ny; ++iy)
                 for (int iz = 0; iz < nz; ++iz) {
-                    double a, b, c, T, Tl, TsR, TsL;
-                    if (!(tin >> a >> b >> c >> T >> Tl >> TsR >> TsL)) return SLD_ERR_IO;
+                    // centre, Te, then [Tl] [Ts_R] [Ts_L] (write_config.cpp:154-166)
+                    double a, b, c, T, x;
+                    if (!(tin >> a >> b >> c >> T)) return SLD_ERR_IO;
+                    const int extra = (latt ? 1 : 0) + (spin ? 1 : 0) + (hl ? 1 : 0);
+                    for (int q = 0; q < extra; ++q)
+                        if (!(tin >> x)) return SLD_ERR_IO;
                     te[ix + iy * nx + iz * nx * ny] = T;
                 }
     }

@@ -102,6 +102,7 @@ __device__ __forceinline__ double3 spin_integrate_dS(const Dev& D, double3 s, do
                                                      double dt, double3& HL) {
     HL = make_double3(0.0, 0.0, 0.0);
     if (!D.spinlang) return spin_rotation(H, s, dt);
+    if (!D.hc) sumJ = 0.0;   // the exchange correction of the Landau field is SLDHL's
     double dt_half = dt / 2.0, dt_quad = dt / 4.0, g = D.gamma_S_HL;
     double L[4];
     for (int k = 0; k < 4; ++k) L[k] = interp_const(D.landau[k], rho, D.inv_rho);
@@ -124,8 +125,44 @@ __device__ __forceinline__ double3 spin_integrate_dS(const Dev& D, double3 s, do
 }
 
 // The noise increment of one visit at temperature T (eV): the normals xi
-// scaled by sqrt(2 T gamma_S_HL / dt) (calculate_spin_CPU.cpp:157-167).
+// scaled by sqrt(2 T gamma_S_HL / dt) (calculate_spin_CPU.cpp:157-167), or
+// for the Heisenberg scheme the random field sqrt(2 T gamma_S_H hbar / dt) xi
+// (calculate_spin_CPU.cpp:78-87).
 __device__ __forceinline__ double3 spin_noise_dS(const Dev& D, double T, double3 xi, double dt) {
-    double amp = sqrt(2.0 * T * D.gamma_S_HL / dt);
+    double amp = D.hint ? sqrt(2.0 * T * D.gamma_S_H * SLD_HBAR / dt) : sqrt(2.0 * T * D.gamma_S_HL / dt);
     return make_double3(amp * xi.x, amp * xi.y, amp * xi.z);
+}
+
+// The damped precession of a spin of length s0 about H over a half step, in
+// closed form (calculate_spin_CPU.cpp:55-74): ca, sa = cos, sin of the
+// precession angle, eb = the damping factor exp(-|H| s0 gamma_S_H dt/2 / hbar).
+__device__ __forceinline__ double3 llg_half(double3 s, double3 H, double H0, double s0, double ca,
+                                           double sa, double eb) {
+    const double e2b = eb * eb;
+    double3 x = make_double3(s.y * H.z - s.z * H.y, s.z * H.x - s.x * H.z, s.x * H.y - s.y * H.x);
+    double n = 0.0;
+    if (s0 > 0.0 && H0 > 0.0) n = (s.x * H.x + s.y * H.y + s.z * H.z) / s0 / H0;
+    double den = (1e0 + e2b + n * (1e0 - e2b)) * H0;
+    double fac = (1e0 - e2b + n * (1e0 + e2b - 2e0 * ca * eb)) * s0;
+    double a = 2e0 * ca * eb * H0, b = 2e0 * sa * eb;
+    return make_double3((a * s.x + b * x.x + fac * H.x) / den, (a * s.y + b * x.y + fac * H.y) / den,
+                        (a * s.z + b * x.z + fac * H.z) / den);
+}
+
+// One visit of the Heisenberg Hamiltonians (SDH, SLDH): NVE rotation, or the
+// three-part Langevin scheme (calculate_spin_CPU.cpp:49-101; P.-W. Ma and
+// S. L. Dudarev, Phys. Rev. B 83, 134418 (2011)): damped precession for dt/2,
+// a rotation about the random field dh for dt, damped precession for dt/2.
+// s0 is the spin's stored length.
+__device__ __forceinline__ double3 spin_integrate_H(const Dev& D, double3 s, double s0, double3 H,
+                                                    double3 dh, double dt) {
+    if (!D.spinlang) return spin_rotation(H, s, dt);
+    const double dt_half = dt / 2e0;
+    const double H0 = sqrt(H.x * H.x + H.y * H.y + H.z * H.z);
+    double sa, ca;
+    sincos(H0 * (dt_half / SLD_HBAR), &sa, &ca);
+    const double eb = exp(-H0 * s0 * D.gamma_S_H * (dt_half / SLD_HBAR));
+    s = llg_half(s, H, H0, s0, ca, sa, eb);
+    s = spin_rotation(dh, s, dt);
+    return llg_half(s, H, H0, s0, ca, sa, eb);
 }

@@ -18,6 +18,9 @@ LIB_PATH = os.path.join(HERE, "_lib", "libsld_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "sld.h")
 
 FP64, SPLIT, FP64_ANALYTIC = 0, 1, 2
+# control.h's Hamiltonian switch
+SLDHL, SLDH, MD, SDH, SDHL = 0, 1, 2, 3, 4
+HAMILTONIANS = {"SLDHL": SLDHL, "SLDH": SLDH, "MD": MD, "SDH": SDH, "SDHL": SDHL}
 
 ERRORS = {
     -1: "SLD_ERR_ARG", -2: "SLD_ERR_CUDA", -3: "SLD_ERR_GEOMETRY",
@@ -52,6 +55,7 @@ class Params(C.Structure):
         ("interval_of_scale_stress", C.c_int), ("pressure", C.c_double),
         ("stress", C.c_double * 6), ("baro_damping_time", C.c_double),
         ("displace_limit", C.c_double), ("phi_limit", C.c_double),
+        ("hamiltonian", C.c_int), ("gamma_S_H", C.c_double),
     ]
 
 
@@ -121,7 +125,7 @@ def make_params(params, *, spinlang=False, lattlang=False, eltemp=False,
                 localcolmot=False, renormalize=False, te_mesh=0, te_nloop=50,
                 precision=FP64, device=0, interval_of_print_out=1, replica=0,
                 interval_of_config_out=1000, pressure_control=False,
-                stress_control=False, change_step=False):
+                stress_control=False, change_step=False, hamiltonian=SLDHL):
     """sld_params from a variables.in-style dict plus the control switches."""
     P = Params()
     lib().sld_params_default(C.byref(P))
@@ -141,6 +145,9 @@ def make_params(params, *, spinlang=False, lattlang=False, eltemp=False,
     P.interval_of_config_out = int(interval_of_config_out)
     P.pressure_control, P.stress_control = int(pressure_control), int(stress_control)
     P.change_step = int(change_step)
+    P.hamiltonian = HAMILTONIANS[hamiltonian] if isinstance(hamiltonian, str) else int(hamiltonian)
+    if "gamma_S_H" in params:
+        P.gamma_S_H = float(params["gamma_S_H"])
     # barostat / time-step variables, variables.in names (read_variables.cpp:197-241)
     for k in ("pressure", "baro_damping_time", "displace_limit", "phi_limit"):
         if k in params:
