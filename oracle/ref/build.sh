@@ -19,6 +19,9 @@
 # each without thermostats and with the Langevin thermostats of its degrees
 # of freedom:
 #   md md_lang  sdh sdh_lang  sdhl sdhl_lang  sldh sldh_lang
+# and each with the electron temperature (+ renormalizeEnergy; SLDH also
+# localcolmot):
+#   md_te  sdh_te  sdhl_te  sldh_te
 #
 # usage: sh oracle/ref/build.sh [reference_dir]
 set -e
@@ -34,7 +37,8 @@ mkdir -p "$OUT"
 CXX=${ORACLE_CXX:-g++}
 BASE="-O3 -fopenmp -U_FORTIFY_SOURCE -D_FORTIFY_SOURCE=0 -DCPU -DOMP -w"
 
-for mode in nve lang langte baro dtstep md md_lang sdh sdh_lang sdhl sdhl_lang sldh sldh_lang; do
+for mode in nve lang langte baro dtstep md md_lang sdh sdh_lang sdhl sdhl_lang sldh sldh_lang \
+           md_te sdh_te sdhl_te sldh_te; do
     case "$mode" in
     md*) ham=MD ;;
     sdhl*) ham=SDHL ;;
@@ -67,6 +71,12 @@ for mode in nve lang langte baro dtstep md md_lang sdh sdh_lang sdhl sdhl_lang s
         md_lang) echo "#define lattlang" ;;
         sdh_lang|sdhl_lang) echo "#define spinlang" ;;
         sldh_lang) echo "#define spinlang"; echo "#define lattlang" ;;
+        md_te) echo "#define lattlang"; echo "#define eltemp"; echo "#define renormalizeEnergy" ;;
+        sdh_te|sdhl_te)
+            echo "#define spinlang"; echo "#define eltemp"; echo "#define renormalizeEnergy" ;;
+        sldh_te)
+            echo "#define spinlang"; echo "#define lattlang"; echo "#define eltemp"
+            echo "#define localcolmot"; echo "#define renormalizeEnergy" ;;
         esac
     } > "$src/control.h.new"
     if ! cmp -s "$src/control.h.new" "$src/control.h"; then

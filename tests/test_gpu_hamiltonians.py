@@ -32,6 +32,13 @@ CASES = {
     "sdhl_lang": ("sdhl_lang", "SDHL", dict(spinlang=True)),
     "sldh": ("sldh", "SLDH", {}),
     "sldh_lang": ("sldh_lang", "SLDH", dict(spinlang=True, lattlang=True)),
+    # with the electron temperature, renormalisation and zero friction (the
+    # noise amplitude is zero; Te moves by diffusion and the renormalisation)
+    "md_te": ("md_te", "MD", dict(lattlang=True, eltemp=True, renormalize=True)),
+    "sdh_te": ("sdh_te", "SDH", dict(spinlang=True, eltemp=True, renormalize=True)),
+    "sdhl_te": ("sdhl_te", "SDHL", dict(spinlang=True, eltemp=True, renormalize=True)),
+    "sldh_te": ("sldh_te", "SLDH", dict(spinlang=True, lattlang=True, eltemp=True,
+                                        localcolmot=True, renormalize=True)),
 }
 
 # what each Hamiltonian has (struct.h:44-118)
@@ -50,18 +57,33 @@ def test_hamiltonian_matches_reference(case, tmp_path):
     build, ham, sw = CASES[case]
     if not rj.available(build):
         pytest.skip("reference build missing")
-    params, r, p, s = initial_state(6, seed=31, tilt=0.3, temperature=300.0)
+    params, r, p, s = initial_state(6, seed=31, tilt=0.35, temperature=300.0)
+    te = None
     if case.endswith("_lang"):
         params = dict(params, temperature=0.0)
     if ham in ("SDH", "SLDH"):
         # the harness passes the spin damping in one slot: gamma_S_H here
         params = dict(params, gamma_S_H=8e-3, gamma_S_HL=8e-3)
+    if case.endswith("_te"):
+        params = dict(params, gamma_L_over_mass=0.0, gamma_S_HL=0.0, gamma_S_H=0.0)
+    E = engine_mod()
+    if case.endswith("_te"):
+        probe = E.Engine(params, r, p, s, hamiltonian=ham, **sw)
+        k = np.arange(probe.ncells)
+        te = 300.0 + 40.0 * (k % 7) + 5.0 * (k % 3)
+        probe.close()
     nsteps = 3
-    dumps, ref = rj.run(build, params, r, p, s, ops=[(rj.OP_STEP, nsteps), (rj.OP_DUMP, 0)],
-                        files=True)
-    e = engine_mod().Engine(params, r, p, s, hamiltonian=ham, interval_of_config_out=1, **sw)
+    dumps, ref = rj.run(build, params, r, p, s, te=te,
+                        ops=[(rj.OP_STEP, nsteps), (rj.OP_DUMP, 0)], files=True)
+    e = E.Engine(params, r, p, s, te=te, hamiltonian=ham, interval_of_config_out=1, **sw)
     d = tmp_path / "out"
     d.mkdir()
+    if sw.get("renormalize"):
+        # the harness's set-up prints the reference energy (check_energy(-1))
+        d0 = tmp_path / "init"
+        d0.mkdir()
+        e.check(d0, "b200", -1)
+        (d / "enr-b200.dat").write_text((d0 / "enr-b200.dat").read_text())
     for k in range(nsteps):
         e.run(1)
         e.check(d, "b200", k)
@@ -90,5 +112,8 @@ def test_hamiltonian_matches_reference(case, tmp_path):
     for name in scal:
         errs[name] = relerr(e.get(name), D.a(name))
         assert errs[name] <= TOL_STATE, f"{case} {name}: {errs[name]:.2e}"
+    if te is not None:
+        errs["Te"] = relerr(e.get("Te"), D.c("Te"))
+        assert errs["Te"] <= TOL_STATE, f"{case} Te: {errs['Te']:.2e}"
     print(case, " ".join(f"{k}:{v:.1e}" for k, v in errs.items()),
           "files", f"{max(worst.values()):.1e}")
