@@ -272,6 +272,23 @@ int sld_adjoint_config(sld_ctx* ctx, const double* theta36, double* out4, double
 int sld_adjoint_trajectory(sld_ctx* ctx, const double* theta36, int nsteps,
                            int checkpoint_every, double* L, double* dL36);
 
+/* External field and force (control.h's extfield and extforce;
+   external_field_CPU.cpp, external_force_CPU.cpp).  H: natom x 3 in eV, caller
+   order: the exchange field of every atom starts at it and the magnetic
+   energy gains -s.H (calculate_spin_CPU.cpp:35-40,
+   calculate_force_energy_CPU.cpp:200-202).  f: natom x 3 in eV/A, added into
+   each atom's force at every kick, which keeps it (core_dp_CPU.cpp:68-71,
+   129-132).  NULL removes either.  A field set before the first step is
+   part of the start state (its force pass, cell temperatures and reference
+   energy are formed again, as initialize() does); later ones act from the
+   next step.  The readers take the reference's
+   extfield.in (Tesla, converted by -g muB) and extforce.in files.  Set them
+   before sld_batch_create: a batch keeps the kernel arguments it captured. */
+int sld_set_external_field(sld_ctx* ctx, const double* H_eV);
+int sld_set_external_force(sld_ctx* ctx, const double* f);
+int sld_read_external_field(sld_ctx* ctx, const char* path);
+int sld_read_external_force(sld_ctx* ctx, const char* path);
+
 /* out[0..5] = natom, ncells, ngroups, n_te_cells, nx, ny (link cells). */
 int sld_info(sld_ctx* ctx, int* out6);
 

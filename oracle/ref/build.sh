@@ -22,6 +22,8 @@
 # and each with the electron temperature (+ renormalizeEnergy; SLDH also
 # localcolmot):
 #   md_te  sdh_te  sdhl_te  sldh_te
+# and SLDHL with an external field and force read from files:
+#   extf
 #
 # usage: sh oracle/ref/build.sh [reference_dir]
 set -e
@@ -38,7 +40,7 @@ CXX=${ORACLE_CXX:-g++}
 BASE="-O3 -fopenmp -U_FORTIFY_SOURCE -D_FORTIFY_SOURCE=0 -DCPU -DOMP -w"
 
 for mode in nve lang langte baro dtstep md md_lang sdh sdh_lang sdhl sdhl_lang sldh sldh_lang \
-           md_te sdh_te sdhl_te sldh_te; do
+           md_te sdh_te sdhl_te sldh_te extf; do
     case "$mode" in
     md*) ham=MD ;;
     sdhl*) ham=SDHL ;;
@@ -77,6 +79,7 @@ for mode in nve lang langte baro dtstep md md_lang sdh sdh_lang sdhl sdhl_lang s
         sldh_te)
             echo "#define spinlang"; echo "#define lattlang"; echo "#define eltemp"
             echo "#define localcolmot"; echo "#define renormalizeEnergy" ;;
+        extf) echo "#define extfield"; echo "#define extforce" ;;
         esac
     } > "$src/control.h.new"
     if ! cmp -s "$src/control.h.new" "$src/control.h"; then

@@ -266,6 +266,12 @@ int main(int argc, char** argv) {
 #endif
         a->element[0] = 'F'; a->element[1] = 'e';
     }
+#ifdef extfield
+    external_field(-1);   /* initial.cpp:58-60: extfield.in in the working directory */
+#endif
+#ifdef extforce
+    external_force(-1);   /* initial.cpp:61-63: extforce.in */
+#endif
     box_length.x = fabs(d.xx);
     box_length.y = sqrt(d.yx * d.yx + d.yy * d.yy);
     box_length.z = sqrt(d.zx * d.zx + d.zy * d.zy + d.zz * d.zz);

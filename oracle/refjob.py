@@ -134,10 +134,12 @@ def read_dumps(path):
 
 
 def run(mode, params, r, p, s, te=None, ops=(), threads=1, timeout=3600,
-        files=False):
+        files=False, inputs=None):
     """Run the reference harness in a scratch directory; return the dumps,
     and with ``files`` also a dict of the ``.dat`` files the reference wrote
-    there (name -> text: its enr-/tmp-/.../con-/cel- output)."""
+    there (name -> text: its enr-/tmp-/.../con-/cel- output).  ``inputs``
+    (name -> text) are written into the working directory first, e.g. the
+    extfield.in / extforce.in files the extf build reads."""
     exe = binary(mode)
     if not os.access(exe, os.X_OK):
         raise FileNotFoundError(f"{exe} missing: run sh oracle/ref/build.sh")
@@ -145,6 +147,9 @@ def run(mode, params, r, p, s, te=None, ops=(), threads=1, timeout=3600,
         job = os.path.join(tmp, "job.bin")
         out = os.path.join(tmp, "out.bin")
         write_job(job, params, r, p, s, te, ops, threads)
+        for name, text in (inputs or {}).items():
+            with open(os.path.join(tmp, name), "w") as fh:
+                fh.write(text)
         env = dict(os.environ, OMP_NUM_THREADS=str(threads))
         res = subprocess.run([exe, job, out], cwd=tmp, env=env,
                              stdout=subprocess.PIPE, stderr=subprocess.PIPE,
@@ -157,7 +162,7 @@ def run(mode, params, r, p, s, te=None, ops=(), threads=1, timeout=3600,
             return dumps
         texts = {}
         for name in sorted(os.listdir(tmp)):
-            if name.endswith(".dat"):
+            if name.endswith(".dat") and name not in (inputs or {}):
                 with open(os.path.join(tmp, name)) as fh:
                     texts[name] = fh.read()
         return dumps, texts

@@ -28,6 +28,12 @@ __global__ void __launch_bounds__(256) k_dp_nve(Dev D, double dt) {
     double px = 0, py = 0, pz = 0;
     if (i < D.natom) {
         double4 p = D.p[i], f = D.f[i];
+        if (D.fext) {
+            // core_dp_CPU.cpp:68-71: the external force is added into f itself
+            double4 e = D.fext[i];
+            f.x = f.x + e.x; f.y = f.y + e.y; f.z = f.z + e.z;
+            D.f[i] = f;
+        }
         p.x = p.x + dt * f.x; p.y = p.y + dt * f.y; p.z = p.z + dt * f.z;
         D.p[i] = p;
         px = p.x; py = p.y; pz = p.z;
@@ -116,6 +122,11 @@ __device__ __forceinline__ double3 dp_cell(const Dev& D, const P& P_, const int*
         double3 xi = normals3(D.seed, D.replica, (unsigned)D.id[i], epoch);
         double fx = amp * xi.x, fy = amp * xi.y, fz = amp * xi.z;
         double4 f = D.f[i];
+        if (D.fext) {   // core_dp_CPU.cpp:129-132
+            double4 e = D.fext[i];
+            f.x = f.x + e.x; f.y = f.y + e.y; f.z = f.z + e.z;
+            D.f[i] = f;
+        }
         double3 p = P_.get(m);
         p.x = p.x + dt * (f.x + fx); p.y = p.y + dt * (f.y + fy); p.z = p.z + dt * (f.z + fz);
         P_.set(m, p);

@@ -224,6 +224,10 @@ __device__ __forceinline__ void force_finish(const Dev& D, int i, double si_sq, 
         D.pe[i] = pe;
     }
     if (PART & PART_MAG) {
+        if (D.hext) {   // calculate_force_energy_CPU.cpp:200-202
+            double4 s = D.s[i], h = D.hext[i];
+            me -= s.x * h.x + s.y * h.y + s.z * h.z;
+        }
         if (D.landau_on) {   // the Heisenberg-Landau Hamiltonians
             double A = interp_const(D.landau[0], rho_i, D.inv_rho);
             double B = interp_const(D.landau[1], rho_i, D.inv_rho);

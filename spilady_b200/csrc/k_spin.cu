@@ -379,6 +379,12 @@ template <bool SPLIT, bool CG>
 __device__ __forceinline__ void visit_field(const Dev& D, const VisitRegs<SPLIT>& v, double3& H,
                                             double& sumJ) {
     double hx = 0, hy = 0, hz = 0, hj = 0;
+    double4 hext = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (D.hext) {
+        // the reference starts the field at the external one (calculate_spin_CPU.cpp:35-40)
+        hext = D.hext[v.i];
+        if constexpr (!SPLIT) { hx = hext.x; hy = hext.y; hz = hext.z; }
+    }
     float ks[4] = {0, 0, 0, 0}, kc[4] = {0, 0, 0, 0};
     auto add32 = [&](float J, float4 s) { exch_add32(ks, kc, J, s); };
     auto add64 = [&](double J, double4 s) { exch_add64(hx, hy, hz, hj, J, s); };
@@ -394,9 +400,9 @@ __device__ __forceinline__ void visit_field(const Dev& D, const VisitRegs<SPLIT>
         else add64(D.jv[at], ld_spin<CG>(D.s + j));
     }
     if constexpr (SPLIT) {
-        hx = (double)ks[0] - (double)kc[0];
-        hy = (double)ks[1] - (double)kc[1];
-        hz = (double)ks[2] - (double)kc[2];
+        hx = hext.x + ((double)ks[0] - (double)kc[0]);
+        hy = hext.y + ((double)ks[1] - (double)kc[1]);
+        hz = hext.z + ((double)ks[2] - (double)kc[2]);
         hj = (double)ks[3] - (double)kc[3];
     }
     H = make_double3(hx, hy, hz);

@@ -301,7 +301,7 @@ int check_ctx(sld_ctx* c) {
     const sld_params& P = c->P;
     // the NVE spin-lattice step of the reference: no thermostats, no electrons
     if (P.spinlang || P.lattlang || P.eltemp || P.change_step || P.pressure_control ||
-        P.stress_control)
+        P.stress_control || P.hamiltonian != SLD_HAM_SLDHL || c->D.hext || c->D.fext)
         return SLD_ERR_ARG;
     return SLD_OK;
 }

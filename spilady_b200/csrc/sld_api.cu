@@ -1314,6 +1314,110 @@ int sld_scale(sld_ctx* c, int current_step, double* out3) {
     return SLD_OK;
 }
 
+// ---------------------------------------------------------------------
+// external field and force (control.h's extfield, extforce)
+
+// kernel arguments changed: the step graphs are captured again at the next run
+static void drop_step_graphs(sld_ctx* c) {
+    cudaStreamSynchronize(c->st);
+    for (int k = 0; k < 2; ++k)
+        if (c->step_graphs[k]) {
+            cudaGraphExecDestroy(c->step_graphs[k]);
+            c->step_graphs[k] = nullptr;
+        }
+}
+
+// caller-order natom x 3 values, times k, into a slot-order device array
+static int set_per_atom(sld_ctx* c, double4** buf, double4** dev_ptr, const double* v, double k) {
+    if (!v) {
+        if (*dev_ptr) {
+            *dev_ptr = nullptr;
+            drop_step_graphs(c);
+        }
+        return SLD_OK;
+    }
+    const size_t n = (size_t)c->D.natom;
+    if (!*buf && c->alloc(buf, n) != SLD_OK) return SLD_ERR_NOMEM;
+    std::vector<double4> h(n);
+    for (size_t q = 0; q < n; ++q) {
+        const double* x = v + 3 * (size_t)c->id_of_slot[q];
+        h[q] = make_double4(k * x[0], k * x[1], k * x[2], 0.0);
+    }
+    CK(cudaMemcpyAsync(*buf, h.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (*dev_ptr != *buf) {
+        *dev_ptr = *buf;
+        drop_step_graphs(c);
+    }
+    return SLD_OK;
+}
+
+int sld_set_external_field(sld_ctx* c, const double* H) {
+    if (!c) return SLD_ERR_ARG;
+    if (H && !c->D.spin) return SLD_ERR_ARG;
+    int rc = set_per_atom(c, &c->hext_buf, &c->D.hext, H, 1.0);
+    if (rc) return rc;
+    // Before the first step this is the reference's initialize(), which sets
+    // the field before the first force pass, cell temperatures and reference
+    // energy (initial.cpp:58-60,78-87): those are formed again.  Later the
+    // field takes effect from the next step.
+    long long steps = 0;
+    CK(cudaMemcpy(&steps, &c->D.ctl->steps, sizeof steps, cudaMemcpyDeviceToHost));
+    if (steps != 0) return SLD_OK;
+    fresh_lists(c);
+    launch_force(c->D, c->st);
+    c->force_volume = c->D.box_volume;
+    if (c->P.eltemp) {
+        launch_temperature(c->D, c->st);
+        if (c->P.renormalize_energy) launch_energy_check(c->D, c->st, 0);
+    }
+    return launch_status();
+}
+
+int sld_set_external_force(sld_ctx* c, const double* f) {
+    if (!c) return SLD_ERR_ARG;
+    if (f && !c->D.latt) return SLD_ERR_ARG;
+    return set_per_atom(c, &c->fext_buf, &c->D.fext, f, 1.0);
+}
+
+// extfield.in / extforce.in (external_field_CPU.cpp:37-49,
+// external_force_CPU.cpp:37-48): natom, then one line "i x y z" per atom in
+// atom order; fields in Tesla, converted to eV by -g muB
+static int read_per_atom(sld_ctx* c, const char* path, std::vector<double>& v) {
+    if (!path) return SLD_ERR_ARG;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return SLD_ERR_IO;
+    long n = 0;
+    int rc = SLD_OK;
+    if (std::fscanf(f, "%ld", &n) != 1 || n != c->D.natom) rc = SLD_ERR_IO;
+    v.assign(3 * (size_t)c->D.natom, 0.0);
+    for (long i = 0; i < n && rc == SLD_OK; ++i) {
+        long idx;
+        if (std::fscanf(f, "%ld %lf %lf %lf", &idx, &v[3 * i], &v[3 * i + 1], &v[3 * i + 2]) != 4)
+            rc = SLD_ERR_IO;
+    }
+    std::fclose(f);
+    return rc;
+}
+
+int sld_read_external_field(sld_ctx* c, const char* path) {
+    if (!c) return SLD_ERR_ARG;
+    std::vector<double> v;
+    int rc = read_per_atom(c, path, v);
+    if (rc) return rc;
+    const double el_g = 2.0023193043622e0, muB = 5.7883817555e-5;   // spilady.h:59-60
+    for (double& x : v) x = (-el_g * muB) * x;
+    return sld_set_external_field(c, v.data());
+}
+
+int sld_read_external_force(sld_ctx* c, const char* path) {
+    if (!c) return SLD_ERR_ARG;
+    std::vector<double> v;
+    int rc = read_per_atom(c, path, v);
+    if (rc) return rc;
+    return sld_set_external_force(c, v.data());
+}
+
 int sld_info(sld_ctx* c, int* o) {
     if (!c || !o) return SLD_ERR_ARG;
     o[0] = c->D.natom; o[1] = c->G.ncells; o[2] = c->G.ngroups; o[3] = c->G.nte;

@@ -83,6 +83,8 @@ struct Dev {
     const double *tF, *tdF, *tf, *tdf, *tphi, *tdphi, *tJ, *tdJ;
     // atoms
     double4 *r, *p, *f, *s, *H, *HL;
+    double4* hext;                // external field per atom (eV), or null (extfield)
+    double4* fext;                // external force per atom (eV/A), or null (extforce)
     float4* s32;                  // split form: s rounded to FP32, written with s by every
                                   // spin writer; the FP32 exchange sums gather it
     float4* r32s;                 // positions rounded to FP32 in cell-list order (slot
@@ -367,6 +369,11 @@ __device__ __forceinline__ void exchange_field(const Dev& D, int i, double3& H, 
                                                Skip skip, OnSkip on_skip) {
     const int nj = D.jl_n[i];
     double hx = 0, hy = 0, hz = 0, hj = 0;
+    // the reference starts the field at the external one (calculate_spin_CPU.cpp:35-40)
+    if (D.hext && !D.split) {
+        double4 h = D.hext[i];
+        hx = h.x; hy = h.y; hz = h.z;
+    }
     float ks[4] = {0, 0, 0, 0}, kc[4] = {0, 0, 0, 0};   // Kahan sums (split form)
     for (int e0 = 0; e0 < nj; e0 += SLD_GB) {
         int jj[SLD_GB];
@@ -415,6 +422,10 @@ __device__ __forceinline__ void exchange_field(const Dev& D, int i, double3& H, 
         hy = (double)ks[1] - (double)kc[1];
         hz = (double)ks[2] - (double)kc[2];
         hj = (double)ks[3] - (double)kc[3];
+        if (D.hext) {   // the external field added in FP64
+            double4 h = D.hext[i];
+            hx = h.x + hx; hy = h.y + hy; hz = h.z + hz;
+        }
     }
     H = make_double3(hx, hy, hz);
     sumJ = hj;

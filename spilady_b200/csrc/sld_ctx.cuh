@@ -21,6 +21,8 @@ struct sld_ctx {
     unsigned char* d_te_color = nullptr;
     double* d_avg = nullptr;
     double* d_chk = nullptr;           // check() sums: per-block partials, then totals
+    double4* hext_buf = nullptr;       // external field / force per atom, slot order;
+    double4* fext_buf = nullptr;       // D.hext / D.fext point here while set
     // what the last sld_check printed and the barostats read (check_pressure,
     // check_stress), and the barostats' clocks (initial.cpp:92-97)
     double pressure0 = 0.0, ave_stress[6] = {0, 0, 0, 0, 0, 0};

@@ -102,6 +102,10 @@ def lib():
         L.sld_batch_destroy.restype = None
         L.sld_check.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int]
         L.sld_scale.argtypes = [vp, C.c_int, P]
+        for n in ("sld_set_external_field", "sld_set_external_force"):
+            getattr(L, n).argtypes = [vp, P]
+        for n in ("sld_read_external_field", "sld_read_external_force"):
+            getattr(L, n).argtypes = [vp, C.c_char_p]
         L.sld_write_config.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int, C.c_int]
         L.sld_adjoint_theta_default.argtypes = [P]
         L.sld_adjoint_config.argtypes = [vp, P, P, P, P]
@@ -305,6 +309,24 @@ class Engine:
                                        int(current_step), 1 if heff_as_reference else 0),
                "write_config")
 
+    def set_external_field(self, H):
+        """Per-atom external field (natom x 3, eV), or None to remove."""
+        a = None if H is None else np.ascontiguousarray(H, np.float64).reshape(-1, 3)
+        _check(self.L.sld_set_external_field(self.h, None if a is None else _dp(a)),
+               "set_external_field")
+
+    def set_external_force(self, f):
+        """Per-atom external force (natom x 3, eV/A), or None to remove."""
+        a = None if f is None else np.ascontiguousarray(f, np.float64).reshape(-1, 3)
+        _check(self.L.sld_set_external_force(self.h, None if a is None else _dp(a)),
+               "set_external_force")
+
+    def read_external_field(self, path):
+        _check(self.L.sld_read_external_field(self.h, str(path).encode()), "read_external_field")
+
+    def read_external_force(self, path):
+        _check(self.L.sld_read_external_force(self.h, str(path).encode()), "read_external_force")
+
     def scale(self, current_step):
         """scale(current_step): barostats and adaptive time step; returns
         (displace_max, phi_max, new step)."""
@@ -362,6 +384,24 @@ class Batch:
         _check(self.L.sld_write_config(self.h, str(out_dir).encode(), out_body.encode(),
                                        int(current_step), 1 if heff_as_reference else 0),
                "write_config")
+
+    def set_external_field(self, H):
+        """Per-atom external field (natom x 3, eV), or None to remove."""
+        a = None if H is None else np.ascontiguousarray(H, np.float64).reshape(-1, 3)
+        _check(self.L.sld_set_external_field(self.h, None if a is None else _dp(a)),
+               "set_external_field")
+
+    def set_external_force(self, f):
+        """Per-atom external force (natom x 3, eV/A), or None to remove."""
+        a = None if f is None else np.ascontiguousarray(f, np.float64).reshape(-1, 3)
+        _check(self.L.sld_set_external_force(self.h, None if a is None else _dp(a)),
+               "set_external_force")
+
+    def read_external_field(self, path):
+        _check(self.L.sld_read_external_field(self.h, str(path).encode()), "read_external_field")
+
+    def read_external_force(self, path):
+        _check(self.L.sld_read_external_force(self.h, str(path).encode()), "read_external_force")
 
     def scale(self, current_step):
         """scale(current_step): barostats and adaptive time step; returns
