@@ -116,6 +116,13 @@ typedef struct {
     double baro_damping_time;    /* s                             default.h:192 */
     double displace_limit;       /* Angstrom per step             default.h:218 */
     double phi_limit;            /* rad per step                  default.h:219 */
+    int quantum_noise;           /* control.h's quantumnoise: the lattice
+                                    thermostat's noise coloured to the quantum
+                                    spectrum (quantum_noise_CPU.cpp) */
+    int msteps_quantum;          /* the coloured noise changes every M kicks
+                                                                  default.h:223 */
+    int nfrequency_quantum;      /* frequency intervals of its filter
+                                                                  default.h:224 */
     int hamiltonian;             /* sld_hamiltonian */
     double gamma_S_H;            /* spin Langevin, Heisenberg (SDH, SLDH), unitless
                                                                   default.h:172 */
@@ -288,6 +295,11 @@ int sld_set_external_field(sld_ctx* ctx, const double* H_eV);
 int sld_set_external_force(sld_ctx* ctx, const double* f);
 int sld_read_external_field(sld_ctx* ctx, const char* path);
 int sld_read_external_force(sld_ctx* ctx, const char* path);
+
+/* The quantum thermostat's filter (initial_quantum_noise,
+   quantum_noise_CPU.cpp:75-104): 2 nfrequency_quantum coefficients into out
+   (capacity n).  Returns the count, or a negative code without quantum_noise. */
+int sld_quantum_filter(sld_ctx* ctx, double* out, int n);
 
 /* out[0..5] = natom, ncells, ngroups, n_te_cells, nx, ny (link cells). */
 int sld_info(sld_ctx* ctx, int* out6);

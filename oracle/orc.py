@@ -29,6 +29,7 @@ class Params(C.Structure):
         ("localcolmot", C.c_int), ("renormalize", C.c_int), ("rng", C.c_int),
         ("te_mesh", C.c_int), ("te_nloop", C.c_int),
         ("interval_of_print_out", C.c_int),
+        ("quantum", C.c_int), ("msteps_quantum", C.c_int), ("nfrequency_quantum", C.c_int),
     ]
 
 
@@ -55,6 +56,7 @@ def lib():
             getattr(L, name).argtypes = [C.c_void_p, C.c_double]
         L.orc_run.argtypes = [C.c_void_p, C.c_int]
         L.orc_averages.argtypes = [C.c_void_p, P]
+        L.orc_quantum_filter.argtypes = [C.c_void_p, P, C.c_int]
         for name in ("orc_natom", "orc_ncells", "orc_nte", "orc_ngroups"):
             getattr(L, name).argtypes = [C.c_void_p]
             getattr(L, name).restype = C.c_int
@@ -76,7 +78,8 @@ def _dp(a):
 
 def make_params(params, *, spinlang=False, lattlang=False, eltemp=False,
                 localcolmot=False, renormalize=False, rng=RNG_PHILOX,
-                te_mesh=0, te_nloop=50):
+                te_mesh=0, te_nloop=50, quantum=False, msteps_quantum=50,
+                nfrequency_quantum=150):
     P = Params()
     P.box[:] = list(params["box"])
     for k in ("step", "temperature", "atmass", "gamma_L_over_mass",
@@ -88,6 +91,8 @@ def make_params(params, *, spinlang=False, lattlang=False, eltemp=False,
     P.localcolmot, P.renormalize = int(localcolmot), int(renormalize)
     P.rng, P.te_mesh, P.te_nloop = rng, te_mesh, te_nloop
     P.interval_of_print_out = 1
+    P.quantum, P.msteps_quantum = int(quantum), int(msteps_quantum)
+    P.nfrequency_quantum = int(nfrequency_quantum)
     return P
 
 
@@ -151,6 +156,11 @@ class System:
         out = np.empty(10, np.float64)
         self.L.orc_averages(self.h, _dp(out))
         return dict(zip(["pe", "ke", "me", "me0", "Ee", "Tl", "Te", "sx", "sy", "sz"], out))
+
+    def quantum_filter(self):
+        out = np.zeros(100000)
+        n = self.L.orc_quantum_filter(self.h, _dp(out), len(out))
+        return out[:n]
 
 
 def philox4x32(ctr, key):

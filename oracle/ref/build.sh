@@ -22,8 +22,9 @@
 # and each with the electron temperature (+ renormalizeEnergy; SLDH also
 # localcolmot):
 #   md_te  sdh_te  sdhl_te  sldh_te
-# and SLDHL with an external field and force read from files:
-#   extf
+# and SLDHL with an external field and force read from files, and with the
+# quantum thermostat on the lattice:
+#   extf  quant
 #
 # usage: sh oracle/ref/build.sh [reference_dir]
 set -e
@@ -40,7 +41,7 @@ CXX=${ORACLE_CXX:-g++}
 BASE="-O3 -fopenmp -U_FORTIFY_SOURCE -D_FORTIFY_SOURCE=0 -DCPU -DOMP -w"
 
 for mode in nve lang langte baro dtstep md md_lang sdh sdh_lang sdhl sdhl_lang sldh sldh_lang \
-           md_te sdh_te sdhl_te sldh_te extf; do
+           md_te sdh_te sdhl_te sldh_te extf quant; do
     case "$mode" in
     md*) ham=MD ;;
     sdhl*) ham=SDHL ;;
@@ -80,6 +81,7 @@ for mode in nve lang langte baro dtstep md md_lang sdh sdh_lang sdhl sdhl_lang s
             echo "#define spinlang"; echo "#define lattlang"; echo "#define eltemp"
             echo "#define localcolmot"; echo "#define renormalizeEnergy" ;;
         extf) echo "#define extfield"; echo "#define extforce" ;;
+        quant) echo "#define lattlang"; echo "#define quantumnoise" ;;
         esac
     } > "$src/control.h.new"
     if ! cmp -s "$src/control.h.new" "$src/control.h"; then

@@ -62,10 +62,13 @@ enum {
     OP_DP = 5, OP_DR = 6, OP_DTE = 7, OP_TEMP = 8, OP_CORE = 9,
     OP_CHECK_ENERGY = 10, OP_STEP = 11, OP_CONFIG_INTERVAL = 12, OP_WRITE_CONFIG = 13,
     OP_CHECK = 14,
+    /* quantum build: initial_quantum_noise() after the OP_SET ops of its
+       variables (initial.cpp:102-104), and its filter written to qfilter.dat */
+    OP_QINIT = 15, OP_QFILTER = 16,
     /* OP_SET + k sets input variable k (read_variables.cpp:197-241):
        0 pressure, 1 baro_damping_time, 2-7 stress_xx yx yy zx zy zz,
        8 interval_of_scale_pressure, 9 interval_of_scale_stress,
-       10 displace_limit, 11 phi_limit */
+       10 displace_limit, 11 phi_limit, 12 Msteps_quantum, 13 Nfrequency_quantum */
     OP_SET = 100
 };
 
@@ -388,6 +391,20 @@ int main(int argc, char** argv) {
 #ifdef changestep
         case OP_SET + 10: displace_limit = arg; break;
         case OP_SET + 11: phi_limit = arg; break;
+#endif
+#ifdef quantumnoise
+        case OP_SET + 12: Msteps_quantum = (int)arg; break;
+        case OP_SET + 13:
+            Nfrequency_quantum = (int)arg;
+            Nfrequency_quantum_2 = 2 * Nfrequency_quantum;   /* read_variables.cpp:247-250 */
+            break;
+        case OP_QINIT: initial_quantum_noise(); break;
+        case OP_QFILTER: {
+            FILE* q = fopen("qfilter.dat", "w");
+            for (int k = 0; k < Nfrequency_quantum_2; ++k) fprintf(q, "%.17g\n", H_ptr[k]);
+            fclose(q);
+            break;
+        }
 #endif
         default: die("unknown op");
         }

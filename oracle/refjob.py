@@ -20,13 +20,14 @@ REF_DIR = os.path.join(HERE, "_ref")
 
 OP_DUMP, OP_LINKS, OP_RHO, OP_FORCE, OP_DS, OP_DP, OP_DR, OP_DTE, OP_TEMP, \
     OP_CORE, OP_CHECK_ENERGY, OP_STEP, OP_CONFIG_INTERVAL, OP_WRITE_CONFIG, \
-    OP_CHECK = range(15)
+    OP_CHECK, OP_QINIT, OP_QFILTER = range(17)
 # OP_SET + k sets an input variable of the baro / dtstep builds (harness.cpp)
 OP_SET = 100
 SET_VARS = {"pressure": 0, "baro_damping_time": 1, "stress_xx": 2, "stress_yx": 3,
             "stress_yy": 4, "stress_zx": 5, "stress_zy": 6, "stress_zz": 7,
             "interval_of_scale_pressure": 8, "interval_of_scale_stress": 9,
-            "displace_limit": 10, "phi_limit": 11}
+            "displace_limit": 10, "phi_limit": 11, "Msteps_quantum": 12,
+            "Nfrequency_quantum": 13}
 
 
 def set_ops(**values):

@@ -28,6 +28,7 @@
 #define UTOEV (931.494028e6 / C_LIGHT / C_LIGHT)
 #define LENGTH_SCALE 1e-10
 #define HBAR 6.58211899e-16
+#define PI_NUM 3.141592653589793238462e0            /* spilady.h:61 */
 #define EVTOJ 1.602176487e-19
 #define NINPUT 1000000                          /* global.h:67 */
 
@@ -270,7 +271,16 @@ struct orc_sys {
     int spare;
     double rand1, rand2;
     unsigned long long epoch;
+    /* quantum thermostat */
+    double* qH;                  /* the filter, 2 Nfrequency_quantum values */
+    int qNf2;
+    double* qnoise;              /* current coloured noise per degree of freedom */
+    long long qcount;            /* calls of the kick's A part so far */
 };
+
+/* the quantum thermostat's normals: epoch QEPOCH + t, with t >= -Nf2 the
+   index of the draw in each degree of freedom's history */
+#define QEPOCH (1ULL << 62)
 
 /* ---- geometry: periodic_CPU.cpp:31-50, find_image_CPU.cpp:31-53 ---- */
 static v3 to_frac(const orc_sys* S, v3 r) {
@@ -713,14 +723,44 @@ void orc_core_ds(orc_sys* S, double dt) {
 
 /* ---- lattice: core_dp_CPU.cpp:51-312, core_dr_CPU.cpp:33-44 ---- */
 static void kick_atom(orc_sys* S, int i, double dt, v3* noise_out) {
-    double amp = sqrt(2e0 * atom_T(S, i) * S->gamma_L / dt);
-    v3 xi = normals3(S, i);
-    v3 ff = vmul(amp, xi);
+    v3 ff;
+    if (S->P.quantum) {
+        /* core_dp_CPU.cpp:137-147: sqrt(2 gamma_L / h) times the coloured noise */
+        double h = dt * S->P.msteps_quantum;
+        ff = vmul(sqrt(2e0 * S->gamma_L / h), ld(S->qnoise, i));
+    } else {
+        double amp = sqrt(2e0 * atom_T(S, i) * S->gamma_L / dt);
+        ff = vmul(amp, normals3(S, i));
+    }
     st(S->p, i, vadd(ld(S->p, i), vmul(dt, vadd(ld(S->f, i), ff))));
     *noise_out = ff;
 }
 
+/* quantum_noise_CPU.cpp:56-72 for every degree of freedom at once (their
+   counters advance together): every Msteps_quantum calls, the filter over
+   the history of normals, newest first, then one new normal.  With
+   counter-based normals the history is the draws t = u - Nf2 .. u - 1 of
+   update u; the reference's initial history is the draws before update 0. */
+static void quantum_update(orc_sys* S) {
+    if (S->qcount % S->P.msteps_quantum == 0) {
+        long long u = S->qcount / S->P.msteps_quantum;
+        int Nf2 = S->qNf2;
+        for (int i = 0; i < S->n; ++i) {
+            double q[3] = {0e0, 0e0, 0e0};
+            for (int k = 0; k < Nf2; ++k) {
+                double o[3];
+                orc_philox_normals((unsigned)S->P.random_seed, 0u, (unsigned)i,
+                                   QEPOCH + (unsigned long long)(u - 1 - k + Nf2), o);
+                for (int c = 0; c < 3; ++c) q[c] += S->qH[k] * o[c];
+            }
+            st(S->qnoise, i, vinit(q[0], q[1], q[2]));
+        }
+    }
+    ++S->qcount;
+}
+
 static void dp_A(orc_sys* S, double dt) {                 /* :94-188 */
+    if (S->P.quantum) quantum_update(S);
     if (S->P.localcolmot) {
         for (int g = 0; g < S->ngroups; ++g)
             for (int k = S->gstart[g]; k < S->gstart[g + 1]; ++k) {
@@ -1042,9 +1082,46 @@ void orc_averages(orc_sys* S, double* out) {
 }
 
 /* ---- set-up: initial.cpp:31-106 with the state given in memory ---- */
+/* initial_quantum_noise (quantum_noise_CPU.cpp:75-104): the filter of the
+   coloured noise, from the quantum spectrum hbar w (1/2 + n(w)) at Nf2
+   frequencies up to pi/h, h = Msteps_quantum step/2 */
+static void quantum_filter(orc_sys* S) {
+    int Nf = S->P.nfrequency_quantum, Nf2 = 2 * Nf;
+    double h = S->P.msteps_quantum * S->P.step / 2e0;
+    double wmax = PI_NUM / h, dw = wmax / (double)Nf, T = S->temperature;
+    double* Ht = (double*)malloc(sizeof(double) * Nf2);
+    for (int i = 0; i < Nf2; ++i) {
+        int k = i - Nf;
+        double w = dw * (double)k;
+        Ht[i] = sqrt(HBAR * fabs(w) * (0.5e0 + 1e0 / expm1(HBAR * fabs(w) / T)));
+        Ht[i] *= (w * h / 2e0) / sin(w * h / 2e0);
+        if (k == 0) Ht[i] = sqrt(T);
+    }
+    S->qNf2 = Nf2;
+    S->qH = (double*)malloc(sizeof(double) * Nf2);
+    for (int i = 0; i < Nf2; ++i) {
+        S->qH[i] = 0e0;
+        for (int j = 0; j < Nf2; ++j) {
+            int k = j - Nf;
+            S->qH[i] += Ht[j] * cos(PI_NUM / (double)Nf * (double)k * (double)(i - Nf));
+        }
+        S->qH[i] /= (double)Nf2;
+    }
+    free(Ht);
+    S->qnoise = (double*)calloc(3 * (size_t)S->n, sizeof(double));
+}
+
+int orc_quantum_filter(orc_sys* S, double* out, int n) {
+    if (!S->qH || n < S->qNf2) return -1;
+    memcpy(out, S->qH, sizeof(double) * S->qNf2);
+    return S->qNf2;
+}
+
 orc_sys* orc_create(const orc_params* prm, int natom, const double* r,
                     const double* p, const double* s, const double* te_K) {
     if (natom <= 0) return NULL;
+    if (prm->quantum && (!prm->lattlang || prm->msteps_quantum < 1 || prm->nfrequency_quantum < 1))
+        return NULL;
     if (prm->eltemp && !(prm->lattlang && prm->spinlang)) return NULL;
     orc_sys* S = (orc_sys*)calloc(1, sizeof(orc_sys));
     S->P = *prm;
@@ -1067,6 +1144,7 @@ orc_sys* orc_create(const orc_params* prm, int natom, const double* r,
     S->temperature = prm->temperature * BOLTZ;
     S->gamma_L = prm->gamma_L_over_mass * S->atmass;
     S->gamma_S_HL = prm->gamma_S_HL;
+    if (prm->quantum) quantum_filter(S);
     S->rcut_pot = prm->rcut_pot;
     S->rcut_mag = prm->rcut_mag;
     S->rcut_max = prm->rcut_max;
@@ -1163,7 +1241,7 @@ void orc_destroy(orc_sys* S) {
     double* dp[] = {S->r, S->p, S->f, S->s, S->s0, S->H, S->HL, S->HC, S->rho, S->pe,
                     S->ke, S->me, S->me0, S->vir, S->stress, S->sumJ, S->lv, S->ave_ff,
                     S->Te, S->Ee, S->Tl, S->TsR, S->TsL, S->Gel, S->Ges, S->sRup,
-                    S->sRdn, S->sLup, S->sLdn, S->ave_p};
+                    S->sRdn, S->sLup, S->sLdn, S->ave_p, S->qH, S->qnoise};
     for (size_t k = 0; k < sizeof(dp) / sizeof(dp[0]); ++k) free(dp[k]);
     int* ip[] = {S->cell, S->old_cell, S->next, S->prev, S->node, S->head, S->tail,
                  S->count, S->neigh, S->gstart, S->gcells};

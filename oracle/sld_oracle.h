@@ -34,6 +34,10 @@ typedef struct {
     int te_mesh;              /* 0: Te on link cells; n > 0: n^3 Te mesh */
     int te_nloop;             /* Te substeps per core_dTe call (reference: 50) */
     int interval_of_print_out;
+    /* quantum thermostat (control.h's quantumnoise, quantum_noise_CPU.cpp):
+       the lattice noise coloured by an FIR filter; Msteps_quantum,
+       Nfrequency_quantum (default.h:222-225) */
+    int quantum, msteps_quantum, nfrequency_quantum;
 } orc_params;
 
 typedef struct orc_sys orc_sys;
@@ -57,6 +61,8 @@ void orc_temperature(orc_sys*);
 void orc_run(orc_sys*, int nsteps);
 /* averages: pe, ke, me, me0, Ee, Tl, Te(K), <sx>, <sy>, <sz> */
 void orc_averages(orc_sys*, double* out10);
+/* the quantum thermostat's filter (2 Nfrequency_quantum coefficients) */
+int orc_quantum_filter(orc_sys*, double* out, int n);
 
 int orc_natom(const orc_sys*);
 int orc_ncells(const orc_sys*);

@@ -117,10 +117,18 @@ __device__ __forceinline__ double3 dp_cell(const Dev& D, const P& P_, const int*
     double ax = 0.0, ay = 0.0, az = 0.0;
     for (int m = 0; m < n; ++m) {            // A: force + noise
         int i = a[m];
-        double T = D.eltemp ? D.Te[D.node[i]] : D.temperature;
-        double amp = sqrt(2.0 * T * D.gamma_L / dt);
-        double3 xi = normals3(D.seed, D.replica, (unsigned)D.id[i], epoch);
-        double fx = amp * xi.x, fy = amp * xi.y, fz = amp * xi.z;
+        double fx, fy, fz;
+        if (D.quantum) {
+            // core_dp_CPU.cpp:137-147: sqrt(2 gamma_L / h) times the coloured noise
+            double amp = sqrt(2.0 * D.gamma_L / (dt * D.qM));
+            double4 q = D.qnoise[i];
+            fx = amp * q.x; fy = amp * q.y; fz = amp * q.z;
+        } else {
+            double T = D.eltemp ? D.Te[D.node[i]] : D.temperature;
+            double amp = sqrt(2.0 * T * D.gamma_L / dt);
+            double3 xi = normals3(D.seed, D.replica, (unsigned)D.id[i], epoch);
+            fx = amp * xi.x; fy = amp * xi.y; fz = amp * xi.z;
+        }
         double4 f = D.f[i];
         if (D.fext) {   // core_dp_CPU.cpp:129-132
             double4 e = D.fext[i];
@@ -246,11 +254,38 @@ __global__ void __launch_bounds__(256) k_dr(Dev D, double dt) {
     D.r32s[D.cell_slot[i]] = make_float4((float)x.x, (float)x.y, (float)x.z, 0.f);
 }
 
+// quantum_noise_CPU.cpp:56-72 for every degree of freedom at once (their
+// counters advance together): every M kicks, each atom's coloured noise is
+// the filter over its history of normals, newest first.  With counter-based
+// normals the history of update u is the draws t = u - Nf2 .. u - 1; the
+// reference's initial history is the draws before update 0.
+__global__ void __launch_bounds__(256) k_quantum_update(Dev D) {
+    const long long c = D.ctl->qcount;
+    if (c % D.qM != 0) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.natom) return;
+    const long long u = c / D.qM;
+    double qx = 0.0, qy = 0.0, qz = 0.0;
+    for (int k = 0; k < D.qNf2; ++k) {
+        const double h = __ldg(D.qH + k);
+        double3 x = normals3(D.seed, D.replica, (unsigned)D.id[i],
+                             SLD_QEPOCH + (unsigned long long)(u - 1 - k + D.qNf2));
+        qx += h * x.x; qy += h * x.y; qz += h * x.z;
+    }
+    D.qnoise[i] = make_double4(qx, qy, qz, 0.0);
+}
+
+__global__ void k_quantum_tick(Dev D) {
+    if (threadIdx.x == 0) ++D.ctl->qcount;
+}
+
 void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off) {
     int nb;
     if (D.lattlang) {
+        if (D.quantum) k_quantum_update<<<div_up(D.natom, 256), 256, 0, st>>>(D);
         nb = div_up(D.ncells, KDP_BLOCK);
         k_dp_lang<<<nb, KDP_BLOCK, 0, st>>>(D, dt, epoch_off);
+        if (D.quantum) k_quantum_tick<<<1, 32, 0, st>>>(D);
     } else {
         nb = div_up(D.natom, 256);
         k_dp_nve<<<nb, 256, 0, st>>>(D, dt);

@@ -218,6 +218,34 @@ float pair_margin(const sld::HostGeom& G) {
     return (float)(2.0 * bound);
 }
 
+// initial_quantum_noise (quantum_noise_CPU.cpp:75-104): the quantum
+// thermostat's filter from the spectrum hbar w (1/2 + n(w)) at 2 Nf
+// frequencies up to pi/h, h = Msteps_quantum step/2 (Dammak et al., Phys.
+// Rev. Lett. 103, 190601 (2009); Barrat and Rodney, J. Stat. Phys. 144, 679
+// (2011))
+std::vector<double> quantum_filter(const sld_params& P) {
+    const double hbar = 6.58211899e-16, pi = 3.141592653589793238462e0;
+    const int Nf = P.nfrequency_quantum, Nf2 = 2 * Nf;
+    const double h = P.msteps_quantum * P.step / 2e0;
+    const double dw = pi / h / (double)Nf, T = P.temperature * kBoltz;
+    std::vector<double> Ht(Nf2), H(Nf2, 0.0);
+    for (int i = 0; i < Nf2; ++i) {
+        int k = i - Nf;
+        double w = dw * (double)k;
+        Ht[i] = std::sqrt(hbar * std::fabs(w) * (0.5e0 + 1e0 / std::expm1(hbar * std::fabs(w) / T)));
+        Ht[i] *= (w * h / 2e0) / std::sin(w * h / 2e0);
+        if (k == 0) Ht[i] = std::sqrt(T);
+    }
+    for (int i = 0; i < Nf2; ++i) {
+        for (int j = 0; j < Nf2; ++j) {
+            int k = j - Nf;
+            H[i] += Ht[j] * std::cos(pi / (double)Nf * (double)k * (double)(i - Nf));
+        }
+        H[i] /= (double)Nf2;
+    }
+    return H;
+}
+
 // the box or the time step changes between steps (sld_scale)
 bool dynamic_step(const sld_ctx* c) {
     return c->P.change_step || c->P.pressure_control || c->P.stress_control;
@@ -237,6 +265,11 @@ int validate(const sld_params* p) {
     if (p->eltemp && !((p->spinlang || !spin) && (p->lattlang || !latt))) return SLD_ERR_ARG;
     if (p->localcolmot && !p->lattlang) return SLD_ERR_ARG;
     if ((p->pressure_control || p->stress_control) && !latt) return SLD_ERR_ARG;
+    // the quantum thermostat colours the lattice noise; its filter is made for
+    // one time step (quantum_noise_CPU.cpp:79-81)
+    if (p->quantum_noise &&
+        (!p->lattlang || p->change_step || p->msteps_quantum < 1 || p->nfrequency_quantum < 1))
+        return SLD_ERR_ARG;
     if (p->precision != SLD_FP64 && p->precision != SLD_SPLIT &&
         p->precision != SLD_FP64_ANALYTIC)
         return SLD_ERR_ARG;
@@ -318,6 +351,8 @@ int sld_params_default(sld_params* o) {
     o->gamma_S_HL = 5.88e13;
     o->gamma_S_H = 8e-3;
     o->hamiltonian = SLD_HAM_SLDHL;
+    o->msteps_quantum = 50;
+    o->nfrequency_quantum = 150;
     o->rcut_pot = 4.1001;
     o->rcut_mag = 3.7501;
     o->rcut_max = 4.1001;
@@ -402,6 +437,8 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     D.landau_on = (D.ham == SLD_HAM_SLDHL || D.ham == SLD_HAM_SDHL) ? 1 : 0;
     D.hc = D.ham == SLD_HAM_SLDHL ? 1 : 0;
     D.hint = (D.ham == SLD_HAM_SDH || D.ham == SLD_HAM_SLDH) ? 1 : 0;
+    D.quantum = prm->quantum_noise ? 1 : 0;
+    D.qM = prm->msteps_quantum;
     D.step = prm->step;
     D.inv_r = T.inv_r;
     D.inv_rho = T.inv_rho;
@@ -486,6 +523,14 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     ok = ok && c->alloc(&D.red, 8 * (size_t)c->red_cap) == 0;
     ok = ok && c->alloc(&D.ctl, 1) == 0 && c->alloc(&c->d_avg, 16) == 0;
     ok = ok && c->alloc(&c->d_chk, SLD_CHK_ATOM * (size_t)div_up(natom, 256) + SLD_CHK_N) == 0;
+    if (ok && prm->quantum_noise) {
+        std::vector<double> h = quantum_filter(*prm);
+        double* qH = nullptr;
+        ok = c->alloc(&qH, h.size()) == 0 && c->alloc(&D.qnoise, n) == 0 &&
+             cudaMemcpy(qH, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+        D.qH = qH;
+        D.qNf2 = (int)h.size();
+    }
     ok = ok && c->alloc(&c->d_gcells, (size_t)G.ncells) == 0;
     ok = ok && c->alloc(&c->d_te_gcells, (size_t)nte) == 0 &&
          c->alloc(&c->d_te_gstart, G.te_gstart.size()) == 0 &&
@@ -1416,6 +1461,14 @@ int sld_read_external_force(sld_ctx* c, const char* path) {
     int rc = read_per_atom(c, path, v);
     if (rc) return rc;
     return sld_set_external_force(c, v.data());
+}
+
+int sld_quantum_filter(sld_ctx* c, double* out, int n) {
+    if (!c || !out) return SLD_ERR_ARG;
+    if (!c->D.quantum) return SLD_ERR_STATE;
+    if (n < c->D.qNf2) return SLD_ERR_ARG;
+    CK(cudaMemcpy(out, c->D.qH, sizeof(double) * c->D.qNf2, cudaMemcpyDeviceToHost));
+    return c->D.qNf2;
 }
 
 int sld_info(sld_ctx* c, int* o) {

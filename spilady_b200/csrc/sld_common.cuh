@@ -44,6 +44,7 @@ struct Ctl {
     // me, me0, Ee per atom) and the step it ran at, as step + 2 (0: none)
     double chk[5];
     long long chk_tag;
+    long long qcount;             // kicks of the quantum thermostat so far
 };
 
 // data of the quintic that joins the ZBL core to the cubic knots of the
@@ -72,6 +73,11 @@ struct Dev {
     // field (SLDHL only), the Heisenberg Langevin scheme (SDH, SLDH)
     int ham, latt, spin, landau_on, hc, hint;
     double gamma_S_H;
+    // quantum thermostat: the filter (qNf2 values), the coloured noise of each
+    // atom, its update interval in kicks
+    int quantum, qM, qNf2;
+    const double* qH;
+    double4* qnoise;
     int te_nloop;
     int small_grid;               // a link-cell axis of 3: every pair gets the minimum image
     int split;                    // 1: split-precision form (FP32 pair terms)
@@ -458,6 +464,9 @@ bool sweep_uses_flow();
 void launch_sweep_flow(const Dev& D, cudaStream_t st, const SweepFlow& F, double dt,
                        bool fields);
 void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off);
+// the quantum thermostat's normals: Philox epoch SLD_QEPOCH + t, t >= -Nf2 the
+// index of the draw in each atom's history
+#define SLD_QEPOCH (1ULL << 62)
 void launch_dr(const Dev& D, cudaStream_t st, double dt);
 // barostat position rescaling (D holds the new box) and the adaptive time
 // step's maxima (k_lattice.cu)

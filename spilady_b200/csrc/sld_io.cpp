@@ -72,6 +72,9 @@ extern "C" int sld_read_variables(const char* path, sld_params* P) {
         else if (key == "PRESSURE") P->pressure_control = iv;
         else if (key == "STRESS") P->stress_control = iv;
         else if (key == "changestep") P->change_step = iv;
+        else if (key == "quantumnoise") P->quantum_noise = iv;
+        else if (key == "Msteps_quantum") P->msteps_quantum = iv;
+        else if (key == "Nfrequency_quantum") P->nfrequency_quantum = iv;
         else if (key == "te_mesh") P->te_mesh = iv;
         else if (key == "te_nloop") P->te_nloop = iv;
         else if (key == "precision") P->precision = (val == "split" || iv == 1) ? SLD_SPLIT : SLD_FP64;

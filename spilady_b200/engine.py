@@ -55,6 +55,8 @@ class Params(C.Structure):
         ("interval_of_scale_stress", C.c_int), ("pressure", C.c_double),
         ("stress", C.c_double * 6), ("baro_damping_time", C.c_double),
         ("displace_limit", C.c_double), ("phi_limit", C.c_double),
+        ("quantum_noise", C.c_int), ("msteps_quantum", C.c_int),
+        ("nfrequency_quantum", C.c_int),
         ("hamiltonian", C.c_int), ("gamma_S_H", C.c_double),
     ]
 
@@ -102,6 +104,7 @@ def lib():
         L.sld_batch_destroy.restype = None
         L.sld_check.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int]
         L.sld_scale.argtypes = [vp, C.c_int, P]
+        L.sld_quantum_filter.argtypes = [vp, P, C.c_int]
         for n in ("sld_set_external_field", "sld_set_external_force"):
             getattr(L, n).argtypes = [vp, P]
         for n in ("sld_read_external_field", "sld_read_external_force"):
@@ -129,7 +132,8 @@ def make_params(params, *, spinlang=False, lattlang=False, eltemp=False,
                 localcolmot=False, renormalize=False, te_mesh=0, te_nloop=50,
                 precision=FP64, device=0, interval_of_print_out=1, replica=0,
                 interval_of_config_out=1000, pressure_control=False,
-                stress_control=False, change_step=False, hamiltonian=SLDHL):
+                stress_control=False, change_step=False, hamiltonian=SLDHL,
+                quantum_noise=False, msteps_quantum=50, nfrequency_quantum=150):
     """sld_params from a variables.in-style dict plus the control switches."""
     P = Params()
     lib().sld_params_default(C.byref(P))
@@ -150,6 +154,8 @@ def make_params(params, *, spinlang=False, lattlang=False, eltemp=False,
     P.pressure_control, P.stress_control = int(pressure_control), int(stress_control)
     P.change_step = int(change_step)
     P.hamiltonian = HAMILTONIANS[hamiltonian] if isinstance(hamiltonian, str) else int(hamiltonian)
+    P.quantum_noise, P.msteps_quantum = int(quantum_noise), int(msteps_quantum)
+    P.nfrequency_quantum = int(nfrequency_quantum)
     if "gamma_S_H" in params:
         P.gamma_S_H = float(params["gamma_S_H"])
     # barostat / time-step variables, variables.in names (read_variables.cpp:197-241)
@@ -309,6 +315,13 @@ class Engine:
                                        int(current_step), 1 if heff_as_reference else 0),
                "write_config")
 
+    def quantum_filter(self):
+        out = np.zeros(100000)
+        n = self.L.sld_quantum_filter(self.h, _dp(out), len(out))
+        if n < 0:
+            raise SldError(int(n), "quantum_filter")
+        return out[:n]
+
     def set_external_field(self, H):
         """Per-atom external field (natom x 3, eV), or None to remove."""
         a = None if H is None else np.ascontiguousarray(H, np.float64).reshape(-1, 3)
@@ -384,6 +397,13 @@ class Batch:
         _check(self.L.sld_write_config(self.h, str(out_dir).encode(), out_body.encode(),
                                        int(current_step), 1 if heff_as_reference else 0),
                "write_config")
+
+    def quantum_filter(self):
+        out = np.zeros(100000)
+        n = self.L.sld_quantum_filter(self.h, _dp(out), len(out))
+        if n < 0:
+            raise SldError(int(n), "quantum_filter")
+        return out[:n]
 
     def set_external_field(self, H):
         """Per-atom external field (natom x 3, eV), or None to remove."""
