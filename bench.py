@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--size", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the built-in launch shapes instead of sld_autotune's")
     ap.add_argument("--small", action="store_true",
                     help="short run for profiler captures: no CPU baseline, no e2e leg, "
                          "one phase-profile step")
@@ -400,6 +402,9 @@ def main():
             "fp64-analytic": engine.FP64_ANALYTIC}[args.precision]
     e = engine.Engine(params, r, p, s, te=te, device=local, precision=prec, **sw)
     natom = e.natom
+    # launch shapes by the autotuner (outside the timed region; the state is
+    # put back afterwards)
+    shapes = None if args.no_autotune else e.autotune(steps=8)
     e.run(args.warmup)
     e.sync()
     import torch
@@ -482,6 +487,7 @@ def main():
                                " dt 0.5 fs",
                    "precision": args.precision, "natom": natom,
                    "l2": "state (~1 GB) larger than L2; no flush needed",
+                   "launch_shapes": shapes,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": kernels_per_step * args.steps, "clocks": clk,

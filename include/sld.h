@@ -301,6 +301,18 @@ int sld_read_external_force(sld_ctx* ctx, const char* path);
    (capacity n).  Returns the count, or a negative code without quantum_noise. */
 int sld_quantum_filter(sld_ctx* ctx, double* out, int n);
 
+/* Autotuner of the launch shapes (no reference counterpart): times `steps`
+   captured steps twice for each candidate and keeps one that is faster by
+   more than 1% than the best so far, by coordinate
+   descent over the cells per block of the spin sweeps, the atoms per block
+   of the pair/list and force passes, and, with eltemp, the core_dTe kernel
+   (one CTA, a cluster, or the hub cluster) and the Te-mesh temperature pass.
+   The state is copied first and put back, so the context continues exactly
+   as if it had not run.  out5 (may be NULL): the chosen sweep, pair, force
+   and temperature block sizes (0: default) and core_dTe kernel (-1: default).
+   Not with sld_scale's switches (their steps are not captured). */
+int sld_autotune(sld_ctx* ctx, int steps, int* out5);
+
 /* out[0..5] = natom, ncells, ngroups, n_te_cells, nx, ny (link cells). */
 int sld_info(sld_ctx* ctx, int* out6);
 

@@ -470,12 +470,13 @@ template <bool FAST>
 static void launch_dte_form(const Dev& D, cudaStream_t st, double dt) {
     cudaLaunchAttribute at[1];
     const int hub_per = (D.nte + HUB_CL - 1) / HUB_CL;
-    if (g_dte_mode == 2 && g_hub_ok && D.nte <= kHubMaxCells && hub_per <= 4 * 1024) {
+    const int mode = D.tune.dte_mode >= 0 ? D.tune.dte_mode : g_dte_mode;
+    if (mode == 2 && g_hub_ok && D.nte <= kHubMaxCells && hub_per <= 4 * 1024) {
         cudaLaunchConfig_t cfg = cluster_cfg(HUB_CL, 1024, hub_smem(D.nte), st, at);
         cudaLaunchKernelEx(&cfg, k_dte_hub<FAST>, D, dt, hub_per);
         return;
     }
-    if (g_dte_mode >= 1 && g_dte_cluster > 0) {
+    if (mode >= 1 && g_dte_cluster > 0) {
         cudaLaunchConfig_t cfg = cluster_cfg(g_dte_cluster, 256, 0, st, at);
         cudaLaunchKernelEx(&cfg, k_dte_cluster<FAST>, D, dt);
         return;

@@ -417,18 +417,20 @@ __global__ void __launch_bounds__(128) k_force32(Dev D) {
 
 template <int PART>
 static void launch_force_part(const Dev& D, cudaStream_t st) {
-    int nb = div_up(D.natom, 128);
-    if (D.split) k_force32<PART><<<nb, 128, 0, st>>>(D);
-    else if (D.analytic) k_force64<true, PART><<<nb, 128, 0, st>>>(D);
-    else k_force64<false, PART><<<nb, 128, 0, st>>>(D);
+    const int bs = D.tune.force_block > 0 ? D.tune.force_block : 128;
+    int nb = div_up(D.natom, bs);
+    if (D.split) k_force32<PART><<<nb, bs, 0, st>>>(D);
+    else if (D.analytic) k_force64<true, PART><<<nb, bs, 0, st>>>(D);
+    else k_force64<false, PART><<<nb, bs, 0, st>>>(D);
 }
 
 void launch_pairs(const Dev& D, cudaStream_t st, bool write_rho) {
     int w = write_rho ? 1 : 0;
-    int nb = div_up(D.natom, 128);
-    if (D.split) k_pairs<1><<<nb, 128, 0, st>>>(D, w);
-    else if (D.analytic) k_pairs<2><<<nb, 128, 0, st>>>(D, w);
-    else k_pairs<0><<<nb, 128, 0, st>>>(D, w);
+    const int bs = D.tune.pair_block > 0 ? D.tune.pair_block : 128;
+    int nb = div_up(D.natom, bs);
+    if (D.split) k_pairs<1><<<nb, bs, 0, st>>>(D, w);
+    else if (D.analytic) k_pairs<2><<<nb, bs, 0, st>>>(D, w);
+    else k_pairs<0><<<nb, bs, 0, st>>>(D, w);
 }
 void launch_embed(const Dev& D, cudaStream_t st) {
     int nb = div_up(D.natom, 256);

@@ -646,16 +646,18 @@ void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g,
         // 255 registers allow 8 warps, 2 blocks of 4.  The Heisenberg
         // Hamiltonians' visit has its own instance (the other sweep variants
         // have only the Heisenberg-Landau visit).
+        const int bs = D.tune.sweep_block > 0 ? D.tune.sweep_block : (D.split ? 96 : 128);
+        const int nb = div_up(ncell_g, bs);
         if (D.split) {
             if (D.hint)
-                k_sweep_pipe<true, 1><<<div_up(ncell_g, 96), 96, 0, st>>>(D, gcells, ncell_g, dt, b);
+                k_sweep_pipe<true, 1><<<nb, bs, 0, st>>>(D, gcells, ncell_g, dt, b);
             else
-                k_sweep_pipe<true, 0><<<div_up(ncell_g, 96), 96, 0, st>>>(D, gcells, ncell_g, dt, b);
+                k_sweep_pipe<true, 0><<<nb, bs, 0, st>>>(D, gcells, ncell_g, dt, b);
         } else {
             if (D.hint)
-                k_sweep_pipe<false, 1><<<div_up(ncell_g, 128), 128, 0, st>>>(D, gcells, ncell_g, dt, b);
+                k_sweep_pipe<false, 1><<<nb, bs, 0, st>>>(D, gcells, ncell_g, dt, b);
             else
-                k_sweep_pipe<false, 0><<<div_up(ncell_g, 128), 128, 0, st>>>(D, gcells, ncell_g, dt, b);
+                k_sweep_pipe<false, 0><<<nb, bs, 0, st>>>(D, gcells, ncell_g, dt, b);
         }
         return;
     }

@@ -148,7 +148,8 @@ __global__ void k_temp_node(Dev D) {
 void launch_temperature(const Dev& D, cudaStream_t st) {
     if (D.te_mesh > 0) {
         cudaMemsetAsync(D.acc, 0, sizeof(double) * 9 * (size_t)D.nte, st);
-        k_temp_atom<<<div_up(D.natom, 128), 128, 0, st>>>(D);
+        const int bs = D.tune.temp_block > 0 ? D.tune.temp_block : 128;
+        k_temp_atom<<<div_up(D.natom, bs), bs, 0, st>>>(D);
         k_temp_node<<<div_up(D.nte, 128), 128, 0, st>>>(D);
     } else {
         k_temp_cell<<<div_up(D.ncells, 128), 128, 0, st>>>(D);

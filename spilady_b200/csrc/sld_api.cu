@@ -437,6 +437,7 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     D.landau_on = (D.ham == SLD_HAM_SLDHL || D.ham == SLD_HAM_SDHL) ? 1 : 0;
     D.hc = D.ham == SLD_HAM_SLDHL ? 1 : 0;
     D.hint = (D.ham == SLD_HAM_SDH || D.ham == SLD_HAM_SLDH) ? 1 : 0;
+    D.tune = Tune{0, 0, 0, 0, -1};
     D.quantum = prm->quantum_noise ? 1 : 0;
     D.qM = prm->msteps_quantum;
     D.step = prm->step;
@@ -1469,6 +1470,109 @@ int sld_quantum_filter(sld_ctx* c, double* out, int n) {
     if (n < c->D.qNf2) return SLD_ERR_ARG;
     CK(cudaMemcpy(out, c->D.qH, sizeof(double) * c->D.qNf2, cudaMemcpyDeviceToHost));
     return c->D.qNf2;
+}
+
+// ---------------------------------------------------------------------
+// autotuner of the launch shapes
+
+// every device allocation of the context, for a tuning run that leaves the
+// state as it found it
+struct StateCopy {
+    std::vector<void*> buf;
+    int cur = 0;
+    bool lists_stale = false;
+    double force_volume = 0.0;
+};
+
+static int state_save(sld_ctx* c, StateCopy& s) {
+    s.cur = c->cur;
+    s.lists_stale = c->lists_stale;
+    s.force_volume = c->force_volume;
+    for (size_t k = 0; k < c->allocs.size(); ++k) {
+        void* q = nullptr;
+        if (cudaMalloc(&q, c->alloc_bytes[k]) != cudaSuccess) return SLD_ERR_NOMEM;
+        s.buf.push_back(q);
+        CK(cudaMemcpyAsync(q, c->allocs[k], c->alloc_bytes[k], cudaMemcpyDeviceToDevice, c->st));
+    }
+    CK(cudaStreamSynchronize(c->st));
+    return SLD_OK;
+}
+
+static int state_restore(sld_ctx* c, const StateCopy& s) {
+    for (size_t k = 0; k < s.buf.size(); ++k)
+        CK(cudaMemcpyAsync(c->allocs[k], s.buf[k], c->alloc_bytes[k], cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    use_set(c, s.cur);
+    c->lists_stale = s.lists_stale;
+    c->force_volume = s.force_volume;
+    return SLD_OK;
+}
+
+static void state_free(StateCopy& s) {
+    for (void* q : s.buf) cudaFree(q);
+    s.buf.clear();
+}
+
+// device milliseconds of `steps` steps with the current launch shapes, from
+// the saved state: one untimed step first (the graph capture), then the
+// faster of two timed runs
+static int trial(sld_ctx* c, const StateCopy& s, int steps, double* ms) {
+    drop_step_graphs(c);
+    int rc = state_restore(c, s);
+    if (rc) return rc;
+    if ((rc = sld_run(c, 1)) || (rc = sld_sync(c))) return rc;
+    *ms = 1e300;
+    for (int rep = 0; rep < 2; ++rep) {
+        double t = 0.0;
+        if ((rc = sld_run(c, steps)) || (rc = sld_sync(c)) || (rc = sld_last_run_ms(c, &t)))
+            return rc;
+        *ms = std::min(*ms, t);
+    }
+    return SLD_OK;
+}
+
+int sld_autotune(sld_ctx* c, int steps, int* out5) {
+    if (!c || steps < 1) return SLD_ERR_ARG;
+    if (dynamic_step(c)) return SLD_ERR_ARG;   // no captured step to time
+    StateCopy s;
+    int rc = state_save(c, s);
+    if (rc) { state_free(s); return rc; }
+    Tune& T = c->D.tune;
+    double best = 0.0;
+    rc = trial(c, s, steps, &best);
+    // coordinate descent over the shapes, each from the current best
+    struct Axis { int* field; std::vector<int> values; };
+    std::vector<Axis> axes = {{&T.sweep_block, {64, 96, 128}},
+                              {&T.pair_block, {64, 96, 128}},
+                              {&T.force_block, {64, 96, 128}}};
+    if (c->P.eltemp) {
+        axes.push_back({&T.dte_mode, {0, 1, 2}});
+        if (c->P.te_mesh > 0) axes.push_back({&T.temp_block, {64, 128}});
+    }
+    for (auto& ax : axes) {
+        if (rc) break;
+        int keep = *ax.field;
+        for (int v : ax.values) {
+            if (v == keep) continue;
+            *ax.field = v;
+            double ms = 0.0;
+            rc = trial(c, s, steps, &ms);
+            if (rc) break;
+            // a shape must win by 1%: run-to-run noise is about that
+            if (ms < 0.99 * best) { best = ms; keep = v; }
+        }
+        *ax.field = keep;
+    }
+    drop_step_graphs(c);
+    int rc2 = state_restore(c, s);
+    state_free(s);
+    if (rc) return rc;
+    if (rc2) return rc2;
+    if (out5) {
+        out5[0] = T.sweep_block; out5[1] = T.pair_block; out5[2] = T.force_block;
+        out5[3] = T.temp_block; out5[4] = T.dte_mode;
+    }
+    return SLD_OK;
 }
 
 int sld_info(sld_ctx* c, int* o) {

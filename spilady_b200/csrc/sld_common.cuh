@@ -54,6 +54,15 @@ struct Pot32 {
     float zbl_as;   // ZBL screening length
 };
 
+// launch shapes chosen by sld_autotune (0: the built-in default)
+struct Tune {
+    int sweep_block;   // cells per block of the pipelined spin sweep (a thread a cell)
+    int pair_block;    // atoms per block of the pair and list pass
+    int force_block;   // atoms per block of the force passes
+    int temp_block;    // atoms per block of the cell-temperature pass on a Te mesh
+    int dte_mode;      // core_dTe kernel: 0 one CTA, 1 cluster, 2 hub; -1 default
+};
+
 struct Dev {
     // box (struct.h box_vector order: xx yx yy zx zy zz) and inverse
     double d[6], inv[6];
@@ -80,6 +89,7 @@ struct Dev {
     double4* qnoise;
     int te_nloop;
     int small_grid;               // a link-cell axis of 3: every pair gets the minimum image
+    Tune tune;
     int split;                    // 1: split-precision form (FP32 pair terms)
     int analytic;                 // 1: the split form's kernels in FP64
     Pot32 pot32;

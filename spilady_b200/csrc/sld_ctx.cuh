@@ -14,6 +14,7 @@ struct sld_ctx {
     std::vector<int> id_of_slot, slot_of_id;
     Dev D{};
     std::vector<void*> allocs;
+    std::vector<size_t> alloc_bytes;   // size of each allocation (a whole-state snapshot)
     int* d_gcells = nullptr;
     SweepFlow flow{};                  // data-flow schedule of the spin sweeps
     int* d_te_gcells = nullptr;
@@ -57,6 +58,7 @@ struct sld_ctx {
         if (cudaMalloc(&q, n * sizeof(T)) != cudaSuccess) return SLD_ERR_NOMEM;
         cudaMemset(q, 0, n * sizeof(T));
         allocs.push_back(q);
+        alloc_bytes.push_back(n * sizeof(T));
         *p = static_cast<T*>(q);
         return SLD_OK;
     }

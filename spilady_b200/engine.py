@@ -105,6 +105,7 @@ def lib():
         L.sld_check.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int]
         L.sld_scale.argtypes = [vp, C.c_int, P]
         L.sld_quantum_filter.argtypes = [vp, P, C.c_int]
+        L.sld_autotune.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
         for n in ("sld_set_external_field", "sld_set_external_force"):
             getattr(L, n).argtypes = [vp, P]
         for n in ("sld_read_external_field", "sld_read_external_force"):
@@ -315,6 +316,14 @@ class Engine:
                                        int(current_step), 1 if heff_as_reference else 0),
                "write_config")
 
+    def autotune(self, steps=3):
+        """Choose the launch shapes by timing captured steps; the state is
+        left unchanged.  Returns the chosen shapes."""
+        out = (C.c_int * 5)()
+        _check(self.L.sld_autotune(self.h, int(steps), out), "autotune")
+        return dict(zip(("sweep_block", "pair_block", "force_block", "temp_block",
+                         "dte_mode"), list(out)))
+
     def quantum_filter(self):
         out = np.zeros(100000)
         n = self.L.sld_quantum_filter(self.h, _dp(out), len(out))
@@ -397,6 +406,14 @@ class Batch:
         _check(self.L.sld_write_config(self.h, str(out_dir).encode(), out_body.encode(),
                                        int(current_step), 1 if heff_as_reference else 0),
                "write_config")
+
+    def autotune(self, steps=3):
+        """Choose the launch shapes by timing captured steps; the state is
+        left unchanged.  Returns the chosen shapes."""
+        out = (C.c_int * 5)()
+        _check(self.L.sld_autotune(self.h, int(steps), out), "autotune")
+        return dict(zip(("sweep_block", "pair_block", "force_block", "temp_block",
+                         "dte_mode"), list(out)))
 
     def quantum_filter(self):
         out = np.zeros(100000)

@@ -47,3 +47,23 @@ def test_replicas_draw_different_noise():
     a.run(1)
     b.run(1)
     assert not np.array_equal(a.get("p"), b.get("p"))
+
+
+def test_autotune_keeps_the_state_and_the_results():
+    # launch shapes change no arithmetic (a thread per cell or atom whatever
+    # the block), so the tuned context steps on with the same bits
+    from spilady_b200 import engine
+    from spilady_b200.lattice import initial_state
+    params, r, p, s = initial_state(8, seed=61, tilt=0.2)
+    a = engine.Engine(params, r, p, s, spinlang=True, lattlang=True, precision=engine.SPLIT)
+    b = engine.Engine(params, r, p, s, spinlang=True, lattlang=True, precision=engine.SPLIT)
+    a.run(2)
+    b.run(2)
+    shapes = a.autotune(steps=2)
+    assert shapes["sweep_block"] in (0, 64, 96, 128)
+    for n in ("r", "p", "s"):
+        assert np.array_equal(a.get(n), b.get(n)), n
+    a.run(3)
+    b.run(3)
+    for n in ("r", "p", "s", "f"):
+        assert np.array_equal(a.get(n), b.get(n)), n
