@@ -25,6 +25,11 @@
 # and SLDHL with an external field and force read from files, and with the
 # quantum thermostat on the lattice:
 #   extf  quant
+# and NVE SLDHL whose potential's 36 constants are read from theta.in, for
+# finite differences of the reference's own code in them: DD05.cpp and
+# JijFe.cpp are replaced at link time by oracle/ref/param_pot.cpp, which
+# restates their forms:
+#   param
 #
 # usage: sh oracle/ref/build.sh [reference_dir]
 set -e
@@ -41,7 +46,7 @@ CXX=${ORACLE_CXX:-g++}
 BASE="-O3 -fopenmp -U_FORTIFY_SOURCE -D_FORTIFY_SOURCE=0 -DCPU -DOMP -w"
 
 for mode in nve lang langte baro dtstep md md_lang sdh sdh_lang sdhl sdhl_lang sldh sldh_lang \
-           md_te sdh_te sdhl_te sldh_te extf quant; do
+           md_te sdh_te sdhl_te sldh_te extf quant param; do
     case "$mode" in
     md*) ham=MD ;;
     sdhl*) ham=SDHL ;;
@@ -57,6 +62,9 @@ for mode in nve lang langte baro dtstep md md_lang sdh sdh_lang sdhl sdhl_lang s
     for f in "$REF"/*.cpp "$REF"/*.h; do
         b=$(basename "$f")
         case "$b" in control.h|spilady.cpp) continue ;; esac
+        if [ "$mode" = param ]; then
+            case "$b" in DD05.cpp|JijFe.cpp) continue ;; esac
+        fi
         ln -s "$f" "$src/$b"
     done
     {
@@ -90,7 +98,9 @@ for mode in nve lang langte baro dtstep md md_lang sdh sdh_lang sdhl sdhl_lang s
         rm -f "$src/control.h.new"
     fi
     pids=""
-    for f in "$src"/*.cpp "$HERE/harness.cpp"; do
+    extra=""
+    if [ "$mode" = param ]; then extra="$HERE/param_pot.cpp"; fi
+    for f in "$src"/*.cpp "$HERE/harness.cpp" $extra; do
         b=$(basename "$f" .cpp)
         o="$obj/$b.o"
         if [ ! -f "$o" ] || [ "$f" -nt "$o" ] || [ "$src/control.h" -nt "$o" ]; then

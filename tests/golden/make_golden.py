@@ -5,7 +5,8 @@ Each fixture holds the synthetic input state and the reference's output
 arrays at a few points of the run, with one OpenMP thread (the reference's
 Langevin noise stream depends on the thread count).  Run from the repo root:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # the trajectory fixtures
+    python tests/golden/make_golden.py adjoint    # the reference's FD gradient
 """
 from __future__ import annotations
 
@@ -63,6 +64,61 @@ def make(name):
     print(name, mode, "atoms", r.shape[0], "groups", dumps[0].ngroups)
 
 
+def make_adjoint_fd(path=os.path.join(HERE, "adjoint_ref_fd.npz"), K=10, threads=16):
+    """The reference's own gradient of L = sum |f|^2 + |Heff_H|^2 in the 36
+    potential parameters, by FP64 central differences (h = 1e-6 of each, 1e-6
+    for a zero one) of its CPU code: the "param" build reads the parameters
+    from theta.in.  One configuration (bcc Fe 8^3 cells, positions +N(0, 0.05
+    A), spin tilt 0.2 rad), and after K NVE steps of 1 fs.  Heff_H is the
+    field check_temperature recomputes for every atom."""
+    from concurrent.futures import ThreadPoolExecutor
+    params, r, p, s = initial_state(8, seed=21, tilt=0.2, temperature=300.0, pos_sigma=0.05)
+    theta = np.array(DEFAULT_THETA)
+    h = np.where(theta != 0.0, 1e-6 * np.abs(theta), 1e-6)
+
+    def loss(th, steps):
+        ops = ([(rj.OP_CORE, steps)] if steps else []) + [(rj.OP_CHECK, steps - 1),
+                                                          (rj.OP_DUMP, 0)]
+        d = rj.run("param", params, r, p, s, ops=ops,
+                   inputs={"theta.in": " ".join("%.17g" % x for x in th)})[-1]
+        return float((d.vec("f") ** 2).sum() + (d.vec("H") ** 2).sum())
+
+    jobs = []
+    for steps in (0, K):
+        for k in range(len(theta)):
+            for sgn in (1.0, -1.0):
+                t = theta.copy()
+                t[k] += sgn * h[k]
+                jobs.append((t, steps))
+    with ThreadPoolExecutor(threads) as ex:
+        vals = list(ex.map(lambda j: loss(*j), jobs))
+    v = np.array(vals).reshape(2, len(theta), 2)
+    fd = (v[:, :, 0] - v[:, :, 1]) / (2 * h)
+    np.savez_compressed(path, theta=theta, h=h, K=K, dL_config=fd[0], dL_traj=fd[1],
+                        L_config=loss(theta, 0), L_traj=loss(theta, K))
+    print("adjoint_ref_fd", path)
+
+
+# the potential's 36 constants in sld_adjoint_theta_default's order (DD05.cpp,
+# JijFe.cpp): F a, b; f coefficients, knots; phi coefficients, knots; J A, rc;
+# Landau A, B, C, D
+DEFAULT_THETA = [
+    4.100199340884814, 1.565647547483517,
+    0.9332056681088162, -1.162558782567700, -0.3502026949249225, 0.4287820835430028,
+    4.907925057809273, -5.307049068415304,
+    3.0, 2.8666666666666666, 2.7333333333333333, 2.6, 2.4, 2.3,
+    -0.1960674387419232, 0.3687525935422963, -1.505333614924853, 4.948907078156191,
+    -4.894613262753399, 3.468897724782442, -1.792218099820337, 80.22069592246987,
+    4.1, 3.8, 3.5, 3.2, 2.9, 2.6, 2.4, 2.3,
+    0.870, 3.75,
+    -0.744824, 0.345295, -0.00790205, 0.0,
+]
+
+
 if __name__ == "__main__":
-    for n in (sys.argv[1:] or CASES):
-        make(n)
+    args = sys.argv[1:]
+    if args == ["adjoint"]:
+        make_adjoint_fd()
+    else:
+        for n in (args or CASES):
+            make(n)

@@ -137,3 +137,26 @@ def test_split_forward_gradient_tracks_fp64():
     err = np.max(np.abs(gs - g64)) / np.max(np.abs(g64))
     print(f"split forward: L rel {abs(Ls - L64) / L64:.1e}, gradient rel {err:.1e}")
     assert err <= 1e-4
+
+
+def test_gradients_against_the_references_finite_differences():
+    # tests/golden/adjoint_ref_fd.npz: central differences of the reference's
+    # own CPU code (its potential's constants read from a file), same system.
+    # The reference evaluates tabulated forms with seven-point derivatives
+    # (dx = r/1000), which differ from the exact forms near the knots of the
+    # cubic pieces; that difference bounds the agreement.
+    from conftest import load_golden
+    g = load_golden("adjoint_ref_fd")
+    params, r, p, s, e = system()
+    th = E().adjoint_theta_default()
+    assert np.array_equal(th, g["theta"])
+    out, _, dLc = e.adjoint_config(th)
+    assert abs(out[1] - float(g["L_config"])) <= 1e-6 * out[1]
+    K = int(g["K"])
+    L, dLt = e.adjoint_trajectory(th, K, 4)
+    assert abs(L - float(g["L_traj"])) <= 1e-6 * L
+    ec = np.max(np.abs(dLc - g["dL_config"])) / np.max(np.abs(g["dL_config"]))
+    et = np.max(np.abs(dLt - g["dL_traj"])) / np.max(np.abs(g["dL_traj"]))
+    print(f"vs the reference's FD: config {ec:.1e}, {K} steps {et:.1e}")
+    # measured 3.6e-5 and 1.3e-5
+    assert ec <= 2e-4 and et <= 2e-4
