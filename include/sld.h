@@ -270,6 +270,14 @@ int sld_adjoint_theta_default(double* theta36);
 int sld_adjoint_config(sld_ctx* ctx, const double* theta36, double* out4, double* dE36,
                        double* dL36);
 
+/* Jacobians of one configuration's forces and exchange fields in theta,
+   forward mode in FP64: dF and dH (natom x 3 x 36, caller order, the
+   parameter index fastest; dH may be NULL) with d f_i / d theta_k and
+   d Heff_H,i / d theta_k; f and H (natom x 3, may be NULL) the forces and
+   fields themselves. */
+int sld_adjoint_jacobians(sld_ctx* ctx, const double* theta36, double* f, double* H,
+                          double* dF, double* dH);
+
 /* Through a trajectory: nsteps NVE main-loop steps (core.cpp:55-63) from
    the context's current state with the parameters theta; *L = the loss of
    the final configuration and dL36 (may be NULL: forward only) its gradient

@@ -352,6 +352,100 @@ __global__ void __launch_bounds__(128) k_adj_energy_grad(Dev D, AdjDev A, AdjCon
     block_theta(loc, 0, ADJ_NTHETA, A.thb + (size_t)blockIdx.x * ADJ_NTHETA, sh);
 }
 
+// Forward-mode Jacobians of one configuration.  d rho_i / d theta over the
+// density's 12 parameters (theta 2..13): natom x 12.
+__global__ void __launch_bounds__(128) k_adj_rho_tan(Dev D, AdjDev A, AdjConst K, double* drho) {
+    typedef Dual<12> T;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.natom) return;
+    ThSeed<12> th{K.th, -TH_DA, TH_DA, TH_DA + 12};
+    double4 ri = D.r[i];
+    T rho = dconst<12>(0.0);
+    int nn = D.nbr_n[i];
+    for (int e = 0; e < nn; ++e) {
+        double4 rj;
+        double3 d = adj_pair_vec(D, ri, D.nbr[(size_t)e * D.natom + i], rj);
+        double r0 = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
+        if (r0 < D.rcut_pot) {
+            T f, df;
+            adj_dens(dconst<12>(r0), th, f, df);
+            rho += f;
+        }
+    }
+    for (int k = 0; k < 12; ++k) drho[12 * (size_t)i + k] = rho.d[k];
+}
+
+// d f_i / d theta and d Heff_H,i / d theta: natom x 3 x 36 each, slot order.
+// The densities carry their parameter partials (drho), so F'(rho) takes both
+// its own parameters' and the density parameters' partials.
+#define ADJ_NJ TH_LANDAU
+__global__ void __launch_bounds__(128) k_adj_force_tan(Dev D, AdjDev A, AdjConst K,
+                                                       const double* __restrict__ drho,
+                                                       double* df, double* dh) {
+    typedef Dual<ADJ_NJ> T;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.natom) return;
+    ThSeed<ADJ_NJ> th{K.th, 0, 0, ADJ_NJ};
+    auto rho_of = [&](int a) {
+        T x = dconst<ADJ_NJ>(A.rho[a]);
+        for (int k = 0; k < 12; ++k) x.d[TH_DA + k] = drho[12 * (size_t)a + k];
+        return x;
+    };
+    double4 ri = D.r[i], si = D.s[i];
+    double si_sq = si.x * si.x + si.y * si.y + si.z * si.z;
+    T F_i, dF_i;
+    adj_emb(rho_of(i), th, F_i, dF_i);
+    T fx = dconst<ADJ_NJ>(0.0), fy = fx, fz = fx, hx = fx, hy = fx, hz = fx;
+    int nn = D.nbr_n[i];
+    for (int e = 0; e < nn; ++e) {
+        int pk = D.nbr[(size_t)e * D.natom + i];
+        int j = pk & SLD_JMASK;
+        double4 rj;
+        double3 d = adj_pair_vec(D, ri, pk, rj);
+        double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
+        double r0 = sqrt(rsq);
+        T r = dconst<ADJ_NJ>(r0);
+        T dudr = dconst<ADJ_NJ>(0.0);
+        if (r0 < D.rcut_pot) {
+            T f, dfr, phi, dphi, F_j, dF_j;
+            adj_dens(r, th, f, dfr);
+            adj_pair(K, r, th, phi, dphi);
+            adj_emb(rho_of(j), th, F_j, dF_j);
+            dudr = (dF_i + dF_j) * dfr + dphi;
+        }
+        T J, dJ;
+        adj_exch(r, th, J, dJ);
+        double4 sj = D.s[j];
+        if (r0 < D.rcut_mag) {
+            double sdot = si.x * sj.x + si.y * sj.y + si.z * sj.z;
+            double stimes = sqrt(si_sq * (sj.x * sj.x + sj.y * sj.y + sj.z * sj.z));
+            dudr = dudr - dJ * (sdot - stimes);
+        }
+        if (rsq < D.rcut_mag_sq) {
+            hx += J * sj.x; hy += J * sj.y; hz += J * sj.z;
+        }
+        T force = -dudr / r0;
+        fx += force * d.x; fy += force * d.y; fz += force * d.z;
+    }
+    const T* fv[3] = {&fx, &fy, &fz};
+    const T* hv[3] = {&hx, &hy, &hz};
+    for (int c = 0; c < 3; ++c) {
+        double* o = df + (3 * (size_t)i + c) * ADJ_NTHETA;
+        double* q = dh + (3 * (size_t)i + c) * ADJ_NTHETA;
+        for (int k = 0; k < ADJ_NTHETA; ++k) {
+            o[k] = k < ADJ_NJ ? fv[c]->d[k] : 0.0;   // the Landau constants move no force
+            q[k] = k < ADJ_NJ ? hv[c]->d[k] : 0.0;
+        }
+    }
+}
+
+void adj_jacobians(const Dev& D, const AdjDev& A, const AdjConst& K, cudaStream_t st, double* drho,
+                   double* df, double* dh) {
+    int nb = (D.natom + 127) / 128;
+    k_adj_rho_tan<<<nb, 128, 0, st>>>(D, A, K, drho);
+    k_adj_force_tan<<<nb, 128, 0, st>>>(D, A, K, drho, df, dh);
+}
+
 // ---------------------------------------------------------------------
 // reverse
 

@@ -377,6 +377,46 @@ int sld_adjoint_config(sld_ctx* c, const double* theta, double* out4, double* dE
     return SLD_OK;
 }
 
+int sld_adjoint_jacobians(sld_ctx* c, const double* theta, double* f, double* H, double* dF,
+                          double* dH) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    if (!theta || !dF) return SLD_ERR_ARG;
+    Adj a;
+    rc = alloc_adj(a, c, theta);
+    if (rc) return rc;
+    cudaStream_t st = c->st;
+    const size_t n = a.n, w = 3 * ADJ_NTHETA;
+    double4* f_keep = a.pool.get<double4>(n);
+    double* drho = a.pool.get<double>(12 * n);
+    double* ddf = a.pool.get<double>(w * n);
+    double* ddh = a.pool.get<double>(w * n);
+    if (!a.pool.ok) return SLD_ERR_NOMEM;
+    ACK(cudaDeviceSynchronize());   // the pool's clearing memsets
+    dcopy(f_keep, c->D.f, n, st);
+    launch_pairs(c->D, st, false);
+    fields(a);
+    adj_jacobians(c->D, a.A, a.K, st, drho, ddf, ddh);
+    std::vector<double> hf(w * n), hh(w * n);
+    std::vector<double4> fv(n), Hv(n);
+    ACK(cudaMemcpyAsync(hf.data(), ddf, sizeof(double) * w * n, cudaMemcpyDeviceToHost, st));
+    ACK(cudaMemcpyAsync(hh.data(), ddh, sizeof(double) * w * n, cudaMemcpyDeviceToHost, st));
+    ACK(cudaMemcpyAsync(fv.data(), c->D.f, sizeof(double4) * n, cudaMemcpyDeviceToHost, st));
+    ACK(cudaMemcpyAsync(Hv.data(), a.A.H, sizeof(double4) * n, cudaMemcpyDeviceToHost, st));
+    dcopy(c->D.f, f_keep, n, st);
+    rc = finish(c);
+    if (rc) return rc;
+    // slot order to the caller's atom order
+    for (size_t q = 0; q < n; ++q) {
+        size_t i = (size_t)c->id_of_slot[q];
+        std::copy(hf.begin() + q * w, hf.begin() + (q + 1) * w, dF + i * w);
+        if (dH) std::copy(hh.begin() + q * w, hh.begin() + (q + 1) * w, dH + i * w);
+        if (f) { f[3 * i] = fv[q].x; f[3 * i + 1] = fv[q].y; f[3 * i + 2] = fv[q].z; }
+        if (H) { H[3 * i] = Hv[q].x; H[3 * i + 1] = Hv[q].y; H[3 * i + 2] = Hv[q].z; }
+    }
+    return SLD_OK;
+}
+
 int sld_adjoint_trajectory(sld_ctx* c, const double* theta, int nsteps, int checkpoint_every,
                            double* L, double* dL) {
     int rc = check_ctx(c);

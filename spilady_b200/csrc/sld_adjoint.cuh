@@ -22,6 +22,8 @@ void adj_force(const Dev& D, const AdjDev& A, const AdjConst& K, cudaStream_t st
 void adj_sweep(const Dev& D, const AdjConst& K, cudaStream_t st, const int* cells, int n, double dt,
                bool backward);
 void adj_kick(const Dev& D, cudaStream_t st, double h, double4* ppre);
+void adj_jacobians(const Dev& D, const AdjDev& A, const AdjConst& K, cudaStream_t st, double* drho,
+                   double* df, double* dh);
 void adj_energy_grad(const Dev& D, const AdjDev& A, const AdjConst& K, cudaStream_t st);
 void adj_force_rev(const Dev& D, const AdjDev& A, const AdjConst& K, cudaStream_t st);
 void adj_field_rev(const Dev& D, const AdjDev& A, const AdjConst& K, cudaStream_t st);

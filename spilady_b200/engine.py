@@ -114,6 +114,7 @@ def lib():
         L.sld_adjoint_theta_default.argtypes = [P]
         L.sld_adjoint_config.argtypes = [vp, P, P, P, P]
         L.sld_adjoint_trajectory.argtypes = [vp, P, C.c_int, C.c_int, P, P]
+        L.sld_adjoint_jacobians.argtypes = [vp, P, P, P, P, P]
         L.sld_error_string.argtypes = [C.c_int]
         L.sld_error_string.restype = C.c_char_p
         _lib = L
@@ -365,6 +366,17 @@ class Engine:
                "adjoint_config")
         return out, dE, dL
 
+    def adjoint_jacobians(self, theta):
+        """Forces f, fields H (natom x 3) and their Jacobians in theta
+        (natom x 3 x 36 each)."""
+        th = np.ascontiguousarray(theta, np.float64)
+        n = self.natom
+        f, H = np.zeros((n, 3)), np.zeros((n, 3))
+        dF, dH = np.zeros((n, 3, ADJ_NTHETA)), np.zeros((n, 3, ADJ_NTHETA))
+        _check(self.L.sld_adjoint_jacobians(self.h, _dp(th), _dp(f), _dp(H), _dp(dF), _dp(dH)),
+               "adjoint_jacobians")
+        return f, H, dF, dH
+
     def adjoint_trajectory(self, theta, nsteps, checkpoint_every=20, grad=True):
         """Loss after nsteps NVE steps and (grad) its gradient in theta."""
         th = np.ascontiguousarray(theta, np.float64)
@@ -455,6 +467,17 @@ class Batch:
         _check(self.L.sld_adjoint_config(self.h, _dp(th), _dp(out), _dp(dE), _dp(dL)),
                "adjoint_config")
         return out, dE, dL
+
+    def adjoint_jacobians(self, theta):
+        """Forces f, fields H (natom x 3) and their Jacobians in theta
+        (natom x 3 x 36 each)."""
+        th = np.ascontiguousarray(theta, np.float64)
+        n = self.natom
+        f, H = np.zeros((n, 3)), np.zeros((n, 3))
+        dF, dH = np.zeros((n, 3, ADJ_NTHETA)), np.zeros((n, 3, ADJ_NTHETA))
+        _check(self.L.sld_adjoint_jacobians(self.h, _dp(th), _dp(f), _dp(H), _dp(dF), _dp(dH)),
+               "adjoint_jacobians")
+        return f, H, dF, dH
 
     def adjoint_trajectory(self, theta, nsteps, checkpoint_every=20, grad=True):
         """Loss after nsteps NVE steps and (grad) its gradient in theta."""

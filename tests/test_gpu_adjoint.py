@@ -160,3 +160,28 @@ def test_gradients_against_the_references_finite_differences():
     print(f"vs the reference's FD: config {ec:.1e}, {K} steps {et:.1e}")
     # measured 3.6e-5 and 1.3e-5
     assert ec <= 2e-4 and et <= 2e-4
+
+
+def test_force_and_field_jacobians_against_finite_differences():
+    params, r, p, s, e = system()
+    th = E().adjoint_theta_default()
+    f, H, dF, dH = e.adjoint_jacobians(th)
+    h = steps(th)
+    worst = 0.0
+    for k in range(36):
+        tp, tm = th.copy(), th.copy()
+        tp[k] += h[k]
+        tm[k] -= h[k]
+        fp, Hp, _, _ = e.adjoint_jacobians(tp)
+        fm, Hm, _, _ = e.adjoint_jacobians(tm)
+        for name, g, a, b in (("dF", dF[:, :, k], fp, fm), ("dH", dH[:, :, k], Hp, Hm)):
+            fd = (a - b) / (2 * h[k])
+            scale = max(np.max(np.abs(fd)), 1e-30)
+            err = np.max(np.abs(g - fd)) / scale
+            if np.max(np.abs(fd)) > 0:
+                worst = max(worst, err)
+                assert err <= 1e-6, f"{name} theta[{k}]: {err:.2e}"
+            else:
+                assert np.all(g == 0.0), f"{name} theta[{k}] should vanish"
+    print(f"jacobians: worst {worst:.1e}")
+
