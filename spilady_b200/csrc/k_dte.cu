@@ -471,8 +471,11 @@ static void launch_dte_form(const Dev& D, cudaStream_t st, double dt) {
     cudaLaunchAttribute at[1];
     const int hub_per = (D.nte + HUB_CL - 1) / HUB_CL;
     const int mode = D.tune.dte_mode >= 0 ? D.tune.dte_mode : g_dte_mode;
+    // a hub thread keeps the energies of at most four of its CTA's cells
+    int threads = D.tune.dte_threads > 0 ? D.tune.dte_threads : 1024;
+    if (hub_per > 4 * threads) threads = 1024;
     if (mode == 2 && g_hub_ok && D.nte <= kHubMaxCells && hub_per <= 4 * 1024) {
-        cudaLaunchConfig_t cfg = cluster_cfg(HUB_CL, 1024, hub_smem(D.nte), st, at);
+        cudaLaunchConfig_t cfg = cluster_cfg(HUB_CL, threads, hub_smem(D.nte), st, at);
         cudaLaunchKernelEx(&cfg, k_dte_hub<FAST>, D, dt, hub_per);
         return;
     }

@@ -437,7 +437,7 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     D.landau_on = (D.ham == SLD_HAM_SLDHL || D.ham == SLD_HAM_SDHL) ? 1 : 0;
     D.hc = D.ham == SLD_HAM_SLDHL ? 1 : 0;
     D.hint = (D.ham == SLD_HAM_SDH || D.ham == SLD_HAM_SLDH) ? 1 : 0;
-    D.tune = Tune{0, 0, 0, 0, -1};
+    D.tune = Tune{0, 0, 0, 0, -1, 0};
     D.quantum = prm->quantum_noise ? 1 : 0;
     D.qM = prm->msteps_quantum;
     D.step = prm->step;
@@ -1531,7 +1531,7 @@ static int trial(sld_ctx* c, const StateCopy& s, int steps, double* ms) {
     return SLD_OK;
 }
 
-int sld_autotune(sld_ctx* c, int steps, int* out5) {
+int sld_autotune(sld_ctx* c, int steps, int* out6) {
     if (!c || steps < 1) return SLD_ERR_ARG;
     if (dynamic_step(c)) return SLD_ERR_ARG;   // no captured step to time
     StateCopy s;
@@ -1547,6 +1547,7 @@ int sld_autotune(sld_ctx* c, int steps, int* out5) {
                               {&T.force_block, {64, 96, 128}}};
     if (c->P.eltemp) {
         axes.push_back({&T.dte_mode, {0, 1, 2}});
+        axes.push_back({&T.dte_threads, {256, 512, 1024}});
         if (c->P.te_mesh > 0) axes.push_back({&T.temp_block, {64, 128}});
     }
     for (auto& ax : axes) {
@@ -1568,9 +1569,9 @@ int sld_autotune(sld_ctx* c, int steps, int* out5) {
     state_free(s);
     if (rc) return rc;
     if (rc2) return rc2;
-    if (out5) {
-        out5[0] = T.sweep_block; out5[1] = T.pair_block; out5[2] = T.force_block;
-        out5[3] = T.temp_block; out5[4] = T.dte_mode;
+    if (out6) {
+        out6[0] = T.sweep_block; out6[1] = T.pair_block; out6[2] = T.force_block;
+        out6[3] = T.temp_block; out6[4] = T.dte_mode; out6[5] = T.dte_threads;
     }
     return SLD_OK;
 }

@@ -61,6 +61,7 @@ struct Tune {
     int force_block;   // atoms per block of the force passes
     int temp_block;    // atoms per block of the cell-temperature pass on a Te mesh
     int dte_mode;      // core_dTe kernel: 0 one CTA, 1 cluster, 2 hub; -1 default
+    int dte_threads;   // threads per CTA of the hub core_dTe kernel
 };
 
 struct Dev {
