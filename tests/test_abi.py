@@ -74,3 +74,39 @@ def test_error_strings_cover_every_code():
         assert msg and msg != "unknown error", code
         if code < 0:
             assert code in engine.ERRORS, code
+
+
+def test_read_variables_other_switches(tmp_path):
+    # the keys of the switches that are compile-time in the reference
+    # (control.h) and of the variables behind them (read_variables.cpp:197-250)
+    f = tmp_path / "variables.in"
+    f.write_text("hamiltonian SDHL\ngamma_S_H 0.02\nPRESSURE 1\nSTRESS 1\nchangestep 1\n"
+                 "pressure 2.5\nstress_yx -0.5\nbaro_damping_time 3e-13\n"
+                 "interval_of_scale_pressure 7\ndisplace_limit 0.02\nphi_limit 0.3\n"
+                 "quantumnoise 1\nMsteps_quantum 20\nNfrequency_quantum 64\n"
+                 "interval_of_config_out 25\n")
+    P = engine.Params()
+    L = engine.lib()
+    L.sld_params_default(C.byref(P))
+    assert P.interval_of_config_out == 1000 and P.msteps_quantum == 50
+    assert P.nfrequency_quantum == 150 and P.baro_damping_time == 1e-13
+    assert L.sld_read_variables(str(f).encode(), C.byref(P)) == 0
+    assert P.hamiltonian == engine.SDHL and P.gamma_S_H == 0.02
+    assert P.pressure_control == 1 and P.stress_control == 1 and P.change_step == 1
+    assert P.pressure == 2.5 and P.stress[1] == -0.5 and P.baro_damping_time == 3e-13
+    assert P.interval_of_scale_pressure == 7 and P.displace_limit == 0.02
+    assert P.phi_limit == 0.3 and P.quantum_noise == 1 and P.msteps_quantum == 20
+    assert P.nfrequency_quantum == 64 and P.interval_of_config_out == 25
+
+
+def test_hamiltonian_switch_combinations_rejected():
+    from spilady_b200.lattice import initial_state
+    params, r, p, s = initial_state(5, seed=1)
+    E = engine
+    assert _create(params, r, p, s, hamiltonian=E.MD, spinlang=True) == -1     # no spins
+    assert _create(params, r, p, s, hamiltonian=E.SDH, lattlang=True) == -1    # no lattice
+    assert _create(params, r, p, s, hamiltonian=E.SDHL, pressure_control=True) == -1
+    assert _create(params, r, p, s, hamiltonian=E.MD, lattlang=True, eltemp=True,
+                   spinlang=False, quantum_noise=True, change_step=True) == -1
+    assert _create(params, r, p, s, quantum_noise=True) == -1                  # needs lattlang
+    assert _create(params, r, p, s, hamiltonian=7) == -1

@@ -3,12 +3,18 @@ own CPU build: the committed golden fixtures (tests/golden, made by
 tests/golden/make_golden.py from oracle/_ref) and, where the reference build
 is present, a live run.  With the reference's random stream (MWC, one
 thread) the restatement reproduces the reference bit for bit."""
+import os
+import sys
+
 import numpy as np
 import pytest
 
 from conftest import load_golden, relerr
 from oracle import orc, refjob
-from spilady_b200.lattice import default_params
+from oracle import refjob as rj
+from spilady_b200.lattice import default_params, initial_state
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 SWITCHES = {
     "nve": {},
@@ -121,3 +127,35 @@ def test_oracle_rejects_two_cell_box():
     params, r, p, s = initial_state(2, seed=1)
     with pytest.raises(ValueError):
         orc.System(params, r, p, s)
+
+
+def test_quantum_filter_matches_the_references():
+    # initial_quantum_noise's filter, as the reference built with quantumnoise
+    # makes it, against the oracle's restatement: bit for bit
+    from oracle import orc
+    if not rj.available("quant"):
+        pytest.skip("reference build missing")
+    params, r, p, s = initial_state(6, seed=5)
+    ops = rj.set_ops(Msteps_quantum=3, Nfrequency_quantum=12) + [(rj.OP_QINIT, 0),
+                                                                 (rj.OP_QFILTER, 0)]
+    _, t = rj.run("quant", params, r, p, s, ops=ops, files=True)
+    ref = np.array([float(x) for x in t["qfilter.dat"].split()])
+    o = orc.System(params, r, p, s, lattlang=True, quantum=True, msteps_quantum=3,
+                   nfrequency_quantum=12)
+    assert len(ref) == 24 and np.array_equal(o.quantum_filter(), ref)
+
+
+def test_param_build_is_the_stock_build_at_the_default_constants():
+    # the param build (the potential's constants from theta.in, for finite
+    # differences of the reference's code) gives the stock build's forces
+    # and fields at the default constants, bit for bit
+    if not (rj.available("param") and rj.available("nve")):
+        pytest.skip("reference build missing")
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_golden import DEFAULT_THETA
+    params, r, p, s = initial_state(6, seed=6, tilt=0.2, pos_sigma=0.05)
+    ops = [(rj.OP_CORE, 2), (rj.OP_CHECK, 1), (rj.OP_DUMP, 0)]
+    a = rj.run("param", params, r, p, s, ops=ops,
+               inputs={"theta.in": " ".join("%.17g" % x for x in DEFAULT_THETA)})[0]
+    b = rj.run("nve", params, r, p, s, ops=ops)[0]
+    assert np.array_equal(a.atoms, b.atoms)
