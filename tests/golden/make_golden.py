@@ -7,6 +7,7 @@ Langevin noise stream depends on the thread count).  Run from the repo root:
 
     python tests/golden/make_golden.py            # the trajectory fixtures
     python tests/golden/make_golden.py adjoint    # the reference's FD gradient
+    python tests/golden/make_golden.py long       # the reference's long runs
 """
 from __future__ import annotations
 
@@ -99,6 +100,38 @@ def make_adjoint_fd(path=os.path.join(HERE, "adjoint_ref_fd.npz"), K=10, threads
     print("adjoint_ref_fd", path)
 
 
+def read_lines(text):
+    return np.array([[float(x) for x in l.split()] for l in text.splitlines() if l.strip()])
+
+
+def make_long_runs(path=os.path.join(HERE, "long_runs_ref.npz"), threads=16):
+    """The reference's long runs, for the statistical checks: its print-out
+    lines every step (check.cpp with interval_of_print_out 1).
+      NVE: bcc Fe 16^3 cells (8,192 atoms), spins tilted 0.05 rad, 300 K
+           momenta, dt 1 fs, 1,000 steps: the total energy per atom (pe + ke +
+           me + me0), whose drift the engine's may not exceed;
+      Langevin spin + lattice at 300 K: 10^3 cells (2,000 atoms), 3,000 steps:
+           Tl, Ts_R, Ts_L and |<m>|, whose equilibrium averages the engine's
+           must match within their error bars (the noise streams differ).
+    OpenMP threads change only the rounding of NVE and the reference's own
+    noise stream of the Langevin run."""
+    never = [(rj.OP_CONFIG_INTERVAL, 10**9)]
+    params, r, p, s = initial_state(16, seed=4, tilt=0.05, temperature=300.0)
+    _, t = rj.run("nve", params, r, p, s, ops=never + [(rj.OP_STEP, 1000)], threads=threads,
+                  files=True)
+    enr = read_lines(t["enr-ref.dat"])
+    e_nve = enr[:, 2] + enr[:, 3] + enr[:, 4] + enr[:, 5]
+    params, r, p, s = initial_state(10, seed=7, tilt=0.05, temperature=300.0)
+    _, t = rj.run("lang", params, r, p, s, ops=never + [(rj.OP_STEP, 3000)], threads=threads,
+                  files=True)
+    tmp = read_lines(t["tmp-ref.dat"])
+    spn = read_lines(t["spn-ref.dat"])
+    np.savez_compressed(path, nve_E=e_nve, nve_steps=1000,
+                        lang_Tl=tmp[:, 2], lang_TsR=tmp[:, 3], lang_TsL=tmp[:, 4],
+                        lang_m=spn[:, 9], lang_steps=3000)
+    print("long_runs_ref", path)
+
+
 # the potential's 36 constants in sld_adjoint_theta_default's order (DD05.cpp,
 # JijFe.cpp): F a, b; f coefficients, knots; phi coefficients, knots; J A, rc;
 # Landau A, B, C, D
@@ -119,6 +152,8 @@ if __name__ == "__main__":
     args = sys.argv[1:]
     if args == ["adjoint"]:
         make_adjoint_fd()
+    elif args == ["long"]:
+        make_long_runs()
     else:
         for n in (args or CASES):
             make(n)
