@@ -340,13 +340,13 @@ def run_adjoint(args, world, rank, local):
     ((Lk, dLk), ms_traj) = timed(lambda: e.adjoint_trajectory(th, K, C), 1)
     (_, ms_fwd) = timed(lambda: e.adjoint_trajectory(th, K, C, grad=False), 1)
 
-    def fd(fn):
+    def fd(fn, scale=1.0):
         g = np.zeros(len(th))
         for k in range(len(th)):
             tp, tm = th.copy(), th.copy()
-            tp[k] += h[k]
-            tm[k] -= h[k]
-            g[k] = (fn(tp) - fn(tm)) / (2 * h[k])
+            tp[k] += scale * h[k]
+            tm[k] -= scale * h[k]
+            g[k] = (fn(tp) - fn(tm)) / (2 * scale * h[k])
         return g
 
     def err(g, f):
@@ -359,6 +359,15 @@ def run_adjoint(args, world, rank, local):
     fdE = fd(lambda t: e64.adjoint_config(t)[0][0])
     fdL = fd(lambda t: e64.adjoint_config(t)[0][1])
     fdT = fd(lambda t: e64.adjoint_trajectory(t, K, C, grad=False))
+    # A sharper check of the trajectory gradient.  Through 200 steps the
+    # rounding of every step is amplified with the trajectory's separation,
+    # which makes L(theta) noisy on the scale of h = 1e-6; central differences
+    # with 100x larger steps (1e-4 and 5e-5 of each parameter) see 100x less of
+    # that noise, and Richardson's extrapolation of the two removes their
+    # O(h^2) truncation error.
+    fdA = fd(lambda t: e64.adjoint_trajectory(t, K, C, grad=False), 100.0)
+    fdB = fd(lambda t: e64.adjoint_trajectory(t, K, C, grad=False), 50.0)
+    fdTR = (4.0 * fdB - fdA) / 3.0
     _, dLk64 = e64.adjoint_trajectory(th, K, C)
     line = {
         "metric": f"ms per gradient of L in 36 potential parameters through {K} NVE steps, "
@@ -374,8 +383,12 @@ def run_adjoint(args, world, rank, local):
         "vs_finite_differences": {"dE_config": err(dE, fdE), "dL_config": err(dL, fdL),
                                   f"dL_{K}_steps": err(dLk, fdT),
                                   f"dL_{K}_steps_fp64_forward": err(dLk64, fdT),
+                                  f"dL_{K}_steps_fp64_forward_vs_richardson": err(dLk64, fdTR),
+                                  f"dL_{K}_steps_vs_richardson": err(dLk, fdTR),
+                                  "fd_h_vs_richardson": err(fdT, fdTR),
                                   "how": "max |adjoint - FD| / max |FD| over the 36 parameters; "
-                                         "FD: FP64 central differences, h = 1e-6 relative"},
+                                         "FD: FP64 central differences, h = 1e-6 relative; "
+                                         "richardson: from h = 1e-4 and 5e-5 relative"},
         "roofline": None, "cpu_baseline": None, "e2e": None,
     }
     print(json.dumps(line))
