@@ -415,6 +415,20 @@ def main():
             "fp64-analytic": engine.FP64_ANALYTIC}[args.precision]
     e = engine.Engine(params, r, p, s, te=te, device=local, precision=prec, **sw)
     natom = e.natom
+    # The split form's error against the FP64 run of the same kernels, on the
+    # start state: forces, exchange fields and per-atom energies (BASELINE's
+    # bound: 1e-5 relative).
+    split_err = None
+    if prec == engine.SPLIT and not args.small:
+        ref = engine.Engine(params, r, p, s, te=te, device=local,
+                            precision=engine.FP64_ANALYTIC, **sw)
+        rel = lambda a, b: float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+        split_err = {"force": rel(e.get("f"), ref.get("f")),
+                     "field": rel(e.get("H"), ref.get("H")),
+                     "pe": rel(e.get("pe"), ref.get("pe")),
+                     "me": rel(e.get("me"), ref.get("me")),
+                     "how": "max |split - fp64| / max |fp64| over all atoms, start state"}
+        ref.close()
     # launch shapes by the autotuner (outside the timed region; the state is
     # put back afterwards)
     shapes = None if args.no_autotune else e.autotune(steps=8)
@@ -501,6 +515,7 @@ def main():
                    "precision": args.precision, "natom": natom,
                    "l2": "state (~1 GB) larger than L2; no flush needed",
                    "launch_shapes": shapes,
+                   "split_vs_fp64": split_err,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": kernels_per_step * args.steps, "clocks": clk,
