@@ -8,7 +8,7 @@ temperature on a 16^3 mesh (8^3 unit cells per node) with a Gaussian hot spot
 (3,000 K peak, sigma 2 nm, 300 K background), energy renormalisation every
 step, dt = 0.5 fs.  Synthetic seeded initial state; spins tilted by a
 Gaussian polar angle of 0.35 rad so that the spin temperature starts near
-300 K (see DESIGN.md).  The state (about 1 GB) is far larger than L2, so
+300 K.  The state (about 1 GB) is far larger than L2, so
 every step streams it from HBM.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -416,8 +416,8 @@ def main():
     e = engine.Engine(params, r, p, s, te=te, device=local, precision=prec, **sw)
     natom = e.natom
     # The split form's error against the FP64 run of the same kernels, on the
-    # start state: forces, exchange fields and per-atom energies (BASELINE's
-    # bound: 1e-5 relative).
+    # start state: forces, exchange fields and per-atom energies (the split
+    # form is held to 1e-5 relative).
     split_err = None
     if prec == engine.SPLIT and not args.small:
         ref = engine.Engine(params, r, p, s, te=te, device=local,

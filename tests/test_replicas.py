@@ -1,4 +1,5 @@
-"""Replicas across ranks (the path does not shard): bench.py's
+"""Replicas across ranks (the path does not shard: the colour-ordered spin
+sweeps would need a halo exchange per colour group): bench.py's
 process-group plumbing, run as two gloo ranks on the CPU.  Each rank times
 its own replica; the job's time is the maximum over ranks."""
 import os
