@@ -57,15 +57,24 @@ __device__ __forceinline__ Nbr6 te_nbr6(const Dev& D, int k) {
 }
 
 // core_dTe_CPU.cpp:158-171: the Laplacian term of one cell (the fitted
-// form multiplies by the reciprocal squared edges instead of dividing)
+// form multiplies by the reciprocal squared edges instead of dividing, with
+// every rounding written out, so that the hub's two sweep schedules, whose
+// code the compiler contracts differently, form the same bits)
 template <bool FAST>
 __device__ __forceinline__ double te_lap(const DteGeom& g, double T, double xp, double xm,
                                          double yp, double ym, double zp, double zm) {
-    double ex = xp + xm - 2.0 * T;
-    double ey = yp + ym - 2.0 * T;
-    double ez = zp + zm - 2.0 * T;
-    if constexpr (FAST) return g.pre * (ex * g.idx2 + ey * g.idy2 + ez * g.idz2);
-    else return g.pre * (ex / g.dx2 + ey / g.dy2 + ez / g.dz2);
+    if constexpr (FAST) {
+        const double t2 = 2.0 * T;
+        const double ex = __dsub_rn(__dadd_rn(xp, xm), t2);
+        const double ey = __dsub_rn(__dadd_rn(yp, ym), t2);
+        const double ez = __dsub_rn(__dadd_rn(zp, zm), t2);
+        return __dmul_rn(g.pre, __fma_rn(ez, g.idz2, __fma_rn(ey, g.idy2, __dmul_rn(ex, g.idx2))));
+    } else {
+        double ex = xp + xm - 2.0 * T;
+        double ey = yp + ym - 2.0 * T;
+        double ez = zp + zm - 2.0 * T;
+        return g.pre * (ex / g.dx2 + ey / g.dy2 + ez / g.dz2);
+    }
 }
 
 // Gel Tl + Ges Ts_L and (Gel + Ges) hh / boltz of cell k
@@ -243,154 +252,233 @@ __global__ void __launch_bounds__(256) k_dte_cluster(Dev D, double dt) {
 // Cluster "hub" form: every CTA of an 8-CTA cluster does the cell-local A and
 // B parts for its share of the cells in parallel; CTA 0 holds all Te and
 // Te_to_Ee(Te) in its shared memory (the others read and write them through
-// distributed shared memory) and runs C's colour phases with block barriers.
-// Two cluster barriers per substep instead of one per colour phase.
+// distributed shared memory) and runs C's diffusion sweep with block
+// barriers.  Two cluster barriers per substep instead of one per colour
+// phase.
+//   - The cells are stored in colour order (position m holds te_gcells[m]),
+//     so the cells of a colour group are consecutive and so, in a regular
+//     mesh, are their neighbours in each direction: a warp's shared-memory
+//     loads of the sweep hit distinct banks.  A table gives each position
+//     the positions of its six face neighbours, one 16-byte record.
 //   - Each CTA keeps its cells' coupling source Gel Tl + Ges Ts_L and rate
 //     (Gel + Ges) h/2/boltz in its own shared memory: they do not change
 //     during core_dTe, so the substeps read no global memory.
-//   - The hub also keeps the colour lists and a table of each cell's six
-//     neighbours in its shared memory.
-//   - Reference expressions: in a colour phase, half of the hub's threads
-//     update the Te of the phase's cells (the chain the next phase waits for)
-//     while the other half evaluate Te_to_Ee for the cells of the previous
-//     phase, which no cell of this phase reads.  The one exception is the
-//     last forward colour, updated again right away by the backward pass:
-//     its Te_to_Ee is evaluated in place.  Every value is the one of the
-//     plain sequence.
+//   - The sweep runs by colour phases (one barrier per phase) or by levels
+//     (te_levels: one barrier per level, fewer than the phases).
+//   - Reference expressions: half of the hub's threads update the Te of a
+//     phase's (level's) cells, the chain the next one waits for, while the
+//     other half evaluate Te_to_Ee for the cells of the previous one, which
+//     nothing of this one reads.  A cell updated in two consecutive phases
+//     (the last forward colour) has its Te_to_Ee evaluated in place; by
+//     levels, such a pair of updates is one task.  Every value is the one of
+//     the plain sequence.
 //   - Fitted expressions: an update keeps the energy it converts to Te (what
 //     Te_to_Ee would return, up to rounding), so the sweep evaluates no
 //     Te_to_Ee at all.
-static const int kHubMaxCells = 6400;    // 8 (2 n + 2 + 2 n / 8) + 16 n bytes of shared memory
+static const int kHubMaxCells = 6000;   // 8 (2 n + 2 + 2 n / 8) + 16 n + 4 n bytes of shared memory
 
-template <bool FAST>
+// the positions of the six face neighbours of position m
+__device__ __forceinline__ void hub_nb(const uint4* sNb, int m, int (&q)[6]) {
+    const uint4 v = sNb[m];
+    q[0] = (int)(v.x & 0xffffu);
+    q[1] = (int)(v.x >> 16);
+    q[2] = (int)(v.y & 0xffffu);
+    q[3] = (int)(v.y >> 16);
+    q[4] = (int)(v.z & 0xffffu);
+    q[5] = (int)(v.z >> 16);
+}
+
+// one update of the fitted form (two for a double task) at position t & 0x7fff:
+// its new Te and energy, which it returns; nothing is stored
+__device__ __forceinline__ int hub_task_fast(const double* hsm, int n, const uint4* sNb, unsigned t,
+                                             const DteGeom& gm, double& T, double& x) {
+    const int m = (int)(t & 0x7fffu);
+    int q[6];
+    hub_nb(sNb, m, q);
+    const double a0 = hsm[q[0]], a1 = hsm[q[1]], a2 = hsm[q[2]], a3 = hsm[q[3]], a4 = hsm[q[4]],
+                 a5 = hsm[q[5]];
+    T = hsm[m];
+    x = __dadd_rn(hsm[n + m], te_lap<true>(gm, T, a0, a1, a2, a3, a4, a5));
+    T = te_T<true>(x);
+    if (t & 0x8000u) {
+        x = __dadd_rn(x, te_lap<true>(gm, T, a0, a1, a2, a3, a4, a5));
+        T = te_T<true>(x);
+    }
+    return m;
+}
+
+// one update (two for a double task) of the reference form: the new Te
+__device__ __forceinline__ int hub_task_ref(const double* hsm, int n, const uint4* sNb, unsigned t,
+                                            const DteGeom& gm, double& T) {
+    const int m = (int)(t & 0x7fffu);
+    int q[6];
+    hub_nb(sNb, m, q);
+    const double a0 = hsm[q[0]], a1 = hsm[q[1]], a2 = hsm[q[2]], a3 = hsm[q[3]], a4 = hsm[q[4]],
+                 a5 = hsm[q[5]];
+    T = hsm[m];
+    T = te_T<false>(hsm[n + m] + te_lap<false>(gm, T, a0, a1, a2, a3, a4, a5));
+    if (t & 0x8000u) {
+        const double E = te_E<false>(T);
+        T = te_T<false>(E + te_lap<false>(gm, T, a0, a1, a2, a3, a4, a5));
+    }
+    return m;
+}
+
+// C's diffusion sweep on the hub.  By levels (LEV) the tasks of a level read
+// no value another task of the level writes; by phases a phase is one colour
+// group, positions te_gstart[g]..te_gstart[g+1].  The fitted form takes two
+// tasks per thread and iteration, whose chains interleave.  The reference
+// form splits the threads into workers and helpers (above).
+template <bool FAST, bool LEV>
+__device__ __forceinline__ void hub_sweep(const Dev& D, double* hsm, int n,
+                                          const unsigned short* sTk, const uint4* sNb,
+                                          const DteGeom& gm) {
+    const int G = D.te_ngroups;
+    const int nph = LEV ? D.te_nlevels : 2 * G;
+    // tasks of phase (level) l: [b, e), as positions (phases) or task entries
+    auto range = [&](int l, int& b, int& e) {
+        if constexpr (LEV) {
+            b = D.te_lstart[l];
+            e = D.te_lstart[l + 1];
+        } else {
+            const int g = l < G ? l : 2 * G - 1 - l;
+            b = D.te_gstart[g];
+            e = D.te_gstart[g + 1];
+        }
+    };
+    auto task = [&](int m) -> unsigned { return LEV ? (unsigned)sTk[m] : (unsigned)m; };
+    if constexpr (FAST) {
+        const int bd = blockDim.x;
+        for (int l = 0; l < nph; ++l) {
+            int b, e;
+            range(l, b, e);
+            for (int m = b + threadIdx.x; m < e; m += 2 * bd) {
+                if (m + bd < e) {   // two tasks: both chains in flight together
+                    double T1, x1, T2, x2;
+                    const int k1 = hub_task_fast(hsm, n, sNb, task(m), gm, T1, x1);
+                    const int k2 = hub_task_fast(hsm, n, sNb, task(m + bd), gm, T2, x2);
+                    hsm[k1] = T1;
+                    hsm[n + k1] = x1;
+                    hsm[k2] = T2;
+                    hsm[n + k2] = x2;
+                } else {
+                    double T1, x1;
+                    const int k1 = hub_task_fast(hsm, n, sNb, task(m), gm, T1, x1);
+                    hsm[k1] = T1;
+                    hsm[n + k1] = x1;
+                }
+            }
+            __syncthreads();
+        }
+    } else {
+        const int half = blockDim.x / 2;
+        const bool worker = threadIdx.x < half;
+        const int lane = worker ? threadIdx.x : threadIdx.x - half;
+        int pb = 0, pe = 0;   // the previous phase's tasks, whose Te_to_Ee is due
+        for (int l = 0; l < nph; ++l) {
+            int b, e;
+            range(l, b, e);
+            // by phases, the last forward colour is updated again at once
+            const bool inplace = !LEV && l == G - 1;
+            if (worker) {
+                for (int m = b + lane; m < e; m += half) {
+                    double T;
+                    const int k = hub_task_ref(hsm, n, sNb, task(m), gm, T);
+                    hsm[k] = T;
+                    if (inplace) hsm[n + k] = te_E<false>(T);
+                }
+            } else {
+                for (int m = pb + lane; m < pe; m += half) {
+                    const int k = (int)(task(m) & 0x7fffu);
+                    hsm[n + k] = te_E<false>(hsm[k]);
+                }
+            }
+            __syncthreads();
+            pb = inplace ? 0 : b;
+            pe = inplace ? 0 : e;
+        }
+        for (int m = pb + threadIdx.x; m < pe; m += blockDim.x) {
+            const int k = (int)(task(m) & 0x7fffu);
+            hsm[n + k] = te_E<false>(hsm[k]);
+        }
+    }
+}
+
+template <bool FAST, bool LEV>
 __global__ void __launch_bounds__(1024) k_dte_hub(Dev D, double dt, int per) {
     cg::cluster_group cl = cg::this_cluster();
     extern __shared__ __align__(16) double hsm[];
     const int n = D.nte;
     const int rank = (int)cl.block_rank();
-    double* hT = cl.map_shared_rank(hsm, 0);   // the hub's arrays
+    double* hT = cl.map_shared_rank(hsm, 0);   // the hub's arrays, by position
     double* hE = hT + n;
     double* hfac = hT + 2 * n;
-    double* mySrc = hsm + 2 * n + 2;           // this CTA's own cells
+    double* mySrc = hsm + 2 * n + 2;           // this CTA's own positions
     double* myG = mySrc + per;
-    int* sGc = reinterpret_cast<int*>(myG + per);                        // hub: colour lists
-    unsigned short* sNb = reinterpret_cast<unsigned short*>(sGc + n);    // hub: 6 neighbours
+    uint4* sNb = reinterpret_cast<uint4*>(myG + per);                      // hub: neighbours
+    unsigned short* sTk = reinterpret_cast<unsigned short*>(sNb + n);      // hub: level tasks
     __shared__ double sh[32];
-    const int k0 = rank * per, k1 = min(n, k0 + per);
+    const int p0 = rank * per, p1 = min(n, p0 + per);
     int nloop = D.te_nloop > 0 ? D.te_nloop : 50;
     double h = dt / nloop, hh = h / 2.0;
-    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+    for (int m = p0 + threadIdx.x; m < p1; m += blockDim.x) {
+        const int k = D.te_gcells[m];
         double T = D.Te[k];
-        hT[k] = T;
-        hE[k] = te_E<FAST>(T);
-        mySrc[k - k0] = te_src(D, k);
-        myG[k - k0] = te_rate(D, k, hh);
+        hT[m] = T;
+        hE[m] = te_E<FAST>(T);
+        mySrc[m - p0] = te_src(D, k);
+        myG[m - p0] = te_rate(D, k, hh);
     }
     if (rank == 0) {
-        for (int m = threadIdx.x; m < n; m += blockDim.x) {
-            sGc[m] = D.te_gcells[m];
-            const Nbr6 q = te_nbr6(D, m);
-            unsigned short* o = sNb + 6 * m;
-            o[0] = (unsigned short)q.xp; o[1] = (unsigned short)q.xm; o[2] = (unsigned short)q.yp;
-            o[3] = (unsigned short)q.ym; o[4] = (unsigned short)q.zp; o[5] = (unsigned short)q.zm;
+        for (int m = threadIdx.x; m < n; m += blockDim.x) sNb[m] = D.te_lnb[m];
+        if constexpr (LEV) {
+            for (int m = threadIdx.x; m < D.te_lstart[D.te_nlevels]; m += blockDim.x)
+                sTk[m] = D.te_ltasks[m];
         }
     }
     cl.sync();
     const DteGeom gm = dte_geom(D, h);
     double lastE[4];   // this thread's last A-step energies (per <= 4096 -> <= 4 per thread)
     for (int it = 0; it < nloop; ++it) {
-        for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {   // A(h/2), B(h/2)
-            double T = te_T<FAST>(hE[k] + hh * mySrc[k - k0]);
-            T = te_rk4<FAST>(T, myG[k - k0], hh);
-            hT[k] = T;
-            hE[k] = te_E<FAST>(T);
+        for (int m = p0 + threadIdx.x; m < p1; m += blockDim.x) {   // A(h/2), B(h/2)
+            double T = te_T<FAST>(hE[m] + hh * mySrc[m - p0]);
+            T = te_rk4<FAST>(T, myG[m - p0], hh);
+            hT[m] = T;
+            hE[m] = te_E<FAST>(T);
         }
         cl.sync();
         if (rank == 0) {   // C(h) on the hub
             double acc = 0.0;
-            for (int k = threadIdx.x; k < n; k += blockDim.x) acc += hsm[n + k];
+            for (int m = threadIdx.x; m < n; m += blockDim.x) acc += hsm[n + m];
             double t = block_sum(acc, sh);
             __shared__ double tot;
             if (threadIdx.x == 0) tot = t;
             __syncthreads();
-            double start = tot;
-            const int G = D.te_ngroups;
-            if constexpr (FAST) {
-                // the fitted form keeps the energy each update converts, the
-                // value Te_to_Ee(Te) returns up to rounding, so no thread
-                // evaluates Te_to_Ee during the sweep
-                for (int p = 0; p < 2 * G; ++p) {
-                    const int g = p < G ? p : 2 * G - 1 - p;
-                    const int b = D.te_gstart[g], e = D.te_gstart[g + 1];
-                    for (int m = b + threadIdx.x; m < e; m += blockDim.x) {
-                        int k = sGc[m];
-                        const unsigned short* q = sNb + 6 * k;
-                        const double* sT = hsm;
-                        double T = sT[k];
-                        double x = hsm[n + k] + te_lap<FAST>(gm, T, sT[q[0]], sT[q[1]], sT[q[2]],
-                                                             sT[q[3]], sT[q[4]], sT[q[5]]);
-                        hsm[k] = te_T<FAST>(x);
-                        hsm[n + k] = x;
-                    }
-                    __syncthreads();
-                }
-            } else {
-                const int half = blockDim.x / 2;
-                const bool worker = threadIdx.x < half;
-                const int lane = worker ? threadIdx.x : threadIdx.x - half;
-                int pb = 0, pe = 0;   // cells of the previous phase whose Te_to_Ee is due
-                for (int p = 0; p < 2 * G; ++p) {
-                    const int g = p < G ? p : 2 * G - 1 - p;
-                    const int b = D.te_gstart[g], e = D.te_gstart[g + 1];
-                    if (worker) {
-                        for (int m = b + lane; m < e; m += half) {
-                            int k = sGc[m];
-                            const unsigned short* q = sNb + 6 * k;
-                            const double* sT = hsm;
-                            double T = sT[k];
-                            T = te_T<FAST>(hsm[n + k] + te_lap<FAST>(gm, T, sT[q[0]], sT[q[1]],
-                                                                     sT[q[2]], sT[q[3]], sT[q[4]],
-                                                                     sT[q[5]]));
-                            hsm[k] = T;
-                            if (p == G - 1) hsm[n + k] = te_E<FAST>(T);
-                        }
-                    } else {
-                        for (int m = pb + lane; m < pe; m += half) {
-                            int k = sGc[m];
-                            hsm[n + k] = te_E<FAST>(hsm[k]);
-                        }
-                    }
-                    __syncthreads();
-                    pb = p == G - 1 ? 0 : b;
-                    pe = p == G - 1 ? 0 : e;
-                }
-                for (int m = pb + threadIdx.x; m < pe; m += blockDim.x) {
-                    int k = sGc[m];
-                    hsm[n + k] = te_E<FAST>(hsm[k]);
-                }
-            }
+            const double start = tot;
+            hub_sweep<FAST, LEV>(D, hsm, n, sTk, sNb, gm);
             __syncthreads();
             acc = 0.0;
-            for (int k = threadIdx.x; k < n; k += blockDim.x) acc += hsm[n + k];
+            for (int m = threadIdx.x; m < n; m += blockDim.x) acc += hsm[n + m];
             t = block_sum(acc, sh);
             if (threadIdx.x == 0) hsm[2 * n] = start / t;
         }
         cl.sync();
         double fac = *hfac;
         int q = 0;
-        for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x, ++q) {   // rescale, B, A
-            double T = te_T<FAST>(hE[k] * fac);
-            T = te_rk4<FAST>(T, myG[k - k0], hh);
-            double Ee = te_E<FAST>(T) + hh * mySrc[k - k0];
+        for (int m = p0 + threadIdx.x; m < p1; m += blockDim.x, ++q) {   // rescale, B, A
+            double T = te_T<FAST>(hE[m] * fac);
+            T = te_rk4<FAST>(T, myG[m - p0], hh);
+            double Ee = te_E<FAST>(T) + hh * mySrc[m - p0];
             T = te_T<FAST>(Ee);
-            hT[k] = T;
-            hE[k] = te_E<FAST>(T);
+            hT[m] = T;
+            hE[m] = te_E<FAST>(T);
             if (q < 4) lastE[q] = Ee;
         }
     }
     int q = 0;
-    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x, ++q) {
-        D.Te[k] = hT[k];
+    for (int m = p0 + threadIdx.x; m < p1; m += blockDim.x, ++q) {
+        const int k = D.te_gcells[m];
+        D.Te[k] = hT[m];
         if (q < 4) D.Ee[k] = lastE[q];
     }
     cl.sync();   // keep the hub's shared memory alive until every CTA is done
@@ -401,15 +489,17 @@ __global__ void __launch_bounds__(1024) k_dte_hub(Dev D, double dt, int per) {
 
 static bool g_dte_inited = false;
 static int g_dte_cluster = 0;   // cluster size of k_dte_cluster, 0: clusters unavailable
-static int g_dte_mode = 2;      // 2: hub when the mesh fits; 1: cluster; 0: one CTA
+static int g_dte_mode = 3;      // 3: hub by levels when the mesh fits, 2: hub by colour
+                                // phases; 1: cluster; 0: one CTA
 static bool g_hub_ok = false;
 
 // dynamic shared memory of k_dte_hub for n Te cells: the hub's Te, f(Te) and
-// factor, and each CTA's own source and rate
+// factor, each CTA's own source and rate, the hub's neighbour records and
+// level tasks
 static size_t hub_smem(int n) {
     const int per = (n + HUB_CL - 1) / HUB_CL;
-    return sizeof(double) * (2 * (size_t)n + 2 + 2 * (size_t)per) + sizeof(int) * (size_t)n +
-           sizeof(unsigned short) * 6 * (size_t)n;
+    return sizeof(double) * (2 * (size_t)n + 2 + 2 * (size_t)per) + sizeof(uint4) * (size_t)n +
+           sizeof(unsigned short) * 2 * (size_t)n;
 }
 
 static cudaLaunchConfig_t cluster_cfg(int cs, int threads, size_t smem, cudaStream_t st,
@@ -430,27 +520,36 @@ static cudaLaunchConfig_t cluster_cfg(int cs, int threads, size_t smem, cudaStre
 
 template <bool FAST>
 static void dte_attributes() {
-    cudaFuncSetAttribute(k_dte_hub<FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_dte_hub<FAST, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)hub_smem(kHubMaxCells));
+    cudaFuncSetAttribute(k_dte_hub<FAST, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)hub_smem(kHubMaxCells));
     cudaFuncSetAttribute(k_dte_cluster<FAST>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
 }
 
 int dte_init(int device) {
     (void)device;
+    // the kernel choice is read at every context creation (tests switch it)
+    const char* m = getenv("SLD_DTE_MODE");
+    g_dte_mode = m && m[0] >= '0' && m[0] <= '3' ? m[0] - '0' : 3;
     if (g_dte_inited) return g_dte_cluster;
     g_dte_inited = true;
     dte_attributes<false>();
     dte_attributes<true>();
-    const char* m = getenv("SLD_DTE_MODE");
-    if (m && m[0] >= '0' && m[0] <= '2') g_dte_mode = m[0] - '0';
     cudaLaunchAttribute at[1];
     {
         cudaLaunchConfig_t cfg = cluster_cfg(HUB_CL, 1024, hub_smem(kHubMaxCells), nullptr, at);
         int nclu = 0, nclu2 = 0;
-        g_hub_ok = cudaOccupancyMaxActiveClusters(&nclu, k_dte_hub<false>, &cfg) == cudaSuccess &&
-                   nclu > 0 &&
-                   cudaOccupancyMaxActiveClusters(&nclu2, k_dte_hub<true>, &cfg) == cudaSuccess &&
-                   nclu2 > 0;
+        int nclu3 = 0, nclu4 = 0;
+        g_hub_ok =
+            cudaOccupancyMaxActiveClusters(&nclu, k_dte_hub<false, false>, &cfg) == cudaSuccess &&
+            nclu > 0 &&
+            cudaOccupancyMaxActiveClusters(&nclu2, k_dte_hub<true, false>, &cfg) == cudaSuccess &&
+            nclu2 > 0 &&
+            cudaOccupancyMaxActiveClusters(&nclu3, k_dte_hub<false, true>, &cfg) == cudaSuccess &&
+            nclu3 > 0 &&
+            cudaOccupancyMaxActiveClusters(&nclu4, k_dte_hub<true, true>, &cfg) == cudaSuccess &&
+            nclu4 > 0;
         cudaGetLastError();
     }
     for (int cs : {16, 8, 4}) {
@@ -474,9 +573,13 @@ static void launch_dte_form(const Dev& D, cudaStream_t st, double dt) {
     // a hub thread keeps the energies of at most four of its CTA's cells
     int threads = D.tune.dte_threads > 0 ? D.tune.dte_threads : 1024;
     if (hub_per > 4 * threads) threads = 1024;
-    if (mode == 2 && g_hub_ok && D.nte <= kHubMaxCells && hub_per <= 4 * 1024) {
+    if (mode >= 2 && g_hub_ok && D.nte <= kHubMaxCells && D.te_nlevels > 0 &&
+        hub_per <= 4 * 1024) {
         cudaLaunchConfig_t cfg = cluster_cfg(HUB_CL, threads, hub_smem(D.nte), st, at);
-        cudaLaunchKernelEx(&cfg, k_dte_hub<FAST>, D, dt, hub_per);
+        if (mode == 3)
+            cudaLaunchKernelEx(&cfg, k_dte_hub<FAST, true>, D, dt, hub_per);
+        else
+            cudaLaunchKernelEx(&cfg, k_dte_hub<FAST, false>, D, dt, hub_per);
         return;
     }
     if (mode >= 1 && g_dte_cluster > 0) {

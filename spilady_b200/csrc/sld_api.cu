@@ -535,8 +535,19 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     ok = ok && c->alloc(&c->d_gcells, (size_t)G.ncells) == 0;
     ok = ok && c->alloc(&c->d_te_gcells, (size_t)nte) == 0 &&
          c->alloc(&c->d_te_gstart, G.te_gstart.size()) == 0 &&
-         c->alloc(&c->d_te_color, (size_t)nte) == 0;
+         c->alloc(&c->d_te_color, (size_t)nte) == 0 &&
+         c->alloc(&c->d_te_ltasks, G.te_ltasks.size()) == 0 &&
+         c->alloc(&c->d_te_lstart, G.te_lstart.size()) == 0 &&
+         c->alloc(&c->d_te_lnb, G.te_lnb.size() / 8) == 0;
     if (!ok) { sld_destroy(c); return SLD_ERR_NOMEM; }
+    if (G.te_nlevels > 0) {
+        cudaMemcpy(c->d_te_lnb, G.te_lnb.data(), sizeof(unsigned short) * G.te_lnb.size(),
+                   cudaMemcpyHostToDevice);
+        cudaMemcpy(c->d_te_ltasks, G.te_ltasks.data(), sizeof(unsigned short) * G.te_ltasks.size(),
+                   cudaMemcpyHostToDevice);
+        cudaMemcpy(c->d_te_lstart, G.te_lstart.data(), sizeof(int) * G.te_lstart.size(),
+                   cudaMemcpyHostToDevice);
+    }
     cudaMemcpy(c->d_gcells, G.gcells.data(), sizeof(int) * G.ncells, cudaMemcpyHostToDevice);
     cudaMemcpy(c->d_te_gcells, G.te_gcells.data(), sizeof(int) * nte, cudaMemcpyHostToDevice);
     cudaMemcpy(c->d_te_gstart, G.te_gstart.data(), sizeof(int) * G.te_gstart.size(),
@@ -577,6 +588,10 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     D.te_gcells = c->d_te_gcells;
     D.te_gstart = c->d_te_gstart;
     D.te_ngroups = G.te_ngroups;
+    D.te_ltasks = c->d_te_ltasks;
+    D.te_lstart = c->d_te_lstart;
+    D.te_lnb = c->d_te_lnb;
+    D.te_nlevels = G.te_nlevels;
 
     // Te per Te cell (map_cells.cpp:128-158), stored in eV as the reference does
     std::vector<double> te(nte);
@@ -1546,7 +1561,7 @@ int sld_autotune(sld_ctx* c, int steps, int* out6) {
                               {&T.pair_block, {64, 96, 128}},
                               {&T.force_block, {64, 96, 128}}};
     if (c->P.eltemp) {
-        axes.push_back({&T.dte_mode, {0, 1, 2}});
+        axes.push_back({&T.dte_mode, {0, 1, 2, 3}});
         axes.push_back({&T.dte_threads, {256, 512, 1024}});
         if (c->P.te_mesh > 0) axes.push_back({&T.temp_block, {64, 128}});
     }

@@ -60,7 +60,8 @@ struct Tune {
     int pair_block;    // atoms per block of the pair and list pass
     int force_block;   // atoms per block of the force passes
     int temp_block;    // atoms per block of the cell-temperature pass on a Te mesh
-    int dte_mode;      // core_dTe kernel: 0 one CTA, 1 cluster, 2 hub; -1 default
+    int dte_mode;      // core_dTe kernel: 0 one CTA, 1 cluster, 2 hub by colour
+                       // phases, 3 hub by levels; -1 default
     int dte_threads;   // threads per CTA of the hub core_dTe kernel
 };
 
@@ -120,6 +121,15 @@ struct Dev {
     const int *te_gcells, *te_gstart;
     const unsigned char* te_color;   // colour group of each Te cell
     int te_ngroups;
+    // the diffusion sweep as levels of independent tasks, the cells named by
+    // their position in te_gcells (position | 0x8000 for two updates in a
+    // row), te_lstart[l]..te_lstart[l+1] for level l; te_lnb: per position,
+    // the positions of the six face neighbours (+x -x +y -y +z -z, then two
+    // zeros); 0 levels when the mesh is too large for them
+    const unsigned short* te_ltasks;
+    const int* te_lstart;
+    const uint4* te_lnb;
+    int te_nlevels;
     // per-step neighbour lists (built after every drift by k_pairs):
     //   nbr  [SLD_MAXNB][natom]  j | (1<<30 when the pair crosses the box)
     //        for r_ij < rcut_max, in the reference's traversal order; entry

@@ -20,6 +20,9 @@ struct sld_ctx {
     int* d_te_gcells = nullptr;
     int* d_te_gstart = nullptr;
     unsigned char* d_te_color = nullptr;
+    unsigned short* d_te_ltasks = nullptr;
+    uint4* d_te_lnb = nullptr;
+    int* d_te_lstart = nullptr;
     double* d_avg = nullptr;
     double* d_chk = nullptr;           // check() sums: per-block partials, then totals
     double4* hext_buf = nullptr;       // external field / force per atom, slot order;

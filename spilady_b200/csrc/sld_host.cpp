@@ -59,6 +59,64 @@ int colour_grid(int nx, int ny, int nz, std::vector<int>& gstart, std::vector<in
     return (int)gstart.size() - 1;
 }
 
+int te_levels(int nx, int ny, int nz, const std::vector<int>& gstart,
+              const std::vector<int>& gcells, std::vector<int>& lstart,
+              std::vector<unsigned short>& tasks, std::vector<unsigned short>& nbp) {
+    lstart.clear();
+    tasks.clear();
+    nbp.clear();
+    const int nc = nx * ny * nz;
+    if (nc >= 0x8000) return 0;
+    const int G = (int)gstart.size() - 1;
+    std::vector<int> pos(nc);
+    for (int m = 0; m < nc; ++m) pos[gcells[m]] = m;
+    auto nb6 = [&](int c, int* nb) {
+        const int x = c % nx, y = (c / nx) % ny, z = c / (nx * ny);
+        nb[0] = (x + 1) % nx + (y + z * ny) * nx;
+        nb[1] = (x + nx - 1) % nx + (y + z * ny) * nx;
+        nb[2] = x + ((y + 1) % ny + z * ny) * nx;
+        nb[3] = x + ((y + ny - 1) % ny + z * ny) * nx;
+        nb[4] = x + (y + ((z + 1) % nz) * ny) * nx;
+        nb[5] = x + (y + ((z + nz - 1) % nz) * ny) * nx;
+    };
+    nbp.assign(8 * (size_t)nc, 0);
+    for (int m = 0; m < nc; ++m) {
+        int nb[6];
+        nb6(gcells[m], nb);
+        for (int j = 0; j < 6; ++j) nbp[8 * (size_t)m + j] = (unsigned short)pos[nb[j]];
+    }
+    std::vector<int> last(nc, 0);      // level of the cell's latest update (0: none yet)
+    std::vector<int> at(nc, -1);       // that update's index in its level's list
+    std::vector<std::vector<unsigned short>> lv;
+    for (int pass = 0; pass < 2; ++pass)
+        for (int gg = 0; gg < G; ++gg) {
+            const int g = pass == 0 ? gg : G - 1 - gg;
+            for (int m = gstart[g]; m < gstart[g + 1]; ++m) {
+                const int c = gcells[m];
+                int nb[6];
+                nb6(c, nb);
+                int l = last[c];
+                for (int j : nb)
+                    if (j != c) l = std::max(l, last[j]);
+                if (last[c] > 0 && l == last[c]) {   // nothing read changed since: same task
+                    lv[l - 1][at[c]] |= 0x8000;
+                    continue;
+                }
+                ++l;
+                if ((int)lv.size() < l) lv.resize(l);
+                at[c] = (int)lv[l - 1].size();
+                lv[l - 1].push_back((unsigned short)m);
+                last[c] = l;
+            }
+        }
+    lstart.push_back(0);
+    for (const auto& v : lv) {
+        tasks.insert(tasks.end(), v.begin(), v.end());
+        lstart.push_back((int)tasks.size());
+    }
+    return (int)lv.size();
+}
+
 void box_derived(HostGeom& G) {
     const double* d = G.d;
     // vec_utils_CPU.cpp:135-148
@@ -108,6 +166,8 @@ int setup_geometry(const sld_params& P, int natom, const std::vector<double>& r,
         G.te_gstart = G.gstart;
         G.te_gcells = G.gcells;
     }
+    G.te_nlevels = te_levels(G.tx, G.ty, G.tz, G.te_gstart, G.te_gcells, G.te_lstart, G.te_ltasks,
+                             G.te_lnb);
     // initial_links_CPU (links_CPU.cpp:33-83): wrap, bin; each cell's list
     // holds its atoms in descending index order
     std::vector<int> cell(natom);

@@ -276,10 +276,11 @@ def test_sweep_schedules_give_identical_bits(monkeypatch, precision):
 
 
 # ------------------------------------------------------ core_dTe kernels
-@pytest.mark.parametrize("mode", [2, 1, 0])
+@pytest.mark.parametrize("mode", [3, 2, 1, 0])
 @pytest.mark.parametrize("precision", [0, 2])
 def test_core_dte_kernels_and_forms(monkeypatch, mode, precision):
-    # hub (2), cluster (1) and one-CTA (0) kernels, with the reference's
+    # hub by levels (3) and by colour phases (2), cluster (1) and one-CTA (0)
+    # kernels, with the reference's
     # heat-capacity expressions (FP64 form) and with the fitted ones (the
     # split form's, here in its FP64 twin): one core_dTe and one full step
     monkeypatch.setenv("SLD_DTE_MODE", str(mode))
@@ -297,3 +298,29 @@ def test_core_dte_kernels_and_forms(monkeypatch, mode, precision):
         o.run(1)
         e.run(1)
         compare(o, e, ATOM + ["Te", "Tl"], 1e-10, f"step, dTe mode {mode}")
+
+
+@pytest.mark.parametrize("cells", [10, 8])
+@pytest.mark.parametrize("precision", [0, 2])
+def test_core_dte_levels_give_the_phase_bits(monkeypatch, cells, precision):
+    # the hub's sweep by levels against the same hub by colour phases: every
+    # update reads the values of the sequential sweep, so the bits agree.  Te
+    # on the link cells (6^3 at 10^3 unit cells: 8 colours, 7 levels; 5^3 at
+    # 8^3: 20 colours, irregular levels and double tasks inside the sweep),
+    # whose lattice and spin temperatures are fixed-order sums (a Te mesh
+    # sums them with atomics, whose order is not fixed)
+    from spilady_b200.lattice import hot_spot_te
+    sw = dict(spinlang=True, lattlang=True, eltemp=True, localcolmot=True, renormalize=True)
+    params, r, p, s = initial_state(cells, seed=16, tilt=0.35)
+    mesh = {10: 6, 8: 5}[cells]
+    te = hot_spot_te(mesh, params["box"][0], peak=3000.0, background=300.0, sigma=6.0)
+    out = {}
+    for mode in (2, 3):
+        monkeypatch.setenv("SLD_DTE_MODE", str(mode))
+        e = engine_mod().Engine(params, r, p, s, te=te, precision=precision, **sw)
+        assert e.ncells == mesh ** 3
+        e.core_dTe(5e-16)
+        out[mode] = {n: e.get(n) for n in ("Te", "Ee")}
+        e.close()
+    for n in ("Te", "Ee"):
+        assert np.array_equal(out[2][n], out[3][n]), n
