@@ -312,15 +312,17 @@ int sld_quantum_filter(sld_ctx* ctx, double* out, int n);
 /* Autotuner of the launch shapes (no reference counterpart): times `steps`
    captured steps twice for each candidate and keeps one that is faster by
    more than 1% than the best so far, by coordinate
-   descent over the cells per block of the spin sweeps, the atoms per block
-   of the pair/list and force passes, and, with eltemp, the core_dTe kernel
-   (one CTA, a cluster, or the hub cluster), the hub's threads per CTA and
-   the Te-mesh temperature pass.  The state is copied first and put back, so
-   the context continues exactly as if it had not run.  out6 (may be NULL):
-   the chosen sweep, pair, force and temperature block sizes (0: default),
-   core_dTe kernel (-1: default) and hub threads (0: default).  Not with
-   sld_scale's switches (their steps are not captured). */
-int sld_autotune(sld_ctx* ctx, int steps, int* out6);
+   descent over the cells per block of the spin sweeps and their CTAs per
+   SM, the atoms per block of the pair/list and force passes, and, with
+   eltemp, the core_dTe kernel (one CTA, a cluster, or the hub cluster by
+   colour phases or by levels), the hub's threads per CTA and the Te-mesh
+   temperature pass.  The state is copied first and put back, so the context
+   continues exactly as if it had not run.  out8 (may be NULL): the chosen
+   sweep, pair, force and temperature block sizes (0: default), core_dTe
+   kernel (-1: default), hub threads (0: default), sweep CTAs per SM (0: no
+   cap) and 0.  Not with sld_scale's switches (their steps are not
+   captured). */
+int sld_autotune(sld_ctx* ctx, int steps, int* out8);
 
 /* out[0..5] = natom, ncells, ngroups, n_te_cells, nx, ny (link cells). */
 int sld_info(sld_ctx* ctx, int* out6);

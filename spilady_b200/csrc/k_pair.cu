@@ -14,6 +14,7 @@
 // image is applied with the reference's arithmetic (find_image) and only to
 // pairs whose cells are neighbours across the periodic boundary; for all
 // other pairs the reference's find_image leaves the vector unchanged.
+#include <algorithm>
 #include <cstdlib>
 
 #include "sld_pot32.cuh"
@@ -184,8 +185,9 @@ __device__ void pairs_one(const Dev& D, int i, int write_rho) {
 
 template <int MODE>
 __global__ void __launch_bounds__(128) k_pairs(Dev D, int write_rho) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < D.natom) pairs_one<MODE>(D, i, write_rho);
+    // one atom per thread; a capped grid walks several atoms per thread
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x)
+        pairs_one<MODE>(D, i, write_rho);
 }
 
 // F'(rho) per atom (the force pass needs it for both atoms of every pair)
@@ -263,9 +265,7 @@ __device__ __forceinline__ void force_finish(const Dev& D, int i, double si_sq, 
 
 // FP64 force pass; AN: the analytic forms instead of the tables
 template <bool AN, int PART>
-__global__ void __launch_bounds__(128) k_force64(Dev D) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= D.natom) return;
+__device__ __forceinline__ void force64_one(const Dev& D, int i) {
     unsigned* err = &D.ctl->err;
     const int N = D.natom;
     double4 ri = D.r[i];
@@ -355,10 +355,14 @@ __global__ void __launch_bounds__(128) k_force64(Dev D) {
 }
 
 // split form: FP32 pair terms from the analytic potential, Kahan sums
+template <bool AN, int PART>
+__global__ void __launch_bounds__(128) k_force64(Dev D) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x)
+        force64_one<AN, PART>(D, i);
+}
+
 template <int PART>
-__global__ void __launch_bounds__(128) k_force32(Dev D) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= D.natom) return;
+__device__ __forceinline__ void force32_one(const Dev& D, int i) {
     const int N = D.natom;
     double4 ri = D.r[i];
     double4 si = (PART & PART_MAG) ? D.s[i] : make_double4(0, 0, 0, 0);
@@ -416,9 +420,32 @@ __global__ void __launch_bounds__(128) k_force32(Dev D) {
 }
 
 template <int PART>
+__global__ void __launch_bounds__(128) k_force32(Dev D) {
+    // one atom per thread; a capped grid walks several atoms per thread
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x)
+        force32_one<PART>(D, i);
+}
+
+// a cap on the CTAs per SM (0: none) for the kernels of the step graph's side
+// branch, which run beside the spin sweeps: a capped grid leaves room for the
+// sweep's next launch instead of filling every free slot
+static int capped_grid(int nb, int cap) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            sms <= 0)
+            sms = 148;
+    }
+    return cap > 0 ? std::min(nb, cap * sms) : nb;
+}
+
+template <int PART>
 static void launch_force_part(const Dev& D, cudaStream_t st) {
     const int bs = D.tune.force_block > 0 ? D.tune.force_block : 128;
     int nb = div_up(D.natom, bs);
+    if (PART == PART_EAM) nb = capped_grid(nb, D.tune.force_cap);
     if (D.split) k_force32<PART><<<nb, bs, 0, st>>>(D);
     else if (D.analytic) k_force64<true, PART><<<nb, bs, 0, st>>>(D);
     else k_force64<false, PART><<<nb, bs, 0, st>>>(D);
@@ -427,7 +454,7 @@ static void launch_force_part(const Dev& D, cudaStream_t st) {
 void launch_pairs(const Dev& D, cudaStream_t st, bool write_rho) {
     int w = write_rho ? 1 : 0;
     const int bs = D.tune.pair_block > 0 ? D.tune.pair_block : 128;
-    int nb = div_up(D.natom, bs);
+    int nb = capped_grid(div_up(D.natom, bs), D.tune.pair_cap);
     if (D.split) k_pairs<1><<<nb, bs, 0, st>>>(D, w);
     else if (D.analytic) k_pairs<2><<<nb, bs, 0, st>>>(D, w);
     else k_pairs<0><<<nb, bs, 0, st>>>(D, w);

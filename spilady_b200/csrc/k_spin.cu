@@ -19,6 +19,7 @@
 // A block whose cells hold more atoms (or in-cell neighbours) than its
 // shared-memory tables falls back to one thread per cell reading everything
 // from global memory, with the same arithmetic.
+#include <algorithm>
 #include <cstdlib>
 #include <type_traits>
 
@@ -482,9 +483,9 @@ __device__ __forceinline__ void cell_walk(const Dev& D, int c, double dt, int ba
 template <bool SPLIT, int INTEG>
 __global__ void __launch_bounds__(128) k_sweep_pipe(Dev D, const int* __restrict__ gcells,
                                                     int ncell_g, double dt, int backward) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ncell_g) return;
-    cell_walk<SPLIT, false, INTEG>(D, gcells[t], dt, backward);
+    // one cell per thread; a capped grid walks several cells per thread
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ncell_g; t += gridDim.x * blockDim.x)
+        cell_walk<SPLIT, false, INTEG>(D, gcells[t], dt, backward);
 }
 
 // ---------------------------------------------------------------------
@@ -615,6 +616,7 @@ void launch_sweep_flow(const Dev& D, cudaStream_t st, const SweepFlow& F, double
 }
 
 static size_t sweep_smem() { return sizeof(SweepShared); }
+static int g_sms = 148;        // SMs of the device (capped sweep grids)
 static int g_sweep_mode = 2;   // 0: two-level (shared memory), 1: one thread per cell,
                                // 2: one thread per cell, pipelined; one launch per group
                                // 3: the pipelined walk, scheduled by data flow
@@ -626,6 +628,7 @@ void sweep_init() {
     int dev = 0, sms = 0, b0 = 0, b1 = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms > 0) g_sms = sms;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_sweep_flow<false>, 128, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_sweep_flow<true>, 128, 0);
     g_flow_blocks[0] = (b0 > 0 ? b0 : 1) * sms;
@@ -647,7 +650,11 @@ void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g,
         // Hamiltonians' visit has its own instance (the other sweep variants
         // have only the Heisenberg-Landau visit).
         const int bs = D.tune.sweep_block > 0 ? D.tune.sweep_block : (D.split ? 96 : 128);
-        const int nb = div_up(ncell_g, bs);
+        int nb = div_up(ncell_g, bs);
+        // a cap on the CTAs per SM leaves registers for the kernels of the
+        // graph's other branch (the pair pass, the EAM forces, core_dTe),
+        // which then run beside the sweep instead of after it
+        if (D.tune.sweep_cap > 0) nb = std::min(nb, D.tune.sweep_cap * g_sms);
         if (D.split) {
             if (D.hint)
                 k_sweep_pipe<true, 1><<<nb, bs, 0, st>>>(D, gcells, ncell_g, dt, b);

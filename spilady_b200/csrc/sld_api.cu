@@ -437,7 +437,27 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     D.landau_on = (D.ham == SLD_HAM_SLDHL || D.ham == SLD_HAM_SDHL) ? 1 : 0;
     D.hc = D.ham == SLD_HAM_SLDHL ? 1 : 0;
     D.hint = (D.ham == SLD_HAM_SDH || D.ham == SLD_HAM_SLDH) ? 1 : 0;
-    D.tune = Tune{0, 0, 0, 0, -1, 0};
+    D.tune = Tune{0, 0, 0, 0, -1, 0, 0, 0, 0, 1};
+    {
+        // starting launch shapes: caps on the CTAs per SM of the sweeps and
+        // of the side branch's pair and EAM passes, the hub core_dTe kernel's
+        // threads (tests compare shapes; the autotuner chooses its own)
+        auto cap = [](const char* name) {
+            const char* v = getenv(name);
+            const int k = v ? atoi(v) : 0;
+            return k > 0 && k <= 32 ? k : 0;
+        };
+        D.tune.sweep_cap = cap("SLD_SWEEP_CAP");
+        D.tune.pair_cap = cap("SLD_PAIR_CAP");
+        D.tune.force_cap = cap("SLD_FORCE_CAP");
+        const char* gp = getenv("SLD_GRAPH_PRIO");
+        if (gp && gp[0] == '0') D.tune.graph_prio = 0;
+        const char* t = getenv("SLD_DTE_THREADS");
+        if (t) {
+            const int k = atoi(t);
+            if (k == 256 || k == 512 || k == 1024) D.tune.dte_threads = k;
+        }
+    }
     D.quantum = prm->quantum_noise ? 1 : 0;
     D.qM = prm->msteps_quantum;
     D.step = prm->step;
@@ -754,7 +774,10 @@ int sld_run(sld_ctx* c, int nsteps) {
         CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
         enqueue_step(c);
         CK(cudaStreamEndCapture(c->st, &g));
-        CK(cudaGraphInstantiate(&c->step_graphs[k], g, 0));
+        // with node priorities the sweeps' branch (the high-priority stream)
+        // gets its CTAs dispatched before the side branch's waiting ones
+        CK(cudaGraphInstantiate(&c->step_graphs[k], g,
+                                c->D.tune.graph_prio ? cudaGraphInstantiateFlagUseNodePriority : 0));
         cudaGraphDestroy(g);
         use_set(c, saved);
     }
@@ -809,7 +832,11 @@ static int batch_capture(sld_batch* b, int k) {
         }
         if (cudaStreamEndCapture(b->st, &g) != cudaSuccess) rc = SLD_ERR_CUDA;
     }
-    if (rc == SLD_OK && cudaGraphInstantiate(&b->graphs[k], g, 0) != cudaSuccess) rc = SLD_ERR_CUDA;
+    if (rc == SLD_OK &&
+        cudaGraphInstantiate(&b->graphs[k], g,
+                             b->ctx[0]->D.tune.graph_prio ? cudaGraphInstantiateFlagUseNodePriority
+                                                          : 0) != cudaSuccess)
+        rc = SLD_ERR_CUDA;
     if (g) cudaGraphDestroy(g);
     for (size_t q = 0; q < b->ctx.size(); ++q) use_set(b->ctx[q], saved[q]);
     return rc;
@@ -1546,7 +1573,7 @@ static int trial(sld_ctx* c, const StateCopy& s, int steps, double* ms) {
     return SLD_OK;
 }
 
-int sld_autotune(sld_ctx* c, int steps, int* out6) {
+int sld_autotune(sld_ctx* c, int steps, int* out8) {
     if (!c || steps < 1) return SLD_ERR_ARG;
     if (dynamic_step(c)) return SLD_ERR_ARG;   // no captured step to time
     StateCopy s;
@@ -1558,6 +1585,7 @@ int sld_autotune(sld_ctx* c, int steps, int* out6) {
     // coordinate descent over the shapes, each from the current best
     struct Axis { int* field; std::vector<int> values; };
     std::vector<Axis> axes = {{&T.sweep_block, {64, 96, 128}},
+                              {&T.sweep_cap, {0, 2, 3}},
                               {&T.pair_block, {64, 96, 128}},
                               {&T.force_block, {64, 96, 128}}};
     if (c->P.eltemp) {
@@ -1584,9 +1612,10 @@ int sld_autotune(sld_ctx* c, int steps, int* out6) {
     state_free(s);
     if (rc) return rc;
     if (rc2) return rc2;
-    if (out6) {
-        out6[0] = T.sweep_block; out6[1] = T.pair_block; out6[2] = T.force_block;
-        out6[3] = T.temp_block; out6[4] = T.dte_mode; out6[5] = T.dte_threads;
+    if (out8) {
+        out8[0] = T.sweep_block; out8[1] = T.pair_block; out8[2] = T.force_block;
+        out8[3] = T.temp_block; out8[4] = T.dte_mode; out8[5] = T.dte_threads;
+        out8[6] = T.sweep_cap; out8[7] = 0;
     }
     return SLD_OK;
 }

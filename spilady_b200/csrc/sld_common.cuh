@@ -63,6 +63,12 @@ struct Tune {
     int dte_mode;      // core_dTe kernel: 0 one CTA, 1 cluster, 2 hub by colour
                        // phases, 3 hub by levels; -1 default
     int dte_threads;   // threads per CTA of the hub core_dTe kernel
+    int sweep_cap;     // CTAs per SM of a spin-sweep launch (0: one thread per cell),
+                       // leaving room for the other graph branch's kernels
+    int pair_cap;      // CTAs per SM of the pair/list pass (0: one thread per atom)
+    int force_cap;     // CTAs per SM of the EAM force pass (0: one thread per atom)
+    int graph_prio;    // 1: the step graph keeps its streams' priorities (the spin
+                       // sweeps' branch first), 0: every node at the launch priority
 };
 
 struct Dev {

@@ -320,10 +320,10 @@ class Engine:
     def autotune(self, steps=3):
         """Choose the launch shapes by timing captured steps; the state is
         left unchanged.  Returns the chosen shapes."""
-        out = (C.c_int * 6)()
+        out = (C.c_int * 8)()
         _check(self.L.sld_autotune(self.h, int(steps), out), "autotune")
         return dict(zip(("sweep_block", "pair_block", "force_block", "temp_block",
-                         "dte_mode", "dte_threads"), list(out)))
+                         "dte_mode", "dte_threads", "sweep_cap"), list(out)))
 
     def quantum_filter(self):
         out = np.zeros(100000)
@@ -422,10 +422,10 @@ class Batch:
     def autotune(self, steps=3):
         """Choose the launch shapes by timing captured steps; the state is
         left unchanged.  Returns the chosen shapes."""
-        out = (C.c_int * 6)()
+        out = (C.c_int * 8)()
         _check(self.L.sld_autotune(self.h, int(steps), out), "autotune")
         return dict(zip(("sweep_block", "pair_block", "force_block", "temp_block",
-                         "dte_mode", "dte_threads"), list(out)))
+                         "dte_mode", "dte_threads", "sweep_cap"), list(out)))
 
     def quantum_filter(self):
         out = np.zeros(100000)

@@ -67,3 +67,43 @@ def test_autotune_keeps_the_state_and_the_results():
     b.run(3)
     for n in ("r", "p", "s", "f"):
         assert np.array_equal(a.get(n), b.get(n)), n
+
+
+def test_capped_sweep_grid_gives_the_same_bits(monkeypatch):
+    # a cap on the sweep's CTAs per SM makes each thread walk several cells
+    # of its colour group; the cells of a group are independent, so the
+    # result is the same bit for bit.  96^3 unit cells: 66^3 link cells,
+    # colour groups of 35,937 cells, more than one CTA per SM's threads
+    from spilady_b200 import engine
+    from spilady_b200.lattice import initial_state
+    params, r, p, s = initial_state(96, seed=62, tilt=0.2)
+    out = {}
+    for cap in ("0", "1"):
+        monkeypatch.setenv("SLD_SWEEP_CAP", cap)
+        e = engine.Engine(params, r, p, s, spinlang=True, lattlang=True, precision=engine.SPLIT)
+        assert e.ngroups == 8
+        e.run(2)
+        out[cap] = {n: e.get(n) for n in ("s", "H", "p")}
+        e.close()
+    for n in ("s", "H", "p"):
+        assert np.array_equal(out["0"][n], out["1"][n]), n
+
+
+def test_capped_side_branch_grids_give_the_same_bits(monkeypatch):
+    # caps on the CTAs per SM of the sweeps, the pair pass and the EAM force
+    # pass (each thread then takes several cells or atoms) change no
+    # arithmetic: the step ends with the same bits
+    from spilady_b200 import engine
+    from spilady_b200.lattice import initial_state
+    params, r, p, s = initial_state(48, seed=63, tilt=0.2)
+    out = {}
+    for caps in (("0", "0", "0"), ("2", "1", "1")):
+        for name, v in zip(("SLD_SWEEP_CAP", "SLD_PAIR_CAP", "SLD_FORCE_CAP"), caps):
+            monkeypatch.setenv(name, v)
+        e = engine.Engine(params, r, p, s, spinlang=True, lattlang=True, precision=engine.SPLIT)
+        e.run(2)
+        out[caps] = {n: e.get(n) for n in ("s", "p", "r", "f", "rho")}
+        e.close()
+    a, b = out.values()
+    for n in a:
+        assert np.array_equal(a[n], b[n]), n
