@@ -168,15 +168,23 @@ __global__ void __launch_bounds__(KDP_BLOCK) k_dp_lang(Dev D, double dt, int epo
         const unsigned long long epoch = D.ctl->epoch + (unsigned long long)epoch_off;
         if (n > 0 && n <= KDP_MAXA) {
             const PShared P_{sp + threadIdx.x};
-            for (int m = 0; m < n; ++m) {
-                const double4 p = D.p[a[m]];
-                P_.set(m, make_double3(p.x, p.y, p.z));
-            }
+            // all of the cell's loads in flight at once: the indices, then the momenta
+            int idx[KDP_MAXA];
+#pragma unroll
+            for (int m = 0; m < KDP_MAXA; ++m) idx[m] = m < n ? __ldg(a + m) : 0;
+#pragma unroll
+            for (int m = 0; m < KDP_MAXA; ++m)
+                if (m < n) {
+                    const double4 p = D.p[idx[m]];
+                    P_.set(m, make_double3(p.x, p.y, p.z));
+                }
             ps = dp_cell(D, P_, a, n, dt, epoch);
-            for (int m = 0; m < n; ++m) {
-                const double3 p = P_.get(m);
-                D.p[a[m]] = make_double4(p.x, p.y, p.z, 0.0);
-            }
+#pragma unroll
+            for (int m = 0; m < KDP_MAXA; ++m)
+                if (m < n) {
+                    const double3 p = P_.get(m);
+                    D.p[idx[m]] = make_double4(p.x, p.y, p.z, 0.0);
+                }
         } else if (n > 0) {
             ps = dp_cell(D, PGlobal{D, a}, a, n, dt, epoch);
         }
