@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(256) k_dte_cluster(Dev D, double dt) {
 //   - Fitted expressions: an update keeps the energy it converts to Te (what
 //     Te_to_Ee would return, up to rounding), so the sweep evaluates no
 //     Te_to_Ee at all.
-static const int kHubMaxCells = 6000;   // 8 (2 n + 2 + 2 n / 8) + 16 n + 4 n bytes of shared memory
+static const int kHubMaxCells = 6000;   // 8 (2 n + 10 + 2 n / 8) + 16 n + 4 n bytes of shared memory
 
 // the positions of the six face neighbours of position m
 __device__ __forceinline__ void hub_nb(const uint4* sNb, int m, int (&q)[6]) {
@@ -413,7 +413,8 @@ __global__ void __launch_bounds__(1024) k_dte_hub(Dev D, double dt, int per) {
     double* hT = cl.map_shared_rank(hsm, 0);   // the hub's arrays, by position
     double* hE = hT + n;
     double* hfac = hT + 2 * n;
-    double* mySrc = hsm + 2 * n + 2;           // this CTA's own positions
+    double* hpart = hT + 2 * n + 2;            // each CTA's sum of Ee after A and B
+    double* mySrc = hsm + 2 * n + 2 + HUB_CL;  // this CTA's own positions
     double* myG = mySrc + per;
     uint4* sNb = reinterpret_cast<uint4*>(myG + per);                      // hub: neighbours
     unsigned short* sTk = reinterpret_cast<unsigned short*>(sNb + n);      // hub: level tasks
@@ -439,27 +440,29 @@ __global__ void __launch_bounds__(1024) k_dte_hub(Dev D, double dt, int per) {
     cl.sync();
     const DteGeom gm = dte_geom(D, h);
     double lastE[4];   // this thread's last A-step energies (per <= 4096 -> <= 4 per thread)
+    const int ncta = (int)cl.num_blocks();
     for (int it = 0; it < nloop; ++it) {
+        double part = 0.0;   // C's starting energy, summed per CTA
         for (int m = p0 + threadIdx.x; m < p1; m += blockDim.x) {   // A(h/2), B(h/2)
             double T = te_T<FAST>(hE[m] + hh * mySrc[m - p0]);
             T = te_rk4<FAST>(T, myG[m - p0], hh);
             hT[m] = T;
-            hE[m] = te_E<FAST>(T);
+            const double E = te_E<FAST>(T);
+            hE[m] = E;
+            part += E;
         }
+        part = block_sum(part, sh);
+        if (threadIdx.x == 0) hpart[rank] = part;
         cl.sync();
         if (rank == 0) {   // C(h) on the hub
-            double acc = 0.0;
-            for (int m = threadIdx.x; m < n; m += blockDim.x) acc += hsm[n + m];
-            double t = block_sum(acc, sh);
-            __shared__ double tot;
-            if (threadIdx.x == 0) tot = t;
-            __syncthreads();
-            const double start = tot;
+            double start = 0.0;   // valid in thread 0, the one that uses it
+            if (threadIdx.x == 0)
+                for (int r = 0; r < ncta; ++r) start += hsm[2 * n + 2 + r];
             hub_sweep<FAST, LEV>(D, hsm, n, sTk, sNb, gm);
             __syncthreads();
-            acc = 0.0;
+            double acc = 0.0;
             for (int m = threadIdx.x; m < n; m += blockDim.x) acc += hsm[n + m];
-            t = block_sum(acc, sh);
+            const double t = block_sum(acc, sh);
             if (threadIdx.x == 0) hsm[2 * n] = start / t;
         }
         cl.sync();
@@ -469,9 +472,15 @@ __global__ void __launch_bounds__(1024) k_dte_hub(Dev D, double dt, int per) {
             double T = te_T<FAST>(hE[m] * fac);
             T = te_rk4<FAST>(T, myG[m - p0], hh);
             double Ee = te_E<FAST>(T) + hh * mySrc[m - p0];
-            T = te_T<FAST>(Ee);
-            hT[m] = T;
-            hE[m] = te_E<FAST>(T);
+            if (FAST && it + 1 < nloop) {
+                // the fitted form keeps the energy: the next substep's A
+                // continues from it without the round trip through Te
+                hE[m] = Ee;
+            } else {
+                T = te_T<FAST>(Ee);
+                hT[m] = T;
+                hE[m] = te_E<FAST>(T);
+            }
             if (q < 4) lastE[q] = Ee;
         }
     }
@@ -493,12 +502,12 @@ static int g_dte_mode = 3;      // 3: hub by levels when the mesh fits, 2: hub b
                                 // phases; 1: cluster; 0: one CTA
 static bool g_hub_ok = false;
 
-// dynamic shared memory of k_dte_hub for n Te cells: the hub's Te, f(Te) and
-// factor, each CTA's own source and rate, the hub's neighbour records and
-// level tasks
+// dynamic shared memory of k_dte_hub for n Te cells: the hub's Te, f(Te),
+// factor and the CTAs' partial sums, each CTA's own source and rate, the
+// hub's neighbour records and level tasks
 static size_t hub_smem(int n) {
     const int per = (n + HUB_CL - 1) / HUB_CL;
-    return sizeof(double) * (2 * (size_t)n + 2 + 2 * (size_t)per) + sizeof(uint4) * (size_t)n +
+    return sizeof(double) * (2 * (size_t)n + 2 + HUB_CL + 2 * (size_t)per) + sizeof(uint4) * (size_t)n +
            sizeof(unsigned short) * 2 * (size_t)n;
 }
 

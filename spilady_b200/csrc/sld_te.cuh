@@ -39,10 +39,16 @@ __device__ __forceinline__ double Ee_to_te_fast(double E) {
     return sqrt(y * te_poly_inv_logcosh(t)) * (1.0 / TE_B);
 }
 
-// exp(x) - 1: the Taylor series through x^8/8! for |x| < 2^-8 (truncation
-// below 2e-21 relative there), else expm1.  B's decay exponent is of order
-// 1e-5 for femtosecond substeps.
+// exp(x) - 1: the Taylor series through x^4/4! for |x| < 2^-14 (truncation
+// below 2e-19 relative there), through x^8/8! for |x| < 2^-8 (below 2e-21),
+// else expm1.  B's decay exponent is of order 1e-5 for femtosecond substeps.
 __device__ __forceinline__ double te_expm1(double x) {
+    if (fabs(x) < 6.103515625e-05) {
+        double p = 1.0 / 24.0;
+        p = fma(p, x, 1.0 / 6.0);
+        p = fma(p, x, 0.5);
+        return fma(x * x, p, x);
+    }
     if (fabs(x) < 0.00390625) {
         double p = 1.0 / 40320.0;
         p = fma(p, x, 1.0 / 5040.0);
