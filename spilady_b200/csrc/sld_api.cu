@@ -69,10 +69,12 @@ int launch_status() {
 // passes false where the same step overwrites them before anything reads
 // them (the first core_ds of a step; with eltemp, calculate_temperature
 // recomputes all three).
-void enqueue_ds(sld_ctx* c, const Dev& D, double dt, int& eoff, bool fields = true) {
+// noise_drawn: the caller launched this call's visit records already
+void enqueue_ds(sld_ctx* c, const Dev& D, double dt, int& eoff, bool fields = true,
+                bool noise_drawn = false) {
     const auto& G = c->G;
     double dt_half = dt / 2e0;
-    if (c->P.spinlang) launch_spin_noise(D, c->st, eoff, dt_half);
+    if (c->P.spinlang && !noise_drawn) launch_spin_noise(D, c->st, eoff, dt_half);
     if (sweep_uses_flow() && !D.hint) {
         launch_sweep_flow(D, c->st, c->flow, dt_half, fields);
         if (c->P.spinlang) eoff += 2;
@@ -99,7 +101,7 @@ void enqueue_dp(sld_ctx* c, double dt, int& eoff) { enqueue_dp(c, c->D, dt, eoff
 // two branches of one graph.  The second branch runs what does not read the
 // spins beside the sweeps:
 //   main:   links | dp(dt/2) | ds(dt/2) ........ | ds(dt/2) | force(magnetic) | dp(dt/2) | Te ...
-//   second:  core_dTe(dt/2) |  dr | rho + lists | force(EAM)
+//   second:  core_dTe(dt/2), visit records of the first ds | dr | rho + lists | force(EAM)
 // The lists and rho of this step go to the other buffer set, so the first
 // sweep still reads the previous ones; the step ends with that set current.
 // MD (core.cpp:38-56 without spins): links | dp | dr | rho | forces | dp
@@ -154,14 +156,30 @@ void enqueue_step(sld_ctx* c) {
     static const bool one_stream = getenv("SLD_ONE_STREAM") && getenv("SLD_ONE_STREAM")[0] == '1';
     cudaStream_t M = c->st, A = one_stream ? c->st : c->st2;
     cudaEvent_t* ev = c->fork_ev;
+    // The first core_ds's visit records read Te, rho and the noise counters,
+    // not the momenta: the side branch writes them while the main branch
+    // runs the first kick (the second core_ds's must wait for the first
+    // sweep, which reads the same records, and stay in place)
+    const bool early_noise = c->P.spinlang != 0;
+    const int eoff_ds1 = eoff + (c->P.lattlang ? 1 : 0);   // after the first kick's draw
     if (c->P.eltemp) {
         cudaEventRecord(ev[0], M);
         cudaStreamWaitEvent(A, ev[0], 0);
         launch_dte(Dc, A, dt / 2e0);
         cudaEventRecord(ev[1], A);
+        if (early_noise) {
+            launch_spin_noise(Dc, A, eoff_ds1, dt / 2e0 / 2e0);
+            cudaEventRecord(ev[4], A);
+        }
         launch_links(Dc, M, false, c->scan_blocks);
         cudaStreamWaitEvent(M, ev[1], 0);
     } else {
+        if (early_noise) {
+            cudaEventRecord(ev[0], M);
+            cudaStreamWaitEvent(A, ev[0], 0);
+            launch_spin_noise(Dc, A, eoff_ds1, dt / 2e0 / 2e0);
+            cudaEventRecord(ev[4], A);
+        }
         launch_links(Dc, M, false, c->scan_blocks);
     }
     enqueue_dp(c, Dc, dt / 2e0, eoff);
@@ -172,7 +190,8 @@ void enqueue_step(sld_ctx* c) {
     cudaEventRecord(ev[2], A);
     launch_force_eam(Dn, A);
     cudaEventRecord(ev[3], A);
-    enqueue_ds(c, Dc, dt / 2e0, eoff, false);
+    if (early_noise) cudaStreamWaitEvent(M, ev[4], 0);
+    enqueue_ds(c, Dc, dt / 2e0, eoff, false, early_noise);
     cudaStreamWaitEvent(M, ev[2], 0);
     enqueue_ds(c, Dn, dt / 2e0, eoff, !c->P.eltemp);
     cudaStreamWaitEvent(M, ev[3], 0);
@@ -409,7 +428,7 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
         sld_destroy(c);
         return SLD_ERR_CUDA;
     }
-    for (int k = 0; k < 4; ++k) cudaEventCreateWithFlags(&c->fork_ev[k], cudaEventDisableTiming);
+    for (int k = 0; k < 5; ++k) cudaEventCreateWithFlags(&c->fork_ev[k], cudaEventDisableTiming);
 
     DevTables T;
     rc = device_tables(prm->device, G.rcut_max, &T);
@@ -675,7 +694,7 @@ void sld_destroy(sld_ctx* c) {
     if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
     for (int k = 0; k < 2; ++k)
         if (c->step_graphs[k]) cudaGraphExecDestroy(c->step_graphs[k]);
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < 5; ++k)
         if (c->fork_ev[k]) cudaEventDestroy(c->fork_ev[k]);
     if (c->st2) cudaStreamDestroy(c->st2);
     for (void* q : c->allocs) cudaFree(q);

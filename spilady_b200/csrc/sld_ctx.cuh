@@ -36,7 +36,7 @@ struct sld_ctx {
     double force_volume = 0.0;
     cudaStream_t st = nullptr;
     cudaStream_t st2 = nullptr;        // second branch of the step graph
-    cudaEvent_t fork_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t fork_ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     cudaGraphExec_t step_graph = nullptr;
     cudaGraphExec_t step_graphs[2] = {nullptr, nullptr};   // by current buffer set
     // exchange lists and rho are double buffered: the list pass of a step
