@@ -35,21 +35,30 @@ sys.path.insert(0, ROOT)
 
 METRIC = "atom-steps/s, 4.19M-atom bcc Fe SLD: split-FP32 vs plain FP64 on one B200"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
-# Algorithmic HBM bytes per atom and step for each phase: each atom's own data
-# and list rows read or written once, neighbour data (spins, positions) reused
-# on chip or in L2.  core_ds: a visit reads its spin (32 B) and writes it
-# (32 B + the 16 B FP32 copy), reads its exchange row (14 pairs x 8 B) and its
-# visit record (32 B) = 224 B; backward visits also write H, HL, sum J (72 B);
-# 4 visits per step, 2 backward, plus the visit records (64 B, twice) = 1168.
-ALGO_BYTES = {"links": 70, "calculate_rho": 264, "calculate_force_energy": 290,
-              "core_ds": 1168, "core_dp": 340, "core_dr": 112,
-              "calculate_temperature": 290, "check_energy": 32, "core_dTe": 0,
-              "bookkeeping": 0}
-# DRAM bytes per atom and step of core_ds from an ncu capture (bcc Fe 64^3
-# cells, split form, cold caches as ncu replays them): one sweep launch of
-# 10,648 cells (65,536 visits) read 33.32 MB and wrote 0.03 MB (508 B per
-# visit); the visit-record pass read 8.41 MB for 524,288 atoms (16 B per atom).
-CORE_DS_TRAFFIC_PER_ATOM = 4 * 508.4 + 2 * 16.0
+# Algorithmic HBM bytes per atom and step (compulsory SoA traffic: each
+# atom's own state read or written once per pass, neighbour data reused on
+# chip).  Per form and pass: bin 28; rho 32 / 16 (FP64 / split); forces (r, s,
+# rho in, f out) 80 / 40; four spin visits (r, s, rho in, s out) 4 x 80 / 4 x
+# 64; two kicks with the rescale 2 x 120 / 2 x 108; drift 72 / 84.  Totals
+# 772 / 640 B per atom-step.
+ALGO = {
+    "fp64": {"links": 28, "calculate_rho": 32, "calculate_force_energy": 80, "core_ds": 320,
+             "core_dp": 240, "core_dr": 72, "step": 772},
+    "split": {"links": 28, "calculate_rho": 16, "calculate_force_energy": 40, "core_ds": 256,
+              "core_dp": 216, "core_dr": 84, "step": 640},
+}
+# The bytes this design moves on purpose for core_ds (its visit records and
+# exchange rows, which the count above treats as on-chip reuse): a visit
+# reads its spin (32 B) and writes it (32 B + the 16 B FP32 copy), reads its
+# exchange row (14 pairs x 8 B) and visit record (32 B) = 224 B; backward
+# visits also write H, HL and sum J (72 B); 4 visits per step, 2 backward,
+# plus the visit records (64 B, twice) = 1,168 B per atom-step.
+DESIGN_BYTES_CORE_DS = 1168
+# DRAM bytes per atom and step of core_ds measured by ncu (dram__bytes_read.sum
+# + dram__bytes_write.sum); the capture is summarised in profiles/.
+CORE_DS_TRAFFIC_PER_ATOM = {"split": 4 * 508.4 + 2 * 16.0}
+CORE_DS_TRAFFIC_SOURCE = ("ncu dram__bytes at 64^3 (one sweep launch, 65,536 visits, 508 B "
+                          "per visit; visit-record pass 16 B per atom), scaled per visit")
 ROOFLINE_KERNEL = {"core_ds": "k_sweep_pipe + k_spin_noise (core_ds: 72 sweep launches "
                               "and 2 visit-record passes per step)"}
 
@@ -64,11 +73,14 @@ def parse():
     ap.add_argument("--size", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64-arm", action="store_true",
+                    help="time only the form given by --precision (the default run also "
+                         "times the plain FP64 form on the same state for split / FP64)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the built-in launch shapes instead of sld_autotune's")
     ap.add_argument("--small", action="store_true",
                     help="short run for profiler captures: no CPU baseline, no e2e leg, "
-                         "one phase-profile step")
+                         "no FP64 arm, no error check, one phase-profile step")
     ap.add_argument("--workload", default="single", choices=["single", "replicas", "adjoint"],
                     help="single: the 128^3 spin-lattice-electron system; replicas: many "
                          "independent small systems advanced as one batch; adjoint: gradients "
@@ -147,28 +159,38 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ reference
-def reference_sample(steps, threads):
-    """The reference's own CPU build (oracle/_ref) on a bounded sample of the
-    workload: 24^3 cells, same physics, Te on link cells (the reference keeps
-    Te per link cell; it has no decoupled mesh).  Returns (atom-steps/s,
-    natom, seconds)."""
+def reference_sample(size, steps, warm, threads):
+    """The reference's own CPU build (oracle/_ref) on the benchmark's system:
+    bcc Fe size^3 cells, the same physics and start state, Te on the link
+    cells (the reference keeps Te per link cell; it has no decoupled mesh).
+    ``warm`` untimed steps, then ``steps`` steps timed around core() inside
+    the reference's process.  Returns (atom-steps/s, natom, seconds)."""
     from oracle import refjob
     from spilady_b200.lattice import initial_state
-    params, r, p, s = initial_state(24, seed=2026, tilt=0.35)
+    params, r, p, s = initial_state(size, seed=2026, tilt=0.35)
     params["step"] = 0.5e-15
-    ops = [(refjob.OP_CORE, 1), (refjob.OP_CORE, steps), (refjob.OP_DUMP, 0)]
+    ops = [(refjob.OP_CORE, warm), (refjob.OP_STATS, 0), (refjob.OP_CORE, steps),
+           (refjob.OP_STATS, 0)]
     d = refjob.run("langte", params, r, p, s, ops=ops, threads=threads)[-1]
     return r.shape[0] * steps / d.wall, r.shape[0], d.wall
 
 
-def cpu_baseline_block(steps=10):
+# The reference's CPU step at 128^3 takes about 11 s on 16 host cores, so its
+# timed samples are bounded: the baseline inside our arm times 2 steps after 1
+# warm-up step (about 40 s with the set-up); the reference arm times up to
+# REF_MAX_STEPS steps after one warm-up step (about 4 min).
+REF_MAX_STEPS = 20
+
+
+def cpu_baseline_block(size, steps=2):
     threads = os.cpu_count() or 1
     from oracle import refjob
     if refjob.available("langte"):
-        v, n, t = reference_sample(steps, threads)
+        v, n, t = reference_sample(size, steps, 1, threads)
         return {"value": v, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
-                "sample": f"reference CPU build, 24^3 cells ({n} atoms), {steps} steps, "
-                          f"same physics with Te on link cells, {t:.1f} s of core()"}
+                "sample": f"reference CPU build, {size}^3 cells ({n} atoms), {steps} steps "
+                          f"after 1 warm-up step, same physics with Te on link cells, "
+                          f"{t:.1f} s of core()"}
     return {"value": None, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
             "sample": "reference build absent (oracle/ref/build.sh not run)"}
 
@@ -209,16 +231,22 @@ def run_reference(args, world, rank):
         print(json.dumps({"impl": "reference", "unavailable":
                           "reference CPU build missing (sh oracle/ref/build.sh)"}))
         return
-    v, n, t = reference_sample(args.steps, threads)
+    steps = max(1, min(args.steps, REF_MAX_STEPS))
+    warm = 1 if args.warmup > 0 else 0
+    v, n, t = reference_sample(args.size, steps, warm, threads)
     line = {"metric": METRIC, "value": v, "unit": "atom-steps/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "steps": steps, "warmup": warm, "ms_per_step": 1e3 * t / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"bcc Fe 24^3 cells ({n} atoms) sample of the 128^3 "
-                                   "spin-lattice-electron workload, Te on link cells",
-                       "parallelism": "OpenMP host threads"},
+            "config": {"workload": f"bcc Fe {args.size}^3 cells ({n} atoms) spin-lattice-electron,"
+                                   " Langevin spin+lattice, localcolmot, Te on link cells"
+                                   " (the reference has no decoupled Te mesh), dt 0.5 fs",
+                       "natom": n, "parallelism": f"OpenMP, {threads} host threads",
+                       "steps_note": f"{steps} timed steps (at most {REF_MAX_STEPS}) after "
+                                     f"{warm} warm-up step; each step is the whole system"},
             "cpu_baseline": {"value": v, "unit": "atom-steps/s", "cores": threads,
-                             "kind": "reference", "sample": f"{n} atoms x {args.steps} steps"},
+                             "kind": "reference",
+                             "sample": f"{n} atoms x {steps} steps, {t:.1f} s of core()"},
             "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -410,76 +438,67 @@ def main():
         run_adjoint(args, world, rank, local)
         return
     from spilady_b200 import engine
-    params, r, p, s, te, sw = workload(args.size)
-    prec = {"fp64": engine.FP64, "split": engine.SPLIT,
-            "fp64-analytic": engine.FP64_ANALYTIC}[args.precision]
-    e = engine.Engine(params, r, p, s, te=te, device=local, precision=prec, **sw)
-    natom = e.natom
-    # The split form's error against the FP64 run of the same kernels, on the
-    # start state: forces, exchange fields and per-atom energies (the split
-    # form is held to 1e-5 relative).
-    split_err = None
-    if prec == engine.SPLIT and not args.small:
-        ref = engine.Engine(params, r, p, s, te=te, device=local,
-                            precision=engine.FP64_ANALYTIC, **sw)
-        rel = lambda a, b: float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
-        split_err = {"force": rel(e.get("f"), ref.get("f")),
-                     "field": rel(e.get("H"), ref.get("H")),
-                     "pe": rel(e.get("pe"), ref.get("pe")),
-                     "me": rel(e.get("me"), ref.get("me")),
-                     "how": "max |split - fp64| / max |fp64| over all atoms, start state"}
-        ref.close()
-    # launch shapes by the autotuner (outside the timed region; the state is
-    # put back afterwards)
-    shapes = None if args.no_autotune else e.autotune(steps=8)
-    e.run(args.warmup)
-    e.sync()
     import torch
     torch.cuda.set_device(local)
-    clocks = ClockSampler(local)
-    barrier(world)
-    torch.cuda.synchronize()
-    clocks.start()
-    e.run(args.steps)
-    ms = e.last_run_ms()
-    torch.cuda.synchronize()
-    barrier(world)
-    clk = clocks.stop()
-    e.sync()
-    ms = allmax(world, ms)
-    value = natom * args.steps * world / (ms / 1e3)
-    kernels_per_step = e.step_kernel_count()
+    params, r, p, s, te, sw = workload(args.size)
+    forms = {"fp64": engine.FP64, "split": engine.SPLIT, "fp64-analytic": engine.FP64_ANALYTIC}
+    prec = forms[args.precision]
+    # The split form's error against the FP64 run of the same kernels and
+    # against the reference's arithmetic (the FP64 form), on the start state:
+    # forces, exchange fields and per-atom energies (held to 1e-5 relative).
+    split_err = None
+    if prec == engine.SPLIT and not args.small:
+        e = engine.Engine(params, r, p, s, te=te, device=local, precision=prec, **sw)
+        ref = engine.Engine(params, r, p, s, te=te, device=local, precision=engine.FP64, **sw)
+        rel = lambda a, b: float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+        split_err = {q: rel(e.get(n), ref.get(n)) for q, n in
+                     (("force", "f"), ("field", "H"), ("rho", "rho"), ("pe", "pe"),
+                      ("me", "me"))}
+        split_err["force_abs_eV_per_A"] = float(np.max(np.abs(e.get("f") - ref.get("f"))))
+        split_err["how"] = ("max |split - fp64| / max |fp64| over all atoms, start state; the "
+                            "FP64 form is the reference's arithmetic (its tables)")
+        ref.close()
+        e.close()
 
-    # per-phase device time (CUDA events on the engine's stream), a few steps
-    prof = {}
-    nprof = 1 if args.small else 5
-    for _ in range(nprof):
-        for k, v in e.profile_step().items():
-            prof[k] = prof.get(k, 0.0) + v / nprof
-    dom = max(prof, key=prof.get)
-    peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
-    hbm = peaks.get("hbm_gbs", 6650.0)
-    step_s = prof[dom] / 1e3
-    achieved = ALGO_BYTES.get(dom, 0) * natom / step_s / 1e9 if prof[dom] > 0 else 0.0
-    traffic = CORE_DS_TRAFFIC_PER_ATOM * natom if dom == "core_ds" else None
-    roofline = {"bound": "hbm", "kernel": ROOFLINE_KERNEL.get(dom, dom), "achieved": achieved,
-                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "traffic": traffic,
-                "per": "one step of the phase (algorithmic bytes and traffic per step)",
-                "algorithmic_bytes": ALGO_BYTES.get(dom, 0) * natom,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at 64^3, "
-                                  "scaled per visit" if traffic else None,
-                "peak_source": "measured (burst copy)" if peaks else "fallback",
-                "timing": f"CUDA events around each phase on the engine stream, {nprof} "
-                          "sequential steps after the timed region",
-                "phase_ms": {k: round(v, 4) for k, v in prof.items()}}
+    def timed_form(form, with_e2e):
+        """One form: autotune, warm up, time args.steps graph steps (CUDA
+        events on the engine stream), profile the phases; optionally the e2e
+        leg through the public API.  Returns a dict."""
+        e = engine.Engine(params, r, p, s, te=te, device=local, precision=form, **sw)
+        shapes = None if args.no_autotune else e.autotune(steps=8)
+        e.run(args.warmup)
+        e.sync()
+        clocks = ClockSampler(local)
+        barrier(world)
+        torch.cuda.synchronize()
+        clocks.start()
+        e.run(args.steps)
+        ms = e.last_run_ms()
+        torch.cuda.synchronize()
+        barrier(world)
+        clk = clocks.stop()
+        e.sync()
+        ms = allmax(world, ms)
+        out = {"ms": ms, "value": e.natom * args.steps * world / (ms / 1e3), "clocks": clk,
+               "shapes": shapes, "kernels_per_step": e.step_kernel_count(), "natom": e.natom}
+        prof = {}
+        nprof = 1 if args.small else 5
+        for _ in range(nprof):
+            for k, v in e.profile_step().items():
+                prof[k] = prof.get(k, 0.0) + v / nprof
+        out["prof"], out["nprof"] = prof, nprof
+        if with_e2e:
+            out["e2e"] = e2e_leg(e)
+        e.close()
+        return out
 
-    # end to end through the public API with host buffers: upload the state
-    # from pinned host memory, then every step run it and read the check()
-    # averages back
-    e2e = None
-    if not args.no_e2e:
-        import torch
+    def e2e_leg(e):
+        # End to end through the public API with host buffers: upload the
+        # state from pinned host memory (sld_set_state), then every step run
+        # it and read the check() averages back, as the reference's main loop
+        # prints them every step at interval_of_print_out 1.  The state stays
+        # on the device between steps, as it does behind the reference's
+        # core() with a device backend.
         host = {}
         for name, a in (("r", r), ("p", p), ("s", s)):
             host[name] = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
@@ -491,18 +510,57 @@ def main():
             e.run(1)
             e.averages()
         t1 = time.perf_counter()
-        e2e = {"value": natom * k / (t1 - t0), "unit": "atom-steps/s",
-               "h2d_bytes_per_step": int(natom * 72 / k), "d2h_bytes_per_step": 80,
-               "steps": k,
-               "note": "one upload of r, p, s per sample of k steps (the state stays on the "
-                       "device between steps), averages read back every step"}
-    e.close()
+        nat = e.natom
+        return {"value": nat * k / (t1 - t0), "unit": "atom-steps/s",
+                "h2d_bytes_per_step": int(nat * 72 / k), "d2h_bytes_per_step": 80, "steps": k,
+                "note": f"per sample of {k} steps: r, p, s uploaded from pinned host memory "
+                        "once (sld_set_state), then sld_run(1) and the averages read back "
+                        "every step"}
+
+    main_arm = timed_form(prec, not args.no_e2e)
+    fp64_arm = None
+    if prec == engine.SPLIT and not (args.no_fp64_arm or args.small):
+        fp64_arm = timed_form(engine.FP64, False)
+    natom = main_arm["natom"]
+    ms, value, prof, nprof = main_arm["ms"], main_arm["value"], main_arm["prof"], main_arm["nprof"]
+    key = "split" if prec == engine.SPLIT else "fp64"
+    dom = max((k for k in prof if k in ALGO[key]), key=prof.get)
+    peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    achieved = ALGO[key][dom] * natom / (prof[dom] / 1e3) / 1e9 if prof[dom] > 0 else 0.0
+    traffic = None
+    if dom == "core_ds" and key in CORE_DS_TRAFFIC_PER_ATOM:
+        traffic = CORE_DS_TRAFFIC_PER_ATOM[key] * natom
+    step_achieved = ALGO[key]["step"] * natom / (ms / args.steps / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": ROOFLINE_KERNEL.get(dom, dom), "achieved": achieved,
+                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                "per": "one step of the phase (algorithmic bytes and traffic per step)",
+                "algorithmic_bytes": ALGO[key][dom] * natom,
+                "algorithmic_bytes_per_atom": ALGO[key][dom],
+                "traffic_source": CORE_DS_TRAFFIC_SOURCE if traffic else None,
+                "design_bytes": {"per_atom": DESIGN_BYTES_CORE_DS,
+                                 "achieved": DESIGN_BYTES_CORE_DS * natom / (prof[dom] / 1e3) / 1e9,
+                                 "what": "core_ds with this design's visit records and "
+                                         "exchange rows counted"} if dom == "core_ds" else None,
+                "whole_step": {"bytes_per_atom": ALGO[key]["step"], "achieved": step_achieved,
+                               "frac": step_achieved / hbm},
+                "peak_source": "measured (burst copy)" if peaks else "fallback",
+                "timing": f"CUDA events around each phase on the engine stream, {nprof} "
+                          "sequential steps after the timed region",
+                "phase_ms": {k: round(v, 4) for k, v in prof.items()}}
+    fp64_block = None
+    if fp64_arm is not None:
+        fp64_block = {"value": fp64_arm["value"], "ms_per_step": fp64_arm["ms"] / args.steps,
+                      "phase_ms": {k: round(v, 4) for k, v in fp64_arm["prof"].items()},
+                      "launch_shapes": fp64_arm["shapes"], "clocks": fp64_arm["clocks"],
+                      "how": "the plain FP64 form (the reference's arithmetic) on the same "
+                             "state, box and steps, timed the same way"}
 
     if rank != 0:
         return
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_block()
+        cpu = cpu_baseline_block(args.size)
     line = {
         "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -513,12 +571,14 @@ def main():
                                f" Langevin spin+lattice, localcolmot, Te mesh {sw['te_mesh']}^3,"
                                " dt 0.5 fs",
                    "precision": args.precision, "natom": natom,
-                   "l2": "state (~1 GB) larger than L2; no flush needed",
-                   "launch_shapes": shapes,
-                   "split_vs_fp64": split_err,
+                   "l2": "state (~3 GB) larger than L2; no flush needed",
+                   "launch_shapes": main_arm["shapes"],
+                   "split_error": split_err,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-        "gpu_launches": kernels_per_step * args.steps, "clocks": clk,
+        "fp64": fp64_block,
+        "split_over_fp64": (value / fp64_arm["value"]) if fp64_arm else None,
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": main_arm.get("e2e"),
+        "gpu_launches": main_arm["kernels_per_step"] * args.steps, "clocks": main_arm["clocks"],
     }
     print(json.dumps(line))
 

@@ -53,10 +53,12 @@ extern "C" {
 #define SLD_MAX_CELL_ATOMS 64
 
 /* SLD_FP64: the reference's arithmetic (FP64, interpolated 10^6-point
-   tables); SLD_SPLIT: FP32 pair terms from the analytic potential with
-   compensated sums, FP64 integration and reductions; SLD_FP64_ANALYTIC: the
-   split form's kernels evaluated in FP64 (the error reference for
-   SLD_SPLIT). */
+   tables); SLD_SPLIT: FP32 pair terms with compensated sums, the same
+   functions as the reference's tables (the functional forms with the
+   tables' seven-point derivatives; F(rho) from the tables), FP64 integration
+   and reductions; SLD_FP64_ANALYTIC: the functional forms in FP64 with their
+   exact derivatives (the model the adjoint differentiates; near the knots of
+   the cubics it differs from the tables' derivatives by about 1e-4). */
 typedef enum { SLD_FP64 = 0, SLD_SPLIT = 1, SLD_FP64_ANALYTIC = 2 } sld_precision;
 
 /* The Hamiltonian, control.h's mode switch (control.h:8-12; core.cpp:31-76):

@@ -31,9 +31,10 @@
 # restates their forms:
 #   param
 #
-# usage: sh oracle/ref/build.sh [reference_dir]
+# usage: sh oracle/ref/build.sh [reference_dir]   (default: $SPILADY_REFERENCE,
+# else the reference tree mounted at /root/reference)
 set -e
-REF=${1:-/root/reference}
+REF=${1:-${SPILADY_REFERENCE:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT=$(cd "$HERE/.." && pwd)/_ref
 if [ ! -f "$REF/core.cpp" ]; then

@@ -65,6 +65,9 @@ enum {
     /* quantum build: initial_quantum_noise() after the OP_SET ops of its
        variables (initial.cpp:102-104), and its filter written to qfilter.dat */
     OP_QINIT = 15, OP_QFILTER = 16,
+    /* a dump record without the arrays (natom = ncells = 0): the time and
+       the wall time of the last OP_CORE, for timing runs of large systems */
+    OP_STATS = 17,
     /* OP_SET + k sets input variable k (read_variables.cpp:197-241):
        0 pressure, 1 baro_damping_time, 2-7 stress_xx yx yy zx zy zz,
        8 interval_of_scale_pressure, 9 interval_of_scale_stress,
@@ -324,6 +327,15 @@ int main(int argc, char** argv) {
         rd(f, &arg, 1);
         switch (code) {
         case OP_DUMP: dump(out); break;
+        case OP_STATS: {
+            int32_t hdr[4] = {0x44554d50, 0, 0, ngroups};
+            wr(out, hdr, 4);
+            double sc[2] = {total_time, g_last_wall};
+            wr(out, sc, 2);
+            int32_t none[2] = {0, 0};   /* no list entries, no groups */
+            wr(out, none, 2);
+            break;
+        }
         case OP_LINKS: links(); break;
         case OP_FORCE: calculate_force_energy(); break;
 #ifdef H_LATT

@@ -20,7 +20,7 @@ REF_DIR = os.path.join(HERE, "_ref")
 
 OP_DUMP, OP_LINKS, OP_RHO, OP_FORCE, OP_DS, OP_DP, OP_DR, OP_DTE, OP_TEMP, \
     OP_CORE, OP_CHECK_ENERGY, OP_STEP, OP_CONFIG_INTERVAL, OP_WRITE_CONFIG, \
-    OP_CHECK, OP_QINIT, OP_QFILTER = range(17)
+    OP_CHECK, OP_QINIT, OP_QFILTER, OP_STATS = range(18)
 # OP_SET + k sets an input variable of the baro / dtstep builds (harness.cpp)
 OP_SET = 100
 SET_VARS = {"pressure": 0, "baro_damping_time": 1, "stress_xx": 2, "stress_yx": 3,
@@ -111,10 +111,10 @@ def read_dumps(path):
         total_time, wall = struct.unpack_from("<2d", data, off)
         off += 16
         na = natom * len(ATOM_FIELDS)
-        atoms = np.frombuffer(data, np.float64, na, off).reshape(natom, -1)
+        atoms = np.frombuffer(data, np.float64, na, off).reshape(natom, len(ATOM_FIELDS))
         off += 8 * na
         nc = ncells * len(CELL_FIELDS)
-        cells = np.frombuffer(data, np.float64, nc, off).reshape(ncells, -1)
+        cells = np.frombuffer(data, np.float64, nc, off).reshape(ncells, len(CELL_FIELDS))
         off += 8 * nc
         (nl,) = struct.unpack_from("<i", data, off)
         off += 4

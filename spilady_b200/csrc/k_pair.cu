@@ -190,16 +190,14 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, int write_rho) {
         pairs_one<MODE>(D, i, write_rho);
 }
 
-// F'(rho) per atom (the force pass needs it for both atoms of every pair)
+// F'(rho) per atom (the force pass needs it for both atoms of every pair):
+// from the reference's FP64 tables (FP64 and split forms), or the analytic
+// derivative (FP64_ANALYTIC)
 template <int MODE>
 __global__ void __launch_bounds__(256) k_embed(Dev D) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= D.natom) return;
-    if constexpr (MODE == 1) {
-        float F, dF;
-        emb32((float)D.rho[i], F, dF);
-        D.dF[i] = (double)dF;
-    } else if constexpr (MODE == 2) {
+    if constexpr (MODE == 2) {
         double F, dF;
         emb64(D.rho[i], F, dF);
         D.dF[i] = dF;
@@ -411,11 +409,11 @@ __device__ __forceinline__ void force32_one(const Dev& D, int i) {
         st6f[3] += gx * dy; st6f[4] += gy * dz; st6f[5] += gz * dx;
         vir += -force * rsq;
     }
-    float F = 0.f, dF;
-    if (PART & PART_EAM) emb32((float)rho_i, F, dF);
+    double F = 0.0;
+    if (PART & PART_EAM) F = interp(D.tF, rho_i, D.inv_rho, &D.ctl->err);
     double st6[6];
     for (int k = 0; k < 6; ++k) st6[k] = st6f[k];
-    force_finish<PART>(D, i, si_sq, rho_i, (double)F, fx.value(), fy.value(), fz.value(),
+    force_finish<PART>(D, i, si_sq, rho_i, F, fx.value(), fy.value(), fz.value(),
                        pe.value(), me.value(), me0.value(), (double)vir, st6);
 }
 

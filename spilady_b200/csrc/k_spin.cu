@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(128) k_sweep_pipe(Dev D, const int* __restrict
 // and every warp leaves; the host reports SLD_ERR_TIMEOUT.
 // Tags grow by 2 per call (sync[0]); flags and tags are never reset, so
 // stale flags from earlier calls are always below this call's tags.
-#define FLOW_POLLS (1 << 21)     // polls of one cell's waits (~0.2 s with the sleeps)
+#define FLOW_POLLS (1 << 21)     // default polls of one cell's waits (~0.2 s with the sleeps)
 
 __device__ __forceinline__ int ld_flag(const int* p) {
     return *reinterpret_cast<const volatile int*>(p);
@@ -535,7 +535,7 @@ __device__ __forceinline__ bool flow_wait_one(const Dev& D, const int* flag, int
 // the flags not yet set are polled.
 __device__ bool flow_wait(const Dev& D, const SweepFlow& F, int c, int g, bool bwd, int tagF,
                           int tagB) {
-    int budget = FLOW_POLLS;
+    int budget = F.polls;
     int cx, cy, cz;
     cell_xyz(D, c, cx, cy, cz);
     int nb[26], fl[26], gr[26];
@@ -564,7 +564,10 @@ __device__ bool flow_wait(const Dev& D, const SweepFlow& F, int c, int g, bool b
 template <bool SPLIT>
 __global__ void __launch_bounds__(128) k_sweep_flow(Dev D, SweepFlow F, double dt, int flags) {
     const int lane = threadIdx.x & 31;
-    const int tagF = F.sync[0] + 1, tagB = tagF + 1;
+    // the tags this call's waits need (F.stall > 0 asks for tags no warp
+    // writes: every wait on a neighbour then runs out)
+    const int tagF = F.sync[0] + 1 + F.stall, tagB = tagF + 1;
+    const int putF = F.sync[0] + 1, putB = putF + 1;
     int task = 0;
     if (lane == 0) task = atomicAdd(F.sync + 1, 1);
     task = __shfl_sync(0xffffffffu, task, 0);
@@ -589,7 +592,7 @@ __global__ void __launch_bounds__(128) k_sweep_flow(Dev D, SweepFlow F, double d
             __threadfence();                  // the flags above before the spins below
             cell_walk<SPLIT, true>(D, c, dt, (bwd ? SW_BACKWARD : 0) | flags);
             __threadfence();                  // this cell's spins before its flag
-            atomicExch(F.cell_flag + c, bwd ? tagB : tagF);
+            atomicExch(F.cell_flag + c, bwd ? putB : putF);
         }
         task = __shfl_sync(0xffffffffu, next, 0);
     }
@@ -604,8 +607,16 @@ __global__ void k_flow_next(SweepFlow F) {
 }
 
 static int g_flow_blocks[2] = {0, 0};
+// the waits' bound and the stall of the data-flow schedule, from the
+// environment at context creation (SLD_FLOW_POLLS, SLD_FLOW_STALL): a test
+// makes the waits run out with a small bound and a stall, and expects
+// SLD_ERR_TIMEOUT instead of a hang
+static int g_flow_polls = FLOW_POLLS, g_flow_stall = 0;
 
-void launch_sweep_flow(const Dev& D, cudaStream_t st, const SweepFlow& F, double dt, bool fields) {
+void launch_sweep_flow(const Dev& D, cudaStream_t st, const SweepFlow& F0, double dt, bool fields) {
+    SweepFlow F = F0;
+    F.polls = g_flow_polls;
+    F.stall = g_flow_stall;
     const int flags = fields ? 0 : SW_NO_FIELDS;
     const int k = D.split ? 1 : 0;
     if (D.split)
@@ -625,6 +636,16 @@ void sweep_init() {
     cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem());
     const char* v = getenv("SLD_SWEEP_MODE");
     if (v && v[0] >= '0' && v[0] <= '3') g_sweep_mode = v[0] - '0';
+    g_flow_polls = FLOW_POLLS;
+    g_flow_stall = 0;
+    if (const char* q = getenv("SLD_FLOW_POLLS")) {
+        long n = strtol(q, nullptr, 10);
+        if (n >= 1 && n <= FLOW_POLLS) g_flow_polls = (int)n;
+    }
+    if (const char* q = getenv("SLD_FLOW_STALL")) {
+        long n = strtol(q, nullptr, 10);
+        if (n >= 0 && n <= 1000) g_flow_stall = (int)n;
+    }
     int dev = 0, sms = 0, b0 = 0, b1 = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

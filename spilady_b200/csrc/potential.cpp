@@ -163,13 +163,15 @@ void pot_join_data(double o[7]) {
 }
 
 static void cubic_pieces(const double* a, const double* k, int n, float* K, float* C, double* K64,
-                         double* C64) {
+                         double* C64, float* A, double* A64) {
     // knots ascending (the arrays here are given descending)
     std::vector<int> ord(n);
     for (int i = 0; i < n; ++i) ord[i] = n - 1 - i;
     for (int i = 0; i < n; ++i) {
         K[i] = (float)k[ord[i]];
         K64[i] = (double)K[i];
+        A[i] = (float)a[ord[i]];
+        A64[i] = a[ord[i]];
     }
     for (int m = 0; m <= n; ++m) {
         double c[4] = {0, 0, 0, 0};
@@ -196,8 +198,8 @@ void pot_cubic_tables(float out[kCubicFloats], double o64[kCubicFloats]) {
     static const double da[6] = {0.9332056681088162, -1.162558782567700, -0.3502026949249225,
                                  0.4287820835430028, 4.907925057809273, -5.307049068415304};
     static const double dk[6] = {3.0, 2.8666666666666666, 2.7333333333333333, 2.6, 2.4, 2.3};
-    cubic_pieces(kPV, kPK, 8, out, out + 8, o64, o64 + 8);
-    cubic_pieces(da, dk, 6, out + 44, out + 50, o64 + 44, o64 + 50);
+    cubic_pieces(kPV, kPK, 8, out, out + 8, o64, o64 + 8, out + 78, o64 + 78);
+    cubic_pieces(da, dk, 6, out + 44, out + 50, o64 + 44, o64 + 50, out + 86, o64 + 86);
 }
 
 }  // namespace sld

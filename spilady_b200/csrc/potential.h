@@ -31,8 +31,11 @@ void pot_join_data(double out[7]);
 // base stored as FP32.  Layout (floats): pair knots [0,8), pair coefficients
 // [8,44) (9 intervals x c0..c3), density knots [44,50), density coefficients
 // [50,78) (7 intervals).  Interval m holds r with m knots <= r; its base is
-// knot m-1 (knot 0 for m = 0); the last interval is zero.
-constexpr int kCubicFloats = 78;
+// knot m-1 (knot 0 for m = 0); the last interval is zero.  Then the amplitude
+// a_i of each knot's term a_i (k_i - r)^3, in the same ascending knot order:
+// pair [78,86), density [86,92) (the seven-point derivative near a knot needs
+// the one term that changes form there).
+constexpr int kCubicFloats = 92;
 void pot_cubic_tables(float out[kCubicFloats], double out64[kCubicFloats]);
 
 }  // namespace sld

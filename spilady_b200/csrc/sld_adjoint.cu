@@ -333,6 +333,7 @@ int sld_adjoint_theta_default(double* theta) {
 int sld_adjoint_config(sld_ctx* c, const double* theta, double* out4, double* dE, double* dL) {
     int rc = check_ctx(c);
     if (rc) return rc;
+    SLD_DEVICE_OF(c);
     if (!theta || !out4) return SLD_ERR_ARG;
     Adj a;
     rc = alloc_adj(a, c, theta);
@@ -381,6 +382,7 @@ int sld_adjoint_jacobians(sld_ctx* c, const double* theta, double* f, double* H,
                           double* dH) {
     int rc = check_ctx(c);
     if (rc) return rc;
+    SLD_DEVICE_OF(c);
     if (!theta || !dF) return SLD_ERR_ARG;
     Adj a;
     rc = alloc_adj(a, c, theta);
@@ -421,6 +423,7 @@ int sld_adjoint_trajectory(sld_ctx* c, const double* theta, int nsteps, int chec
                            double* L, double* dL) {
     int rc = check_ctx(c);
     if (rc) return rc;
+    SLD_DEVICE_OF(c);
     if (!theta || !L || nsteps < 0 || checkpoint_every < 1) return SLD_ERR_ARG;
     Adj a;
     rc = alloc_adj(a, c, theta);

@@ -411,7 +411,8 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     if (rc) { delete c; return rc; }
     const auto& G = c->G;
 
-    if (cudaSetDevice(prm->device) != cudaSuccess) { delete c; return SLD_ERR_CUDA; }
+    DevGuard dev_guard(prm->device);   // the caller's device is current again on return
+    if (!dev_guard.ok) { delete c; return SLD_ERR_CUDA; }
     sweep_init();
     dte_init(prm->device);
     // the main branch (spin sweeps: few, latency-bound blocks) gets the
@@ -650,6 +651,7 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
 
 int sld_set_state(sld_ctx* c, const double* r, const double* p, const double* s) {
     if (!c || !r || !p || !s) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     Dev& D = c->D;
     const size_t n = (size_t)D.natom;
     // The caller's arrays go to the device as they are, into the neighbour
@@ -690,6 +692,7 @@ int sld_set_state(sld_ctx* c, const double* r, const double* p, const double* s)
 
 void sld_destroy(sld_ctx* c) {
     if (!c) return;
+    DevGuard sld_dev_guard_(c->P.device);
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
     for (int k = 0; k < 2; ++k)
@@ -706,12 +709,14 @@ void sld_destroy(sld_ctx* c) {
 
 int sld_links(sld_ctx* c) {
     if (!c) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     launch_links(c->D, c->st, false, c->scan_blocks);
     return launch_status();
 }
 
 int sld_calculate_rho(sld_ctx* c) {
     if (!c) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     launch_pairs(c->D, c->st, true);
     c->lists_stale = false;
     return launch_status();
@@ -727,6 +732,7 @@ static void fresh_lists(sld_ctx* c) {
 
 int sld_calculate_force_energy(sld_ctx* c) {
     if (!c) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     fresh_lists(c);
     launch_force(c->D, c->st);
     c->force_volume = c->D.box_volume;
@@ -735,6 +741,7 @@ int sld_calculate_force_energy(sld_ctx* c) {
 
 int sld_core_ds(sld_ctx* c, double dt) {
     if (!c) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     fresh_lists(c);
     int eoff = 0;
     enqueue_ds(c, dt, eoff);
@@ -744,6 +751,7 @@ int sld_core_ds(sld_ctx* c, double dt) {
 
 int sld_core_dp(sld_ctx* c, double dt) {
     if (!c) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     int eoff = 0;
     enqueue_dp(c, dt, eoff);
     launch_advance(c->D, c->st, eoff, 0);
@@ -752,6 +760,7 @@ int sld_core_dp(sld_ctx* c, double dt) {
 
 int sld_core_dr(sld_ctx* c, double dt) {
     if (!c) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     launch_dr(c->D, c->st, dt);
     c->lists_stale = true;
     return launch_status();
@@ -759,6 +768,7 @@ int sld_core_dr(sld_ctx* c, double dt) {
 
 int sld_core_dTe(sld_ctx* c, double dt) {
     if (!c) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     if (!c->P.eltemp) return SLD_OK;
     launch_dte(c->D, c->st, dt);
     return launch_status();
@@ -766,6 +776,7 @@ int sld_core_dTe(sld_ctx* c, double dt) {
 
 int sld_calculate_temperature(sld_ctx* c) {
     if (!c) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     if (!c->P.eltemp) return SLD_OK;
     fresh_lists(c);
     launch_temperature(c->D, c->st);
@@ -774,6 +785,7 @@ int sld_calculate_temperature(sld_ctx* c) {
 
 int sld_run(sld_ctx* c, int nsteps) {
     if (!c || nsteps < 0) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     fresh_lists(c);
     if (dynamic_step(c)) {
         // box or time step set by sld_scale between steps: launch directly
@@ -790,15 +802,25 @@ int sld_run(sld_ctx* c, int nsteps) {
         int saved = c->cur;
         use_set(c, k);
         cudaGraph_t g = nullptr;
-        CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-        enqueue_step(c);
-        CK(cudaStreamEndCapture(c->st, &g));
+        cudaError_t e = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            enqueue_step(c);
+            // always end the capture, so that the stream leaves capture mode
+            // even when a launch inside it failed
+            e = cudaStreamEndCapture(c->st, &g);
+        }
         // with node priorities the sweeps' branch (the high-priority stream)
         // gets its CTAs dispatched before the side branch's waiting ones
-        CK(cudaGraphInstantiate(&c->step_graphs[k], g,
-                                c->D.tune.graph_prio ? cudaGraphInstantiateFlagUseNodePriority : 0));
-        cudaGraphDestroy(g);
+        if (e == cudaSuccess)
+            e = cudaGraphInstantiate(&c->step_graphs[k], g,
+                                     c->D.tune.graph_prio ? cudaGraphInstantiateFlagUseNodePriority : 0);
+        if (g) cudaGraphDestroy(g);
         use_set(c, saved);
+        if (e != cudaSuccess) {
+            c->step_graphs[k] = nullptr;
+            cudaGetLastError();
+            return SLD_ERR_CUDA;
+        }
     }
     CK(cudaEventRecord(c->ev0, c->st));
     for (int k = 0; k < nsteps; ++k) {
@@ -875,7 +897,8 @@ int sld_batch_create(sld_batch** out, sld_ctx* const* ctxs, int n) {
     b->ctx = v;
     b->device = v[0]->P.device;
     b->join.assign(n, nullptr);
-    bool ok = cudaSetDevice(b->device) == cudaSuccess &&
+    DevGuard dev_guard(b->device);
+    bool ok = dev_guard.ok &&
               cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreateWithFlags(&b->root, cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess &&
@@ -892,7 +915,8 @@ int sld_batch_create(sld_batch** out, sld_ctx* const* ctxs, int n) {
 
 int sld_batch_run(sld_batch* b, int nsteps) {
     if (!b || nsteps < 0) return SLD_ERR_ARG;
-    CK(cudaSetDevice(b->device));
+    DevGuard dev_guard(b->device);
+    if (!dev_guard.ok) return SLD_ERR_CUDA;
     // the batch stream follows whatever is queued on each context's stream
     for (size_t q = 0; q < b->ctx.size(); ++q) {
         sld_ctx* c = b->ctx[q];
@@ -952,6 +976,7 @@ void sld_batch_destroy(sld_batch* b) {
 
 int sld_profile_step(sld_ctx* c, double* ms) {
     if (!c || !ms) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     if (!c->D.latt || !c->D.spin) return SLD_ERR_ARG;   // the spin-lattice step's phases
     fresh_lists(c);
     cudaEvent_t ev[2];
@@ -994,6 +1019,7 @@ int sld_profile_step(sld_ctx* c, double* ms) {
 
 int sld_step_kernel_count(sld_ctx* c, int* out) {
     if (!c || !out) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     cudaGraph_t g = nullptr;
     fresh_lists(c);
     CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
@@ -1016,6 +1042,7 @@ int sld_step_kernel_count(sld_ctx* c, int* out) {
 
 int sld_last_run_ms(sld_ctx* c, double* out) {
     if (!c || !out) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     CK(cudaEventSynchronize(c->ev1));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
@@ -1025,6 +1052,7 @@ int sld_last_run_ms(sld_ctx* c, double* out) {
 
 int sld_sync(sld_ctx* c) {
     if (!c) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     int rc = launch_status();
     if (rc) return rc;
     return check_flags(c);
@@ -1032,6 +1060,7 @@ int sld_sync(sld_ctx* c) {
 
 long sld_get(sld_ctx* c, const char* field, double* out, long cap) {
     if (!c || !field || !out) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     Dev& D = c->D;
     size_t n = (size_t)D.natom;
     std::string f(field);
@@ -1117,6 +1146,7 @@ long sld_get(sld_ctx* c, const char* field, double* out, long cap) {
 
 int sld_get_cell_lists(sld_ctx* c, int* out) {
     if (!c || !out) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     size_t n = (size_t)c->D.natom;
     CK(cudaStreamSynchronize(c->st));
     std::vector<int> h(n);
@@ -1127,6 +1157,7 @@ int sld_get_cell_lists(sld_ctx* c, int* out) {
 
 int sld_averages(sld_ctx* c, double* out10) {
     if (!c || !out10) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     launch_averages(c->D, c->st, c->d_avg);
     CK(cudaMemcpyAsync(out10, c->d_avg, sizeof(double) * 10, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -1135,6 +1166,7 @@ int sld_averages(sld_ctx* c, double* out10) {
 
 int sld_virial(sld_ctx* c, double* out) {
     if (!c || !out) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     launch_virial(c->D, c->st);
     CK(cudaMemcpyAsync(out, &c->D.ctl->virial, sizeof(double), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -1143,6 +1175,7 @@ int sld_virial(sld_ctx* c, double* out) {
 
 int sld_total_time(sld_ctx* c, double* out) {
     if (!c || !out) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     CK(cudaMemcpyAsync(out, &c->D.ctl->total_time, sizeof(double), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     return SLD_OK;
@@ -1155,6 +1188,7 @@ int sld_total_time(sld_ctx* c, double* out) {
 // check_pressure_CPU.cpp:35-59, check_spin_CPU.cpp:35-76).
 int sld_check(sld_ctx* c, const char* dir, const char* out_body, int current_step) {
     if (!c || !out_body) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     if ((current_step + 1) % c->P.interval_of_print_out != 0) return SLD_OK;
     const Dev& D = c->D;
     double* part = c->d_chk;
@@ -1247,6 +1281,7 @@ int sld_check(sld_ctx* c, const char* dir, const char* out_body, int current_ste
 int sld_write_config(sld_ctx* c, const char* dir, const char* out_body, int current_step,
                      int flags) {
     if (!c || !out_body) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     const int every = c->P.interval_of_config_out;
     if (!(current_step == -1 || current_step == -2 || (current_step + 1) % every == 0))
         return SLD_OK;
@@ -1349,6 +1384,7 @@ static void apply_box(sld_ctx* c, const double* d) {
 
 int sld_scale(sld_ctx* c, int current_step, double* out3) {
     if (!c) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     const sld_params& P = c->P;
     double t = 0.0;
     int rc = sld_total_time(c, &t);
@@ -1461,6 +1497,7 @@ static int set_per_atom(sld_ctx* c, double4** buf, double4** dev_ptr, const doub
 
 int sld_set_external_field(sld_ctx* c, const double* H) {
     if (!c) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     if (H && !c->D.spin) return SLD_ERR_ARG;
     int rc = set_per_atom(c, &c->hext_buf, &c->D.hext, H, 1.0);
     if (rc) return rc;
@@ -1483,6 +1520,7 @@ int sld_set_external_field(sld_ctx* c, const double* H) {
 
 int sld_set_external_force(sld_ctx* c, const double* f) {
     if (!c) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     if (f && !c->D.latt) return SLD_ERR_ARG;
     return set_per_atom(c, &c->fext_buf, &c->D.fext, f, 1.0);
 }
@@ -1509,6 +1547,7 @@ static int read_per_atom(sld_ctx* c, const char* path, std::vector<double>& v) {
 
 int sld_read_external_field(sld_ctx* c, const char* path) {
     if (!c) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     std::vector<double> v;
     int rc = read_per_atom(c, path, v);
     if (rc) return rc;
@@ -1519,6 +1558,7 @@ int sld_read_external_field(sld_ctx* c, const char* path) {
 
 int sld_read_external_force(sld_ctx* c, const char* path) {
     if (!c) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     std::vector<double> v;
     int rc = read_per_atom(c, path, v);
     if (rc) return rc;
@@ -1527,6 +1567,7 @@ int sld_read_external_force(sld_ctx* c, const char* path) {
 
 int sld_quantum_filter(sld_ctx* c, double* out, int n) {
     if (!c || !out) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     if (!c->D.quantum) return SLD_ERR_STATE;
     if (n < c->D.qNf2) return SLD_ERR_ARG;
     CK(cudaMemcpy(out, c->D.qH, sizeof(double) * c->D.qNf2, cudaMemcpyDeviceToHost));
@@ -1594,6 +1635,7 @@ static int trial(sld_ctx* c, const StateCopy& s, int steps, double* ms) {
 
 int sld_autotune(sld_ctx* c, int steps, int* out8) {
     if (!c || steps < 1) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     if (dynamic_step(c)) return SLD_ERR_ARG;   // no captured step to time
     StateCopy s;
     int rc = state_save(c, s);
@@ -1641,6 +1683,7 @@ int sld_autotune(sld_ctx* c, int steps, int* out8) {
 
 int sld_info(sld_ctx* c, int* o) {
     if (!c || !o) return SLD_ERR_ARG;
+    SLD_DEVICE_OF(c);
     o[0] = c->D.natom; o[1] = c->G.ncells; o[2] = c->G.ngroups; o[3] = c->G.nte;
     o[4] = c->G.nx; o[5] = c->G.ny;
     return SLD_OK;

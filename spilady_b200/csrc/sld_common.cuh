@@ -486,6 +486,9 @@ struct SweepFlow {
     const unsigned char* cell_group;  // colour group of each link cell
     int* cell_flag;                   // tag of each cell's last finished sweep
     int* sync;                        // [0] tag base of the next call, [1] next task
+    int polls;                        // bound on the polls of one cell's waits
+    int stall;                        // added to every tag a wait needs (0; a test
+                                      // sets it to make the waits run out)
 };
 bool sweep_uses_flow();
 void launch_sweep_flow(const Dev& D, cudaStream_t st, const SweepFlow& F, double dt,

@@ -67,6 +67,28 @@ struct sld_ctx {
     }
 };
 
+// Makes the context's device current for the duration of an entry point and
+// gives the caller's current device back afterwards: a context's buffers,
+// streams and graphs belong to the device it was created on, whatever device
+// the calling thread has made current since.
+struct DevGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DevGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
+        else prev = -1;   // already current: nothing to give back
+    }
+    ~DevGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    DevGuard(const DevGuard&) = delete;
+    DevGuard& operator=(const DevGuard&) = delete;
+};
+#define SLD_DEVICE_OF(c)                 \
+    DevGuard sld_dev_guard_((c)->P.device); \
+    if (!sld_dev_guard_.ok) return SLD_ERR_CUDA
+
 // the device state with buffer set k of the exchange lists and rho
 inline Dev dev_set(const sld_ctx* c, int k) {
     Dev D = c->D;

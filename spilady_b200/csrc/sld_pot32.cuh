@@ -3,11 +3,20 @@
 //
 // The FP64 form reads the reference's 10^6-point tables (built from the
 // DD05.cpp / JijFe.cpp forms, with seven-point numerical derivatives); here
-// the same functional forms and their exact derivatives are evaluated
-// directly in FP32, which needs no table traffic.  The pair term between
-// 1.8 and 2.0 A is the quintic that joins the ZBL core to the cubic knots
-// (its Hermite data is computed on the host in FP64); below 1.8 A it is the
-// ZBL screened Coulomb term itself.
+// the same functions are evaluated directly in FP32, which needs no table
+// traffic.  The values are the functional forms themselves (linear
+// interpolation between table entries 4.1e-6 A apart changes them by less
+// than FP64 rounding).  The derivatives are the reference's: its derivative
+// tables hold the seven-point central difference with step dx = x/1000
+// (potential_CPU.cpp:159-170), which for a piecewise cubic equals the exact
+// derivative except within 3 dx of a knot, where the stencil straddles the
+// knot; there the one term a (k - x)^3_+ that changes form adds the
+// stencil's difference from its exact derivative (knot_stencil32 below).
+// The embedding function F(rho) and F'(rho) are read from the reference's
+// tables per atom, in FP64.  The pair term between 1.8 and 2.0 A is the
+// quintic that joins the ZBL core to the cubic knots (its Hermite data is
+// computed on the host in FP64); below 1.8 A it is the ZBL screened Coulomb
+// term itself.
 #pragma once
 #include "sld_common.cuh"
 
@@ -24,39 +33,6 @@ struct Kahan {
     __device__ __forceinline__ double value() const { return (double)s - (double)c; }
 };
 
-// DD05 density f(r) = sum a_i (r_i - r)^3 for r < r_i, and f'(r)
-__device__ __forceinline__ void dens32(float r, float& f, float& df) {
-    const float a[6] = {0.9332056681088162f, -1.162558782567700f, -0.3502026949249225f,
-                        0.4287820835430028f, 4.907925057809273f, -5.307049068415304f};
-    const float k[6] = {3.0f, 2.8666666666666666f, 2.7333333333333333f, 2.6f, 2.4f, 2.3f};
-    f = 0.f;
-    df = 0.f;
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        float u = k[i] - r;
-        if (u > 0.f) {
-            float u2 = u * u;
-            f = fmaf(a[i] * u2, u, f);
-            df = fmaf(-3.f * a[i], u2, df);
-        }
-    }
-}
-
-// DD05 embedding F(rho) and F'(rho)
-__device__ __forceinline__ void emb32(float rho, float& F, float& dF) {
-    const float a = 4.100199340884814f, b = 1.565647547483517f;
-    const float b_ln2 = 1.565647547483517f / 0.69314718055994531f;
-    float sq = sqrtf(rho);
-    F = -a * sq;
-    dF = -0.5f * a / sq;
-    if (rho < 1.f) {
-        float l = logf(2.f - rho);
-        F -= b_ln2 * (1.f - sq) * l;
-        dF -= b_ln2 * ((-0.5f / sq) * l - (1.f - sq) / (2.f - rho));
-    }
-    (void)b;
-}
-
 __device__ __forceinline__ void zbl32(const Pot32& P, float r, float& v, float& dv) {
     const float z2 = 26.f * 26.f * 14.3992f;
     float x = r / P.zbl_as;
@@ -69,26 +45,9 @@ __device__ __forceinline__ void zbl32(const Pot32& P, float r, float& v, float& 
     dv = z2 * (ds * r - s) / (r * r);
 }
 
-// DD05 pair term phi(r) and phi'(r)
+// DD05 pair term phi(r) and phi'(r) at r <= 2 A: the ZBL core below 1.8 A
+// and the quintic join between 1.8 and 2.0 A
 __device__ __forceinline__ void pair32(const Pot32& P, float r, float& v, float& dv) {
-    const float V[8] = {-0.1960674387419232f, 0.3687525935422963f, -1.505333614924853f,
-                        4.948907078156191f,   -4.894613262753399f, 3.468897724782442f,
-                        -1.792218099820337f,  80.22069592246987f};
-    const float K[8] = {4.1f, 3.8f, 3.5f, 3.2f, 2.9f, 2.6f, 2.4f, 2.3f};
-    if (r > 2.0f) {
-        v = 0.f;
-        dv = 0.f;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            float u = K[i] - r;
-            if (u > 0.f) {
-                float u2 = u * u;
-                v = fmaf(V[i] * u2, u, v);
-                dv = fmaf(-3.f * V[i], u2, dv);
-            }
-        }
-        return;
-    }
     if (r <= 1.8f) {
         zbl32(P, r, v, dv);
         return;
@@ -107,56 +66,73 @@ __device__ __forceinline__ void pair32(const Pot32& P, float r, float& v, float&
           w * w * (g20 * P.zbl_c1 + g21 * P.knot_c2)) / w;
 }
 
-// Fe exchange J(r) = 0.870 (1 - r/3.75)^3 for r < 3.75, and J'(r)
-__device__ __forceinline__ void exch32(float r, float& J, float& dJ) {
-    const float A = 0.870f, rc = 3.75f;
-    float u = 1.f - r / rc;
-    if (u > 0.f) {
-        J = A * u * u * u;
-        dJ = -3.f * A / rc * u * u;
-    } else {
-        J = 0.f;
-        dJ = 0.f;
-    }
+// The seven-point derivative (potential_CPU.cpp:159-170) of x -> (k - x)^3_+
+// at x = r with step dx, less the exact derivative -3 (k - r)^2_+, for
+// u = k - r.  Zero (up to rounding) for |u| >= 3 dx, where the stencil sees
+// one cubic.  The terms are of size dx^3 and the result of size dx^2, so FP32
+// keeps it to about 1e-7 relative.
+__device__ __forceinline__ float cube_pos32(float x) { return x > 0.f ? x * x * x : 0.f; }
+__device__ __forceinline__ float knot_stencil32(float u, float dx) {
+    float s = 45.f * (cube_pos32(u - dx) - cube_pos32(u + dx)) -
+              9.f * (cube_pos32(u - 2.f * dx) - cube_pos32(u + 2.f * dx)) +
+              (cube_pos32(u - 3.f * dx) - cube_pos32(u + 3.f * dx));
+    float up = fmaxf(u, 0.f);
+    return s / (60.f * dx) + 3.f * up * up;
 }
-
-// One piecewise cubic (knots K[0..n), coefficients C[4*(n+1)]) at r, with
-// t = r - base formed in FP64 so that it carries FP32 relative precision.
+// One piecewise cubic (knots K[0..n) ascending, coefficients C[4*(n+1)],
+// knot amplitudes A[0..n)) at an FP32 distance r: t = r - base is exact in
+// FP32 (r and the knot are within a factor of two).  df is the reference's
+// seven-point derivative: near the knots just below and above r (knots are
+// 0.1 A or more apart, the stencil spans 6 r/1000 < 0.025 A) the stencil
+// term of that knot is added.
 __device__ __forceinline__ void cubic_eval(const float* __restrict__ K, const float* __restrict__ C,
-                                           int n, double r, float& f, float& df) {
+                                           const float* __restrict__ A, int n, float r, float& f,
+                                           float& df) {
     int m = 0;
-    for (int i = 0; i < n; ++i) m += r >= (double)__ldg(K + i);
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        if (i < n) m += r >= __ldg(K + i);
+    const float dx = r * 1e-3f;
     if (m == n) {
         f = 0.f;
         df = 0.f;
+    } else {
+        const float t = r - __ldg(K + (m == 0 ? 0 : m - 1));
+        const float* c = C + 4 * m;
+        float c0 = __ldg(c), c1 = __ldg(c + 1), c2 = __ldg(c + 2), c3 = __ldg(c + 3);
+        f = fmaf(fmaf(fmaf(c3, t, c2), t, c1), t, c0);
+        df = fmaf(fmaf(3.f * c3, t, 2.f * c2), t, c1);
+        const float ua = __ldg(K + m) - r;   // > 0
+        if (ua < 3.f * dx) df = fmaf(__ldg(A + m), knot_stencil32(ua, dx), df);
+    }
+    if (m > 0) {
+        const float ub = __ldg(K + m - 1) - r;   // <= 0
+        if (ub > -3.f * dx) df = fmaf(__ldg(A + m - 1), knot_stencil32(ub, dx), df);
+    }
+}
+
+// density f and the reference's f' at an FP32 distance
+__device__ __forceinline__ void dens32f(const Dev& D, float r, float& f, float& df) {
+    cubic_eval(D.cubic + 44, D.cubic + 50, D.cubic + 86, 6, r, f, df);
+}
+
+// pair term phi and the reference's phi' at an FP32 distance (ZBL core and
+// join below 2 A; within 3 r/1000 of 1.8 and 2.0 A the reference's stencil
+// also straddles the joins, which only close collisions reach: there the
+// exact derivative of the join is used)
+__device__ __forceinline__ void pair32f(const Dev& D, float r, float& v, float& dv) {
+    if (r > 2.0f) {
+        cubic_eval(D.cubic, D.cubic + 8, D.cubic + 78, 8, r, v, dv);
         return;
     }
-    double base = (double)__ldg(K + (m == 0 ? 0 : m - 1));
-    float t = (float)(r - base);
-    const float* c = C + 4 * m;
-    float c0 = __ldg(c), c1 = __ldg(c + 1), c2 = __ldg(c + 2), c3 = __ldg(c + 3);
-    f = fmaf(fmaf(fmaf(c3, t, c2), t, c1), t, c0);
-    df = fmaf(fmaf(3.f * c3, t, 2.f * c2), t, c1);
+    pair32(D.pot32, r, v, dv);
 }
 
-// density f and f' at an FP64 distance
-__device__ __forceinline__ void dens32r(const Dev& D, double r, float& f, float& df) {
-    cubic_eval(D.cubic + 44, D.cubic + 50, 6, r, f, df);
-}
-
-// pair term phi and phi' at an FP64 distance (ZBL core and join below 2 A)
-__device__ __forceinline__ void pair32r(const Dev& D, double r, float& v, float& dv) {
-    if (r > 2.0) {
-        cubic_eval(D.cubic, D.cubic + 8, 8, r, v, dv);
-        return;
-    }
-    pair32(D.pot32, (float)r, v, dv);
-}
-
-// exchange J and J' at an FP64 distance
-__device__ __forceinline__ void exch32r(double r, float& J, float& dJ) {
-    const float A = 0.870f, rc = 3.75f;
-    float u = (float)(1.0 - r * (1.0 / 3.75));
+// Fe exchange J(r) = 0.870 (1 - r/3.75)^3 = a (3.75 - r)^3 for r < 3.75, and
+// the reference's J'(r) (its stencil straddles the knot for |r - 3.75| < 3 dx)
+__device__ __forceinline__ void exch32f(float r, float& J, float& dJ) {
+    const float A = 0.870f, rc = 3.75f, a = 0.870f / (3.75f * 3.75f * 3.75f);
+    float u = 1.f - r * (1.f / 3.75f);
     if (u > 0.f) {
         J = A * u * u * u;
         dJ = -3.f * A / rc * u * u;
@@ -164,9 +140,29 @@ __device__ __forceinline__ void exch32r(double r, float& J, float& dJ) {
         J = 0.f;
         dJ = 0.f;
     }
+    const float dx = r * 1e-3f, uk = rc - r;
+    if (fabsf(uk) < 3.f * dx) dJ = fmaf(a, knot_stencil32(uk, dx), dJ);
 }
 
-// ---- the same forms in FP64 (the split form's error reference) ----
+// the same at an FP64 distance (rounded to FP32 first)
+__device__ __forceinline__ void dens32r(const Dev& D, double r, float& f, float& df) {
+    dens32f(D, (float)r, f, df);
+}
+__device__ __forceinline__ void pair32r(const Dev& D, double r, float& v, float& dv) {
+    pair32f(D, (float)r, v, dv);
+}
+__device__ __forceinline__ void exch32r(double r, float& J, float& dJ) { exch32f((float)r, J, dJ); }
+
+// F(rho) and F'(rho) from the reference's FP64 tables (potential_CPU.cpp:172-179)
+__device__ __forceinline__ void emb_tab(const Dev& D, double rho, double& F, double& dF) {
+    F = interp(D.tF, rho, D.inv_rho, &D.ctl->err);
+    dF = interp(D.tdF, rho, D.inv_rho, &D.ctl->err);
+}
+
+// ---- the analytic forms in FP64 with their exact derivatives ----
+// (SLD_FP64_ANALYTIC: the model the adjoint differentiates; it differs from
+// the reference's tables by the tables' seven-point derivatives near the
+// knots, about 1e-4 of the forces)
 __device__ __forceinline__ void cubic_eval64(const double* __restrict__ K, const double* __restrict__ C,
                                              int n, double r, double& f, double& df) {
     int m = 0;

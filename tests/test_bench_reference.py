@@ -15,9 +15,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 @pytest.mark.skipif(not refjob.available("langte"), reason="reference build missing")
 def test_reference_arm_prints_one_contract_line():
-    out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1",
-                          "--warmup", "1"], cwd=ROOT, capture_output=True, text=True,
-                         timeout=600)
+    # a 16^3 box here (the arm's default is the benchmark's 128^3)
+    out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--size", "16",
+                          "--steps", "1", "--warmup", "1"], cwd=ROOT, capture_output=True,
+                         text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1
@@ -42,7 +43,7 @@ def test_reference_arm_under_torchrun_prints_from_rank_zero_only():
     out = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
                           "--nproc-per-node", "2", "--master-addr", "127.0.0.1",
                           "--master-port", str(port), "bench.py", "--impl", "reference",
-                          "--gpus", "2", "--steps", "1", "--warmup", "1"],
+                          "--size", "16", "--gpus", "2", "--steps", "1", "--warmup", "1"],
                          cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]

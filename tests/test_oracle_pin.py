@@ -159,3 +159,22 @@ def test_param_build_is_the_stock_build_at_the_default_constants():
                inputs={"theta.in": " ".join("%.17g" % x for x in DEFAULT_THETA)})[0]
     b = rj.run("nve", params, r, p, s, ops=ops)[0]
     assert np.array_equal(a.atoms, b.atoms)
+
+
+@pytest.mark.skipif(not refjob.available("langte"), reason="reference build absent")
+def test_oracle_matches_live_reference_langte_20cubed():
+    # 20^3 cells: 13^3 link cells in 18 colour groups (the colour count of the
+    # 89^3 link cells of the 128^3 box); three spin-lattice-electron steps
+    # with the reference's own noise stream (MWC, one thread): bit for bit
+    params, r, p, s = initial_state(20, seed=21, tilt=0.35)
+    d = refjob.run("langte", params, r, p, s, ops=[(refjob.OP_CORE, 3), (refjob.OP_DUMP, 0)])[0]
+    o = orc.System(params, r, p, s, rng=orc.RNG_MWC, **SWITCHES["langte"])
+    assert o.ngroups == d.ngroups == 18
+    o.run(3)
+    for n in ("r", "p", "s", "f", "H", "HL"):
+        assert np.array_equal(o.get(n), d.vec(n)), n
+    for n in ("rho", "pe", "me", "me0", "ke"):
+        assert np.array_equal(o.get(n), d.a(SCAL[n])), n
+    for c in ("Te", "Tl", "Ts_L", "Ts_R"):
+        assert np.array_equal(o.get(c), d.c(c)), c
+    assert np.array_equal(o.lists(), d.lists)
