@@ -252,6 +252,50 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
+def replicas_cpu_baseline(systems, nrep=4, steps=5):
+    """The reference's own CPU build (Langevin spin + lattice) run on the
+    first ``nrep`` replicas one after another, ``steps`` steps each after one
+    warm-up step: atom-steps/s of the replicas run one by one on the host."""
+    from oracle import refjob
+    threads = os.cpu_count() or 1
+    if not refjob.available("lang"):
+        return {"value": None, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
+                "sample": "reference build absent (oracle/ref/build.sh not run)"}
+    work, secs, edges = 0, 0.0, []
+    for edge, temp, params, r, p, s in systems[:nrep]:
+        ops = [(refjob.OP_CORE, 1), (refjob.OP_STATS, 0), (refjob.OP_CORE, steps),
+               (refjob.OP_STATS, 0)]
+        d = refjob.run("lang", params, r, p, s, ops=ops, threads=threads)[-1]
+        work += r.shape[0] * steps
+        secs += d.wall
+        edges.append(edge)
+    return {"value": work / secs, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
+            "sample": f"reference CPU build (Langevin spin + lattice), replicas of edges {edges} "
+                      f"one after another, {steps} steps each after 1 warm-up step"}
+
+
+def adjoint_cpu_baseline(params, r, p, s, K, nparam=36, steps=10):
+    """What a gradient by central differences of the reference's own CPU code
+    costs: 2 x nparam K-step NVE trajectories of its param build (the
+    potential's constants read from a file), estimated from ``steps`` timed
+    steps after one warm-up step.  Returns ms per gradient."""
+    from oracle import refjob
+    threads = os.cpu_count() or 1
+    if not refjob.available("param"):
+        return {"value": None, "unit": "ms", "cores": threads, "kind": "reference",
+                "sample": "reference build absent (oracle/ref/build.sh not run)"}
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_golden import DEFAULT_THETA
+    ops = [(refjob.OP_CORE, 1), (refjob.OP_STATS, 0), (refjob.OP_CORE, steps), (refjob.OP_STATS, 0)]
+    d = refjob.run("param", params, r, p, s, ops=ops, threads=threads,
+                   inputs={"theta.in": " ".join("%.17g" % x for x in DEFAULT_THETA)})[-1]
+    per_step = d.wall / steps
+    return {"value": 2 * nparam * K * per_step * 1e3, "unit": "ms", "cores": threads,
+            "kind": "reference",
+            "sample": f"reference CPU build (param, NVE), {r.shape[0]} atoms, {steps} timed steps "
+                      f"({per_step * 1e3:.1f} ms each) x {2 * nparam} trajectories x {K} steps"}
+
+
 def replicas_workload(n, seed=2027):
     """n independent bcc Fe boxes: cubic edge uniform on 8..32 cells,
     temperature uniform on 100..1200 K, Langevin spin and lattice
@@ -306,6 +350,9 @@ def run_replicas(args, world, rank, local):
         per.append({"edge": edge, "natom": e.natom, "T_K": temp, "Tl_K": a["Tl"],
                     "m": float(np.sqrt(a["sx"] ** 2 + a["sy"] ** 2 + a["sz"] ** 2))})
     kernels = sum(e.step_kernel_count() for e in engines)
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = replicas_cpu_baseline(systems)
     batch.close()
     for e in engines:
         e.close()
@@ -328,7 +375,7 @@ def run_replicas(args, world, rank, local):
         "one_by_one": {"value": natom * args.steps * world / (seq_ms / 1e3),
                        "ms_per_step": seq_ms / args.steps,
                        "how": "each replica's own graph replays, one replica after another"},
-        "roofline": None, "cpu_baseline": None, "e2e": None,
+        "roofline": None, "cpu_baseline": cpu, "e2e": None,
         "gpu_launches": kernels * args.steps, "clocks": clk,
     }
     print(json.dumps(line))
@@ -397,6 +444,7 @@ def run_adjoint(args, world, rank, local):
     fdB = fd(lambda t: e64.adjoint_trajectory(t, K, C, grad=False), 50.0)
     fdTR = (4.0 * fdB - fdA) / 3.0
     _, dLk64 = e64.adjoint_trajectory(th, K, C)
+    cpu = None if args.no_cpu_baseline else adjoint_cpu_baseline(params, r, p, s, K)
     line = {
         "metric": f"ms per gradient of L in 36 potential parameters through {K} NVE steps, "
                   f"{e.natom}-atom bcc Fe",
@@ -417,7 +465,7 @@ def run_adjoint(args, world, rank, local):
                                   "how": "max |adjoint - FD| / max |FD| over the 36 parameters; "
                                          "FD: FP64 central differences, h = 1e-6 relative; "
                                          "richardson: from h = 1e-4 and 5e-5 relative"},
-        "roofline": None, "cpu_baseline": None, "e2e": None,
+        "roofline": None, "cpu_baseline": cpu, "e2e": None,
     }
     print(json.dumps(line))
 

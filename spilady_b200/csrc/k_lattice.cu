@@ -256,10 +256,15 @@ __global__ void __launch_bounds__(256) k_dr(Dev D, double dt) {
     if (i >= D.natom) return;
     double k = dt / D.atmass;
     double4 r = D.r[i], p = D.p[i];
-    double3 x = periodic(D, make_double3(r.x + k * p.x, r.y + k * p.y, r.z + k * p.z));
+    const double3 u = make_double3(r.x + k * p.x, r.y + k * p.y, r.z + k * p.z);
+    double3 x = periodic(D, u);
     if (!isfinite(x.x + x.y + x.z)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
     D.r[i] = make_double4(x.x, x.y, x.z, 0.0);
-    D.r32s[D.cell_slot[i]] = make_float4((float)x.x, (float)x.y, (float)x.z, 0.f);
+    // the FP32 copy keeps the unwrapped position, relative to the cell the
+    // atom is linked in until the next links
+    const int4 q = cell_fix(D, D.cell_of[i], u.x, u.y, u.z);
+    D.fxs[D.cell_slot[i]] = q;
+    if (D.fxa) D.fxa[i] = q;
 }
 
 // quantum_noise_CPU.cpp:56-72 for every degree of freedom at once (their
@@ -365,7 +370,9 @@ __global__ void __launch_bounds__(256) k_scale_positions(Dev D, double factor) {
     double4 r = D.r[i];
     double x = __dmul_rn(factor, r.x), y = __dmul_rn(factor, r.y), z = __dmul_rn(factor, r.z);
     D.r[i] = make_double4(x, y, z, 0.0);
-    D.r32s[D.cell_slot[i]] = make_float4((float)x, (float)y, (float)z, 0.f);
+    const int4 q = cell_fix(D, D.cell_of[i], x, y, z);
+    D.fxs[D.cell_slot[i]] = q;
+    if (D.fxa) D.fxa[i] = q;
 }
 
 // scale_stress_CPU.cpp:66-80: fractional coordinates from the old inverse
@@ -384,7 +391,9 @@ __global__ void __launch_bounds__(256) k_reshape_positions(Dev D, InvBox old) {
     double y = __dadd_rn(__dmul_rn(d[2], qy), __dmul_rn(d[4], qz));
     double z = __dmul_rn(d[5], qz);
     D.r[i] = make_double4(x, y, z, 0.0);
-    D.r32s[D.cell_slot[i]] = make_float4((float)x, (float)y, (float)z, 0.f);
+    const int4 q = cell_fix(D, D.cell_of[i], x, y, z);
+    D.fxs[D.cell_slot[i]] = q;
+    if (D.fxa) D.fxa[i] = q;
 }
 
 void launch_scale_positions(const Dev& D, cudaStream_t st, double factor) {

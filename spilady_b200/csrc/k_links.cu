@@ -158,7 +158,9 @@ __global__ void k_cellsort(Dev D) {
         int i = a[k];
         D.cell_slot[i] = st + k;
         double4 r = D.r[i];
-        D.r32s[st + k] = make_float4((float)r.x, (float)r.y, (float)r.z, 0.f);
+        const int4 q = cell_fix(D, c, r.x, r.y, r.z);
+        D.fxs[st + k] = q;
+        if (D.fxa) D.fxa[i] = q;
     }
 }
 

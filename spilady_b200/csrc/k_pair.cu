@@ -1,5 +1,5 @@
-// Pair passes, FP64 form: the per-step neighbour lists with the EAM density,
-// and the force/energy pass.
+// Pair passes: the per-step neighbour lists with the EAM density, and the
+// force/energy pass.
 //
 // The reference finds pairs by walking link cells in every pass: a half
 // shell with OpenMP atomics for rho and forces (calculate_rho_CPU.cpp:33-69,
@@ -10,10 +10,14 @@
 // and records every pair within rcut_max (nbr) and every exchange pair
 // within rcut_mag with its J(r_ij) (jl/jv); the force pass, the spin sweeps
 // and calculate_temperature then read those lists.  Each thread owns one
-// atom and gathers its full shell, so there are no atomics.  The minimum
-// image is applied with the reference's arithmetic (find_image) and only to
-// pairs whose cells are neighbours across the periodic boundary; for all
-// other pairs the reference's find_image leaves the vector unchanged.
+// atom and gathers its full shell, so there are no atomics.
+//
+// Candidates are tested on fixed-point positions relative to their link
+// cell (fxs, cell_fix): the pair vector of an atom and a candidate in
+// neighbour cell k is M (f_i - f_j - delta_k), exact in integers up to the
+// products with the cell matrix, so a neighbour cell across the periodic
+// boundary is its nearest image and the FP32 vector has one rounding per
+// term, whatever the box.
 #include <algorithm>
 #include <cstdlib>
 
@@ -27,41 +31,45 @@ __device__ __forceinline__ double3 pair_d(const Dev& D, double4 ri, int pk) {
     return d;
 }
 
-// MODE 0: FP64 tables (the reference's arithmetic); 1: split form (FP32
-// analytic); 2: the analytic forms in FP64.
+// find_image_CPU.cpp:31-53 with a flag: true when it moved the vector
+__device__ __forceinline__ double3 find_image_f(const Dev& D, double3 rij, bool& moved) {
+    double3 q = to_frac(D, rij.x, rij.y, rij.z);
+    int idx = 0;
+    if (q.x < -0.5) { q.x += 1.0; ++idx; }
+    if (q.x >= 0.5) { q.x -= 1.0; ++idx; }
+    if (q.y < -0.5) { q.y += 1.0; ++idx; }
+    if (q.y >= 0.5) { q.y -= 1.0; ++idx; }
+    if (q.z < -0.5) { q.z += 1.0; ++idx; }
+    if (q.z >= 0.5) { q.z -= 1.0; ++idx; }
+    moved = idx != 0;
+    return moved ? to_cart(D, q) : rij;
+}
+
+// ---------------------------------------------------------------------
+// FP64 forms.  MODE 0: the reference's tables; 2: the analytic forms in
+// FP64 with exact derivatives.
 //
 // Two passes per atom.  The first walks the 27 cells with a loose cutoff
-// test in FP32 on the cell-ordered FP32 positions (one contiguous 16-byte
-// load and a few FP32 operations per candidate; a neighbour cell across the
-// box is shifted by its box vector), writing the slots that pass to the
-// atom's list in traversal order.  The second walks that list, applies the
-// reference's exact test (FP64 pair vector with find_image), compacts the
-// list in place to the atom indices that pass, and does the per-pair work
-// (density, exchange list).  The lists and sums are those of one exact pass.
-// In one pass, some lane of a warp accepts almost every candidate (about 26
-// of 162 pass), so the per-pair body would run, divergent, for nearly every
-// candidate of every lane.
+// test in FP32 on the cell-relative positions (one contiguous 16-byte load
+// and a few FP32 operations per candidate), writing the slots that pass to
+// the atom's list in traversal order.  The second walks that list, applies
+// the reference's exact test (FP64 pair vector of the positions with
+// find_image, which the reference applies to every pair and which leaves a
+// vector that needs no image unchanged), compacts the list in place to the
+// atom indices that pass (with SLD_WRAP where find_image moved the vector),
+// and does the per-pair work (density, exchange list).  The lists and sums
+// are those of one exact pass.  In one pass, some lane of a warp accepts
+// almost every candidate (about 26 of 162 pass), so the per-pair body would
+// run, divergent, for nearly every candidate of every lane.
 //
 // The loose test keeps every pair the exact one keeps: with coordinates
 // below B in magnitude, each FP32 rounding moves a coordinate by at most
-// e = ulp(B)/2; a pair-vector component collects four of them (two
-// positions, the box shift, the difference), so r^2 near the cutoff moves by
-// at most 2 r_max (4 sqrt(3) e) + (4 sqrt(3) e)^2 plus the FP32 rounding of
-// the sum.  D.pair_loose, set on the host from the box, is twice that.
-
-template <int MODE>
-__device__ __forceinline__ bool pair_accept(const Dev& D, double3 d) {
-    if constexpr (MODE == 1) {
-        float dx = (float)d.x, dy = (float)d.y, dz = (float)d.z;
-        return dx * dx + dy * dy + dz * dz < (float)D.rcut_max_sq;
-    } else {
-        return d.x * d.x + d.y * d.y + d.z * d.z < D.rcut_max_sq;
-    }
-}
-
+// e = ulp(B)/2; a pair-vector component collects five of them (two
+// positions, the cell offset, two differences), so r^2 near the cutoff moves
+// by at most 2 r_max (5 sqrt(3) e) + (5 sqrt(3) e)^2 plus the FP32 rounding of
+// the sum.  D.pair_loose, set on the host from the cell size, is twice that.
 template <int MODE>
 __device__ void pairs_one(const Dev& D, int i, int write_rho) {
-    constexpr bool SPLIT = MODE == 1;
     unsigned* err = &D.ctl->err;
     const int N = D.natom;
     const double4 ri = D.r[i];
@@ -70,117 +78,72 @@ __device__ void pairs_one(const Dev& D, int i, int write_rho) {
     // pass 1: loose cutoff test in the reference's traversal order
     int nn = 0;
     const int myslot = D.cell_slot[i];
-    auto keep = [&](int slot, bool wrap) {
-        if (nn < SLD_MAXNB) D.nbr[(size_t)nn * N + i] = slot | (wrap ? SLD_WRAP : 0);
-        ++nn;
-    };
-    if (!D.small_grid) {
-        const float rx = (float)ri.x, ry = (float)ri.y, rz = (float)ri.z;
+    {
+        const int4 fi = __ldg(D.fxs + myslot);
+        const FxMat M = fx_mat(D);
         const float cut = (float)D.rcut_max_sq + D.pair_loose;
-        const float ax = (float)D.d[0];
-        const float bx = (float)D.d[1], by = (float)D.d[2];
-        const float qx = (float)D.d[3], qy = (float)D.d[4], qz = (float)D.d[5];
         for (int k = 0; k < 27; ++k) {
-            int sx = 0, sy = 0, sz = 0;
-            const int c = k == 26 ? c0 : nbr_cell_s(D, cx, cy, cz, k, sx, sy, sz);
-            const bool wrap = (sx | sy | sz) != 0;
-            // this atom seen from the neighbour cell's image (its atoms
-            // + sx a + sy b + sz c)
-            const float ex = rx - (sx * ax + sy * bx + sz * qx);
-            const float ey = ry - (sy * by + sz * qy);
-            const float ez = rz - sz * qz;
+            const int c = k == 26 ? c0 : nbr_cell(D, cx, cy, cz, k);
+            // this atom seen from the neighbour cell
+            const int ex = fi.x - kNbr[k][0] * SLD_FX_ONE, ey = fi.y - kNbr[k][1] * SLD_FX_ONE,
+                      ez = fi.z - kNbr[k][2] * SLD_FX_ONE;
             const int st = __ldg(D.cell_start + c), n = min(__ldg(D.cell_count + c), SLD_MAXC);
             for (int m0 = 0; m0 < n; m0 += 4) {
-                float4 q[4];
+                int4 q[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
-                    q[u] = m0 + u < n ? __ldg(D.r32s + st + m0 + u) : make_float4(1e30f, 0.f, 0.f, 0.f);
+                    q[u] = m0 + u < n ? __ldg(D.fxs + st + m0 + u) : make_int4(ex, ey, ez, 0);
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int slot = st + m0 + u;
-                    const float dx = ex - q[u].x, dy = ey - q[u].y, dz = ez - q[u].z;
-                    if (dx * dx + dy * dy + dz * dz < cut && slot != myslot) keep(slot, wrap);
+                    const float3 d = fx_vec(M, ex - q[u].x, ey - q[u].y, ez - q[u].z);
+                    if (m0 + u < n && d.x * d.x + d.y * d.y + d.z * d.z < cut && slot != myslot) {
+                        if (nn < SLD_MAXNB) D.nbr[(size_t)nn * N + i] = slot;
+                        ++nn;
+                    }
                 }
-            }
-        }
-    } else {
-        // three cells along an axis: the image is the reference's minimum
-        // image of each pair
-        for (int k = 0; k < 27; ++k) {
-            bool wrap = false;
-            const int c = k == 26 ? c0 : nbr_cell_w(D, cx, cy, cz, k, wrap);
-            const int st = D.cell_start[c], n = cell_n(D, c);
-            for (int m = 0; m < n; ++m) {
-                const int slot = st + m;
-                if (slot == myslot) continue;
-                const double4 rj = D.r[D.cell_atoms[slot]];
-                if (pair_accept<MODE>(
-                        D, find_image(D, make_double3(ri.x - rj.x, ri.y - rj.y, ri.z - rj.z))))
-                    keep(slot, true);
             }
         }
     }
     const int nl = nn < SLD_MAXNB ? nn : SLD_MAXNB;
-    // pass 2: density and exchange list over the accepted pairs
+    // pass 2: the exact test, density and exchange list over the candidates
     double rho = 0.0;
-    Kahan rho32;
-    const float rmag2f = (float)D.rcut_mag_sq;
-    const float rpotf = (float)D.rcut_pot;
     int nj = 0, w = 0;
     for (int e = 0; e < nl; ++e) {
         const int ps = D.nbr[(size_t)e * N + i];
-        const int j = D.cell_atoms[ps & SLD_JMASK];
-        const int pk = j | (ps & SLD_WRAP);
-        double3 d = pair_d(D, ri, pk);
-        if (!pair_accept<MODE>(D, d)) continue;
-        D.nbr[(size_t)w * N + i] = pk;
+        const int j = D.cell_atoms[ps];
+        const double4 rj = D.r[j];
+        bool moved;
+        const double3 d = find_image_f(D, make_double3(ri.x - rj.x, ri.y - rj.y, ri.z - rj.z), moved);
+        const double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
+        if (!(rsq < D.rcut_max_sq)) continue;
+        D.nbr[(size_t)w * N + i] = j | (moved ? SLD_WRAP : 0);
         ++w;
-        if constexpr (!SPLIT) {
-            double rsq = d.x * d.x + d.y * d.y + d.z * d.z;
-            double r0 = sqrt(rsq);
-            if (r0 < D.rcut_pot) {
-                if constexpr (MODE == 0) {
-                    rho += interp(D.tf, r0, D.inv_r, err);
-                } else {
-                    double f, df;
-                    dens64(D, r0, f, df);
-                    rho += f;
-                }
+        double r0 = sqrt(rsq);
+        if (r0 < D.rcut_pot) {
+            if constexpr (MODE == 0) {
+                rho += interp(D.tf, r0, D.inv_r, err);
+            } else {
+                double f, df;
+                dens64(D, r0, f, df);
+                rho += f;
             }
-            if (rsq < D.rcut_mag_sq) {
-                if (nj < SLD_MAXJ) {
-                    D.jl[(size_t)i * SLD_MAXJ + nj] = j;
-                    double J, dJ;
-                    if constexpr (MODE == 0) J = interp(D.tJ, r0, D.inv_r, err);
-                    else exch64(r0, J, dJ);
-                    D.jv[(size_t)i * SLD_MAXJ + nj] = J;
-                }
-                ++nj;
+        }
+        if (rsq < D.rcut_mag_sq) {
+            if (nj < SLD_MAXJ) {
+                D.jl[(size_t)i * SLD_MAXJ + nj] = j;
+                double J, dJ;
+                if constexpr (MODE == 0) J = interp(D.tJ, r0, D.inv_r, err);
+                else exch64(r0, J, dJ);
+                D.jv[(size_t)i * SLD_MAXJ + nj] = J;
             }
-        } else {
-            float dx = (float)d.x, dy = (float)d.y, dz = (float)d.z;
-            float rsq = dx * dx + dy * dy + dz * dz;
-            double r64 = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
-            float f, df;
-            if ((float)r64 < rpotf) {
-                dens32r(D, r64, f, df);
-                rho32.add(f);
-            }
-            if (rsq < rmag2f) {
-                if (nj < SLD_MAXJ) {
-                    float J, dJ;
-                    exch32r(r64, J, dJ);
-                    D.jl[(size_t)i * SLD_MAXJ + nj] = j;
-                    D.jvf[(size_t)i * SLD_MAXJ + nj] = J;
-                }
-                ++nj;
-            }
+            ++nj;
         }
     }
     if (nn > SLD_MAXNB || nj > SLD_MAXJ) atomicOr(err, SLD_FLAG_CAPACITY);
     D.nbr_n[i] = w;
     D.jl_n[i] = nj < SLD_MAXJ ? nj : SLD_MAXJ;
-    if (write_rho) D.rho[i] = SPLIT ? rho32.value() : rho;
+    if (write_rho) D.rho[i] = rho;
 }
 
 template <int MODE>
@@ -188,6 +151,107 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, int write_rho) {
     // one atom per thread; a capped grid walks several atoms per thread
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x)
         pairs_one<MODE>(D, i, write_rho);
+}
+
+// ---------------------------------------------------------------------
+// Split form: pair distances in FP32 from the cell-relative positions.
+//
+// Pass 1 walks the 27 cells and keeps every candidate with |d|^2 < rcut_max^2
+// in FP32 (its slot and neighbour cell k, packed slot | k << 27); pass 2
+// forms the same d again from the list, writes the atom index (nbr, with
+// SLD_WRAP on every entry so that FP64 readers apply find_image, which
+// leaves a vector that needs no image unchanged) and k (nbk), and adds the
+// density and the exchange row.  A pair within a few 1e-7 A of the cutoff
+// may be kept or dropped otherwise than in FP64; every term is zero there
+// (the density and pair terms' last knots, 3.0 and 4.1 A, and the exchange's
+// 3.75 A lie inside the cutoffs).
+#define SLD_SPLIT_SLOT_BITS 27
+__device__ void pairs_split_one(const Dev& D, int i, int write_rho) {
+    const int N = D.natom;
+    int c0 = D.cell_of[i], cx, cy, cz;
+    cell_xyz(D, c0, cx, cy, cz);
+    const int myslot = D.cell_slot[i];
+    const int4 fi = __ldg(D.fxs + myslot);
+    const FxMat M = fx_mat(D);
+    const float cut = (float)D.rcut_max_sq;
+    int nn = 0;
+    for (int k = 0; k < 27; ++k) {
+        const int c = k == 26 ? c0 : nbr_cell(D, cx, cy, cz, k);
+        const int ex = fi.x - kNbr[k][0] * SLD_FX_ONE, ey = fi.y - kNbr[k][1] * SLD_FX_ONE,
+                  ez = fi.z - kNbr[k][2] * SLD_FX_ONE;
+        const int st = __ldg(D.cell_start + c), n = min(__ldg(D.cell_count + c), SLD_MAXC);
+        for (int m0 = 0; m0 < n; m0 += 4) {
+            int4 q[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                q[u] = m0 + u < n ? __ldg(D.fxs + st + m0 + u) : make_int4(ex, ey, ez, 0);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int slot = st + m0 + u;
+                const float3 d = fx_vec(M, ex - q[u].x, ey - q[u].y, ez - q[u].z);
+                if (m0 + u < n && d.x * d.x + d.y * d.y + d.z * d.z < cut && slot != myslot) {
+                    if (nn < SLD_MAXNB)
+                        D.nbr[(size_t)nn * N + i] =
+                            (int)((unsigned)slot | ((unsigned)k << SLD_SPLIT_SLOT_BITS));
+                    ++nn;
+                }
+            }
+        }
+    }
+    const int nl = nn < SLD_MAXNB ? nn : SLD_MAXNB;
+    Kahan rho;
+    const float rmag2 = (float)D.rcut_mag_sq, rpot = (float)D.rcut_pot;
+    int nj = 0;
+    for (int e0 = 0; e0 < nl; e0 += 4) {
+        int sb[4], kb[4], jb[4];
+        int4 qb[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int ps = e0 + u < nl ? D.nbr[(size_t)(e0 + u) * N + i] : 0;
+            sb[u] = ps & ((1 << SLD_SPLIT_SLOT_BITS) - 1);
+            kb[u] = (unsigned)ps >> SLD_SPLIT_SLOT_BITS;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            jb[u] = e0 + u < nl ? __ldg(D.cell_atoms + sb[u]) : 0;
+            qb[u] = __ldg(D.fxs + sb[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (e0 + u >= nl) break;
+            const int e = e0 + u, k = kb[u];
+            const float3 d = fx_vec(M, fi.x - kNbr[k][0] * SLD_FX_ONE - qb[u].x,
+                                    fi.y - kNbr[k][1] * SLD_FX_ONE - qb[u].y,
+                                    fi.z - kNbr[k][2] * SLD_FX_ONE - qb[u].z);
+            const float rsq = d.x * d.x + d.y * d.y + d.z * d.z;
+            const float r = sqrtf(rsq);
+            D.nbr[(size_t)e * N + i] = jb[u] | SLD_WRAP;
+            D.nbk[(size_t)e * N + i] = (unsigned char)k;
+            if (r < rpot) {
+                float f, df;
+                dens32f(D, r, f, df);
+                rho.add(f);
+            }
+            if (rsq < rmag2) {
+                if (nj < SLD_MAXJ) {
+                    float J, dJ;
+                    exch32f(r, J, dJ);
+                    D.jl[(size_t)i * SLD_MAXJ + nj] = jb[u];
+                    D.jvf[(size_t)i * SLD_MAXJ + nj] = J;
+                }
+                ++nj;
+            }
+        }
+    }
+    if (nn > SLD_MAXNB || nj > SLD_MAXJ) atomicOr(&D.ctl->err, SLD_FLAG_CAPACITY);
+    D.nbr_n[i] = nl;
+    D.jl_n[i] = nj < SLD_MAXJ ? nj : SLD_MAXJ;
+    if (write_rho) D.rho[i] = rho.value();
+}
+
+__global__ void __launch_bounds__(128) k_pairs_split(Dev D, int write_rho) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x)
+        pairs_split_one(D, i, write_rho);
 }
 
 // F'(rho) per atom (the force pass needs it for both atoms of every pair):
@@ -352,69 +416,92 @@ __device__ __forceinline__ void force64_one(const Dev& D, int i) {
     force_finish<PART>(D, i, si_sq, rho_i, F_i, fx, fy, fz, pe, me, me0, vir, st6);
 }
 
-// split form: FP32 pair terms from the analytic potential, Kahan sums
 template <bool AN, int PART>
 __global__ void __launch_bounds__(128) k_force64(Dev D) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x)
         force64_one<AN, PART>(D, i);
 }
 
+// Split form: FP32 pair vectors from the fixed-point cell positions (fxa, the
+// neighbour cell of each entry in nbk), the potential's FP32 forms with the
+// reference's derivatives, compensated (Kahan) FP32 sums for the forces and
+// energies; the stress and virial products (FP32) are summed in FP64.  Four
+// entries' loads are issued together.
 template <int PART>
 __device__ __forceinline__ void force32_one(const Dev& D, int i) {
     const int N = D.natom;
-    double4 ri = D.r[i];
+    const int4 fi = __ldg(D.fxa + i);
+    const FxMat M = fx_mat(D);
     double4 si = (PART & PART_MAG) ? D.s[i] : make_double4(0, 0, 0, 0);
     double si_sq = si.x * si.x + si.y * si.y + si.z * si.z;
     float sx = (float)si.x, sy = (float)si.y, sz = (float)si.z;
     float si_sqf = sx * sx + sy * sy + sz * sz;
     double rho_i = D.rho[i];
     float dF_i = (PART & PART_EAM) ? (float)D.dF[i] : 0.f;
-    const float rpot = (float)D.rcut_pot, rmag = (float)D.rcut_mag;
+    const float rpot = (float)D.rcut_pot, rmag2 = (float)D.rcut_mag_sq;
     Kahan fx, fy, fz, pe, me, me0;
-    float vir = 0.f, st6f[6] = {0, 0, 0, 0, 0, 0};
-    int nn = D.nbr_n[i];
-    for (int e = 0; e < nn; ++e) {
-        int pk = D.nbr[(size_t)e * N + i];
-        int j = pk & SLD_JMASK;
-        double3 dd = pair_d(D, ri, pk);
-        float dx = (float)dd.x, dy = (float)dd.y, dz = (float)dd.z;
-        double r64 = sqrt(dd.x * dd.x + dd.y * dd.y + dd.z * dd.z);
-        float r0 = (float)r64, rsq = r0 * r0;
-        float dudr = 0.f;
-        if ((PART & PART_EAM) && r0 < rpot) {
-            float f, df, phi, dphi;
-            dens32r(D, r64, f, df);
-            pair32r(D, r64, phi, dphi);
-            dudr = (dF_i + (float)D.dF[j]) * df + dphi;
-            pe.add(0.5f * phi);
+    double st[6] = {0, 0, 0, 0, 0, 0}, vir = 0.0;
+    const int nn = D.nbr_n[i];
+    for (int e0 = 0; e0 < nn; e0 += 4) {
+        int jb[4], kb[4];
+        int4 qb[4];
+        float4 sb[4];
+        float dFb[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const bool in = e0 + u < nn;
+            jb[u] = in ? (D.nbr[(size_t)(e0 + u) * N + i] & SLD_JMASK) : i;
+            kb[u] = in ? D.nbk[(size_t)(e0 + u) * N + i] : 26;
         }
-        if ((PART & PART_MAG) && r0 < rmag) {
-            const float4 sj4 = D.s32[j];   // (float) of the spin
-            float tx = sj4.x, ty = sj4.y, tz = sj4.z;
-            float sj_sq = tx * tx + ty * ty + tz * tz;
-            float dot = sx * tx + sy * ty + sz * tz;
-            float times = sqrtf(si_sqf * sj_sq);
-            float J, dJ;
-            exch32r(r64, J, dJ);
-            dudr += -dJ * (dot - times);
-            float Jh = 0.5f * J;
-            me0.add(Jh * times);
-            me.add(-Jh * dot);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            qb[u] = __ldg(D.fxa + jb[u]);
+            dFb[u] = (PART & PART_EAM) ? (float)__ldg(D.dF + jb[u]) : 0.f;
+            sb[u] = (PART & PART_MAG) ? __ldg(D.s32 + jb[u]) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        if (dudr == 0.f && PART != PART_ALL) continue;
-        float force = -dudr / r0;
-        float gx = force * dx, gy = force * dy, gz = force * dz;
-        fx.add(gx); fy.add(gy); fz.add(gz);
-        st6f[0] += gx * dx; st6f[1] += gy * dy; st6f[2] += gz * dz;
-        st6f[3] += gx * dy; st6f[4] += gy * dz; st6f[5] += gz * dx;
-        vir += -force * rsq;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (e0 + u >= nn) break;
+            const int k = kb[u];
+            const float3 d = fx_vec(M, fi.x - kNbr[k][0] * SLD_FX_ONE - qb[u].x,
+                                    fi.y - kNbr[k][1] * SLD_FX_ONE - qb[u].y,
+                                    fi.z - kNbr[k][2] * SLD_FX_ONE - qb[u].z);
+            const float dx = d.x, dy = d.y, dz = d.z;
+            const float rsq = dx * dx + dy * dy + dz * dz;
+            const float r0 = sqrtf(rsq);
+            float dudr = 0.f;
+            if ((PART & PART_EAM) && r0 < rpot) {
+                float f, df, phi, dphi;
+                dens32f(D, r0, f, df);
+                pair32f(D, r0, phi, dphi);
+                dudr = (dF_i + dFb[u]) * df + dphi;
+                pe.add(0.5f * phi);
+            }
+            if ((PART & PART_MAG) && rsq < rmag2) {
+                const float tx = sb[u].x, ty = sb[u].y, tz = sb[u].z;
+                float sj_sq = tx * tx + ty * ty + tz * tz;
+                float dot = sx * tx + sy * ty + sz * tz;
+                float times = sqrtf(si_sqf * sj_sq);
+                float J, dJ;
+                exch32f(r0, J, dJ);
+                dudr += -dJ * (dot - times);
+                float Jh = 0.5f * J;
+                me0.add(Jh * times);
+                me.add(-Jh * dot);
+            }
+            if (dudr == 0.f && PART != PART_ALL) continue;
+            const float force = -dudr / r0;
+            const float gx = force * dx, gy = force * dy, gz = force * dz;
+            fx.add(gx); fy.add(gy); fz.add(gz);
+            st[0] += (double)(gx * dx); st[1] += (double)(gy * dy); st[2] += (double)(gz * dz);
+            st[3] += (double)(gx * dy); st[4] += (double)(gy * dz); st[5] += (double)(gz * dx);
+            vir += (double)(-force * rsq);
+        }
     }
     double F = 0.0;
     if (PART & PART_EAM) F = interp(D.tF, rho_i, D.inv_rho, &D.ctl->err);
-    double st6[6];
-    for (int k = 0; k < 6; ++k) st6[k] = st6f[k];
     force_finish<PART>(D, i, si_sq, rho_i, F, fx.value(), fy.value(), fz.value(),
-                       pe.value(), me.value(), me0.value(), (double)vir, st6);
+                       pe.value(), me.value(), me0.value(), vir, st);
 }
 
 template <int PART>
@@ -453,7 +540,7 @@ void launch_pairs(const Dev& D, cudaStream_t st, bool write_rho) {
     int w = write_rho ? 1 : 0;
     const int bs = D.tune.pair_block > 0 ? D.tune.pair_block : 128;
     int nb = capped_grid(div_up(D.natom, bs), D.tune.pair_cap);
-    if (D.split) k_pairs<1><<<nb, bs, 0, st>>>(D, w);
+    if (D.split) k_pairs_split<<<nb, bs, 0, st>>>(D, w);
     else if (D.analytic) k_pairs<2><<<nb, bs, 0, st>>>(D, w);
     else k_pairs<0><<<nb, bs, 0, st>>>(D, w);
 }

@@ -6,19 +6,9 @@
 // (calculate_spin_CPU.cpp:33-199) evaluates Heff_H = sum_j J(r_ij) s_j with
 // the spins as they are at that moment.  Cells of one colour share no
 // neighbour, so during a group's launch every spin outside the group's cells
-// is frozen and only a cell's own atoms change while it is walked.  Each block
-// takes 32 cells of the group and works in three phases:
-//   A  one thread per atom: from the exchange list, sum the field of the
-//      neighbours outside the atom's cell (frozen), note the in-cell
-//      neighbours, and draw the visit's noise (counter-based, so the draw
-//      does not depend on the order);
-//   B  one thread per cell: walk the cell in the reference's order, add the
-//      in-cell neighbours' current spins (kept in shared memory) and apply the
-//      integrator (FP64);
-//   C  one thread per atom: write the spins back.
-// A block whose cells hold more atoms (or in-cell neighbours) than its
-// shared-memory tables falls back to one thread per cell reading everything
-// from global memory, with the same arithmetic.
+// is frozen and only a cell's own atoms change while it is walked: a thread
+// walks one cell.  The walks (below) differ in how a visit's neighbour spins
+// reach the thread.
 #include <algorithm>
 #include <cstdlib>
 #include <type_traits>
@@ -26,27 +16,11 @@
 #include "sld_pot32.cuh"
 #include "sld_spin.cuh"
 
-#define SW_CPB 32
-#define SW_THREADS 256
-#define SW_MAXA 256
-#define SW_MAXIN 12
 // the sweep kernels' `backward` argument: bit 0 the backward sweep (tail ->
 // head, the second visit record); bit 1 no H, HL, sum J stores (the step
 // graph overwrites them later in the same step)
 #define SW_BACKWARD 1
 #define SW_NO_FIELDS 2
-
-struct SweepShared {
-    double s[SW_MAXA][4];           // current spin, |s|
-    double h[SW_MAXA][4];           // field of the out-of-cell neighbours, sum J|s|
-    double aux[SW_MAXA][4];         // rho, noise increment x y z
-    double inJ[SW_MAXA][SW_MAXIN];  // J of the in-cell neighbours
-    int slot[SW_MAXA];
-    unsigned char inq[SW_MAXA][SW_MAXIN];   // their position in the cell list
-    unsigned char inn[SW_MAXA];
-    int cell[SW_CPB], cell_n[SW_CPB], cell_start[SW_CPB], cell_base[SW_CPB];
-    int total, overflow;
-};
 
 __device__ __forceinline__ void visit_store(const Dev& D, int i, double3 s, double3 H, double3 HL,
                                             double sumJ, bool fields) {
@@ -105,124 +79,14 @@ __device__ void visit_global(const Dev& D, int i, double dt, int sweep, bool fie
     visit_store(D, i, s, H, HL, sumJ, fields);
 }
 
-__global__ void __launch_bounds__(SW_THREADS) k_sweep(Dev D, const int* __restrict__ gcells,
-                                                      int ncell_g, double dt, int backward) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    SweepShared& S = *reinterpret_cast<SweepShared*>(smem_raw);
-    const int cbeg = blockIdx.x * SW_CPB;
-    const int ncb = min(SW_CPB, ncell_g - cbeg);
-    const bool bwd = (backward & SW_BACKWARD) != 0;
-    const bool fields = bwd && !(backward & SW_NO_FIELDS);   // the backward sweep is each atom's last visit
-    if (threadIdx.x < 32) {
-        int lane = threadIdx.x, n = 0, st = 0, c = -1;
-        if (lane < ncb) {
-            c = gcells[cbeg + lane];
-            n = cell_n(D, c);
-            st = D.cell_start[c];
-        }
-        int inc = n;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int t = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += t;
-        }
-        if (lane < ncb) {
-            S.cell[lane] = c;
-            S.cell_n[lane] = n;
-            S.cell_start[lane] = st;
-            S.cell_base[lane] = inc - n;
-        }
-        int total = __shfl_sync(0xffffffffu, inc, 31);
-        if (lane == 0) {
-            S.total = total;
-            S.overflow = total > SW_MAXA ? 1 : 0;
-        }
-    }
-    __syncthreads();
-    const int total = S.total;
-    if (!S.overflow) {
-        // phase A
-        for (int a = threadIdx.x; a < total; a += blockDim.x) {
-            int q = 0;
-            while (q + 1 < ncb && S.cell_base[q + 1] <= a) ++q;
-            int i = D.cell_atoms[S.cell_start[q] + (a - S.cell_base[q])];
-            int c = S.cell[q];
-            S.slot[a] = i;
-            double4 si = D.s[i];
-            S.s[a][0] = si.x; S.s[a][1] = si.y; S.s[a][2] = si.z; S.s[a][3] = si.w;
-            int nin = 0;
-            const int cst = S.cell_start[q], cn = S.cell_n[q];
-            double3 Ho;
-            double hjo;
-            exchange_field(
-                D, i, Ho, hjo, [&](int j) { return D.cell_of[j] == c; },
-                [&](int j, double J) {
-                    int pos = 0;
-                    while (pos < cn && D.cell_atoms[cst + pos] != j) ++pos;
-                    if (nin < SW_MAXIN) {
-                        S.inq[a][nin] = (unsigned char)pos;
-                        S.inJ[a][nin] = J;
-                    }
-                    ++nin;
-                });
-            S.h[a][0] = Ho.x; S.h[a][1] = Ho.y; S.h[a][2] = Ho.z; S.h[a][3] = hjo;
-            S.inn[a] = (unsigned char)(nin < SW_MAXIN ? nin : SW_MAXIN);
-            if (nin > SW_MAXIN) S.overflow = 1;
-            if (D.spinlang) {
-                const double4 q = visit_record(D, i, bwd ? 1 : 0);
-                S.aux[a][0] = q.x;
-                S.aux[a][1] = q.y; S.aux[a][2] = q.z; S.aux[a][3] = q.w;
-            }
-        }
-        __syncthreads();
-        if (!S.overflow) {
-            // phase B
-            if (threadIdx.x < ncb) {
-                int q = threadIdx.x, n = S.cell_n[q], b = S.cell_base[q];
-                for (int t = 0; t < n; ++t) {
-                    int a = b + (bwd ? n - 1 - t : t);
-                    double3 H = make_double3(S.h[a][0], S.h[a][1], S.h[a][2]);
-                    double sumJ = S.h[a][3];
-                    for (int e = 0; e < S.inn[a]; ++e) {
-                        int a2 = b + S.inq[a][e];
-                        double J = S.inJ[a][e];
-                        H.x += J * S.s[a2][0]; H.y += J * S.s[a2][1]; H.z += J * S.s[a2][2];
-                        sumJ += J * S.s[a2][3];
-                    }
-                    double3 HL;
-                    double3 s = spin_integrate_dS(
-                        D, make_double3(S.s[a][0], S.s[a][1], S.s[a][2]), H, sumJ, S.aux[a][0],
-                        make_double3(S.aux[a][1], S.aux[a][2], S.aux[a][3]), dt, HL);
-                    double s0 = sqrt(s.x * s.x + s.y * s.y + s.z * s.z);
-                    S.s[a][0] = s.x; S.s[a][1] = s.y; S.s[a][2] = s.z; S.s[a][3] = s0;
-                    if (fields) {
-                        int i = S.slot[a];
-                        D.H[i] = make_double4(H.x, H.y, H.z, 0.0);
-                        D.HL[i] = make_double4(HL.x, HL.y, HL.z, 0.0);
-                        if (D.spinlang) D.sumJ[i] = sumJ;
-                    }
-                }
-            }
-            __syncthreads();
-            // phase C
-            for (int a = threadIdx.x; a < total; a += blockDim.x) {
-                double s0 = S.s[a][3];
-                if (!isfinite(s0)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
-                D.s[S.slot[a]] = make_double4(S.s[a][0], S.s[a][1], S.s[a][2], s0);
-                if (D.split)
-                    D.s32[S.slot[a]] = make_float4((float)S.s[a][0], (float)S.s[a][1],
-                                                   (float)S.s[a][2], (float)s0);
-            }
-            return;
-        }
-    }
-    // fallback: one thread per cell, from global memory
-    if (threadIdx.x < ncb) {
-        int q = threadIdx.x, n = S.cell_n[q], st = S.cell_start[q];
-        for (int t = 0; t < n; ++t) {
-            int i = D.cell_atoms[st + (bwd ? n - 1 - t : t)];
-            visit_global(D, i, dt, bwd ? 1 : 0, fields);
-        }
+// the spin as a prefetched neighbour slot holds it (FP32 copy in the split form)
+template <bool SPLIT>
+__device__ __forceinline__ typename std::conditional<SPLIT, float4, double4>::type spin_reg(
+    const double4& s) {
+    if constexpr (SPLIT) {
+        return make_float4((float)s.x, (float)s.y, (float)s.z, (float)s.w);
+    } else {
+        return s;
     }
 }
 
@@ -294,15 +158,6 @@ struct VisitRegs {
     double rho;
     double3 dS;
 };
-
-template <bool SPLIT>
-__device__ __forceinline__ typename VisitRegs<SPLIT>::ST spin_reg(const double4& s) {
-    if constexpr (SPLIT) {
-        return make_float4((float)s.x, (float)s.y, (float)s.z, (float)s.w);
-    } else {
-        return s;
-    }
-}
 
 // Spin loads.  CG: through L2 only (ld.global.cg), for a kernel in which
 // other blocks update spins while it runs, so that no stale copy in this
@@ -626,16 +481,14 @@ void launch_sweep_flow(const Dev& D, cudaStream_t st, const SweepFlow& F0, doubl
     k_flow_next<<<1, 32, 0, st>>>(F);
 }
 
-static size_t sweep_smem() { return sizeof(SweepShared); }
 static int g_sms = 148;        // SMs of the device (capped sweep grids)
-static int g_sweep_mode = 2;   // 0: two-level (shared memory), 1: one thread per cell,
-                               // 2: one thread per cell, pipelined; one launch per group
+static int g_sweep_mode = 2;   // 1: one thread per cell, 2: one thread per cell,
+                               // pipelined; one launch per group
                                // 3: the pipelined walk, scheduled by data flow
 
 void sweep_init() {
-    cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem());
     const char* v = getenv("SLD_SWEEP_MODE");
-    if (v && v[0] >= '0' && v[0] <= '3') g_sweep_mode = v[0] - '0';
+    if (v && v[0] >= '1' && v[0] <= '3') g_sweep_mode = v[0] - '0';
     g_flow_polls = FLOW_POLLS;
     g_flow_stall = 0;
     if (const char* q = getenv("SLD_FLOW_POLLS")) {
@@ -689,9 +542,5 @@ void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g,
         }
         return;
     }
-    if (g_sweep_mode == 1) {
-        k_sweep_cell<<<div_up(ncell_g, 128), 128, 0, st>>>(D, gcells, ncell_g, dt, b);
-        return;
-    }
-    k_sweep<<<div_up(ncell_g, SW_CPB), SW_THREADS, sweep_smem(), st>>>(D, gcells, ncell_g, dt, b);
+    k_sweep_cell<<<div_up(ncell_g, 128), 128, 0, st>>>(D, gcells, ncell_g, dt, b);
 }

@@ -56,8 +56,10 @@ struct Snap {
     double4 *r, *p, *s, *f;
     long long* stamp;
     int *cell_of, *cell_start, *cell_count, *cell_atoms, *cell_slot;
-    float4* r32s;
+    int4* fxs;
+    int4* fxa;                        // split form only
     int *nbr, *nbr_n;
+    unsigned char* nbk;               // split form only
     Ctl* ctl;
 };
 
@@ -137,7 +139,9 @@ int alloc_snap(Pool& pool, const Adj& a, Snap& s) {
     s.cell_count = pool.get<int>(nc);
     s.cell_atoms = pool.get<int>(n);
     s.cell_slot = pool.get<int>(n);
-    s.r32s = pool.get<float4>(n);
+    s.fxs = pool.get<int4>(n);
+    s.fxa = a.c->D.fxa ? pool.get<int4>(n) : nullptr;
+    s.nbk = a.c->D.nbk ? pool.get<unsigned char>(a.nnb) : nullptr;
     s.nbr = pool.get<int>(a.nnb);
     s.nbr_n = pool.get<int>(n);
     s.ctl = pool.get<Ctl>(1);
@@ -174,7 +178,9 @@ void save(const Adj& a, Snap& s) {
     dcopy(s.stamp, D.stamp, n, st); dcopy(s.cell_of, D.cell_of, n, st);
     dcopy(s.cell_start, D.cell_start, nc, st); dcopy(s.cell_count, D.cell_count, nc, st);
     dcopy(s.cell_atoms, D.cell_atoms, n, st); dcopy(s.cell_slot, D.cell_slot, n, st);
-    dcopy(s.r32s, D.r32s, n, st);
+    dcopy(s.fxs, D.fxs, n, st);
+    if (s.fxa) dcopy(s.fxa, D.fxa, n, st);
+    if (s.nbk) dcopy(s.nbk, D.nbk, a.nnb, st);
     dcopy(s.nbr, D.nbr, a.nnb, st); dcopy(s.nbr_n, D.nbr_n, n, st);
     dcopy(s.ctl, D.ctl, 1, st);
 }
@@ -187,7 +193,9 @@ void restore(const Adj& a, const Snap& s) {
     dcopy(D.stamp, s.stamp, n, st); dcopy(D.cell_of, s.cell_of, n, st);
     dcopy(D.cell_start, s.cell_start, nc, st); dcopy(D.cell_count, s.cell_count, nc, st);
     dcopy(D.cell_atoms, s.cell_atoms, n, st); dcopy(D.cell_slot, s.cell_slot, n, st);
-    dcopy(D.r32s, s.r32s, n, st);
+    dcopy(D.fxs, s.fxs, n, st);
+    if (s.fxa) dcopy(D.fxa, s.fxa, n, st);
+    if (s.nbk) dcopy(D.nbk, s.nbk, a.nnb, st);
     dcopy(D.nbr, s.nbr, a.nnb, st); dcopy(D.nbr_n, s.nbr_n, n, st);
     dcopy(D.ctl, s.ctl, 1, st);
 }

@@ -224,16 +224,20 @@ int order_groups_by_count(sld_ctx* c) {
     return SLD_OK;
 }
 
-// FP32 pair pre-test margin (k_pair.cu) for the box of G: coordinates stay
-// below B, each rounding is at most ulp(B) / 2
+// FP32 pair pre-test margin (k_pair.cu) for the cells of G.  A pair-vector
+// component is at most three products M_ab d_b of the cell matrix and
+// fixed-point differences (each below 3 cells), each rounded: with B the
+// largest row sum of |M| over three cells, a component moves by at most
+// e = 4 B 2^-24, and r^2 near the cutoff by 2 r_max sqrt(3) e + 3 e^2 plus the
+// FP32 rounding of the sum.  The margin is twice that.
 float pair_margin(const sld::HostGeom& G) {
-    double B = 0.0;
-    for (int k = 0; k < 6; ++k) B += std::fabs(G.d[k]);
-    B *= 2.0;
-    const double e = std::ldexp(1.0, std::ilogb(B) - 23);   // ulp(B) / 2 in FP32
-    const double dl = 4.0 * std::sqrt(3.0) * e;
-    const double rm = G.rcut_max + dl;
-    const double bound = 2.0 * rm * dl + dl * dl + 4.0 * std::ldexp(rm * rm, -23);
+    const double rx = std::fabs(G.d[0]) / G.nx + std::fabs(G.d[1]) / G.ny + std::fabs(G.d[3]) / G.nz;
+    const double ry = std::fabs(G.d[2]) / G.ny + std::fabs(G.d[4]) / G.nz;
+    const double rz = std::fabs(G.d[5]) / G.nz;
+    const double B = 3.0 * std::max(rx, std::max(ry, rz));
+    const double e = 4.0 * B * std::ldexp(1.0, -24);
+    const double rm = G.rcut_max;
+    const double bound = 2.0 * rm * std::sqrt(3.0) * e + 3.0 * e * e + 4.0 * std::ldexp(rm * rm, -23);
     return (float)(2.0 * bound);
 }
 
@@ -396,6 +400,8 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     *out = nullptr;
     int rc = validate(prm);
     if (rc) return rc;
+    // the split form's neighbour lists pack a slot (27 bits) with a cell code
+    if (prm->precision == SLD_SPLIT && natom >= (1 << 27)) return SLD_ERR_CAPACITY;
     sld_ctx* c = new (std::nothrow) sld_ctx();
     if (!c) return SLD_ERR_NOMEM;
     c->P = *prm;
@@ -530,7 +536,9 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
          c->alloc(&D.dF, n) == 0;
     if (prm->spinlang) ok = ok && c->alloc(&D.vrec, 2 * n) == 0;
     if (prm->precision == SLD_SPLIT) ok = ok && c->alloc(&D.s32, n) == 0;
-    ok = ok && c->alloc(&D.r32s, n) == 0 && c->alloc(&D.cell_slot, n) == 0;
+    ok = ok && c->alloc(&D.fxs, n) == 0 && c->alloc(&D.cell_slot, n) == 0;
+    if (prm->precision == SLD_SPLIT)
+        ok = ok && c->alloc(&D.fxa, n) == 0 && c->alloc(&D.nbk, (size_t)SLD_MAXNB * n) == 0;
     {
         float* cub = nullptr;
         double* cub64 = nullptr;

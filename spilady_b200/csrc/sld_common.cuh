@@ -111,10 +111,18 @@ struct Dev {
     double4* fext;                // external force per atom (eV/A), or null (extforce)
     float4* s32;                  // split form: s rounded to FP32, written with s by every
                                   // spin writer; the FP32 exchange sums gather it
-    float4* r32s;                 // positions rounded to FP32 in cell-list order (slot
-                                  // order), written by links and by every drift
+    int4* fxs;                    // positions in fixed point, relative to the atom's link
+                                  // cell: (fractional coordinate x n - cell index) x 2^29
+                                  // per axis, in cell-list order (slot order); written by
+                                  // links and by every drift (with the drift's unwrapped
+                                  // position, so that an atom the drift wraps across the
+                                  // box stays next to its cell until the next links)
+    int4* fxa;                    // split form: the same in atom order
+    unsigned char* nbk;           // split form: [SLD_MAXNB][natom] the neighbour cell
+                                  // (0..26, map_cells order) of each nbr entry
     int* cell_slot;               // index of each atom in cell_atoms (its slot)
     float pair_loose;             // margin of the FP32 pair pre-test (A^2), k_pair.cu
+                                  // (FP64 form; the split form's FP32 test is its own)
     double *rho, *pe, *ke, *me, *me0, *vir, *sumJ, *stress;
     int *cell_of, *id, *node;
     long long* stamp;
@@ -241,6 +249,40 @@ __device__ __forceinline__ void cell_xyz(const Dev& D, int c, int& cx, int& cy, 
     int t = c / D.nx;
     cy = t % D.ny;
     cz = t / D.ny;
+}
+
+// Fixed-point positions relative to a link cell.  A component is the
+// fractional coordinate times the cells per axis, less the cell's index
+// (within [0, 1) for an atom inside its cell), in units of 2^-29, clamped to
+// [-0.75, 1.75] (an atom never drifts that far between two links): the pair
+// vector r_i - r_j of two atoms whose cells are k apart is
+// M (f_i - f_j - delta_k 2^29), exact in integers, with one rounding to FP32
+// per product of the cell matrix M (the box vectors over the cells per axis
+// and 2^29).
+#define SLD_FX_ONE (1 << 29)
+__device__ __forceinline__ int4 cell_fix(const Dev& D, int c, double x, double y, double z) {
+    int cx, cy, cz;
+    cell_xyz(D, c, cx, cy, cz);
+    const double3 q = to_frac(D, x, y, z);
+    auto f = [](double v) {
+        v = fmin(fmax(v, -0.75), 1.75);
+        return __double2int_rn(v * (double)SLD_FX_ONE);
+    };
+    return make_int4(f(q.x * D.nx - cx), f(q.y * D.ny - cy), f(q.z * D.nz - cz), 0);
+}
+struct FxMat {
+    float xx, xy, xz, yy, yz, zz;
+};
+__device__ __forceinline__ FxMat fx_mat(const Dev& D) {
+    const double u = 1.0 / SLD_FX_ONE;
+    return FxMat{(float)(D.d[0] / D.nx * u), (float)(D.d[1] / D.ny * u), (float)(D.d[3] / D.nz * u),
+                 (float)(D.d[2] / D.ny * u), (float)(D.d[4] / D.nz * u), (float)(D.d[5] / D.nz * u)};
+}
+// the Cartesian vector (FP32) of a fixed-point difference
+__device__ __forceinline__ float3 fx_vec(const FxMat& M, int dx, int dy, int dz) {
+    const float fx = (float)dx, fy = (float)dy, fz = (float)dz;
+    return make_float3(fmaf(M.xz, fz, fmaf(M.xy, fy, M.xx * fx)), fmaf(M.yz, fz, M.yy * fy),
+                       M.zz * fz);
 }
 
 // potential_CPU.cpp:172-179: linear interpolation between entries n-1 and n

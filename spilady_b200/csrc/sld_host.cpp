@@ -23,13 +23,16 @@ void host_periodic(const HostGeom& G, double& x, double& y, double& z) {
     }
 }
 
+// the 26 neighbour offsets in the order of map_cells.cpp:96-121
+static const int kNbrOff[26][3] = {
+    {1, 0, 0},   {1, 1, 0},  {0, 1, 0},   {-1, 1, 0},  {1, 0, -1},  {1, 1, -1}, {0, 1, -1},
+    {-1, 1, -1}, {1, 0, 1},  {1, 1, 1},   {0, 1, 1},   {-1, 1, 1},  {0, 0, 1},  {-1, 0, 0},
+    {0, -1, 0},  {0, 0, -1}, {1, -1, 0},  {-1, -1, 0}, {-1, 0, 1},  {-1, 0, -1}, {0, -1, 1},
+    {0, -1, -1}, {1, -1, 1}, {1, -1, -1}, {-1, -1, 1}, {-1, -1, -1}};
+
 // neighbour k of cell (ix, iy, iz) in the order of map_cells.cpp:96-121
 static int nbr(int nx, int ny, int nz, int ix, int iy, int iz, int k) {
-    static const int O[26][3] = {
-        {1, 0, 0},   {1, 1, 0},  {0, 1, 0},   {-1, 1, 0},  {1, 0, -1},  {1, 1, -1}, {0, 1, -1},
-        {-1, 1, -1}, {1, 0, 1},  {1, 1, 1},   {0, 1, 1},   {-1, 1, 1},  {0, 0, 1},  {-1, 0, 0},
-        {0, -1, 0},  {0, 0, -1}, {1, -1, 0},  {-1, -1, 0}, {-1, 0, 1},  {-1, 0, -1}, {0, -1, 1},
-        {0, -1, -1}, {1, -1, 1}, {1, -1, -1}, {-1, -1, 1}, {-1, -1, -1}};
+    const int (&O)[26][3] = kNbrOff;
     int x = (ix + O[k][0] + nx) % nx, y = (iy + O[k][1] + ny) % ny, z = (iz + O[k][2] + nz) % nz;
     return x + y * nx + z * nx * ny;
 }

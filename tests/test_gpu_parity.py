@@ -281,6 +281,7 @@ def test_sweep_schedules_give_identical_bits(monkeypatch, precision):
     got = _run_with_sweep_mode(2, monkeypatch, precision)
     for n, a in ref.items():
         assert np.array_equal(got[n], a), f"mode 2 {n}"
+
     got = _run_with_sweep_mode(1, monkeypatch, precision)
     for n, a in ref.items():
         if precision == 1:
@@ -338,3 +339,35 @@ def test_core_dte_levels_give_the_phase_bits(monkeypatch, cells, precision):
         e.close()
     for n in ("Te", "Ee"):
         assert np.array_equal(out[2][n], out[3][n]), n
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_atoms_wrapped_by_the_drift_keep_their_pairs(precision):
+    # Atoms that the drift carries across the box's high faces are wrapped to
+    # the low side (periodic_CPU.cpp:31-50) but stay linked in their old cell
+    # until the next links; the reference still finds their pairs (find_image
+    # on every pair).  The lattice is shifted so that the sites of highest x,
+    # y and z sit 0.002 A below the faces, and those atoms move outwards.
+    eng = engine_mod()
+    params, r, p, s = initial_state(6, seed=17, tilt=0.3, temperature=300.0, pos_sigma=0.05)
+    L = params["box"][0]
+    r = r + (L - 0.002 - r.max(axis=0))
+    sigma = p.std()
+    for ax in range(3):
+        sel = r[:, ax] > L - 0.003
+        assert sel.any()
+        p[sel, ax] = 20.0 * sigma   # about 0.04 A per step
+    p -= p.mean(axis=0)
+    o = orc.System(params, r, p, s, rng=orc.RNG_PHILOX)
+    e = eng.Engine(params, r, p, s, precision=precision)
+    tol = 1e-10 if precision == 0 else SPLIT_TOL
+    for k in range(2):
+        o.run(1)
+        e.run(1)
+        e.sync()
+        if k == 0:
+            # some atoms were wrapped by the first drift
+            assert np.any(e.get("r") < 0.1)
+        for n in ("r", "p", "s", "f", "rho", "pe", "me"):
+            err = relerr(e.get(n), o.get(n))
+            assert err <= tol, f"step {k} {n}: {err:.3e}"
