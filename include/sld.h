@@ -145,7 +145,9 @@ int sld_read_variables(const char* path, sld_params* inout);
    readTe input of map_cells.cpp:33-39,136-150.  Then, as initialize()
    (initial.cpp:31-106) does: potential tables, link cells and colour groups,
    rho, forces and energies, cell temperatures, and with renormalize_energy
-   the reference energy of check_energy(-1). */
+   the reference energy of check_energy(-1).  The split form takes at most
+   2^27 - 1 atoms (SLD_ERR_CAPACITY beyond: its neighbour lists pack a
+   27-bit slot with a neighbour-cell code). */
 int sld_create(sld_ctx** out, const sld_params* prm, int natom,
                const double* r, const double* p, const double* s,
                const double* te_K);

@@ -68,7 +68,7 @@ __device__ __forceinline__ double3 find_image_f(const Dev& D, double3 rij, bool&
 // positions, the cell offset, two differences), so r^2 near the cutoff moves
 // by at most 2 r_max (5 sqrt(3) e) + (5 sqrt(3) e)^2 plus the FP32 rounding of
 // the sum.  D.pair_loose, set on the host from the cell size, is twice that.
-template <int MODE>
+template <int MODE, bool ORTHO>
 __device__ void pairs_one(const Dev& D, int i, int write_rho) {
     unsigned* err = &D.ctl->err;
     const int N = D.natom;
@@ -96,7 +96,7 @@ __device__ void pairs_one(const Dev& D, int i, int write_rho) {
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int slot = st + m0 + u;
-                    const float3 d = fx_vec(M, ex - q[u].x, ey - q[u].y, ez - q[u].z);
+                    const float3 d = fx_vec<ORTHO>(M, ex - q[u].x, ey - q[u].y, ez - q[u].z);
                     if (m0 + u < n && d.x * d.x + d.y * d.y + d.z * d.z < cut && slot != myslot) {
                         if (nn < SLD_MAXNB) D.nbr[(size_t)nn * N + i] = slot;
                         ++nn;
@@ -146,11 +146,11 @@ __device__ void pairs_one(const Dev& D, int i, int write_rho) {
     if (write_rho) D.rho[i] = rho;
 }
 
-template <int MODE>
+template <int MODE, bool ORTHO>
 __global__ void __launch_bounds__(128) k_pairs(Dev D, int write_rho) {
     // one atom per thread; a capped grid walks several atoms per thread
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x)
-        pairs_one<MODE>(D, i, write_rho);
+        pairs_one<MODE, ORTHO>(D, i, write_rho);
 }
 
 // ---------------------------------------------------------------------
@@ -166,6 +166,7 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, int write_rho) {
 // (the density and pair terms' last knots, 3.0 and 4.1 A, and the exchange's
 // 3.75 A lie inside the cutoffs).
 #define SLD_SPLIT_SLOT_BITS 27
+template <bool ORTHO>
 __device__ void pairs_split_one(const Dev& D, int i, int write_rho) {
     const int N = D.natom;
     int c0 = D.cell_of[i], cx, cy, cz;
@@ -188,7 +189,7 @@ __device__ void pairs_split_one(const Dev& D, int i, int write_rho) {
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int slot = st + m0 + u;
-                const float3 d = fx_vec(M, ex - q[u].x, ey - q[u].y, ez - q[u].z);
+                const float3 d = fx_vec<ORTHO>(M, ex - q[u].x, ey - q[u].y, ez - q[u].z);
                 if (m0 + u < n && d.x * d.x + d.y * d.y + d.z * d.z < cut && slot != myslot) {
                     if (nn < SLD_MAXNB)
                         D.nbr[(size_t)nn * N + i] =
@@ -201,6 +202,7 @@ __device__ void pairs_split_one(const Dev& D, int i, int write_rho) {
     const int nl = nn < SLD_MAXNB ? nn : SLD_MAXNB;
     Kahan rho;
     const float rmag2 = (float)D.rcut_mag_sq, rpot = (float)D.rcut_pot;
+    const Knots32 K = knots32(D);
     int nj = 0;
     for (int e0 = 0; e0 < nl; e0 += 4) {
         int sb[4], kb[4], jb[4];
@@ -220,16 +222,16 @@ __device__ void pairs_split_one(const Dev& D, int i, int write_rho) {
         for (int u = 0; u < 4; ++u) {
             if (e0 + u >= nl) break;
             const int e = e0 + u, k = kb[u];
-            const float3 d = fx_vec(M, fi.x - kNbr[k][0] * SLD_FX_ONE - qb[u].x,
+            const float3 d = fx_vec<ORTHO>(M, fi.x - kNbr[k][0] * SLD_FX_ONE - qb[u].x,
                                     fi.y - kNbr[k][1] * SLD_FX_ONE - qb[u].y,
                                     fi.z - kNbr[k][2] * SLD_FX_ONE - qb[u].z);
             const float rsq = d.x * d.x + d.y * d.y + d.z * d.z;
-            const float r = sqrtf(rsq);
+            const float r = rsq * rsqrtf(rsq);
             D.nbr[(size_t)e * N + i] = jb[u] | SLD_WRAP;
             D.nbk[(size_t)e * N + i] = (unsigned char)k;
             if (r < rpot) {
                 float f, df;
-                dens32f(D, r, f, df);
+                dens32f(D, K, r, f, df);
                 rho.add(f);
             }
             if (rsq < rmag2) {
@@ -249,9 +251,10 @@ __device__ void pairs_split_one(const Dev& D, int i, int write_rho) {
     if (write_rho) D.rho[i] = rho.value();
 }
 
+template <bool ORTHO>
 __global__ void __launch_bounds__(128) k_pairs_split(Dev D, int write_rho) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x)
-        pairs_split_one(D, i, write_rho);
+        pairs_split_one<ORTHO>(D, i, write_rho);
 }
 
 // F'(rho) per atom (the force pass needs it for both atoms of every pair):
@@ -427,7 +430,7 @@ __global__ void __launch_bounds__(128) k_force64(Dev D) {
 // reference's derivatives, compensated (Kahan) FP32 sums for the forces and
 // energies; the stress and virial products (FP32) are summed in FP64.  Four
 // entries' loads are issued together.
-template <int PART>
+template <int PART, bool ORTHO>
 __device__ __forceinline__ void force32_one(const Dev& D, int i) {
     const int N = D.natom;
     const int4 fi = __ldg(D.fxa + i);
@@ -439,6 +442,7 @@ __device__ __forceinline__ void force32_one(const Dev& D, int i) {
     double rho_i = D.rho[i];
     float dF_i = (PART & PART_EAM) ? (float)D.dF[i] : 0.f;
     const float rpot = (float)D.rcut_pot, rmag2 = (float)D.rcut_mag_sq;
+    const Knots32 K = knots32(D);
     Kahan fx, fy, fz, pe, me, me0;
     double st[6] = {0, 0, 0, 0, 0, 0}, vir = 0.0;
     const int nn = D.nbr_n[i];
@@ -463,17 +467,18 @@ __device__ __forceinline__ void force32_one(const Dev& D, int i) {
         for (int u = 0; u < 4; ++u) {
             if (e0 + u >= nn) break;
             const int k = kb[u];
-            const float3 d = fx_vec(M, fi.x - kNbr[k][0] * SLD_FX_ONE - qb[u].x,
+            const float3 d = fx_vec<ORTHO>(M, fi.x - kNbr[k][0] * SLD_FX_ONE - qb[u].x,
                                     fi.y - kNbr[k][1] * SLD_FX_ONE - qb[u].y,
                                     fi.z - kNbr[k][2] * SLD_FX_ONE - qb[u].z);
             const float dx = d.x, dy = d.y, dz = d.z;
             const float rsq = dx * dx + dy * dy + dz * dz;
-            const float r0 = sqrtf(rsq);
+            const float ir = rsqrtf(rsq);
+            const float r0 = rsq * ir;
             float dudr = 0.f;
             if ((PART & PART_EAM) && r0 < rpot) {
                 float f, df, phi, dphi;
-                dens32f(D, r0, f, df);
-                pair32f(D, r0, phi, dphi);
+                dens32f(D, K, r0, f, df);
+                pair32f(D, K, r0, phi, dphi);
                 dudr = (dF_i + dFb[u]) * df + dphi;
                 pe.add(0.5f * phi);
             }
@@ -490,7 +495,7 @@ __device__ __forceinline__ void force32_one(const Dev& D, int i) {
                 me.add(-Jh * dot);
             }
             if (dudr == 0.f && PART != PART_ALL) continue;
-            const float force = -dudr / r0;
+            const float force = -dudr * ir;
             const float gx = force * dx, gy = force * dy, gz = force * dz;
             fx.add(gx); fy.add(gy); fz.add(gz);
             st[0] += (double)(gx * dx); st[1] += (double)(gy * dy); st[2] += (double)(gz * dz);
@@ -504,11 +509,11 @@ __device__ __forceinline__ void force32_one(const Dev& D, int i) {
                        pe.value(), me.value(), me0.value(), vir, st);
 }
 
-template <int PART>
+template <int PART, bool ORTHO>
 __global__ void __launch_bounds__(128) k_force32(Dev D) {
     // one atom per thread; a capped grid walks several atoms per thread
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x)
-        force32_one<PART>(D, i);
+        force32_one<PART, ORTHO>(D, i);
 }
 
 // a cap on the CTAs per SM (0: none) for the kernels of the step graph's side
@@ -531,7 +536,10 @@ static void launch_force_part(const Dev& D, cudaStream_t st) {
     const int bs = D.tune.force_block > 0 ? D.tune.force_block : 128;
     int nb = div_up(D.natom, bs);
     if (PART == PART_EAM) nb = capped_grid(nb, D.tune.force_cap);
-    if (D.split) k_force32<PART><<<nb, bs, 0, st>>>(D);
+    if (D.split) {
+        if (box_ortho(D)) k_force32<PART, true><<<nb, bs, 0, st>>>(D);
+        else k_force32<PART, false><<<nb, bs, 0, st>>>(D);
+    }
     else if (D.analytic) k_force64<true, PART><<<nb, bs, 0, st>>>(D);
     else k_force64<false, PART><<<nb, bs, 0, st>>>(D);
 }
@@ -540,9 +548,17 @@ void launch_pairs(const Dev& D, cudaStream_t st, bool write_rho) {
     int w = write_rho ? 1 : 0;
     const int bs = D.tune.pair_block > 0 ? D.tune.pair_block : 128;
     int nb = capped_grid(div_up(D.natom, bs), D.tune.pair_cap);
-    if (D.split) k_pairs_split<<<nb, bs, 0, st>>>(D, w);
-    else if (D.analytic) k_pairs<2><<<nb, bs, 0, st>>>(D, w);
-    else k_pairs<0><<<nb, bs, 0, st>>>(D, w);
+    const bool ortho = box_ortho(D);
+    if (D.split) {
+        if (ortho) k_pairs_split<true><<<nb, bs, 0, st>>>(D, w);
+        else k_pairs_split<false><<<nb, bs, 0, st>>>(D, w);
+    } else if (D.analytic) {
+        if (ortho) k_pairs<2, true><<<nb, bs, 0, st>>>(D, w);
+        else k_pairs<2, false><<<nb, bs, 0, st>>>(D, w);
+    } else {
+        if (ortho) k_pairs<0, true><<<nb, bs, 0, st>>>(D, w);
+        else k_pairs<0, false><<<nb, bs, 0, st>>>(D, w);
+    }
 }
 void launch_embed(const Dev& D, cudaStream_t st) {
     int nb = div_up(D.natom, 256);

@@ -162,44 +162,48 @@ void pot_join_data(double o[7]) {
     o[6] = 0.88535e0 * 0.52917720859e0 / (2e0 * std::pow(26e0, 0.23));
 }
 
-static void cubic_pieces(const double* a, const double* k, int n, float* K, float* C, double* K64,
-                         double* C64, float* A, double* A64) {
-    // knots ascending (the arrays here are given descending)
-    std::vector<int> ord(n);
+// the cubics of sum_i a_i (k_i - r)^3 for r < k_i (knots given descending)
+static void cubic_pieces(const double* a, const double* k, int n, float* K, float* blocks,
+                         double* K64, double* C64) {
+    std::vector<int> ord(n);   // ascending
     for (int i = 0; i < n; ++i) ord[i] = n - 1 - i;
     for (int i = 0; i < n; ++i) {
         K[i] = (float)k[ord[i]];
         K64[i] = (double)K[i];
-        A[i] = (float)a[ord[i]];
-        A64[i] = a[ord[i]];
     }
     for (int m = 0; m <= n; ++m) {
         double c[4] = {0, 0, 0, 0};
+        const double base = (double)(m == 0 ? K[0] : K[m - 1]);
         if (m < n) {
-            double base = (double)(m == 0 ? K[0] : K[m - 1]);
-            for (int q = 0; q < n; ++q) {
-                int i = ord[q];
-                if (q < m) continue;          // knot at or below the interval: inactive
-                double dl = k[i] - base;
+            for (int q = m; q < n; ++q) {   // knots above the interval are active
+                const int i = ord[q];
+                const double dl = k[i] - base;
                 c[0] += a[i] * dl * dl * dl;
                 c[1] += -3e0 * a[i] * dl * dl;
                 c[2] += 3e0 * a[i] * dl;
                 c[3] += -a[i];
             }
         }
+        float* b = blocks + 8 * m;
         for (int q = 0; q < 4; ++q) {
-            C[4 * m + q] = (float)c[q];
+            b[q] = (float)c[q];
             C64[4 * m + q] = c[q];
         }
+        b[4] = (float)base;
+        b[5] = m < n ? K[m] : 1e30f;
+        b[6] = m > 0 ? (float)a[ord[m - 1]] : 0.f;
+        b[7] = m < n ? (float)a[ord[m]] : 0.f;
     }
 }
 
-void pot_cubic_tables(float out[kCubicFloats], double o64[kCubicFloats]) {
+void pot_cubic_tables(float out[kCubicFloats], double o64[kCubicDoubles]) {
     static const double da[6] = {0.9332056681088162, -1.162558782567700, -0.3502026949249225,
                                  0.4287820835430028, 4.907925057809273, -5.307049068415304};
     static const double dk[6] = {3.0, 2.8666666666666666, 2.7333333333333333, 2.6, 2.4, 2.3};
-    cubic_pieces(kPV, kPK, 8, out, out + 8, o64, o64 + 8, out + 78, o64 + 78);
-    cubic_pieces(da, dk, 6, out + 44, out + 50, o64 + 44, o64 + 50, out + 86, o64 + 86);
+    for (int k = 0; k < kCubicFloats; ++k) out[k] = 0.f;
+    for (int k = 0; k < kCubicDoubles; ++k) o64[k] = 0.0;
+    cubic_pieces(kPV, kPK, 8, out, out + kPairIv, o64, o64 + 8);
+    cubic_pieces(da, dk, 6, out + kDensKnots, out + kDensIv, o64 + 44, o64 + 50);
 }
 
 }  // namespace sld

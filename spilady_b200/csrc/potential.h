@@ -27,15 +27,25 @@ void pot_theta(double out[36]);
 void pot_join_data(double out[7]);
 
 // Piecewise-cubic form of the DD05 pair term (r > 2 A) and density: between
-// consecutive knots each is one cubic, written here in t = r - base with the
-// base stored as FP32.  Layout (floats): pair knots [0,8), pair coefficients
-// [8,44) (9 intervals x c0..c3), density knots [44,50), density coefficients
-// [50,78) (7 intervals).  Interval m holds r with m knots <= r; its base is
-// knot m-1 (knot 0 for m = 0); the last interval is zero.  Then the amplitude
-// a_i of each knot's term a_i (k_i - r)^3, in the same ascending knot order:
-// pair [78,86), density [86,92) (the seven-point derivative near a knot needs
-// the one term that changes form there).
-constexpr int kCubicFloats = 92;
-void pot_cubic_tables(float out[kCubicFloats], double out64[kCubicFloats]);
+// consecutive knots each is one cubic, written in t = r - base with the base
+// stored as FP32.  Interval m holds r with m knots <= r (knots ascending); its
+// base is knot m-1 (knot 0 for m = 0); the last interval is zero.
+//
+// FP32 table (the split form), kCubicFloats floats: pair knots [0,8), then
+// the pair's 9 intervals as 8-float blocks from kPairIv, density knots at
+// kDensKnots (6 and two unused), then the density's 7 intervals from
+// kDensIv.  A block is {c0, c1, c2, c3, base, upper knot (1e30 for the last
+// interval), amplitude a of the knot below and of the knot above (0 where
+// there is none)} for the terms a (k - r)^3 whose seven-point derivative
+// differs from the exact one near their knot.  Every block starts on 32
+// bytes.
+//
+// FP64 table (the analytic FP64 form), kCubicDoubles doubles: pair knots
+// [0,8), pair coefficients [8,44) (c0..c3 per interval), density knots
+// [44,50), density coefficients [50,78).
+constexpr int kCubicFloats = 144;
+constexpr int kPairIv = 8, kDensKnots = 80, kDensIv = 88;
+constexpr int kCubicDoubles = 78;
+void pot_cubic_tables(float out[kCubicFloats], double out64[kCubicDoubles]);
 
 }  // namespace sld

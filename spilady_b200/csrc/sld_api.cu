@@ -13,6 +13,10 @@
 
 #include "../../include/sld.h"
 #include "potential.h"
+#include "sld_pot32.cuh"
+static_assert(SLD_DENS_KNOTS == sld::kDensKnots && SLD_PAIR_IV == sld::kPairIv &&
+                  SLD_DENS_IV == sld::kDensIv,
+              "split-form potential table offsets");
 #include "sld_common.cuh"
 #include "sld_ctx.cuh"
 #include "sld_host.h"
@@ -510,7 +514,7 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
                         (float)jd[4], (float)jd[5], (float)jd[6]};
     }
     float cubic_h[sld::kCubicFloats];
-    double cubic64_h[sld::kCubicFloats];
+    double cubic64_h[sld::kCubicDoubles];
     sld::pot_cubic_tables(cubic_h, cubic64_h);
 
     size_t n = (size_t)natom;
@@ -542,7 +546,7 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
     {
         float* cub = nullptr;
         double* cub64 = nullptr;
-        ok = ok && c->alloc(&cub, sld::kCubicFloats) == 0 && c->alloc(&cub64, sld::kCubicFloats) == 0;
+        ok = ok && c->alloc(&cub, sld::kCubicFloats) == 0 && c->alloc(&cub64, sld::kCubicDoubles) == 0;
         if (ok) {
             cudaMemcpy(cub, cubic_h, sizeof(cubic_h), cudaMemcpyHostToDevice);
             cudaMemcpy(cub64, cubic64_h, sizeof(cubic64_h), cudaMemcpyHostToDevice);

@@ -278,11 +278,17 @@ __device__ __forceinline__ FxMat fx_mat(const Dev& D) {
     return FxMat{(float)(D.d[0] / D.nx * u), (float)(D.d[1] / D.ny * u), (float)(D.d[3] / D.nz * u),
                  (float)(D.d[2] / D.ny * u), (float)(D.d[4] / D.nz * u), (float)(D.d[5] / D.nz * u)};
 }
-// the Cartesian vector (FP32) of a fixed-point difference
+// the Cartesian vector (FP32) of a fixed-point difference; ORTHO: a box whose
+// off-diagonal components are zero (the same values: fmaf(0, y, x) is x)
+template <bool ORTHO = false>
 __device__ __forceinline__ float3 fx_vec(const FxMat& M, int dx, int dy, int dz) {
     const float fx = (float)dx, fy = (float)dy, fz = (float)dz;
+    if constexpr (ORTHO) return make_float3(M.xx * fx, M.yy * fy, M.zz * fz);
     return make_float3(fmaf(M.xz, fz, fmaf(M.xy, fy, M.xx * fx)), fmaf(M.yz, fz, M.yy * fy),
                        M.zz * fz);
+}
+__host__ __device__ inline bool box_ortho(const Dev& D) {
+    return D.d[1] == 0.0 && D.d[3] == 0.0 && D.d[4] == 0.0;
 }
 
 // potential_CPU.cpp:172-179: linear interpolation between entries n-1 and n

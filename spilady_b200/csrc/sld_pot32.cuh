@@ -20,6 +20,12 @@
 #pragma once
 #include "sld_common.cuh"
 
+// offsets in the split form's potential table (potential.h: kDensKnots,
+// kPairIv, kDensIv)
+#define SLD_DENS_KNOTS 80
+#define SLD_PAIR_IV 8
+#define SLD_DENS_IV 88
+
 // compensated (Kahan) FP32 accumulator
 struct Kahan {
     float s, c;
@@ -79,50 +85,58 @@ __device__ __forceinline__ float knot_stencil32(float u, float dx) {
     float up = fmaxf(u, 0.f);
     return s / (60.f * dx) + 3.f * up * up;
 }
-// One piecewise cubic (knots K[0..n) ascending, coefficients C[4*(n+1)],
-// knot amplitudes A[0..n)) at an FP32 distance r: t = r - base is exact in
-// FP32 (r and the knot are within a factor of two).  df is the reference's
-// seven-point derivative: near the knots just below and above r (knots are
-// 0.1 A or more apart, the stencil spans 6 r/1000 < 0.025 A) the stencil
-// term of that knot is added.
-__device__ __forceinline__ void cubic_eval(const float* __restrict__ K, const float* __restrict__ C,
-                                           const float* __restrict__ A, int n, float r, float& f,
-                                           float& df) {
+// The knots of the pair term and of the density (ascending), held in
+// registers by a thread for its whole pair loop.
+struct Knots32 {
+    float p[8], d[6];
+};
+__device__ __forceinline__ Knots32 knots32(const Dev& D) {
+    Knots32 K;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) K.p[i] = __ldg(D.cubic + i);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) K.d[i] = __ldg(D.cubic + SLD_DENS_KNOTS + i);
+    return K;
+}
+
+// One piecewise cubic at an FP32 distance r: the interval m (the number of
+// knots <= r) from the knots in registers, then its 32-byte block {c0..c3,
+// base, upper knot, amplitudes of the knots below and above} in two loads.
+// t = r - base is exact in FP32 (r and the knot are within a factor of two).
+// df is the reference's seven-point derivative: within 3 r/1000 of the knot
+// below or above (knots are 0.1 A or more apart, the stencil spans
+// 6 r/1000 < 0.025 A) that knot's stencil term is added.
+template <int N>
+__device__ __forceinline__ void cubic_iv(const float (&K)[N], const float* __restrict__ blocks,
+                                         float r, float& f, float& df) {
     int m = 0;
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
-        if (i < n) m += r >= __ldg(K + i);
+    for (int i = 0; i < N; ++i) m += r >= K[i] ? 1 : 0;
+    const float4* b = reinterpret_cast<const float4*>(blocks) + 2 * m;
+    const float4 c = __ldg(b), e = __ldg(b + 1);
+    const float t = r - e.x;
+    f = fmaf(fmaf(fmaf(c.w, t, c.z), t, c.y), t, c.x);
+    df = fmaf(fmaf(3.f * c.w, t, 2.f * c.z), t, c.y);
     const float dx = r * 1e-3f;
-    if (m == n) {
-        f = 0.f;
-        df = 0.f;
-    } else {
-        const float t = r - __ldg(K + (m == 0 ? 0 : m - 1));
-        const float* c = C + 4 * m;
-        float c0 = __ldg(c), c1 = __ldg(c + 1), c2 = __ldg(c + 2), c3 = __ldg(c + 3);
-        f = fmaf(fmaf(fmaf(c3, t, c2), t, c1), t, c0);
-        df = fmaf(fmaf(3.f * c3, t, 2.f * c2), t, c1);
-        const float ua = __ldg(K + m) - r;   // > 0
-        if (ua < 3.f * dx) df = fmaf(__ldg(A + m), knot_stencil32(ua, dx), df);
-    }
-    if (m > 0) {
-        const float ub = __ldg(K + m - 1) - r;   // <= 0
-        if (ub > -3.f * dx) df = fmaf(__ldg(A + m - 1), knot_stencil32(ub, dx), df);
-    }
+    const float ub = e.x - r, ua = e.y - r;
+    if (ub > -3.f * dx && e.z != 0.f) df = fmaf(e.z, knot_stencil32(ub, dx), df);
+    if (ua < 3.f * dx) df = fmaf(e.w, knot_stencil32(ua, dx), df);
 }
 
 // density f and the reference's f' at an FP32 distance
-__device__ __forceinline__ void dens32f(const Dev& D, float r, float& f, float& df) {
-    cubic_eval(D.cubic + 44, D.cubic + 50, D.cubic + 86, 6, r, f, df);
+__device__ __forceinline__ void dens32f(const Dev& D, const Knots32& K, float r, float& f,
+                                        float& df) {
+    cubic_iv<6>(K.d, D.cubic + SLD_DENS_IV, r, f, df);
 }
 
 // pair term phi and the reference's phi' at an FP32 distance (ZBL core and
 // join below 2 A; within 3 r/1000 of 1.8 and 2.0 A the reference's stencil
 // also straddles the joins, which only close collisions reach: there the
 // exact derivative of the join is used)
-__device__ __forceinline__ void pair32f(const Dev& D, float r, float& v, float& dv) {
+__device__ __forceinline__ void pair32f(const Dev& D, const Knots32& K, float r, float& v,
+                                        float& dv) {
     if (r > 2.0f) {
-        cubic_eval(D.cubic, D.cubic + 8, D.cubic + 78, 8, r, v, dv);
+        cubic_iv<8>(K.p, D.cubic + SLD_PAIR_IV, r, v, dv);
         return;
     }
     pair32(D.pot32, r, v, dv);
@@ -143,15 +157,6 @@ __device__ __forceinline__ void exch32f(float r, float& J, float& dJ) {
     const float dx = r * 1e-3f, uk = rc - r;
     if (fabsf(uk) < 3.f * dx) dJ = fmaf(a, knot_stencil32(uk, dx), dJ);
 }
-
-// the same at an FP64 distance (rounded to FP32 first)
-__device__ __forceinline__ void dens32r(const Dev& D, double r, float& f, float& df) {
-    dens32f(D, (float)r, f, df);
-}
-__device__ __forceinline__ void pair32r(const Dev& D, double r, float& v, float& dv) {
-    pair32f(D, (float)r, v, dv);
-}
-__device__ __forceinline__ void exch32r(double r, float& J, float& dJ) { exch32f((float)r, J, dJ); }
 
 // F(rho) and F'(rho) from the reference's FP64 tables (potential_CPU.cpp:172-179)
 __device__ __forceinline__ void emb_tab(const Dev& D, double rho, double& F, double& dF) {
