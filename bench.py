@@ -54,11 +54,16 @@ ALGO = {
 # visits also write H, HL and sum J (72 B); 4 visits per step, 2 backward,
 # plus the visit records (64 B, twice) = 1,168 B per atom-step.
 DESIGN_BYTES_CORE_DS = 1168
-# DRAM bytes per atom and step of core_ds measured by ncu (dram__bytes_read.sum
-# + dram__bytes_write.sum); the capture is summarised in profiles/.
-CORE_DS_TRAFFIC_PER_ATOM = {"split": 4 * 508.4 + 2 * 16.0}
-CORE_DS_TRAFFIC_SOURCE = ("ncu dram__bytes at 64^3 (one sweep launch, 65,536 visits, 508 B "
-                          "per visit; visit-record pass 16 B per atom), scaled per visit")
+# DRAM bytes per atom and step of core_ds measured by ncu at 128^3 (the 72
+# k_sweep_pipe launches and the 2 k_spin_noise launches of one step,
+# dram__bytes_read.sum + dram__bytes_write.sum, ncu's default cache control:
+# caches flushed before every launch, so an upper bound on the graph's own
+# traffic); profiles/step_launches_bcc128.md.
+CORE_DS_TRAFFIC_PER_ATOM = {"split": (9764.2e6 + 556.4e6) / 4194304,
+                            "fp64": (11504.2e6 + 556.5e6) / 4194304}
+CORE_DS_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum over one step's 72 "
+                          "sweep and 2 visit-record launches at 128^3, caches flushed before "
+                          "each launch")
 ROOFLINE_KERNEL = {"core_ds": "k_sweep_pipe + k_spin_noise (core_ds: 72 sweep launches "
                               "and 2 visit-record passes per step)"}
 
