@@ -78,6 +78,9 @@ def parse():
     ap.add_argument("--size", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other workloads the default run also measures (64^3 "
+                         "Langevin in both forms, the batched replicas, the adjoint)")
     ap.add_argument("--no-fp64-arm", action="store_true",
                     help="time only the form given by --precision (the default run also "
                          "times the plain FP64 form on the same state for split / FP64)")
@@ -85,7 +88,8 @@ def parse():
                     help="keep the built-in launch shapes instead of sld_autotune's")
     ap.add_argument("--small", action="store_true",
                     help="short run for profiler captures: no CPU baseline, no e2e leg, "
-                         "no FP64 arm, no error check, one phase-profile step")
+                         "no FP64 arm, no error check, no other workloads, one phase-profile "
+                         "step")
     ap.add_argument("--workload", default="single", choices=["single", "replicas", "adjoint"],
                     help="single: the 128^3 spin-lattice-electron system; replicas: many "
                          "independent small systems advanced as one batch; adjoint: gradients "
@@ -475,11 +479,102 @@ def run_adjoint(args, world, rank, local):
     print(json.dumps(line))
 
 
+def other_configs(local):
+    """The other workloads, measured briefly in the default run (each device-
+    timed with CUDA events on its engine's stream):
+      - 64^3 cells (524,288 atoms), Langevin spin and lattice thermostats at
+        300 K, dt 1 fs, 1,000 steps in each form, with the split form's error
+        against the FP64 form on the start state and their averages at the end;
+      - 96 replicas (edges 8-32 cells, 100-1,200 K, Langevin), 20 steps batched
+        in one graph per step and 20 steps one replica after another;
+      - the adjoint: the gradient of L in the 36 potential parameters through
+        200 NVE steps of a 20^3-cell box (split forward), and its error against
+        FP64 central differences through 10 steps."""
+    from spilady_b200 import engine
+    from spilady_b200.lattice import initial_state
+    out = {}
+    rel = lambda a, b: float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+    # 64^3 Langevin
+    params, r, p, s = initial_state(64, seed=2028, tilt=0.05, temperature=300.0)
+    params["step"] = 1e-15
+    sw = dict(spinlang=True, lattlang=True)
+    n_steps = 1000
+    res, start = {}, {}
+    for name, form in (("split", engine.SPLIT), ("fp64", engine.FP64)):
+        e = engine.Engine(params, r, p, s, device=local, precision=form, **sw)
+        start[name] = {n: e.get(n) for n in ("f", "H", "rho", "pe", "me")}
+        e.run(n_steps)
+        e.sync()
+        ms = e.last_run_ms()
+        a = e.averages()
+        res[name] = {"value": e.natom * n_steps / (ms / 1e3), "ms_per_step": ms / n_steps,
+                     "Tl_K": a["Tl"], "m": float(np.sqrt(a["sx"] ** 2 + a["sy"] ** 2 + a["sz"] ** 2)),
+                     "pe": a["pe"], "me": a["me"]}
+        e.close()
+    out["bcc64_langevin"] = {
+        "workload": "bcc Fe 64^3 cells (524288 atoms), Langevin spin (gamma 0.01) and lattice "
+                    "(1/ps) thermostats at 300 K, dt 1 fs, 1000 steps, first step included",
+        "unit": "atom-steps/s", "split": res["split"], "fp64": res["fp64"],
+        "split_over_fp64": res["split"]["value"] / res["fp64"]["value"],
+        "split_error_start": {n: rel(start["split"][n], start["fp64"][n]) for n in start["fp64"]}}
+    # replicas
+    systems = replicas_workload(96)
+    engines = [engine.Engine(pr, rr, pp, ss, device=local, precision=engine.SPLIT, replica=k, **sw)
+               for k, (edge, temp, pr, rr, pp, ss) in enumerate(systems)]
+    natom = sum(e.natom for e in engines)
+    batch = engine.Batch(engines)
+    batch.run(3)
+    batch.run(20)
+    ms = batch.last_run_ms()
+    seq = 0.0
+    for e in engines:
+        e.run(20)
+        e.sync()
+        seq += e.last_run_ms()
+    batch.close()
+    for e in engines:
+        e.close()
+    out["replicas"] = {"workload": f"96 bcc Fe boxes ({natom} atoms), edges 8-32 cells, 100-1200 K, "
+                                   "Langevin spin + lattice, dt 1 fs, split form, 20 steps",
+                       "unit": "atom-steps/s", "batched": natom * 20 / (ms / 1e3),
+                       "one_by_one": natom * 20 / (seq / 1e3)}
+    # adjoint
+    params, r, p, s = initial_state(20, seed=2029, tilt=0.2, temperature=300.0, pos_sigma=0.05)
+    params["step"] = 1e-15
+    es = engine.Engine(params, r, p, s, device=local, precision=engine.SPLIT)
+    e64 = engine.Engine(params, r, p, s, device=local, precision=engine.FP64_ANALYTIC)
+    th = engine.adjoint_theta_default()
+    es.adjoint_trajectory(th, 200, 20)
+    t0 = time.perf_counter()
+    es.adjoint_trajectory(th, 200, 20)
+    grad_ms = (time.perf_counter() - t0) * 1e3
+    K = 10
+    _, g = e64.adjoint_trajectory(th, K, 5)
+    h = np.where(th != 0.0, 1e-6 * np.abs(th), 1e-6)
+    fd = np.zeros(len(th))
+    for k in range(len(th)):
+        tp, tm = th.copy(), th.copy()
+        tp[k] += h[k]
+        tm[k] -= h[k]
+        fd[k] = (e64.adjoint_trajectory(tp, K, 5, grad=False) -
+                 e64.adjoint_trajectory(tm, K, 5, grad=False)) / (2 * h[k])
+    es.close()
+    e64.close()
+    out["adjoint"] = {"workload": "gradient of L = sum |f|^2 + |H|^2 in 36 potential parameters, "
+                                  "bcc Fe 20^3 cells (16000 atoms), NVE dt 1 fs",
+                      "ms_per_gradient_200_steps_split_forward": grad_ms,
+                      "error_vs_fd_10_steps": float(np.max(np.abs(g - fd)) / np.max(np.abs(fd))),
+                      "how": "max |adjoint - FD| / max |FD|; FD: FP64 central differences, "
+                             "h = 1e-6 relative, on the FP64 analytic model"}
+    return out
+
+
 def main():
     args = parse()
     if args.small:
         args.no_cpu_baseline = True
         args.no_e2e = True
+        args.no_configs = True
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
@@ -611,6 +706,9 @@ def main():
 
     if rank != 0:
         return
+    configs = None
+    if world == 1 and not args.no_configs:
+        configs = other_configs(local)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_block(args.size)
@@ -632,6 +730,7 @@ def main():
         "split_over_fp64": (value / fp64_arm["value"]) if fp64_arm else None,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": main_arm.get("e2e"),
         "gpu_launches": main_arm["kernels_per_step"] * args.steps, "clocks": main_arm["clocks"],
+        "other_workloads": configs,
     }
     print(json.dumps(line))
 

@@ -30,6 +30,11 @@
 # JijFe.cpp are replaced at link time by oracle/ref/param_pot.cpp, which
 # restates their forms:
 #   param
+# and the reference's own main loop (spilady.cpp, reading variables.in and a
+# configuration file), NVE SLDHL, on its CPU step functions and on the B200
+# engine's (oracle/ref/core_B200.cpp linked in front of the reference's
+# objects, against spilady_b200/_lib/libsld_b200.so):
+#   main_nve  b200_nve
 #
 # usage: sh oracle/ref/build.sh [reference_dir]   (default: $SPILADY_REFERENCE,
 # else the reference tree mounted at /root/reference)
@@ -47,7 +52,7 @@ CXX=${ORACLE_CXX:-g++}
 BASE="-O3 -fopenmp -U_FORTIFY_SOURCE -D_FORTIFY_SOURCE=0 -DCPU -DOMP -w"
 
 for mode in nve lang langte baro dtstep md md_lang sdh sdh_lang sdhl sdhl_lang sldh sldh_lang \
-           md_te sdh_te sdhl_te sldh_te extf quant param; do
+           md_te sdh_te sdhl_te sldh_te extf quant param main_nve b200_nve; do
     case "$mode" in
     md*) ham=MD ;;
     sdhl*) ham=SDHL ;;
@@ -62,7 +67,9 @@ for mode in nve lang langte baro dtstep md md_lang sdh sdh_lang sdhl sdhl_lang s
     find "$src" -maxdepth 1 -type l -delete
     for f in "$REF"/*.cpp "$REF"/*.h; do
         b=$(basename "$f")
-        case "$b" in control.h|spilady.cpp) continue ;; esac
+        case "$b" in control.h) continue ;; esac
+        # the reference's own main loop only in the main_* and b200_* builds
+        case "$mode:$b" in main_*:spilady.cpp|b200_*:spilady.cpp) ;; *:spilady.cpp) continue ;; esac
         if [ "$mode" = param ]; then
             case "$b" in DD05.cpp|JijFe.cpp) continue ;; esac
         fi
@@ -90,6 +97,7 @@ for mode in nve lang langte baro dtstep md md_lang sdh sdh_lang sdhl sdhl_lang s
             echo "#define spinlang"; echo "#define lattlang"; echo "#define eltemp"
             echo "#define localcolmot"; echo "#define renormalizeEnergy" ;;
         extf) echo "#define extfield"; echo "#define extforce" ;;
+        main_nve|b200_nve) ;;
         quant) echo "#define lattlang"; echo "#define quantumnoise" ;;
         esac
     } > "$src/control.h.new"
@@ -99,17 +107,31 @@ for mode in nve lang langte baro dtstep md md_lang sdh sdh_lang sdhl sdhl_lang s
         rm -f "$src/control.h.new"
     fi
     pids=""
-    extra=""
-    if [ "$mode" = param ]; then extra="$HERE/param_pot.cpp"; fi
-    for f in "$src"/*.cpp "$HERE/harness.cpp" $extra; do
+    extra="$HERE/harness.cpp"
+    if [ "$mode" = param ]; then extra="$extra $HERE/param_pot.cpp"; fi
+    case "$mode" in
+    main_*) extra="" ;;
+    b200_*) extra="$HERE/core_B200.cpp" ;;
+    esac
+    for f in "$src"/*.cpp $extra; do
         b=$(basename "$f" .cpp)
         o="$obj/$b.o"
         if [ ! -f "$o" ] || [ "$f" -nt "$o" ] || [ "$src/control.h" -nt "$o" ]; then
-            $CXX $FLAGS -I"$src" -c "$f" -o "$o" &
+            $CXX $FLAGS -I"$src" -I"$HERE/../../include" -c "$f" -o "$o" &
             pids="$pids $!"
         fi
     done
     for p in $pids; do wait "$p"; done
-    $CXX -fopenmp "$obj"/*.o -o "$OUT/spilady_ref_$mode" -lm
+    case "$mode" in
+    b200_*)
+        # the backend's definitions first: the linker keeps the first of the
+        # step functions the reference's *_CPU.cpp objects define again
+        lib=$(cd "$HERE/../../spilady_b200/_lib" && pwd)
+        $CXX -fopenmp "$obj/core_B200.o" $(ls "$obj"/*.o | grep -v '/core_B200\.o$') \
+            -Wl,--allow-multiple-definition -L"$lib" -lsld_b200 -Wl,-rpath,'$ORIGIN/../../spilady_b200/_lib' \
+            -o "$OUT/spilady_ref_$mode" -lm ;;
+    *)
+        $CXX -fopenmp "$obj"/*.o -o "$OUT/spilady_ref_$mode" -lm ;;
+    esac
 done
 echo "built: $(ls "$OUT"/spilady_ref_* | tr '\n' ' ')"
