@@ -502,7 +502,7 @@ def other_configs(local):
     res, start = {}, {}
     for name, form in (("split", engine.SPLIT), ("fp64", engine.FP64)):
         e = engine.Engine(params, r, p, s, device=local, precision=form, **sw)
-        start[name] = {n: e.get(n) for n in ("f", "H", "rho", "pe", "me")}
+        start[name] = {n: e.get(n) for n in ("f", "rho", "pe", "me")}
         e.run(n_steps)
         e.sync()
         ms = e.last_run_ms()
@@ -516,7 +516,14 @@ def other_configs(local):
                     "(1/ps) thermostats at 300 K, dt 1 fs, 1000 steps, first step included",
         "unit": "atom-steps/s", "split": res["split"], "fp64": res["fp64"],
         "split_over_fp64": res["split"]["value"] / res["fp64"]["value"],
-        "split_error_start": {n: rel(start["split"][n], start["fp64"][n]) for n in start["fp64"]}}
+        "split_error_start": dict(
+            {n: rel(start["split"][n], start["fp64"][n]) for n in start["fp64"]},
+            f_abs_eV_per_A=float(np.max(np.abs(start["split"]["f"] - start["fp64"]["f"]))),
+            how="max |split - fp64| / max |fp64| on the perfect-lattice start state, whose "
+                "net forces nearly vanish by symmetry (so f_abs is given too)"),
+        "split_vs_fp64_averages_at_end": {
+            q: abs(res["split"][q] - res["fp64"][q]) / abs(res["fp64"][q])
+            for q in ("Tl_K", "m", "pe", "me")}}
     # replicas
     systems = replicas_workload(96)
     engines = [engine.Engine(pr, rr, pp, ss, device=local, precision=engine.SPLIT, replica=k, **sw)
