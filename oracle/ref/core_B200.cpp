@@ -106,7 +106,11 @@ void links() {
     links_CPU();
 }
 void calculate_rho() { ok(sld_calculate_rho(ctx()), "calculate_rho"); }
-void calculate_force_energy() { ok(sld_calculate_force_energy(ctx()), "calculate_force_energy"); }
+void calculate_force_energy() {
+    ok(sld_calculate_force_energy(ctx()), "calculate_force_energy");
+    // the total virial calculate_force_energy_CPU.cpp:296-299 leaves for check_pressure
+    ok(sld_virial(ctx(), &virial), "sld_virial");
+}
 void core_ds(double dt) { ok(sld_core_ds(ctx(), dt), "core_ds"); }
 void core_dp(double dt) { ok(sld_core_dp(ctx(), dt), "core_dp"); }
 void core_dr(double dt) { ok(sld_core_dr(ctx(), dt), "core_dr"); }
