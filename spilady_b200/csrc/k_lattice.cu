@@ -126,7 +126,8 @@ __device__ __forceinline__ double3 dp_cell(const Dev& D, const P& P_, const int*
         } else {
             double T = D.eltemp ? D.Te[D.node[i]] : D.temperature;
             double amp = sqrt(2.0 * T * D.gamma_L / dt);
-            double3 xi = normals3(D.seed, D.replica, (unsigned)D.id[i], epoch);
+            double3 xi = D.split ? normals3_f32(D.seed, D.replica, (unsigned)D.id[i], epoch)
+                                 : normals3(D.seed, D.replica, (unsigned)D.id[i], epoch);
             fx = amp * xi.x; fy = amp * xi.y; fz = amp * xi.z;
         }
         double4 f = D.f[i];

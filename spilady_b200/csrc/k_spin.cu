@@ -48,7 +48,10 @@ __global__ void __launch_bounds__(256) k_spin_noise(Dev D, int epoch_off, double
     double T = D.eltemp ? D.Te[D.node[i]] : D.temperature;
     const double rho = D.rho[i];
     for (int v = 0; v < 2; ++v) {
-        double3 x = spin_noise_dS(D, T, normals3(D.seed, D.replica, (unsigned)D.id[i], e0 + v), dt);
+        const unsigned id = (unsigned)D.id[i];
+        const double3 xi = D.split ? normals3_f32(D.seed, D.replica, id, e0 + v)
+                                   : normals3(D.seed, D.replica, id, e0 + v);
+        double3 x = spin_noise_dS(D, T, xi, dt);
         D.vrec[2 * (size_t)i + v] = make_double4(rho, x.x, x.y, x.z);
     }
 }

@@ -344,6 +344,26 @@ __device__ __forceinline__ double3 normals3(unsigned seed, unsigned replica, uns
     return make_double3(ra * ca, ra * sa, rb * cb);
 }
 
+// The same three normals from the same counter, with the Box-Muller transform
+// in FP32 (the split form's thermostats).  The uniforms are (k + 1/2) 2^-32
+// rounded to FP32, which keeps their relative precision (2^-24) down to the
+// smallest, so each normal differs from the FP64 transform's by about 1e-7
+// relative, in the tails too.  The noise is a stochastic force and field;
+// what the split form keeps in FP64 is the integration it enters.
+__device__ __forceinline__ double3 normals3_f32(unsigned seed, unsigned replica, unsigned atom,
+                                                unsigned long long epoch) {
+    uint32_t c[4] = {atom, (uint32_t)epoch, (uint32_t)(epoch >> 32), 0x53504e53u};
+    philox4x32_10(c, seed, replica);
+    const float s = 2.3283064365386963e-10f;   // 2^-32; u <= 1, so -2 log u >= 0
+    const float u0 = ((float)c[0] + 0.5f) * s, u1 = ((float)c[1] + 0.5f) * s;
+    const float u2 = ((float)c[2] + 0.5f) * s, u3 = ((float)c[3] + 0.5f) * s;
+    const float ra = sqrtf(-2.f * logf(u0)), rb = sqrtf(-2.f * logf(u2));
+    float sa, ca;
+    sincospif(2.f * u1, &sa, &ca);
+    const float cb = cospif(2.f * u3);
+    return make_double3((double)(ra * ca), (double)(ra * sa), (double)(rb * cb));
+}
+
 // ---------------------------------------------------------------------
 // heat capacity of the electrons: heatcapacity_CPU.cpp:34-57
 __device__ __forceinline__ double te_Ce(double Te) {

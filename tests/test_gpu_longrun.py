@@ -51,13 +51,16 @@ def test_nve_energy_drift_no_worse_than_reference(precision, tmp_path):
     assert d_ours <= limit * d_ref
 
 
-def test_langevin_equilibrium_matches_reference(tmp_path):
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_langevin_equilibrium_matches_reference(precision, tmp_path):
+    # the split form too: FP32 pair terms and fields, FP32 Box-Muller normals
     E = engine_mod()
     g = load_golden("long_runs_ref")
     n = int(g["lang_steps"])
     params, r, p, s = initial_state(10, seed=7, tilt=0.05, temperature=300.0)
     reps = 8
-    engines = [E.Engine(params, r, p, s, spinlang=True, lattlang=True, replica=k)
+    prec = E.FP64 if precision == "fp64" else E.SPLIT
+    engines = [E.Engine(params, r, p, s, spinlang=True, lattlang=True, replica=k, precision=prec)
                for k in range(reps)]
     batch = E.Batch(engines)
     for k in range(n):
@@ -75,5 +78,6 @@ def test_langevin_equilibrium_matches_reference(tmp_path):
         # one reference realisation against the mean of eight: the standard
         # deviation of their difference is spread * sqrt(1 + 1/8)
         z = abs(theirs - ours.mean()) / (spread * np.sqrt(1.0 + 1.0 / reps))
-        print(f"{name}: engine {ours.mean():.3f} +- {spread:.3f}, reference {theirs:.3f}, z {z:.2f}")
+        print(f"{precision} {name}: engine {ours.mean():.3f} +- {spread:.3f}, reference "
+              f"{theirs:.3f}, z {z:.2f}")
         assert z <= 4.0, f"{name}: {z:.2f} standard deviations apart"
