@@ -240,6 +240,7 @@ __device__ void pairs_split_one(const Dev& D, int i, int write_rho) {
                     exch32f(r, J, dJ);
                     D.jl[(size_t)i * SLD_MAXJ + nj] = jb[u];
                     D.jvf[(size_t)i * SLD_MAXJ + nj] = J;
+                    D.jlk[(size_t)i * SLD_MAXJ + nj] = (unsigned char)k;
                 }
                 ++nj;
             }
@@ -328,9 +329,16 @@ __device__ __forceinline__ void force_finish(const Dev& D, int i, double si_sq, 
     if (!isfinite(fx + fy + fz + pe)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
 }
 
+// The magnetic part over the exchange rows (ROWS): an exchange entry is
+// appended for a neighbour-list entry exactly when its pair vector passes
+// the exchange cutoff, so the rows hold the neighbour list's magnetic pairs
+// in its order and the sums are those of the pass over the neighbour list,
+// with 14 entries per atom to gather instead of 26 (bcc Fe).
+
 // FP64 force pass; AN: the analytic forms instead of the tables
-template <bool AN, int PART>
+template <bool AN, int PART, bool ROWS = false>
 __device__ __forceinline__ void force64_one(const Dev& D, int i) {
+    static_assert(!ROWS || PART == PART_MAG, "the exchange rows hold the magnetic pairs only");
     unsigned* err = &D.ctl->err;
     const int N = D.natom;
     double4 ri = D.r[i];
@@ -341,13 +349,22 @@ __device__ __forceinline__ void force64_one(const Dev& D, int i) {
     double dF_i = (PART & PART_EAM) ? D.dF[i] : 0.0;
     double fx = 0, fy = 0, fz = 0, pe = 0, me = 0, me0 = 0, vir = 0;
     double st6[6] = {0, 0, 0, 0, 0, 0};
-    int nn = D.nbr_n[i];
+    const int nn = ROWS ? D.jl_n[i] : D.nbr_n[i];
     for (int e0 = 0; e0 < nn; e0 += 4) {
       int pkb[4];
       double4 rjb[4];
       double dFb[4];
+      if constexpr (ROWS) {
+          // find_image on every entry, which leaves a vector that needs no
+          // image unchanged (the list's SLD_WRAP marks where it moves one)
+          const int4 w = __ldg(reinterpret_cast<const int4*>(D.jl + (size_t)i * SLD_MAXJ + e0));
+          const int q[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
-      for (int u = 0; u < 4; ++u) pkb[u] = e0 + u < nn ? D.nbr[(size_t)(e0 + u) * N + i] : -1;
+          for (int u = 0; u < 4; ++u) pkb[u] = e0 + u < nn ? (q[u] | SLD_WRAP) : -1;
+      } else {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) pkb[u] = e0 + u < nn ? D.nbr[(size_t)(e0 + u) * N + i] : -1;
+      }
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
           int j = pkb[u] & SLD_JMASK;
@@ -419,10 +436,10 @@ __device__ __forceinline__ void force64_one(const Dev& D, int i) {
     force_finish<PART>(D, i, si_sq, rho_i, F_i, fx, fy, fz, pe, me, me0, vir, st6);
 }
 
-template <bool AN, int PART>
+template <bool AN, int PART, bool ROWS = false>
 __global__ void __launch_bounds__(128) k_force64(Dev D) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x)
-        force64_one<AN, PART>(D, i);
+        force64_one<AN, PART, ROWS>(D, i);
 }
 
 // Split form: FP32 pair vectors from the fixed-point cell positions (fxa, the
@@ -430,8 +447,9 @@ __global__ void __launch_bounds__(128) k_force64(Dev D) {
 // reference's derivatives, compensated (Kahan) FP32 sums for the forces and
 // energies; the stress and virial products (FP32) are summed in FP64.  Four
 // entries' loads are issued together.
-template <int PART, bool ORTHO>
+template <int PART, bool ORTHO, bool ROWS = false>
 __device__ __forceinline__ void force32_one(const Dev& D, int i) {
+    static_assert(!ROWS || PART == PART_MAG, "the exchange rows hold the magnetic pairs only");
     const int N = D.natom;
     const int4 fi = __ldg(D.fxa + i);
     const FxMat M = fx_mat(D);
@@ -445,17 +463,30 @@ __device__ __forceinline__ void force32_one(const Dev& D, int i) {
     const Knots32 K = knots32(D);
     Kahan fx, fy, fz, pe, me, me0;
     double st[6] = {0, 0, 0, 0, 0, 0}, vir = 0.0;
-    const int nn = D.nbr_n[i];
+    const int nn = ROWS ? D.jl_n[i] : D.nbr_n[i];
     for (int e0 = 0; e0 < nn; e0 += 4) {
         int jb[4], kb[4];
         int4 qb[4];
         float4 sb[4];
         float dFb[4];
+        if constexpr (ROWS) {
+            const size_t at = (size_t)i * SLD_MAXJ + e0;
+            const int4 w = __ldg(reinterpret_cast<const int4*>(D.jl + at));
+            const unsigned kw = __ldg(reinterpret_cast<const unsigned*>(D.jlk + at));
+            const int q[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const bool in = e0 + u < nn;
-            jb[u] = in ? (D.nbr[(size_t)(e0 + u) * N + i] & SLD_JMASK) : i;
-            kb[u] = in ? D.nbk[(size_t)(e0 + u) * N + i] : 26;
+            for (int u = 0; u < 4; ++u) {
+                const bool in = e0 + u < nn;
+                jb[u] = in ? q[u] : i;
+                kb[u] = in ? (int)((kw >> (8 * u)) & 255u) : 26;
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const bool in = e0 + u < nn;
+                jb[u] = in ? (D.nbr[(size_t)(e0 + u) * N + i] & SLD_JMASK) : i;
+                kb[u] = in ? D.nbk[(size_t)(e0 + u) * N + i] : 26;
+            }
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -509,11 +540,11 @@ __device__ __forceinline__ void force32_one(const Dev& D, int i) {
                        pe.value(), me.value(), me0.value(), vir, st);
 }
 
-template <int PART, bool ORTHO>
+template <int PART, bool ORTHO, bool ROWS = false>
 __global__ void __launch_bounds__(128) k_force32(Dev D) {
     // one atom per thread; a capped grid walks several atoms per thread
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x)
-        force32_one<PART, ORTHO>(D, i);
+        force32_one<PART, ORTHO, ROWS>(D, i);
 }
 
 // a cap on the CTAs per SM (0: none) for the kernels of the step graph's side
@@ -578,4 +609,15 @@ void launch_force_eam(const Dev& D, cudaStream_t st) {
     launch_embed(D, st);
     launch_force_part<PART_EAM>(D, st);
 }
-void launch_force_mag(const Dev& D, cudaStream_t st) { launch_force_part<PART_MAG>(D, st); }
+// the magnetic part from the exchange rows of the list pass that ran on the
+// same positions (the step graph's order)
+void launch_force_mag(const Dev& D, cudaStream_t st) {
+    const int bs = D.tune.force_block > 0 ? D.tune.force_block : 128;
+    const int nb = div_up(D.natom, bs);
+    if (D.split) {
+        if (box_ortho(D)) k_force32<PART_MAG, true, true><<<nb, bs, 0, st>>>(D);
+        else k_force32<PART_MAG, false, true><<<nb, bs, 0, st>>>(D);
+    }
+    else if (D.analytic) k_force64<true, PART_MAG, true><<<nb, bs, 0, st>>>(D);
+    else k_force64<false, PART_MAG, true><<<nb, bs, 0, st>>>(D);
+}

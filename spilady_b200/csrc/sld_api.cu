@@ -555,7 +555,9 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
         D.cubic64 = cub64;
     }
     for (int k = 0; k < 2 && ok; ++k) {
-        if (prm->precision == SLD_SPLIT) ok = c->alloc(&c->jvf_set[k], (size_t)SLD_MAXJ * n) == 0;
+        if (prm->precision == SLD_SPLIT)
+            ok = c->alloc(&c->jvf_set[k], (size_t)SLD_MAXJ * n) == 0 &&
+                 c->alloc(&c->jlk_set[k], (size_t)SLD_MAXJ * n) == 0;
         else ok = c->alloc(&c->jv_set[k], (size_t)SLD_MAXJ * n) == 0;
     }
     if (ok) use_set(c, 0);

@@ -154,6 +154,8 @@ struct Dev {
     int *nbr, *nbr_n, *jl, *jl_n;
     double* jv;                   // FP64 form
     float* jvf;                   // split form
+    unsigned char* jlk;           // split form: [natom][SLD_MAXJ] the neighbour cell
+                                  // (0..26) of each exchange entry, as nbk
     double* dF;                   // F'(rho) per atom, refreshed after each rho pass
     double4* vrec;                // [natom][2 sweeps] visit records of one core_ds: rho and
                                   // the noise increment dS of the atom's visit in that sweep

@@ -46,6 +46,7 @@ struct sld_ctx {
     int* jln_set[2] = {nullptr, nullptr};
     double* jv_set[2] = {nullptr, nullptr};
     float* jvf_set[2] = {nullptr, nullptr};
+    unsigned char* jlk_set[2] = {nullptr, nullptr};
     double* rho_set[2] = {nullptr, nullptr};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
@@ -96,6 +97,7 @@ inline Dev dev_set(const sld_ctx* c, int k) {
     D.jl_n = c->jln_set[k];
     D.jv = c->jv_set[k];
     D.jvf = c->jvf_set[k];
+    D.jlk = c->jlk_set[k];
     D.rho = c->rho_set[k];
     return D;
 }
