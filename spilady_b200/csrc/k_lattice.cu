@@ -240,6 +240,9 @@ __global__ void __launch_bounds__(1024) k_factor(Dev D, int nb) {
     }
 }
 
+// TEMP: also the kinetic terms of calculate_temperature (the kinetic energy
+// and the momentum) into the Te-node accumulators
+template <bool TEMP>
 __global__ void __launch_bounds__(256) k_scale(Dev D) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= D.natom) return;
@@ -249,7 +252,12 @@ __global__ void __launch_bounds__(256) k_scale(Dev D) {
     p.y = k * (p.y - D.ctl->avep[1]);
     p.z = k * (p.z - D.ctl->avep[2]);
     D.p[i] = p;
-    D.ke[i] = (p.x * p.x + p.y * p.y + p.z * p.z) / 2.0 / D.atmass;
+    const double ke = (p.x * p.x + p.y * p.y + p.z * p.z) / 2.0 / D.atmass;
+    D.ke[i] = ke;
+    if constexpr (TEMP) {
+        double v[4] = {ke, p.x, p.y, p.z};
+        node_add<4>(D, D.node[i], v, 0);
+    }
 }
 
 __global__ void __launch_bounds__(256) k_dr(Dev D, double dt) {
@@ -293,7 +301,7 @@ __global__ void k_quantum_tick(Dev D) {
     if (threadIdx.x == 0) ++D.ctl->qcount;
 }
 
-void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off) {
+void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off, bool temp) {
     int nb;
     if (D.lattlang) {
         if (D.quantum) k_quantum_update<<<div_up(D.natom, 256), 256, 0, st>>>(D);
@@ -308,7 +316,8 @@ void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off) {
     int na = div_up(D.natom, 256);
     k_ke_partials<<<na, 256, 0, st>>>(D);
     k_factor<<<1, 1024, 0, st>>>(D, na);
-    k_scale<<<na, 256, 0, st>>>(D);
+    if (temp) k_scale<true><<<na, 256, 0, st>>>(D);
+    else k_scale<false><<<na, 256, 0, st>>>(D);
 }
 
 void launch_dr(const Dev& D, cudaStream_t st, double dt) {

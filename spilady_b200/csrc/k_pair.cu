@@ -335,10 +335,14 @@ __device__ __forceinline__ void force_finish(const Dev& D, int i, double si_sq, 
 // in its order and the sums are those of the pass over the neighbour list,
 // with 14 entries per atom to gather instead of 26 (bcc Fe).
 
-// FP64 force pass; AN: the analytic forms instead of the tables
-template <bool AN, int PART, bool ROWS = false>
-__device__ __forceinline__ void force64_one(const Dev& D, int i) {
+// FP64 force pass; AN: the analytic forms instead of the tables.  TEMP
+// (with ROWS): also the spin terms of calculate_temperature into tv[0..3],
+// from the exchange field summed as exchange_field does (the rows' J and the
+// neighbours' spins, in row order).
+template <bool AN, int PART, bool ROWS = false, bool TEMP = false>
+__device__ __forceinline__ void force64_one(const Dev& D, int i, double4& tv) {
     static_assert(!ROWS || PART == PART_MAG, "the exchange rows hold the magnetic pairs only");
+    static_assert(!TEMP || ROWS, "the temperature terms come from the exchange rows");
     unsigned* err = &D.ctl->err;
     const int N = D.natom;
     double4 ri = D.r[i];
@@ -349,11 +353,18 @@ __device__ __forceinline__ void force64_one(const Dev& D, int i) {
     double dF_i = (PART & PART_EAM) ? D.dF[i] : 0.0;
     double fx = 0, fy = 0, fz = 0, pe = 0, me = 0, me0 = 0, vir = 0;
     double st6[6] = {0, 0, 0, 0, 0, 0};
+    double hx = 0, hy = 0, hz = 0, hj = 0;   // the exchange field (TEMP)
+    if (TEMP && D.hext) {
+        const double4 h = D.hext[i];
+        hx = h.x; hy = h.y; hz = h.z;
+    }
     const int nn = ROWS ? D.jl_n[i] : D.nbr_n[i];
     for (int e0 = 0; e0 < nn; e0 += 4) {
       int pkb[4];
       double4 rjb[4];
       double dFb[4];
+      double4 sjb[4];
+      double Jb[4];
       if constexpr (ROWS) {
           // find_image on every entry, which leaves a vector that needs no
           // image unchanged (the list's SLD_WRAP marks where it moves one)
@@ -370,6 +381,15 @@ __device__ __forceinline__ void force64_one(const Dev& D, int i) {
           int j = pkb[u] & SLD_JMASK;
           rjb[u] = pkb[u] >= 0 ? D.r[j] : ri;
           dFb[u] = (pkb[u] >= 0 && (PART & PART_EAM)) ? D.dF[j] : 0.0;
+          if constexpr (TEMP) {
+              sjb[u] = pkb[u] >= 0 ? D.s[j] : make_double4(0, 0, 0, 0);
+              Jb[u] = pkb[u] >= 0 ? D.jv[(size_t)i * SLD_MAXJ + e0 + u] : 0.0;
+          }
+      }
+      if constexpr (TEMP) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+              if (pkb[u] >= 0) exch_add64(hx, hy, hz, hj, Jb[u], sjb[u]);
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
@@ -398,7 +418,9 @@ __device__ __forceinline__ void force64_one(const Dev& D, int i) {
             pe += 0.5 * phi;
         }
         if ((PART & PART_MAG) && r0 < D.rcut_mag) {
-            double4 sj = D.s[j];
+            double4 sj;
+            if constexpr (TEMP) sj = sjb[u];
+            else sj = D.s[j];
             double sj_sq = sj.x * sj.x + sj.y * sj.y + sj.z * sj.z;
             double dot = si.x * sj.x + si.y * sj.y + si.z * sj.z;
             double times = sqrt(si_sq * sj_sq);
@@ -434,12 +456,28 @@ __device__ __forceinline__ void force64_one(const Dev& D, int i) {
         }
     }
     force_finish<PART>(D, i, si_sq, rho_i, F_i, fx, fy, fz, pe, me, me0, vir, st6);
+    if constexpr (TEMP)
+        temp_spin_terms(D, i, make_double3(hx, hy, hz), hj, tv.x, tv.y, tv.z, tv.w);
 }
 
 template <bool AN, int PART, bool ROWS = false>
 __global__ void __launch_bounds__(128) k_force64(Dev D) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x)
-        force64_one<AN, PART, ROWS>(D, i);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x) {
+        double4 unused;
+        force64_one<AN, PART, ROWS>(D, i, unused);
+    }
+}
+
+// the magnetic part and the spin terms of calculate_temperature, one atom a
+// thread (the node sums need the lanes of a warp on consecutive atoms)
+template <bool AN>
+__global__ void __launch_bounds__(128) k_force64_temp(Dev D) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.natom) return;
+    double4 t;
+    force64_one<AN, PART_MAG, true, true>(D, i, t);
+    double v[4] = {t.x, t.y, t.z, t.w};
+    node_add<4>(D, D.node[i], v, 4);
 }
 
 // Split form: FP32 pair vectors from the fixed-point cell positions (fxa, the
@@ -447,9 +485,10 @@ __global__ void __launch_bounds__(128) k_force64(Dev D) {
 // reference's derivatives, compensated (Kahan) FP32 sums for the forces and
 // energies; the stress and virial products (FP32) are summed in FP64.  Four
 // entries' loads are issued together.
-template <int PART, bool ORTHO, bool ROWS = false>
-__device__ __forceinline__ void force32_one(const Dev& D, int i) {
+template <int PART, bool ORTHO, bool ROWS = false, bool TEMP = false>
+__device__ __forceinline__ void force32_one(const Dev& D, int i, double4& tv) {
     static_assert(!ROWS || PART == PART_MAG, "the exchange rows hold the magnetic pairs only");
+    static_assert(!TEMP || ROWS, "the temperature terms come from the exchange rows");
     const int N = D.natom;
     const int4 fi = __ldg(D.fxa + i);
     const FxMat M = fx_mat(D);
@@ -463,16 +502,19 @@ __device__ __forceinline__ void force32_one(const Dev& D, int i) {
     const Knots32 K = knots32(D);
     Kahan fx, fy, fz, pe, me, me0;
     double st[6] = {0, 0, 0, 0, 0, 0}, vir = 0.0;
+    float ks[4] = {0, 0, 0, 0}, kc[4] = {0, 0, 0, 0};   // the exchange field (TEMP)
     const int nn = ROWS ? D.jl_n[i] : D.nbr_n[i];
     for (int e0 = 0; e0 < nn; e0 += 4) {
         int jb[4], kb[4];
         int4 qb[4];
         float4 sb[4];
         float dFb[4];
+        float4 Jw = make_float4(0.f, 0.f, 0.f, 0.f);
         if constexpr (ROWS) {
             const size_t at = (size_t)i * SLD_MAXJ + e0;
             const int4 w = __ldg(reinterpret_cast<const int4*>(D.jl + at));
             const unsigned kw = __ldg(reinterpret_cast<const unsigned*>(D.jlk + at));
+            if constexpr (TEMP) Jw = __ldg(reinterpret_cast<const float4*>(D.jvf + at));
             const int q[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
@@ -493,6 +535,12 @@ __device__ __forceinline__ void force32_one(const Dev& D, int i) {
             qb[u] = __ldg(D.fxa + jb[u]);
             dFb[u] = (PART & PART_EAM) ? (float)__ldg(D.dF + jb[u]) : 0.f;
             sb[u] = (PART & PART_MAG) ? __ldg(D.s32 + jb[u]) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        if constexpr (TEMP) {
+            const float Jq[4] = {Jw.x, Jw.y, Jw.z, Jw.w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (e0 + u < nn) exch_add32(ks, kc, Jq[u], sb[u]);
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -538,13 +586,27 @@ __device__ __forceinline__ void force32_one(const Dev& D, int i) {
     if (PART & PART_EAM) F = interp(D.tF, rho_i, D.inv_rho, &D.ctl->err);
     force_finish<PART>(D, i, si_sq, rho_i, F, fx.value(), fy.value(), fz.value(),
                        pe.value(), me.value(), me0.value(), vir, st);
+    if constexpr (TEMP) {
+        // exchange_field's split-form result: the compensated sums, then the
+        // external field added in FP64
+        double hx = (double)ks[0] - (double)kc[0], hy = (double)ks[1] - (double)kc[1],
+               hz = (double)ks[2] - (double)kc[2];
+        const double hj = (double)ks[3] - (double)kc[3];
+        if (D.hext) {
+            const double4 h = D.hext[i];
+            hx = h.x + hx; hy = h.y + hy; hz = h.z + hz;
+        }
+        temp_spin_terms(D, i, make_double3(hx, hy, hz), hj, tv.x, tv.y, tv.z, tv.w);
+    }
 }
 
 template <int PART, bool ORTHO, bool ROWS = false>
 __global__ void __launch_bounds__(128) k_force32(Dev D) {
     // one atom per thread; a capped grid walks several atoms per thread
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x)
-        force32_one<PART, ORTHO, ROWS>(D, i);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x) {
+        double4 unused;
+        force32_one<PART, ORTHO, ROWS>(D, i, unused);
+    }
 }
 
 // a cap on the CTAs per SM (0: none) for the kernels of the step graph's side
@@ -609,11 +671,33 @@ void launch_force_eam(const Dev& D, cudaStream_t st) {
     launch_embed(D, st);
     launch_force_part<PART_EAM>(D, st);
 }
+template <bool ORTHO>
+__global__ void __launch_bounds__(128) k_force32_temp(Dev D) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.natom) return;
+    double4 t;
+    force32_one<PART_MAG, ORTHO, true, true>(D, i, t);
+    double v[4] = {t.x, t.y, t.z, t.w};
+    node_add<4>(D, D.node[i], v, 4);
+}
+
 // the magnetic part from the exchange rows of the list pass that ran on the
-// same positions (the step graph's order)
-void launch_force_mag(const Dev& D, cudaStream_t st) {
+// same positions (the step graph's order); temp: also the spin terms of
+// calculate_temperature into the Te-node accumulators (launch_temperature_begin
+// zeroes them; the last kick's rescale adds the kinetic terms)
+void launch_force_mag(const Dev& D, cudaStream_t st, bool temp) {
     const int bs = D.tune.force_block > 0 ? D.tune.force_block : 128;
     const int nb = div_up(D.natom, bs);
+    if (temp) {
+        const int nt = div_up(D.natom, 128);
+        if (D.split) {
+            if (box_ortho(D)) k_force32_temp<true><<<nt, 128, 0, st>>>(D);
+            else k_force32_temp<false><<<nt, 128, 0, st>>>(D);
+        }
+        else if (D.analytic) k_force64_temp<true><<<nt, 128, 0, st>>>(D);
+        else k_force64_temp<false><<<nt, 128, 0, st>>>(D);
+        return;
+    }
     if (D.split) {
         if (box_ortho(D)) k_force32<PART_MAG, true, true><<<nb, bs, 0, st>>>(D);
         else k_force32<PART_MAG, false, true><<<nb, bs, 0, st>>>(D);

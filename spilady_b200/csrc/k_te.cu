@@ -17,7 +17,7 @@ __device__ __forceinline__ void gather_field_t(const Dev& D, int i, double3& H, 
 }
 
 // per-atom terms of calculate_temperature; writes H, HL, sumJ and returns
-// the five sums (R_up, R_dn, L_up, L_dn) it contributes
+// the four sums (R_up, R_dn, L_up, L_dn) it contributes
 __device__ __forceinline__ void temp_atom(const Dev& D, int i, double& Rup, double& Rdn, double& Lup,
                                           double& Ldn) {
     Rup = Rdn = Lup = Ldn = 0.0;
@@ -25,32 +25,8 @@ __device__ __forceinline__ void temp_atom(const Dev& D, int i, double& Rup, doub
     double3 H;
     double sumJ;
     gather_field_t(D, i, H, sumJ);
-    double4 s4 = D.s[i];
-    double3 s = make_double3(s4.x, s4.y, s4.z);
-    double cx_ = s.y * H.z - H.y * s.z, cy_ = s.z * H.x - H.z * s.x, cz_ = s.x * H.y - H.x * s.y;
-    Rup = cx_ * cx_ + cy_ * cy_ + cz_ * cz_;
-    Rdn = s.x * H.x + s.y * H.y + s.z * H.z;
-    D.H[i] = make_double4(H.x, H.y, H.z, 0.0);
-    if (!D.landau_on) return;   // the Heisenberg Hamiltonians: no Landau field
-    if (!D.hc) sumJ = 0.0;      // the exchange correction is SLDHL's
-    double rho = D.rho[i];
-    double A = interp_const(D.landau[0], rho, D.inv_rho);
-    double B = interp_const(D.landau[1], rho, D.inv_rho);
-    double C = interp_const(D.landau[2], rho, D.inv_rho);
-    double Dd = interp_const(D.landau[3], rho, D.inv_rho);
-    double s_sq = s.x * s.x + s.y * s.y + s.z * s.z;
-    double s0 = sqrt(s_sq);
-    double c = -(2.0 * A + 4.0 * B * s_sq + 6.0 * C * (s_sq * s_sq) + 8.0 * Dd * (s_sq * s_sq * s_sq));
-    double k = -sumJ / s0;
-    double3 HL = make_double3(c * s.x + k * s.x, c * s.y + k * s.y, c * s.z + k * s.z);
-    double hx = H.x + HL.x, hy = H.y + HL.y, hz = H.z + HL.z;
-    Lup = hx * hx + hy * hy + hz * hz;
-    Ldn = 6.0 * A + 20.0 * B * s_sq + 42.0 * C * (s_sq * s_sq) + 72.0 * Dd * (s_sq * s_sq * s_sq);
-    Ldn += 2.0 * sumJ / s0;
-    D.HL[i] = make_double4(HL.x, HL.y, HL.z, 0.0);
-    if (D.hc) D.sumJ[i] = sumJ;
+    temp_spin_terms(D, i, H, sumJ, Rup, Rdn, Lup, Ldn);
 }
-
 // per-Te-cell results from the sums (calculate_temperature_CPU.cpp:118-142)
 __device__ __forceinline__ void temp_finish(const Dev& D, int k, double n, double sum_ke, double apx,
                                             double apy, double apz, double Rup, double Rdn, double Lup,
@@ -105,37 +81,8 @@ __global__ void __launch_bounds__(128) k_temp_atom(Dev D) {
     double a, b, e, f;
     temp_atom(D, i, a, b, e, f);
     double4 p = D.p[i];
-    // Atoms are stored cell by cell, so neighbouring lanes mostly share a
-    // node: a segmented warp scan (segments = runs of equal node, marked by
-    // head flags) sums each run, and the run's last lane does the atomics.
-    // Lanes past natom have returned; the active lanes are a prefix.
-    int node = D.node[i];
     double v[8] = {D.ke[i], p.x, p.y, p.z, a, b, e, f};
-    const unsigned act = __activemask();
-    const int lane = threadIdx.x & 31;
-    int prev = __shfl_up_sync(act, node, 1);
-    int head = (lane == 0 || prev != node) ? 1 : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int th = __shfl_up_sync(act, head, o);
-        double t[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) t[q] = __shfl_up_sync(act, v[q], o);
-        if (lane >= o) {
-            if (!head) {
-#pragma unroll
-                for (int q = 0; q < 8; ++q) v[q] += t[q];
-            }
-            head |= th;
-        }
-    }
-    int nxt = __shfl_down_sync(act, node, 1);
-    bool last = lane == 31 || !((act >> (lane + 1)) & 1u) || nxt != node;
-    if (last) {
-        double* acc = D.acc + 9 * (size_t)node;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) atomicAdd(acc + q, v[q]);
-    }
+    node_add<8>(D, D.node[i], v, 0);
 }
 
 __global__ void k_temp_node(Dev D) {
@@ -143,6 +90,13 @@ __global__ void k_temp_node(Dev D) {
     if (k >= D.nte) return;
     const double* a = D.acc + 9 * (size_t)k;
     temp_finish(D, k, (double)D.te_count[k], a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7]);
+}
+
+void launch_temperature_begin(const Dev& D, cudaStream_t st) {
+    cudaMemsetAsync(D.acc, 0, sizeof(double) * 9 * (size_t)D.nte, st);
+}
+void launch_temperature_end(const Dev& D, cudaStream_t st) {
+    k_temp_node<<<div_up(D.nte, 128), 128, 0, st>>>(D);
 }
 
 void launch_temperature(const Dev& D, cudaStream_t st) {

@@ -95,8 +95,8 @@ void enqueue_ds(sld_ctx* c, const Dev& D, double dt, int& eoff, bool fields = tr
 }
 void enqueue_ds(sld_ctx* c, double dt, int& eoff) { enqueue_ds(c, c->D, dt, eoff); }
 
-void enqueue_dp(sld_ctx* c, const Dev& D, double dt, int& eoff) {
-    launch_dp(D, c->st, dt, eoff);
+void enqueue_dp(sld_ctx* c, const Dev& D, double dt, int& eoff, bool temp = false) {
+    launch_dp(D, c->st, dt, eoff, temp);
     if (c->P.lattlang) ++eoff;
 }
 void enqueue_dp(sld_ctx* c, double dt, int& eoff) { enqueue_dp(c, c->D, dt, eoff); }
@@ -199,11 +199,18 @@ void enqueue_step(sld_ctx* c) {
     cudaStreamWaitEvent(M, ev[2], 0);
     enqueue_ds(c, Dn, dt / 2e0, eoff, !c->P.eltemp);
     cudaStreamWaitEvent(M, ev[3], 0);
-    launch_force_mag(Dn, M);
+    // On a Te mesh, calculate_temperature's per-atom terms are summed where
+    // their inputs are final: the spin terms by the magnetic force pass
+    // (after the last sweep; the exchange field from the spins it gathers
+    // anyway) and the kinetic ones by the last kick's rescale.
+    const bool temp_fused = c->P.eltemp && Dn.te_mesh > 0;
+    if (temp_fused) launch_temperature_begin(Dn, M);
+    launch_force_mag(Dn, M, temp_fused);
     c->force_volume = Dn.box_volume;
-    enqueue_dp(c, Dn, dt / 2e0, eoff);
+    enqueue_dp(c, Dn, dt / 2e0, eoff, temp_fused);
     if (c->P.eltemp) {
-        launch_temperature(Dn, M);
+        if (temp_fused) launch_temperature_end(Dn, M);
+        else launch_temperature(Dn, M);
         launch_dte(Dn, M, dt / 2e0);
         if (c->P.renormalize_energy) launch_energy_check(Dn, M, 1);
     }

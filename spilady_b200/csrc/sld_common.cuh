@@ -534,6 +534,75 @@ __device__ __forceinline__ void exchange_field(const Dev& D, int i, double3& H, 
     sumJ = hj;
 }
 
+// The per-atom spin terms of calculate_temperature
+// (calculate_temperature_CPU.cpp:72-114) from the atom's exchange field H and
+// sum_j J |s_j|: R_up = |s x H|^2, R_dn = s.H and, for the Heisenberg-Landau
+// Hamiltonians, L_up and L_dn of the Landau field; writes H, HL and sum J.
+__device__ __forceinline__ void temp_spin_terms(const Dev& D, int i, double3 H, double sumJ,
+                                                double& Rup, double& Rdn, double& Lup,
+                                                double& Ldn) {
+    Lup = Ldn = 0.0;
+    double4 s4 = D.s[i];
+    double3 s = make_double3(s4.x, s4.y, s4.z);
+    double cx_ = s.y * H.z - H.y * s.z, cy_ = s.z * H.x - H.z * s.x, cz_ = s.x * H.y - H.x * s.y;
+    Rup = cx_ * cx_ + cy_ * cy_ + cz_ * cz_;
+    Rdn = s.x * H.x + s.y * H.y + s.z * H.z;
+    D.H[i] = make_double4(H.x, H.y, H.z, 0.0);
+    if (!D.landau_on) return;   // the Heisenberg Hamiltonians: no Landau field
+    if (!D.hc) sumJ = 0.0;      // the exchange correction is SLDHL's
+    double rho = D.rho[i];
+    double A = interp_const(D.landau[0], rho, D.inv_rho);
+    double B = interp_const(D.landau[1], rho, D.inv_rho);
+    double C = interp_const(D.landau[2], rho, D.inv_rho);
+    double Dd = interp_const(D.landau[3], rho, D.inv_rho);
+    double s_sq = s.x * s.x + s.y * s.y + s.z * s.z;
+    double s0 = sqrt(s_sq);
+    double c = -(2.0 * A + 4.0 * B * s_sq + 6.0 * C * (s_sq * s_sq) + 8.0 * Dd * (s_sq * s_sq * s_sq));
+    double k = -sumJ / s0;
+    double3 HL = make_double3(c * s.x + k * s.x, c * s.y + k * s.y, c * s.z + k * s.z);
+    double hx = H.x + HL.x, hy = H.y + HL.y, hz = H.z + HL.z;
+    Lup = hx * hx + hy * hy + hz * hz;
+    Ldn = 6.0 * A + 20.0 * B * s_sq + 42.0 * C * (s_sq * s_sq) + 72.0 * Dd * (s_sq * s_sq * s_sq);
+    Ldn += 2.0 * sumJ / s0;
+    D.HL[i] = make_double4(HL.x, HL.y, HL.z, 0.0);
+    if (D.hc) D.sumJ[i] = sumJ;
+}
+
+
+// Adds v[0..NV) into the Te-node accumulators acc[9 node + at + q].  Atoms
+// are stored cell by cell, so neighbouring lanes mostly share a node: a
+// segmented warp scan (segments = runs of equal node, marked by head flags)
+// sums each run, and the run's last lane does the atomics.  The calling
+// lanes must be a prefix of the warp (lanes past natom have returned).
+template <int NV>
+__device__ __forceinline__ void node_add(const Dev& D, int node, double (&v)[NV], int at) {
+    const unsigned act = __activemask();
+    const int lane = threadIdx.x & 31;
+    int prev = __shfl_up_sync(act, node, 1);
+    int head = (lane == 0 || prev != node) ? 1 : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int th = __shfl_up_sync(act, head, o);
+        double t[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) t[q] = __shfl_up_sync(act, v[q], o);
+        if (lane >= o) {
+            if (!head) {
+#pragma unroll
+                for (int q = 0; q < NV; ++q) v[q] += t[q];
+            }
+            head |= th;
+        }
+    }
+    int nxt = __shfl_down_sync(act, node, 1);
+    bool last = lane == 31 || !((act >> (lane + 1)) & 1u) || nxt != node;
+    if (last) {
+        double* acc = D.acc + 9 * (size_t)node + at;
+#pragma unroll
+        for (int q = 0; q < NV; ++q) atomicAdd(acc + q, v[q]);
+    }
+}
+
 // ---------------------------------------------------------------------
 // launch wrappers (host), one file per kernel family
 void launch_links(const Dev& D, cudaStream_t st, bool initial, int scan_blocks);
@@ -542,7 +611,7 @@ void sweep_init();
 void launch_force(const Dev& D, cudaStream_t st);
 void launch_embed(const Dev& D, cudaStream_t st);
 void launch_force_eam(const Dev& D, cudaStream_t st);   // lattice terms (no spins)
-void launch_force_mag(const Dev& D, cudaStream_t st);   // adds the magnetic terms
+void launch_force_mag(const Dev& D, cudaStream_t st, bool temp);   // adds the magnetic terms
 void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g, double dt,
                   bool backward, bool fields);
 void launch_spin_noise(const Dev& D, cudaStream_t st, int epoch_off, double dt);
@@ -563,7 +632,9 @@ struct SweepFlow {
 bool sweep_uses_flow();
 void launch_sweep_flow(const Dev& D, cudaStream_t st, const SweepFlow& F, double dt,
                        bool fields);
-void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off);
+// temp: the last kick of a step whose calculate_temperature is split over the
+// magnetic force pass and this kick (launch_force_mag)
+void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off, bool temp = false);
 // the quantum thermostat's normals: Philox epoch SLD_QEPOCH + t, t >= -Nf2 the
 // index of the draw in each atom's history
 #define SLD_QEPOCH (1ULL << 62)
@@ -574,6 +645,10 @@ void launch_scale_positions(const Dev& D, cudaStream_t st, double factor);
 void launch_reshape_positions(const Dev& D, cudaStream_t st, const double old_inv[6]);
 void launch_max_p_h(const Dev& D, cudaStream_t st, double* part, double* out);
 void launch_temperature(const Dev& D, cudaStream_t st);
+// calculate_temperature on a Te mesh in three parts: zero the node sums; the
+// per-atom terms (launch_force_mag and launch_dp with temp); the nodes
+void launch_temperature_begin(const Dev& D, cudaStream_t st);
+void launch_temperature_end(const Dev& D, cudaStream_t st);
 void launch_dte(const Dev& D, cudaStream_t st, double dt);
 int dte_init(int device);
 void launch_energy_check(const Dev& D, cudaStream_t st, int mode);
