@@ -144,9 +144,9 @@ struct RowIdx {
 __device__ __forceinline__ void row_load(const Dev& D, int i, RowIdx& r) {
     r.i = i;
     r.nj = __ldg(D.jl_n + i);
-    const int4* jl4 = reinterpret_cast<const int4*>(D.jl + (size_t)i * SLD_MAXJ);
+    const int* row = D.jl + (size_t)i * SLD_MAXJ;
 #pragma unroll
-    for (int q = 0; q < SC_ROW / 4; ++q) r.w[q] = __ldg(jl4 + q);
+    for (int q = 0; q < SC_ROW / 8; ++q) ldg32_i8(row + 8 * q, r.w[2 * q], r.w[2 * q + 1]);
 }
 
 template <bool SPLIT>
@@ -167,13 +167,8 @@ struct VisitRegs {
 // SM's L1 is read.
 template <bool CG>
 __device__ __forceinline__ double4 ld_spin(const double4* p) {
-    if constexpr (CG) {
-        const double2* q = reinterpret_cast<const double2*>(p);
-        double2 a = __ldcg(q), b = __ldcg(q + 1);
-        return make_double4(a.x, a.y, b.x, b.y);
-    } else {
-        return *p;
-    }
+    if constexpr (CG) return ld32cg_d4(p);
+    else return ld32_d4(p);
 }
 template <bool CG>
 __device__ __forceinline__ float4 ld_spin(const float4* p) {
@@ -197,10 +192,9 @@ __device__ __forceinline__ void visit_fetch(const Dev& D, const RowIdx& r, int s
     }
     const size_t row = (size_t)i * SLD_MAXJ;
     if constexpr (SPLIT) {
-        const float4* j4 = reinterpret_cast<const float4*>(D.jvf + row);
         float4 jw[SC_ROW / 4];
 #pragma unroll
-        for (int q = 0; q < SC_ROW / 4; ++q) jw[q] = __ldg(j4 + q);
+        for (int q = 0; q < SC_ROW / 8; ++q) ldg32_f8(D.jvf + row + 8 * q, jw[2 * q], jw[2 * q + 1]);
 #pragma unroll
         for (int u = 0; u < SC_PJ; ++u) {
             const float4 w = jw[u / 4];
@@ -210,11 +204,13 @@ __device__ __forceinline__ void visit_fetch(const Dev& D, const RowIdx& r, int s
         for (int u = 0; u < SC_PJ; ++u)
             v.sj[u] = v.jj[u] >= 0 ? ld_spin<CG>(D.s32 + v.jj[u]) : make_float4(0.f, 0.f, 0.f, 0.f);
     } else {
-        const double2* j2 = reinterpret_cast<const double2*>(D.jv + row);
 #pragma unroll
-        for (int q = 0; q < SC_PJ / 2; ++q) {
-            double2 w = __ldg(j2 + q);
-            v.J[2 * q + 0] = w.x; v.J[2 * q + 1] = w.y;
+        for (int q = 0; q < SC_ROW / 4; ++q) {
+            const double4 w = ldg32_d4(D.jv + row + 4 * q);
+            const double e[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (4 * q + u < SC_PJ) v.J[4 * q + u] = e[u];
         }
 #pragma unroll
         for (int u = 0; u < SC_PJ; ++u)
@@ -222,10 +218,9 @@ __device__ __forceinline__ void visit_fetch(const Dev& D, const RowIdx& r, int s
     }
     v.si = ld_spin<CG>(D.s + i);
     if (D.spinlang) {
-        const double2* q = reinterpret_cast<const double2*>(D.vrec + 2 * (size_t)i + sweep);
-        const double2 q0 = __ldg(q), q1 = __ldg(q + 1);
-        v.rho = q0.x;
-        v.dS = make_double3(q0.y, q1.x, q1.y);
+        const double4 q = ldg32_d4(D.vrec + 2 * (size_t)i + sweep);
+        v.rho = q.x;
+        v.dS = make_double3(q.y, q.z, q.w);
     } else {
         v.rho = 0.0;
         v.dS = make_double3(0.0, 0.0, 0.0);
@@ -322,12 +317,12 @@ __device__ __forceinline__ void cell_walk(const Dev& D, int c, double dt, int ba
         double s0 = sqrt(s.x * s.x + s.y * s.y + s.z * s.z);
         if (!isfinite(s0)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
         const double4 s4 = make_double4(s.x, s.y, s.z, s0);
-        D.s[i] = s4;
+        st32_d4(D.s + i, s4);
         const auto sr = spin_reg<SPLIT>(s4);
         if constexpr (SPLIT) D.s32[i] = sr;
         if (fields) {
-            D.H[i] = make_double4(H.x, H.y, H.z, 0.0);
-            if constexpr (INTEG == 0) D.HL[i] = make_double4(HL.x, HL.y, HL.z, 0.0);
+            st32_d4(D.H + i, make_double4(H.x, H.y, H.z, 0.0));
+            if constexpr (INTEG == 0) st32_d4(D.HL + i, make_double4(HL.x, HL.y, HL.z, 0.0));
             if (D.spinlang) D.sumJ[i] = sumJ;
         }
         if (more) {
