@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, int write_rho) {
 // 3.75 A lie inside the cutoffs).
 #define SLD_SPLIT_SLOT_BITS 27
 template <bool ORTHO>
-__device__ void pairs_split_one(const Dev& D, int i, int write_rho) {
+__device__ void pairs_split_one(const Dev& D, const int4* koff, int i, int write_rho) {
     const int N = D.natom;
     int c0 = D.cell_of[i], cx, cy, cz;
     cell_xyz(D, c0, cx, cy, cz);
@@ -222,22 +222,22 @@ __device__ void pairs_split_one(const Dev& D, int i, int write_rho) {
         for (int u = 0; u < 4; ++u) {
             if (e0 + u >= nl) break;
             const int e = e0 + u, k = kb[u];
-            const float3 d = fx_vec<ORTHO>(M, fi.x - kNbr[k][0] * SLD_FX_ONE - qb[u].x,
-                                    fi.y - kNbr[k][1] * SLD_FX_ONE - qb[u].y,
-                                    fi.z - kNbr[k][2] * SLD_FX_ONE - qb[u].z);
+            const int4 o = koff[k];
+            const float3 d = fx_vec<ORTHO>(M, fi.x - o.x - qb[u].x, fi.y - o.y - qb[u].y,
+                                           fi.z - o.z - qb[u].z);
             const float rsq = d.x * d.x + d.y * d.y + d.z * d.z;
-            const float r = rsq * rsqrtf(rsq);
+            const float ir = rsqrtf(rsq), r = rsq * ir;
             D.nbr[(size_t)e * N + i] = jb[u] | SLD_WRAP;
             D.nbk[(size_t)e * N + i] = (unsigned char)k;
             if (r < rpot) {
                 float f, df;
-                dens32f(D, K, r, f, df);
+                dens32f(D, K, r, ir, f, df);
                 rho.add(f);
             }
             if (rsq < rmag2) {
                 if (nj < SLD_MAXJ) {
                     float J, dJ;
-                    exch32f(r, J, dJ);
+                    exch32f(r, ir, J, dJ);
                     D.jl[(size_t)i * SLD_MAXJ + nj] = jb[u];
                     D.jvf[(size_t)i * SLD_MAXJ + nj] = J;
                     D.jlk[(size_t)i * SLD_MAXJ + nj] = (unsigned char)k;
@@ -254,8 +254,10 @@ __device__ void pairs_split_one(const Dev& D, int i, int write_rho) {
 
 template <bool ORTHO>
 __global__ void __launch_bounds__(128) k_pairs_split(Dev D, int write_rho) {
+    __shared__ int4 koff[27];
+    fx_offsets_load(koff);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x)
-        pairs_split_one<ORTHO>(D, i, write_rho);
+        pairs_split_one<ORTHO>(D, koff, i, write_rho);
 }
 
 // F'(rho) per atom (the force pass needs it for both atoms of every pair):
@@ -486,7 +488,7 @@ __global__ void __launch_bounds__(128) k_force64_temp(Dev D) {
 // energies; the stress and virial products (FP32) are summed in FP64.  Four
 // entries' loads are issued together.
 template <int PART, bool ORTHO, bool ROWS = false, bool TEMP = false>
-__device__ __forceinline__ void force32_one(const Dev& D, int i, double4& tv) {
+__device__ __forceinline__ void force32_one(const Dev& D, const int4* koff, int i, double4& tv) {
     static_assert(!ROWS || PART == PART_MAG, "the exchange rows hold the magnetic pairs only");
     static_assert(!TEMP || ROWS, "the temperature terms come from the exchange rows");
     const int N = D.natom;
@@ -545,10 +547,9 @@ __device__ __forceinline__ void force32_one(const Dev& D, int i, double4& tv) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             if (e0 + u >= nn) break;
-            const int k = kb[u];
-            const float3 d = fx_vec<ORTHO>(M, fi.x - kNbr[k][0] * SLD_FX_ONE - qb[u].x,
-                                    fi.y - kNbr[k][1] * SLD_FX_ONE - qb[u].y,
-                                    fi.z - kNbr[k][2] * SLD_FX_ONE - qb[u].z);
+            const int4 o = koff[kb[u]];
+            const float3 d = fx_vec<ORTHO>(M, fi.x - o.x - qb[u].x, fi.y - o.y - qb[u].y,
+                                           fi.z - o.z - qb[u].z);
             const float dx = d.x, dy = d.y, dz = d.z;
             const float rsq = dx * dx + dy * dy + dz * dz;
             const float ir = rsqrtf(rsq);
@@ -556,8 +557,8 @@ __device__ __forceinline__ void force32_one(const Dev& D, int i, double4& tv) {
             float dudr = 0.f;
             if ((PART & PART_EAM) && r0 < rpot) {
                 float f, df, phi, dphi;
-                dens32f(D, K, r0, f, df);
-                pair32f(D, K, r0, phi, dphi);
+                dens32f(D, K, r0, ir, f, df);
+                pair32f(D, K, r0, ir, phi, dphi);
                 dudr = (dF_i + dFb[u]) * df + dphi;
                 pe.add(0.5f * phi);
             }
@@ -567,7 +568,7 @@ __device__ __forceinline__ void force32_one(const Dev& D, int i, double4& tv) {
                 float dot = sx * tx + sy * ty + sz * tz;
                 float times = sqrtf(si_sqf * sj_sq);
                 float J, dJ;
-                exch32f(r0, J, dJ);
+                exch32f(r0, ir, J, dJ);
                 dudr += -dJ * (dot - times);
                 float Jh = 0.5f * J;
                 me0.add(Jh * times);
@@ -603,9 +604,11 @@ __device__ __forceinline__ void force32_one(const Dev& D, int i, double4& tv) {
 template <int PART, bool ORTHO, bool ROWS = false>
 __global__ void __launch_bounds__(128) k_force32(Dev D) {
     // one atom per thread; a capped grid walks several atoms per thread
+    __shared__ int4 koff[27];
+    fx_offsets_load(koff);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.natom; i += gridDim.x * blockDim.x) {
         double4 unused;
-        force32_one<PART, ORTHO, ROWS>(D, i, unused);
+        force32_one<PART, ORTHO, ROWS>(D, koff, i, unused);
     }
 }
 
@@ -673,10 +676,12 @@ void launch_force_eam(const Dev& D, cudaStream_t st) {
 }
 template <bool ORTHO>
 __global__ void __launch_bounds__(128) k_force32_temp(Dev D) {
+    __shared__ int4 koff[27];
+    fx_offsets_load(koff);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= D.natom) return;
     double4 t;
-    force32_one<PART_MAG, ORTHO, true, true>(D, i, t);
+    force32_one<PART_MAG, ORTHO, true, true>(D, koff, i, t);
     double v[4] = {t.x, t.y, t.z, t.w};
     node_add<4>(D, D.node[i], v, 4);
 }

@@ -262,6 +262,18 @@ __device__ __forceinline__ void cell_xyz(const Dev& D, int c, int& cx, int& cy, 
 // per product of the cell matrix M (the box vectors over the cells per axis
 // and 2^29).
 #define SLD_FX_ONE (1 << 29)
+// kNbr[k] * SLD_FX_ONE (k = 0..26) into a block's shared table: a pass over
+// list entries takes a different neighbour cell k in every lane, and constant
+// memory serves the lanes' distinct addresses one at a time.  Every thread of
+// the block must call it (it ends with a barrier).
+__device__ __forceinline__ void fx_offsets_load(int4* koff) {
+    if (threadIdx.x < 27)
+        koff[threadIdx.x] = make_int4(kNbr[threadIdx.x][0] * SLD_FX_ONE,
+                                      kNbr[threadIdx.x][1] * SLD_FX_ONE,
+                                      kNbr[threadIdx.x][2] * SLD_FX_ONE, 0);
+    __syncthreads();
+}
+
 __device__ __forceinline__ int4 cell_fix(const Dev& D, int c, double x, double y, double z) {
     int cx, cy, cz;
     cell_xyz(D, c, cx, cy, cz);

@@ -76,15 +76,19 @@ __device__ __forceinline__ void pair32(const Pot32& P, float r, float& v, float&
 // at x = r with step dx, less the exact derivative -3 (k - r)^2_+, for
 // u = k - r.  Zero (up to rounding) for |u| >= 3 dx, where the stencil sees
 // one cubic.  The terms are of size dx^3 and the result of size dx^2, so FP32
-// keeps it to about 1e-7 relative.
+// keeps it to about 1e-7 relative.  i60dx = 1 / (60 dx), formed by the caller
+// from the pair's 1/r (a few ulp; the stencil's own division would cost a
+// division per knot).
 __device__ __forceinline__ float cube_pos32(float x) { return x > 0.f ? x * x * x : 0.f; }
-__device__ __forceinline__ float knot_stencil32(float u, float dx) {
+__device__ __forceinline__ float knot_stencil32(float u, float dx, float i60dx) {
     float s = 45.f * (cube_pos32(u - dx) - cube_pos32(u + dx)) -
               9.f * (cube_pos32(u - 2.f * dx) - cube_pos32(u + 2.f * dx)) +
               (cube_pos32(u - 3.f * dx) - cube_pos32(u + 3.f * dx));
     float up = fmaxf(u, 0.f);
-    return s / (60.f * dx) + 3.f * up * up;
+    return s * i60dx + 3.f * up * up;
 }
+// 1 / (60 dx) for dx = r / 1000, from ir = 1/r
+__device__ __forceinline__ float stencil_i60(float ir) { return ir * (1.f / 0.06f); }
 // The knots of the pair term and of the density (ascending), held in
 // registers by a thread for its whole pair loop.
 struct Knots32 {
@@ -108,7 +112,7 @@ __device__ __forceinline__ Knots32 knots32(const Dev& D) {
 // 6 r/1000 < 0.025 A) that knot's stencil term is added.
 template <int N>
 __device__ __forceinline__ void cubic_iv(const float (&K)[N], const float* __restrict__ blocks,
-                                         float r, float& f, float& df) {
+                                         float r, float ir, float& f, float& df) {
     int m = 0;
 #pragma unroll
     for (int i = 0; i < N; ++i) m += r >= K[i] ? 1 : 0;
@@ -117,26 +121,26 @@ __device__ __forceinline__ void cubic_iv(const float (&K)[N], const float* __res
     const float t = r - e.x;
     f = fmaf(fmaf(fmaf(c.w, t, c.z), t, c.y), t, c.x);
     df = fmaf(fmaf(3.f * c.w, t, 2.f * c.z), t, c.y);
-    const float dx = r * 1e-3f;
+    const float dx = r * 1e-3f, i60 = stencil_i60(ir);
     const float ub = e.x - r, ua = e.y - r;
-    if (ub > -3.f * dx && e.z != 0.f) df = fmaf(e.z, knot_stencil32(ub, dx), df);
-    if (ua < 3.f * dx) df = fmaf(e.w, knot_stencil32(ua, dx), df);
+    if (ub > -3.f * dx && e.z != 0.f) df = fmaf(e.z, knot_stencil32(ub, dx, i60), df);
+    if (ua < 3.f * dx) df = fmaf(e.w, knot_stencil32(ua, dx, i60), df);
 }
 
-// density f and the reference's f' at an FP32 distance
-__device__ __forceinline__ void dens32f(const Dev& D, const Knots32& K, float r, float& f,
-                                        float& df) {
-    cubic_iv<6>(K.d, D.cubic + SLD_DENS_IV, r, f, df);
+// density f and the reference's f' at an FP32 distance r (ir = 1/r)
+__device__ __forceinline__ void dens32f(const Dev& D, const Knots32& K, float r, float ir,
+                                        float& f, float& df) {
+    cubic_iv<6>(K.d, D.cubic + SLD_DENS_IV, r, ir, f, df);
 }
 
 // pair term phi and the reference's phi' at an FP32 distance (ZBL core and
 // join below 2 A; within 3 r/1000 of 1.8 and 2.0 A the reference's stencil
 // also straddles the joins, which only close collisions reach: there the
 // exact derivative of the join is used)
-__device__ __forceinline__ void pair32f(const Dev& D, const Knots32& K, float r, float& v,
-                                        float& dv) {
+__device__ __forceinline__ void pair32f(const Dev& D, const Knots32& K, float r, float ir,
+                                        float& v, float& dv) {
     if (r > 2.0f) {
-        cubic_iv<8>(K.p, D.cubic + SLD_PAIR_IV, r, v, dv);
+        cubic_iv<8>(K.p, D.cubic + SLD_PAIR_IV, r, ir, v, dv);
         return;
     }
     pair32(D.pot32, r, v, dv);
@@ -144,7 +148,7 @@ __device__ __forceinline__ void pair32f(const Dev& D, const Knots32& K, float r,
 
 // Fe exchange J(r) = 0.870 (1 - r/3.75)^3 = a (3.75 - r)^3 for r < 3.75, and
 // the reference's J'(r) (its stencil straddles the knot for |r - 3.75| < 3 dx)
-__device__ __forceinline__ void exch32f(float r, float& J, float& dJ) {
+__device__ __forceinline__ void exch32f(float r, float ir, float& J, float& dJ) {
     const float A = 0.870f, rc = 3.75f, a = 0.870f / (3.75f * 3.75f * 3.75f);
     float u = 1.f - r * (1.f / 3.75f);
     if (u > 0.f) {
@@ -155,7 +159,7 @@ __device__ __forceinline__ void exch32f(float r, float& J, float& dJ) {
         dJ = 0.f;
     }
     const float dx = r * 1e-3f, uk = rc - r;
-    if (fabsf(uk) < 3.f * dx) dJ = fmaf(a, knot_stencil32(uk, dx), dJ);
+    if (fabsf(uk) < 3.f * dx) dJ = fmaf(a, knot_stencil32(uk, dx, stencil_i60(ir)), dJ);
 }
 
 // F(rho) and F'(rho) from the reference's FP64 tables (potential_CPU.cpp:172-179)
