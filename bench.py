@@ -620,7 +620,7 @@ def main():
         events on the engine stream), profile the phases; optionally the e2e
         leg through the public API.  Returns a dict."""
         e = engine.Engine(params, r, p, s, te=te, device=local, precision=form, **sw)
-        shapes = None if args.no_autotune else e.autotune(steps=8)
+        shapes = None if args.no_autotune else e.autotune(steps=12)
         e.run(args.warmup)
         e.sync()
         clocks = ClockSampler(local)

@@ -1645,7 +1645,7 @@ static int trial(sld_ctx* c, const StateCopy& s, int steps, double* ms) {
     if (rc) return rc;
     if ((rc = sld_run(c, 1)) || (rc = sld_sync(c))) return rc;
     *ms = 1e300;
-    for (int rep = 0; rep < 2; ++rep) {
+    for (int rep = 0; rep < 3; ++rep) {
         double t = 0.0;
         if ((rc = sld_run(c, steps)) || (rc = sld_sync(c)) || (rc = sld_last_run_ms(c, &t)))
             return rc;
