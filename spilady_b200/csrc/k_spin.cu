@@ -146,7 +146,7 @@ __device__ __forceinline__ void row_load(const Dev& D, int i, RowIdx& r) {
     r.nj = __ldg(D.jl_n + i);
     const int* row = D.jl + (size_t)i * SLD_MAXJ;
 #pragma unroll
-    for (int q = 0; q < SC_ROW / 8; ++q) ldg32_i8(row + 8 * q, r.w[2 * q], r.w[2 * q + 1]);
+    for (int q = 0; q < SC_ROW / 8; ++q) ldg32_i8_once(row + 8 * q, r.w[2 * q], r.w[2 * q + 1]);
 }
 
 template <bool SPLIT>
@@ -164,7 +164,8 @@ struct VisitRegs {
 
 // Spin loads.  CG: through L2 only (ld.global.cg), for a kernel in which
 // other blocks update spins while it runs, so that no stale copy in this
-// SM's L1 is read.
+// SM's L1 is read.  The gathered neighbours keep L2's normal priority (the
+// streamed rows and records are marked evict-first instead).
 template <bool CG>
 __device__ __forceinline__ double4 ld_spin(const double4* p) {
     if constexpr (CG) return ld32cg_d4(p);
@@ -174,6 +175,13 @@ template <bool CG>
 __device__ __forceinline__ float4 ld_spin(const float4* p) {
     if constexpr (CG) return __ldcg(p);
     else return *p;
+}
+// a visit's own FP64 spin in the split form (read once per visit and gathered
+// by no one: streamed)
+template <bool CG>
+__device__ __forceinline__ double4 ld_own_spin(const double4* p) {
+    if constexpr (CG) return ld32cg_d4(p);
+    else return ld32_d4_once(p);
 }
 
 // everything of one visit but the indices: couplings, neighbour spins, the
@@ -194,7 +202,7 @@ __device__ __forceinline__ void visit_fetch(const Dev& D, const RowIdx& r, int s
     if constexpr (SPLIT) {
         float4 jw[SC_ROW / 4];
 #pragma unroll
-        for (int q = 0; q < SC_ROW / 8; ++q) ldg32_f8(D.jvf + row + 8 * q, jw[2 * q], jw[2 * q + 1]);
+        for (int q = 0; q < SC_ROW / 8; ++q) ldg32_f8_once(D.jvf + row + 8 * q, jw[2 * q], jw[2 * q + 1]);
 #pragma unroll
         for (int u = 0; u < SC_PJ; ++u) {
             const float4 w = jw[u / 4];
@@ -206,7 +214,7 @@ __device__ __forceinline__ void visit_fetch(const Dev& D, const RowIdx& r, int s
     } else {
 #pragma unroll
         for (int q = 0; q < SC_ROW / 4; ++q) {
-            const double4 w = ldg32_d4(D.jv + row + 4 * q);
+            const double4 w = ldg32_d4_once(D.jv + row + 4 * q);
             const double e[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
             for (int u = 0; u < 4; ++u)
@@ -216,9 +224,10 @@ __device__ __forceinline__ void visit_fetch(const Dev& D, const RowIdx& r, int s
         for (int u = 0; u < SC_PJ; ++u)
             v.sj[u] = v.jj[u] >= 0 ? ld_spin<CG>(D.s + v.jj[u]) : make_double4(0, 0, 0, 0);
     }
-    v.si = ld_spin<CG>(D.s + i);
+    if constexpr (SPLIT) v.si = ld_own_spin<CG>(D.s + i);
+    else v.si = ld_spin<CG>(D.s + i);
     if (D.spinlang) {
-        const double4 q = ldg32_d4(D.vrec + 2 * (size_t)i + sweep);
+        const double4 q = ldg32_d4_once(D.vrec + 2 * (size_t)i + sweep);
         v.rho = q.x;
         v.dS = make_double3(q.y, q.z, q.w);
     } else {
@@ -317,12 +326,13 @@ __device__ __forceinline__ void cell_walk(const Dev& D, int c, double dt, int ba
         double s0 = sqrt(s.x * s.x + s.y * s.y + s.z * s.z);
         if (!isfinite(s0)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
         const double4 s4 = make_double4(s.x, s.y, s.z, s0);
-        st32_d4(D.s + i, s4);
+        if constexpr (SPLIT) st32_d4_once(D.s + i, s4);
+        else st32_d4(D.s + i, s4);
         const auto sr = spin_reg<SPLIT>(s4);
         if constexpr (SPLIT) D.s32[i] = sr;
         if (fields) {
-            st32_d4(D.H + i, make_double4(H.x, H.y, H.z, 0.0));
-            if constexpr (INTEG == 0) st32_d4(D.HL + i, make_double4(HL.x, HL.y, HL.z, 0.0));
+            st32_d4_once(D.H + i, make_double4(H.x, H.y, H.z, 0.0));
+            if constexpr (INTEG == 0) st32_d4_once(D.HL + i, make_double4(HL.x, HL.y, HL.z, 0.0));
             if (D.spinlang) D.sumJ[i] = sumJ;
         }
         if (more) {

@@ -420,27 +420,12 @@ static inline int div_up(long a, long b) { return (int)((a + b - 1) / b); }
 
 // 32-byte global accesses: one instruction on sm_100 where a double4 or two
 // 16-byte vectors take two, so a warp's scattered rows and spins cost half
-// the load requests.  The address must be 32-byte aligned.  ldg32_* read data
-// no thread writes during the kernel (the non-coherent path); ld32_d4 and
+// the load requests.  The address must be 32-byte aligned.  ld32_d4 and
 // st32_d4 are coherent and volatile (kept in program order with each other),
 // for spins that a thread reads after writing them; ld32cg_d4 reads through
-// L2 only, for spins other blocks write during the kernel.
-__device__ __forceinline__ void ldg32_i8(const int* p, int4& a, int4& b) {
-    asm("ld.global.nc.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
-        : "l"(p));
-}
-__device__ __forceinline__ void ldg32_f8(const float* p, float4& a, float4& b) {
-    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
-        : "l"(p));
-}
-__device__ __forceinline__ double4 ldg32_d4(const void* p) {
-    double4 v;
-    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
-        : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w) : "l"(p));
-    return v;
-}
+// L2 only, for spins other blocks write during the kernel.  The *_once
+// variants below are for streamed data; ldg32_*_once read data no thread
+// writes during the kernel (the non-coherent path).
 __device__ __forceinline__ double4 ld32_d4(const double4* p) {
     double4 v;
     asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
@@ -455,6 +440,39 @@ __device__ __forceinline__ double4 ld32cg_d4(const double4* p) {
 }
 __device__ __forceinline__ void st32_d4(double4* p, double4 v) {
     asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};"
+                 :: "l"(p), "d"(v.x), "d"(v.y), "d"(v.z), "d"(v.w) : "memory");
+}
+
+// Streamed data: a sweep reads each visit's row, couplings and record once,
+// while the neighbour spins it gathers (the FP32 copy: 16 B per atom) are read
+// by many visits.  The *_once accesses take L2's evict-first priority and skip
+// L1, so that the streamed bytes leave the caches before the gathered spins.
+__device__ __forceinline__ void ldg32_i8_once(const int* p, int4& a, int4& b) {
+    asm("ld.global.nc.L1::no_allocate.L2::evict_first.v8.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+        : "l"(p));
+}
+__device__ __forceinline__ void ldg32_f8_once(const float* p, float4& a, float4& b) {
+    asm("ld.global.nc.L1::no_allocate.L2::evict_first.v8.f32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+        : "l"(p));
+}
+__device__ __forceinline__ double4 ldg32_d4_once(const void* p) {
+    double4 v;
+    asm("ld.global.nc.L1::no_allocate.L2::evict_first.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ double4 ld32_d4_once(const double4* p) {
+    double4 v;
+    asm volatile("ld.global.L1::no_allocate.L2::evict_first.v4.f64 {%0, %1, %2, %3}, [%4];"
+                 : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ void st32_d4_once(double4* p, double4 v) {
+    asm volatile("st.global.L1::no_allocate.L2::evict_first.v4.f64 [%0], {%1, %2, %3, %4};"
                  :: "l"(p), "d"(v.x), "d"(v.y), "d"(v.z), "d"(v.w) : "memory");
 }
 
