@@ -12,20 +12,28 @@
 // run gives the same bits.
 #include "sld_common.cuh"
 
-__device__ __forceinline__ void block_partials3(const Dev& D, double a, double b, double c) {
+// per-block sums of a kick for rescale_momentum: the momentum and the
+// kinetic energy |p|^2 / 2 / m, each atom's rounded as the reference rounds
+// its ke (core_dp_CPU.cpp:292)
+__device__ __forceinline__ void block_partials4(const Dev& D, double a, double b, double c,
+                                                double k) {
     __shared__ double sh[32];
     double ta = block_sum(a, sh);
     double tb = block_sum(b, sh);
     double tc = block_sum(c, sh);
+    double tk = block_sum(k, sh);
     if (threadIdx.x == 0) {
         double* o = D.red + 4 * (size_t)blockIdx.x;
-        o[0] = ta; o[1] = tb; o[2] = tc;
+        o[0] = ta; o[1] = tb; o[2] = tc; o[3] = tk;
     }
+}
+__device__ __forceinline__ double ke_of(const Dev& D, double px, double py, double pz) {
+    return (px * px + py * py + pz * pz) / 2.0 / D.atmass;
 }
 
 __global__ void __launch_bounds__(256) k_dp_nve(Dev D, double dt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double px = 0, py = 0, pz = 0;
+    double px = 0, py = 0, pz = 0, kk = 0;
     if (i < D.natom) {
         double4 p = D.p[i], f = D.f[i];
         if (D.fext) {
@@ -37,8 +45,9 @@ __global__ void __launch_bounds__(256) k_dp_nve(Dev D, double dt) {
         p.x = p.x + dt * f.x; p.y = p.y + dt * f.y; p.z = p.z + dt * f.z;
         D.p[i] = p;
         px = p.x; py = p.y; pz = p.z;
+        kk = ke_of(D, p.x, p.y, p.z);
     }
-    block_partials3(D, px, py, pz);
+    block_partials4(D, px, py, pz, kk);
 }
 
 __device__ __forceinline__ void add3(double4& a, double k, double x, double y, double z) {
@@ -108,9 +117,9 @@ __device__ __forceinline__ void friction(const Dev& D, const P& P_, int n, doubl
 }
 
 // core_dp_CPU.cpp:51-85 for one cell: C1(dt/2) B(dt/2) A(dt) B(dt/2) C2(dt/2);
-// returns the cell's momentum sum for rescale_momentum
+// returns the cell's momentum and kinetic-energy sums for rescale_momentum
 template <class P>
-__device__ __forceinline__ double3 dp_cell(const Dev& D, const P& P_, const int* a, int n, double dt,
+__device__ __forceinline__ double4 dp_cell(const Dev& D, const P& P_, const int* a, int n, double dt,
                                            unsigned long long epoch) {
     if (D.localcolmot) cell_mix(D, P_, n, dt / 2.0, false);
     friction(D, P_, n, dt / 2.0);
@@ -151,18 +160,19 @@ __device__ __forceinline__ double3 dp_cell(const Dev& D, const P& P_, const int*
     }
     friction(D, P_, n, dt / 2.0);
     if (D.localcolmot) cell_mix(D, P_, n, dt / 2.0, true);
-    double px = 0, py = 0, pz = 0;
+    double px = 0, py = 0, pz = 0, kk = 0;
     for (int m = 0; m < n; ++m) {
         double3 p = P_.get(m);
         px += p.x; py += p.y; pz += p.z;
+        kk += ke_of(D, p.x, p.y, p.z);
     }
-    return make_double3(px, py, pz);
+    return make_double4(px, py, pz, kk);
 }
 
 __global__ void __launch_bounds__(KDP_BLOCK) k_dp_lang(Dev D, double dt, int epoch_off) {
     __shared__ double sp[3 * KDP_MAXA * KDP_BLOCK];
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    double3 ps = make_double3(0.0, 0.0, 0.0);
+    double4 ps = make_double4(0.0, 0.0, 0.0, 0.0);
     if (c < D.ncells) {
         const int n = cell_n(D, c);
         const int* a = D.cell_atoms + D.cell_start[c];
@@ -190,52 +200,33 @@ __global__ void __launch_bounds__(KDP_BLOCK) k_dp_lang(Dev D, double dt, int epo
             ps = dp_cell(D, PGlobal{D, a}, a, n, dt, epoch);
         }
     }
-    block_partials3(D, ps.x, ps.y, ps.z);
+    block_partials4(D, ps.x, ps.y, ps.z, ps.w);
 }
 
-__global__ void __launch_bounds__(1024) k_avep(Dev D, int nb) {
+// rescale_momentum (core_dp_CPU.cpp:268-311) from the kick's block sums: the
+// mean momentum a, the kinetic energy before (sum of |p|^2 / 2m) and after
+// removing a, which is the same sum less N |a|^2 / 2m (the reference sums
+// |p - a|^2 / 2m atom by atom; the two agree to rounding), and the factor
+// sqrt(ke_old / ke_new) that k_scale applies.
+__global__ void __launch_bounds__(1024) k_rescale(Dev D, int nb) {
     __shared__ double sh[32];
-    double a = 0, b = 0, c = 0;
-    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
-        a += D.red[4 * k]; b += D.red[4 * k + 1]; c += D.red[4 * k + 2];
+    double a = 0, b = 0, c = 0, k = 0;
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) {
+        a += D.red[4 * q]; b += D.red[4 * q + 1]; c += D.red[4 * q + 2]; k += D.red[4 * q + 3];
     }
     a = block_sum(a, sh);
     b = block_sum(b, sh);
     c = block_sum(c, sh);
+    k = block_sum(k, sh);
     if (threadIdx.x == 0) {
-        D.ctl->avep[0] = a / D.natom;
-        D.ctl->avep[1] = b / D.natom;
-        D.ctl->avep[2] = c / D.natom;
-    }
-}
-
-__global__ void __launch_bounds__(256) k_ke_partials(Dev D) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double ko = 0, kn = 0;
-    if (i < D.natom) {
-        double4 p = D.p[i];
-        ko = (p.x * p.x + p.y * p.y + p.z * p.z) / 2.0 / D.atmass;
-        double x = p.x - D.ctl->avep[0], y = p.y - D.ctl->avep[1], z = p.z - D.ctl->avep[2];
-        kn = (x * x + y * y + z * z) / 2.0 / D.atmass;
-    }
-    __shared__ double sh[32];
-    double a = block_sum(ko, sh);
-    double b = block_sum(kn, sh);
-    if (threadIdx.x == 0) {
-        D.red[4 * (size_t)blockIdx.x] = a;
-        D.red[4 * (size_t)blockIdx.x + 1] = b;
-    }
-}
-
-__global__ void __launch_bounds__(1024) k_factor(Dev D, int nb) {
-    __shared__ double sh[32];
-    double a = 0, b = 0;
-    for (int k = threadIdx.x; k < nb; k += blockDim.x) { a += D.red[4 * k]; b += D.red[4 * k + 1]; }
-    a = block_sum(a, sh);
-    b = block_sum(b, sh);
-    if (threadIdx.x == 0) {
-        double factor = sqrt(a / b);
-        if (b < 1e-10) factor = 1.0;
+        const double n = (double)D.natom;
+        const double ax = a / n, ay = b / n, az = c / n;
+        D.ctl->avep[0] = ax;
+        D.ctl->avep[1] = ay;
+        D.ctl->avep[2] = az;
+        const double ke_new = k - n * (ax * ax + ay * ay + az * az) / 2.0 / D.atmass;
+        double factor = sqrt(k / ke_new);
+        if (ke_new < 1e-10) factor = 1.0;
         D.ctl->ke_factor = factor;
     }
 }
@@ -312,10 +303,8 @@ void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off, bool tem
         nb = div_up(D.natom, 256);
         k_dp_nve<<<nb, 256, 0, st>>>(D, dt);
     }
-    k_avep<<<1, 1024, 0, st>>>(D, nb);
+    k_rescale<<<1, 1024, 0, st>>>(D, nb);
     int na = div_up(D.natom, 256);
-    k_ke_partials<<<na, 256, 0, st>>>(D);
-    k_factor<<<1, 1024, 0, st>>>(D, na);
     if (temp) k_scale<true><<<na, 256, 0, st>>>(D);
     else k_scale<false><<<na, 256, 0, st>>>(D);
 }
