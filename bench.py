@@ -651,9 +651,11 @@ def main():
         # End to end through the public API with host buffers: upload the
         # state from pinned host memory (sld_set_state), then every step run
         # it and read the check() averages back, as the reference's main loop
-        # prints them every step at interval_of_print_out 1.  The state stays
-        # on the device between steps, as it does behind the reference's
-        # core() with a device backend.
+        # prints them every step at interval_of_print_out 1, and at the end of
+        # the sample read the whole configuration (r, p, s) back into the
+        # pinned buffers, as a configuration file written every k steps
+        # needs.  The state stays on the device between steps, as it does
+        # behind the reference's core() with a device backend.
         host = {}
         for name, a in (("r", r), ("p", p), ("s", s)):
             host[name] = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
@@ -664,13 +666,16 @@ def main():
         for _ in range(k):
             e.run(1)
             e.averages()
+        for name in ("r", "p", "s"):
+            e.get(name, out=host[name].numpy().reshape(-1))
         t1 = time.perf_counter()
         nat = e.natom
         return {"value": nat * k / (t1 - t0), "unit": "atom-steps/s",
-                "h2d_bytes_per_step": int(nat * 72 / k), "d2h_bytes_per_step": 80, "steps": k,
+                "h2d_bytes_per_step": int(nat * 72 / k),
+                "d2h_bytes_per_step": int(80 + nat * 72 / k), "steps": k,
                 "note": f"per sample of {k} steps: r, p, s uploaded from pinned host memory "
-                        "once (sld_set_state), then sld_run(1) and the averages read back "
-                        "every step"}
+                        "once (sld_set_state), sld_run(1) and the averages read back every "
+                        "step, and r, p, s read back into the pinned buffers at the end"}
 
     main_arm = timed_form(prec, not args.no_e2e)
     fp64_arm = None

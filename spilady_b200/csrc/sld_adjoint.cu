@@ -42,7 +42,14 @@ struct Pool {
             ok = false;
             return nullptr;
         }
-        cudaMemset(q, 0, std::max<size_t>(n, 1) * sizeof(T));
+        // cleared on the default stream, which does not order against the
+        // engine's non-blocking stream: finished before any use of it there
+        if (cudaMemset(q, 0, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess ||
+            cudaDeviceSynchronize() != cudaSuccess) {
+            ok = false;
+            cudaFree(q);
+            return nullptr;
+        }
         p.push_back(q);
         return static_cast<T*>(q);
     }

@@ -1079,6 +1079,17 @@ int sld_sync(sld_ctx* c) {
     return check_flags(c);
 }
 
+// a per-atom field in caller order on the device: out[width id(k) + w] for
+// the atom in slot k (x, y, z of a double4 field, or width consecutive doubles)
+__global__ void k_pack_caller(const Dev D, const double* __restrict__ src, int src_width,
+                              int width, double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= D.natom) return;
+    const size_t i = (size_t)D.id[k];
+    const double* a = src + (size_t)src_width * k;
+    for (int w = 0; w < width; ++w) out[(size_t)width * i + w] = a[w];
+}
+
 long sld_get(sld_ctx* c, const char* field, double* out, long cap) {
     if (!c || !field || !out) return SLD_ERR_ARG;
     SLD_DEVICE_OF(c);
@@ -1086,26 +1097,22 @@ long sld_get(sld_ctx* c, const char* field, double* out, long cap) {
     size_t n = (size_t)D.natom;
     std::string f(field);
     if (cudaStreamSynchronize(c->st) != cudaSuccess) return SLD_ERR_CUDA;
-    auto vec4 = [&](double4* src) -> long {
-        if (cap < (long)(3 * n)) return SLD_ERR_ARG;
-        std::vector<double4> h(n);
-        if (cudaMemcpy(h.data(), src, sizeof(double4) * n, cudaMemcpyDeviceToHost)) return SLD_ERR_CUDA;
-        for (size_t k = 0; k < n; ++k) {
-            int i = c->id_of_slot[k];
-            out[3 * i] = h[k].x; out[3 * i + 1] = h[k].y; out[3 * i + 2] = h[k].z;
-        }
-        return (long)(3 * n);
-    };
-    auto scal = [&](double* src, int width) -> long {
+    // per-atom fields are put in caller order on the device and copied out in
+    // one transfer (direct DMA when the caller's buffer is pinned)
+    auto packed = [&](const double* src, int src_width, int width) -> long {
         if (cap < (long)(width * n)) return SLD_ERR_ARG;
-        std::vector<double> h(width * n);
-        if (cudaMemcpy(h.data(), src, sizeof(double) * width * n, cudaMemcpyDeviceToHost)) return SLD_ERR_CUDA;
-        for (size_t k = 0; k < n; ++k) {
-            int i = c->id_of_slot[k];
-            for (int w = 0; w < width; ++w) out[(size_t)width * i + w] = h[(size_t)width * k + w];
-        }
+        if (!c->d_stage && c->alloc(&c->d_stage, 6 * n) != SLD_OK) return SLD_ERR_NOMEM;
+        k_pack_caller<<<div_up((long)n, 256), 256, 0, c->st>>>(D, src, src_width, width, c->d_stage);
+        if (cudaMemcpyAsync(out, c->d_stage, sizeof(double) * width * n, cudaMemcpyDeviceToHost,
+                            c->st) != cudaSuccess ||
+            cudaStreamSynchronize(c->st) != cudaSuccess)
+            return SLD_ERR_CUDA;
         return (long)(width * n);
     };
+    auto vec4 = [&](double4* src) -> long {
+        return packed(reinterpret_cast<const double*>(src), 4, 3);
+    };
+    auto scal = [&](double* src, int width) -> long { return packed(src, width, width); };
     auto percell = [&](double* src, double scale) -> long {
         size_t m = (size_t)D.nte;
         if (cap < (long)m) return SLD_ERR_ARG;

@@ -16,6 +16,8 @@ struct sld_ctx {
     std::vector<void*> allocs;
     std::vector<size_t> alloc_bytes;   // size of each allocation (a whole-state snapshot)
     int* d_gcells = nullptr;
+    double* d_stage = nullptr;     // sld_get's device staging (6 doubles per atom), made
+                                   // at its first use
     SweepFlow flow{};                  // data-flow schedule of the spin sweeps
     int* d_te_gcells = nullptr;
     int* d_te_gstart = nullptr;
@@ -60,7 +62,12 @@ struct sld_ctx {
         void* q = nullptr;
         if (n == 0) n = 1;
         if (cudaMalloc(&q, n * sizeof(T)) != cudaSuccess) return SLD_ERR_NOMEM;
-        cudaMemset(q, 0, n * sizeof(T));
+        // cleared on the default stream, which does not order against the
+        // engine's non-blocking streams: finished before any use of it there
+        if (cudaMemset(q, 0, n * sizeof(T)) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+            cudaFree(q);
+            return SLD_ERR_CUDA;
+        }
         allocs.push_back(q);
         alloc_bytes.push_back(n * sizeof(T));
         *p = static_cast<T*>(q);

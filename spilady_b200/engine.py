@@ -262,10 +262,15 @@ class Engine:
         s = np.ascontiguousarray(s, np.float64)
         _check(self.L.sld_set_state(self.h, _dp(r), _dp(p), _dp(s)), "set_state")
 
-    def get(self, name):
+    def get(self, name, out=None):
+        """A field in caller order; into ``out`` (a C-contiguous float64 array
+        of the field's size, e.g. pinned host memory) when given."""
         width = VEC_FIELDS.get(name, 1)
         n = (self.nte if name in CELL_FIELDS else self.natom) * width
-        out = np.empty(n, np.float64)
+        if out is None:
+            out = np.empty(n, np.float64)
+        elif out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"] or out.size != n:
+            raise ValueError(f"get({name}): out must be C-contiguous float64 of {n} values")
         got = self.L.sld_get(self.h, name.encode(), _dp(out), n)
         if got < 0:
             raise SldError(int(got), f"get({name})")
