@@ -251,11 +251,22 @@ __global__ void __launch_bounds__(256) k_scale(Dev D) {
     }
 }
 
+// SCALE: first finish the kick's rescale_momentum for this atom (as
+// k_scale<false> does), for a step that defers it to the drift
+template <bool SCALE>
 __global__ void __launch_bounds__(256) k_dr(Dev D, double dt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= D.natom) return;
     double k = dt / D.atmass;
     double4 r = D.r[i], p = D.p[i];
+    if constexpr (SCALE) {
+        const double f = D.ctl->ke_factor;
+        p.x = f * (p.x - D.ctl->avep[0]);
+        p.y = f * (p.y - D.ctl->avep[1]);
+        p.z = f * (p.z - D.ctl->avep[2]);
+        D.p[i] = p;
+        D.ke[i] = (p.x * p.x + p.y * p.y + p.z * p.z) / 2.0 / D.atmass;
+    }
     const double3 u = make_double3(r.x + k * p.x, r.y + k * p.y, r.z + k * p.z);
     double3 x = periodic(D, u);
     if (!isfinite(x.x + x.y + x.z)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
@@ -292,7 +303,8 @@ __global__ void k_quantum_tick(Dev D) {
     if (threadIdx.x == 0) ++D.ctl->qcount;
 }
 
-void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off, bool temp) {
+void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off, bool temp,
+               bool defer_scale) {
     int nb;
     if (D.lattlang) {
         if (D.quantum) k_quantum_update<<<div_up(D.natom, 256), 256, 0, st>>>(D);
@@ -304,13 +316,15 @@ void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off, bool tem
         k_dp_nve<<<nb, 256, 0, st>>>(D, dt);
     }
     k_rescale<<<1, 1024, 0, st>>>(D, nb);
+    if (defer_scale) return;
     int na = div_up(D.natom, 256);
     if (temp) k_scale<true><<<na, 256, 0, st>>>(D);
     else k_scale<false><<<na, 256, 0, st>>>(D);
 }
 
-void launch_dr(const Dev& D, cudaStream_t st, double dt) {
-    k_dr<<<div_up(D.natom, 256), 256, 0, st>>>(D, dt);
+void launch_dr(const Dev& D, cudaStream_t st, double dt, bool scale) {
+    if (scale) k_dr<true><<<div_up(D.natom, 256), 256, 0, st>>>(D, dt);
+    else k_dr<false><<<div_up(D.natom, 256), 256, 0, st>>>(D, dt);
 }
 
 // sld_set_state on the device: the caller's r, p, s ([atom][3], caller order)

@@ -544,6 +544,9 @@ __device__ __forceinline__ void force32_one(const Dev& D, const int4* koff, int 
             for (int u = 0; u < 4; ++u)
                 if (e0 + u < nn) exch_add32(ks, kc, Jq[u], sb[u]);
         }
+        // the batch's stress and virial products, summed in FP32 and added
+        // to the FP64 sums once per batch
+        float bst[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             if (e0 + u >= nn) break;
@@ -578,10 +581,13 @@ __device__ __forceinline__ void force32_one(const Dev& D, const int4* koff, int 
             const float force = -dudr * ir;
             const float gx = force * dx, gy = force * dy, gz = force * dz;
             fx.add(gx); fy.add(gy); fz.add(gz);
-            st[0] += (double)(gx * dx); st[1] += (double)(gy * dy); st[2] += (double)(gz * dz);
-            st[3] += (double)(gx * dy); st[4] += (double)(gy * dz); st[5] += (double)(gz * dx);
-            vir += (double)(-force * rsq);
+            bst[0] += gx * dx; bst[1] += gy * dy; bst[2] += gz * dz;
+            bst[3] += gx * dy; bst[4] += gy * dz; bst[5] += gz * dx;
+            bst[6] += -force * rsq;
         }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) st[k] += (double)bst[k];
+        vir += (double)bst[6];
     }
     double F = 0.0;
     if (PART & PART_EAM) F = interp(D.tF, rho_i, D.inv_rho, &D.ctl->err);

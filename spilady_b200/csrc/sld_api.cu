@@ -95,8 +95,9 @@ void enqueue_ds(sld_ctx* c, const Dev& D, double dt, int& eoff, bool fields = tr
 }
 void enqueue_ds(sld_ctx* c, double dt, int& eoff) { enqueue_ds(c, c->D, dt, eoff); }
 
-void enqueue_dp(sld_ctx* c, const Dev& D, double dt, int& eoff, bool temp = false) {
-    launch_dp(D, c->st, dt, eoff, temp);
+void enqueue_dp(sld_ctx* c, const Dev& D, double dt, int& eoff, bool temp = false,
+                bool defer_scale = false) {
+    launch_dp(D, c->st, dt, eoff, temp, defer_scale);
     if (c->P.lattlang) ++eoff;
 }
 void enqueue_dp(sld_ctx* c, double dt, int& eoff) { enqueue_dp(c, c->D, dt, eoff); }
@@ -186,10 +187,13 @@ void enqueue_step(sld_ctx* c) {
         }
         launch_links(Dc, M, false, c->scan_blocks);
     }
-    enqueue_dp(c, Dc, dt / 2e0, eoff);
+    // The first kick's rescale_momentum scales the momenta in the drift, on
+    // the side branch: the main branch reads no momenta before the second
+    // kick, which runs after the side branch's EAM forces
+    enqueue_dp(c, Dc, dt / 2e0, eoff, false, true);
     cudaEventRecord(ev[0], M);
     cudaStreamWaitEvent(A, ev[0], 0);
-    launch_dr(Dc, A, dt);
+    launch_dr(Dc, A, dt, true);
     launch_pairs(Dn, A, true);
     cudaEventRecord(ev[2], A);
     launch_force_eam(Dn, A);

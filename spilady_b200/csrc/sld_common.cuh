@@ -704,11 +704,14 @@ void launch_sweep_flow(const Dev& D, cudaStream_t st, const SweepFlow& F, double
                        bool fields);
 // temp: the last kick of a step whose calculate_temperature is split over the
 // magnetic force pass and this kick (launch_force_mag)
-void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off, bool temp = false);
+// defer_scale: leave rescale_momentum's scaling of the momenta to the next
+// drift (launch_dr with scale), for a step in which nothing reads them before
+void launch_dp(const Dev& D, cudaStream_t st, double dt, int epoch_off, bool temp = false,
+               bool defer_scale = false);
 // the quantum thermostat's normals: Philox epoch SLD_QEPOCH + t, t >= -Nf2 the
 // index of the draw in each atom's history
 #define SLD_QEPOCH (1ULL << 62)
-void launch_dr(const Dev& D, cudaStream_t st, double dt);
+void launch_dr(const Dev& D, cudaStream_t st, double dt, bool scale = false);
 // barostat position rescaling (D holds the new box) and the adaptive time
 // step's maxima (k_lattice.cu)
 void launch_scale_positions(const Dev& D, cudaStream_t st, double factor);
