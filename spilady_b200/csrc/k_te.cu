@@ -27,6 +27,7 @@ __device__ __forceinline__ void temp_atom(const Dev& D, int i, double& Rup, doub
     gather_field_t(D, i, H, sumJ);
     temp_spin_terms(D, i, H, sumJ, Rup, Rdn, Lup, Ldn);
 }
+
 // per-Te-cell results from the sums (calculate_temperature_CPU.cpp:118-142)
 __device__ __forceinline__ void temp_finish(const Dev& D, int k, double n, double sum_ke, double apx,
                                             double apy, double apz, double Rup, double Rdn, double Lup,

@@ -638,7 +638,6 @@ __device__ __forceinline__ void temp_spin_terms(const Dev& D, int i, double3 H, 
     if (D.hc) D.sumJ[i] = sumJ;
 }
 
-
 // Adds v[0..NV) into the Te-node accumulators acc[9 node + at + q].  Atoms
 // are stored cell by cell, so neighbouring lanes mostly share a node: a
 // segmented warp scan (segments = runs of equal node, marked by head flags)
