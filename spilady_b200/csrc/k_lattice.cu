@@ -36,6 +36,10 @@ __global__ void __launch_bounds__(256) k_dp_nve(Dev D, double dt) {
     double px = 0, py = 0, pz = 0, kk = 0;
     if (i < D.natom) {
         double4 p = D.p[i], f = D.f[i];
+        if (D.fm) {   // the magnetic part, kept apart
+            const double4 g = D.fm[i];
+            f.x = f.x + g.x; f.y = f.y + g.y; f.z = f.z + g.z;
+        }
         if (D.fext) {
             // core_dp_CPU.cpp:68-71: the external force is added into f itself
             double4 e = D.fext[i];
@@ -140,6 +144,10 @@ __device__ __forceinline__ double4 dp_cell(const Dev& D, const P& P_, const int*
             fx = amp * xi.x; fy = amp * xi.y; fz = amp * xi.z;
         }
         double4 f = D.f[i];
+        if (D.fm) {   // the magnetic part, kept apart
+            const double4 g = D.fm[i];
+            f.x = f.x + g.x; f.y = f.y + g.y; f.z = f.z + g.z;
+        }
         if (D.fext) {   // core_dp_CPU.cpp:129-132
             double4 e = D.fext[i];
             f.x = f.x + e.x; f.y = f.y + e.y; f.z = f.z + e.z;

@@ -310,11 +310,19 @@ __device__ __forceinline__ void force_finish(const Dev& D, int i, double si_sq, 
         D.me0[i] = me0;
     }
     if (PART == PART_MAG) {
-        // add to what the EAM part wrote
-        double4 f = D.f[i];
-        D.f[i] = make_double4(f.x + fx, f.y + fy, f.z + fz, 0.0);
-        D.vir[i] += 0.5 * vir;
-        for (int k = 0; k < 6; ++k) out[k] += st6[k] / 2.0 / V;
+        if (D.fm) {
+            // the terms that the add below would add, kept apart
+            D.fm[i] = make_double4(fx, fy, fz, 0.0);
+            D.virm[i] = 0.5 * vir;
+            double* om = D.stressm + 6 * (size_t)i;
+            for (int k = 0; k < 6; ++k) om[k] = st6[k] / 2.0 / V;
+        } else {
+            // add to what the EAM part wrote
+            double4 f = D.f[i];
+            D.f[i] = make_double4(f.x + fx, f.y + fy, f.z + fz, 0.0);
+            D.vir[i] += 0.5 * vir;
+            for (int k = 0; k < 6; ++k) out[k] += st6[k] / 2.0 / V;
+        }
         if (!isfinite(fx + fy + fz + me)) atomicOr(&D.ctl->err, SLD_FLAG_NAN);
         return;
     }
@@ -690,6 +698,25 @@ __global__ void __launch_bounds__(128) k_force32_temp(Dev D) {
     force32_one<PART_MAG, ORTHO, true, true>(D, koff, i, t);
     double v[4] = {t.x, t.y, t.z, t.w};
     node_add<4>(D, D.node[i], v, 4);
+}
+
+// f, vir and stress plus the magnetic parts kept apart (D.fm): the same
+// single addition per element as the magnetic pass's add.  f is left out
+// when an external force is set: the kick then stores its f + fm + fext.
+__global__ void __launch_bounds__(256) k_fold_mag(Dev D, int with_f) {
+    const size_t n = (size_t)D.natom;
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < 6 * n) D.stress[t] = D.stress[t] + D.stressm[t];
+    if (t < n) {
+        D.vir[t] = D.vir[t] + D.virm[t];
+        if (with_f) {
+            const double4 f = D.f[t], g = D.fm[t];
+            D.f[t] = make_double4(f.x + g.x, f.y + g.y, f.z + g.z, 0.0);
+        }
+    }
+}
+void launch_fold_mag(const Dev& D, cudaStream_t st) {
+    k_fold_mag<<<div_up(6 * D.natom, 256), 256, 0, st>>>(D, D.fext ? 0 : 1);
 }
 
 // the magnetic part from the exchange rows of the list pass that ran on the

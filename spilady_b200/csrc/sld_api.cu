@@ -107,6 +107,7 @@ void enqueue_dp(sld_ctx* c, double dt, int& eoff) { enqueue_dp(c, c->D, dt, eoff
 // spins beside the sweeps:
 //   main:   links | dp(dt/2) | ds(dt/2) ........ | ds(dt/2) | force(magnetic) | dp(dt/2) | Te ...
 //   second:  core_dTe(dt/2), visit records of the first ds | dr | rho + lists | force(EAM)
+//            ... fold of the magnetic part (beside Te)
 // The lists and rho of this step go to the other buffer set, so the first
 // sweep still reads the previous ones; the step ends with that set current.
 // MD (core.cpp:38-56 without spins): links | dp | dr | rho | forces | dp
@@ -172,11 +173,14 @@ void enqueue_step(sld_ctx* c) {
         cudaStreamWaitEvent(A, ev[0], 0);
         launch_dte(Dc, A, dt / 2e0);
         cudaEventRecord(ev[1], A);
+        launch_links(Dc, M, false, c->scan_blocks);
         if (early_noise) {
+            // the records read each atom's Te node, which the links rewrite
+            cudaEventRecord(ev[5], M);
+            cudaStreamWaitEvent(A, ev[5], 0);
             launch_spin_noise(Dc, A, eoff_ds1, dt / 2e0 / 2e0);
             cudaEventRecord(ev[4], A);
         }
-        launch_links(Dc, M, false, c->scan_blocks);
         cudaStreamWaitEvent(M, ev[1], 0);
     } else {
         if (early_noise) {
@@ -202,22 +206,35 @@ void enqueue_step(sld_ctx* c) {
     enqueue_ds(c, Dc, dt / 2e0, eoff, false, early_noise);
     cudaStreamWaitEvent(M, ev[2], 0);
     enqueue_ds(c, Dn, dt / 2e0, eoff, !c->P.eltemp);
-    cudaStreamWaitEvent(M, ev[3], 0);
+    // The magnetic force pass reads the spins and the exchange rows, not what
+    // the EAM pass writes: it runs beside it, into buffers of its own (Dm).
+    // The last kick adds the two forces; the fold into f, vir and stress runs
+    // on the side branch beside the rest of the step.
     // On a Te mesh, calculate_temperature's per-atom terms are summed where
     // their inputs are final: the spin terms by the magnetic force pass
     // (after the last sweep; the exchange field from the spins it gathers
     // anyway) and the kinetic ones by the last kick's rescale.
+    Dev Dm = Dn;
+    Dm.fm = c->fm;
+    Dm.virm = c->virm;
+    Dm.stressm = c->stressm;
     const bool temp_fused = c->P.eltemp && Dn.te_mesh > 0;
     if (temp_fused) launch_temperature_begin(Dn, M);
-    launch_force_mag(Dn, M, temp_fused);
+    launch_force_mag(Dm, M, temp_fused);
+    cudaStreamWaitEvent(M, ev[3], 0);
     c->force_volume = Dn.box_volume;
-    enqueue_dp(c, Dn, dt / 2e0, eoff, temp_fused);
+    enqueue_dp(c, Dm, dt / 2e0, eoff, temp_fused);
+    cudaEventRecord(ev[0], M);
+    cudaStreamWaitEvent(A, ev[0], 0);
+    launch_fold_mag(Dm, A);
+    cudaEventRecord(ev[1], A);
     if (c->P.eltemp) {
         if (temp_fused) launch_temperature_end(Dn, M);
         else launch_temperature(Dn, M);
         launch_dte(Dn, M, dt / 2e0);
         if (c->P.renormalize_energy) launch_energy_check(Dn, M, 1);
     }
+    cudaStreamWaitEvent(M, ev[1], 0);
     launch_advance(Dn, M, eoff, 1);
 }
 
@@ -450,7 +467,7 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
         sld_destroy(c);
         return SLD_ERR_CUDA;
     }
-    for (int k = 0; k < 5; ++k) cudaEventCreateWithFlags(&c->fork_ev[k], cudaEventDisableTiming);
+    for (int k = 0; k < 6; ++k) cudaEventCreateWithFlags(&c->fork_ev[k], cudaEventDisableTiming);
 
     DevTables T;
     rc = device_tables(prm->device, G.rcut_max, &T);
@@ -550,6 +567,9 @@ int sld_create(sld_ctx** out, const sld_params* prm, int natom, const double* r,
          c->alloc(&c->jln_set[0], n) == 0 && c->alloc(&c->jln_set[1], n) == 0 &&
          c->alloc(&D.dF, n) == 0;
     if (prm->spinlang) ok = ok && c->alloc(&D.vrec, 2 * n) == 0;
+    if (D.spin && D.latt)
+        ok = ok && c->alloc(&c->fm, n) == 0 && c->alloc(&c->virm, n) == 0 &&
+             c->alloc(&c->stressm, 6 * n) == 0;
     if (prm->precision == SLD_SPLIT) ok = ok && c->alloc(&D.s32, n) == 0;
     ok = ok && c->alloc(&D.fxs, n) == 0 && c->alloc(&D.cell_slot, n) == 0;
     if (prm->precision == SLD_SPLIT)
@@ -722,7 +742,7 @@ void sld_destroy(sld_ctx* c) {
     if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
     for (int k = 0; k < 2; ++k)
         if (c->step_graphs[k]) cudaGraphExecDestroy(c->step_graphs[k]);
-    for (int k = 0; k < 5; ++k)
+    for (int k = 0; k < 6; ++k)
         if (c->fork_ev[k]) cudaEventDestroy(c->fork_ev[k]);
     if (c->st2) cudaStreamDestroy(c->st2);
     for (void* q : c->allocs) cudaFree(q);

@@ -159,6 +159,14 @@ struct Dev {
     double* dF;                   // F'(rho) per atom, refreshed after each rho pass
     double4* vrec;                // [natom][2 sweeps] visit records of one core_ds: rho and
                                   // the noise increment dS of the atom's visit in that sweep
+    // The magnetic part of the forces, virial and stress, kept apart while
+    // the EAM part is formed beside it (set in the spin-lattice step only,
+    // null elsewhere): the magnetic pass writes them here instead of adding
+    // them to f, vir and stress; the last kick adds fm to f for its own use,
+    // and launch_fold_mag adds all three in
+    double4* fm;
+    double* virm;
+    double* stressm;
     // control and reduction scratch
     Ctl* ctl;
     double* red;                  // partial sums
@@ -681,6 +689,7 @@ void launch_force(const Dev& D, cudaStream_t st);
 void launch_embed(const Dev& D, cudaStream_t st);
 void launch_force_eam(const Dev& D, cudaStream_t st);   // lattice terms (no spins)
 void launch_force_mag(const Dev& D, cudaStream_t st, bool temp);   // adds the magnetic terms
+void launch_fold_mag(const Dev& D, cudaStream_t st);   // f, vir, stress += fm, virm, stressm
 void launch_sweep(const Dev& D, cudaStream_t st, const int* gcells, int ncell_g, double dt,
                   bool backward, bool fields);
 void launch_spin_noise(const Dev& D, cudaStream_t st, int epoch_off, double dt);

@@ -16,6 +16,11 @@ struct sld_ctx {
     std::vector<void*> allocs;
     std::vector<size_t> alloc_bytes;   // size of each allocation (a whole-state snapshot)
     int* d_gcells = nullptr;
+    // the spin-lattice step's magnetic forces, virial and stress, kept apart
+    // from the EAM part formed beside them (Dev::fm)
+    double4* fm = nullptr;
+    double* virm = nullptr;
+    double* stressm = nullptr;
     double* d_stage = nullptr;     // sld_get's device staging (6 doubles per atom), made
                                    // at its first use
     SweepFlow flow{};                  // data-flow schedule of the spin sweeps
@@ -38,7 +43,7 @@ struct sld_ctx {
     double force_volume = 0.0;
     cudaStream_t st = nullptr;
     cudaStream_t st2 = nullptr;        // second branch of the step graph
-    cudaEvent_t fork_ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t fork_ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     cudaGraphExec_t step_graph = nullptr;
     cudaGraphExec_t step_graphs[2] = {nullptr, nullptr};   // by current buffer set
     // exchange lists and rho are double buffered: the list pass of a step
