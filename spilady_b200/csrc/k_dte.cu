@@ -412,8 +412,13 @@ __global__ void __launch_bounds__(1024) k_dte_hub(Dev D, double dt, int per) {
     const int rank = (int)cl.block_rank();
     double* hT = cl.map_shared_rank(hsm, 0);   // the hub's arrays, by position
     double* hE = hT + n;
-    double* hfac = hT + 2 * n;
     double* hpart = hT + 2 * n + 2;            // each CTA's sum of Ee after A and B
+    double* hfac = hT + 2 * n;
+    // myE: the energy each A step starts from, the value this CTA last gave
+    // the position, in this CTA's own shared memory (every CTA's has the hub's
+    // layout): the hub's Te-to-Ee array on the hub, the unused slots of the
+    // hub's Te array elsewhere
+    double* myE = rank == 0 ? hsm + n : hsm;
     double* mySrc = hsm + 2 * n + 2 + HUB_CL;  // this CTA's own positions
     double* myG = mySrc + per;
     uint4* sNb = reinterpret_cast<uint4*>(myG + per);                      // hub: neighbours
@@ -426,7 +431,7 @@ __global__ void __launch_bounds__(1024) k_dte_hub(Dev D, double dt, int per) {
         const int k = D.te_gcells[m];
         double T = D.Te[k];
         hT[m] = T;
-        hE[m] = te_E<FAST>(T);
+        myE[m] = te_E<FAST>(T);
         mySrc[m - p0] = te_src(D, k);
         myG[m - p0] = te_rate(D, k, hh);
     }
@@ -444,14 +449,15 @@ __global__ void __launch_bounds__(1024) k_dte_hub(Dev D, double dt, int per) {
     for (int it = 0; it < nloop; ++it) {
         double part = 0.0;   // C's starting energy, summed per CTA
         for (int m = p0 + threadIdx.x; m < p1; m += blockDim.x) {   // A(h/2), B(h/2)
-            double T = te_T<FAST>(hE[m] + hh * mySrc[m - p0]);
+            double T = te_T<FAST>(myE[m] + hh * mySrc[m - p0]);
             T = te_rk4<FAST>(T, myG[m - p0], hh);
             hT[m] = T;
             const double E = te_E<FAST>(T);
             hE[m] = E;
             part += E;
         }
-        part = block_sum(part, sh);
+        // sh was last read before the previous cluster barrier
+        part = block_sum_after_barrier(part, sh);
         if (threadIdx.x == 0) hpart[rank] = part;
         cl.sync();
         if (rank == 0) {   // C(h) on the hub
@@ -459,14 +465,14 @@ __global__ void __launch_bounds__(1024) k_dte_hub(Dev D, double dt, int per) {
             if (threadIdx.x == 0)
                 for (int r = 0; r < ncta; ++r) start += hsm[2 * n + 2 + r];
             hub_sweep<FAST, LEV>(D, hsm, n, sTk, sNb, gm);
-            __syncthreads();
+            if constexpr (!FAST) __syncthreads();   // the fitted sweep ends on a barrier
             double acc = 0.0;
             for (int m = threadIdx.x; m < n; m += blockDim.x) acc += hsm[n + m];
-            const double t = block_sum(acc, sh);
+            const double t = block_sum_after_barrier(acc, sh);
             if (threadIdx.x == 0) hsm[2 * n] = start / t;
         }
         cl.sync();
-        double fac = *hfac;
+        const double fac = *hfac;
         int q = 0;
         for (int m = p0 + threadIdx.x; m < p1; m += blockDim.x, ++q) {   // rescale, B, A
             double T = te_T<FAST>(hE[m] * fac);
@@ -475,11 +481,11 @@ __global__ void __launch_bounds__(1024) k_dte_hub(Dev D, double dt, int per) {
             if (FAST && it + 1 < nloop) {
                 // the fitted form keeps the energy: the next substep's A
                 // continues from it without the round trip through Te
-                hE[m] = Ee;
+                myE[m] = Ee;
             } else {
                 T = te_T<FAST>(Ee);
                 hT[m] = T;
-                hE[m] = te_E<FAST>(T);
+                myE[m] = te_E<FAST>(T);
             }
             if (q < 4) lastE[q] = Ee;
         }

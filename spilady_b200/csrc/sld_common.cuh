@@ -424,6 +424,22 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
     return t;
 }
 
+// block_sum for a caller that has passed a block-wide barrier since the last
+// read of `sh`
+__device__ __forceinline__ double block_sum_after_barrier(double v, double* sh) {
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    v = warp_sum(v);
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (w == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        t = lane < nw ? sh[lane] : 0.0;
+        t = warp_sum(t);
+    }
+    return t;
+}
+
 static inline int div_up(long a, long b) { return (int)((a + b - 1) / b); }
 
 // 32-byte global accesses: one instruction on sm_100 where a double4 or two
