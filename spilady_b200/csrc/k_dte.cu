@@ -461,15 +461,20 @@ __global__ void __launch_bounds__(1024) k_dte_hub(Dev D, double dt, int per) {
         if (threadIdx.x == 0) hpart[rank] = part;
         cl.sync();
         if (rank == 0) {   // C(h) on the hub
-            double start = 0.0;   // valid in thread 0, the one that uses it
-            if (threadIdx.x == 0)
+            // C's starting energy, valid in thread 0: the fitted form keeps it in
+            // the slot after the factor's rather than in a register through its
+            // sweep, which holds two updates' chains in flight
+            double start = 0.0;
+            if (threadIdx.x == 0) {
                 for (int r = 0; r < ncta; ++r) start += hsm[2 * n + 2 + r];
+                if constexpr (FAST) hsm[2 * n + 1] = start;
+            }
             hub_sweep<FAST, LEV>(D, hsm, n, sTk, sNb, gm);
             if constexpr (!FAST) __syncthreads();   // the fitted sweep ends on a barrier
             double acc = 0.0;
             for (int m = threadIdx.x; m < n; m += blockDim.x) acc += hsm[n + m];
             const double t = block_sum_after_barrier(acc, sh);
-            if (threadIdx.x == 0) hsm[2 * n] = start / t;
+            if (threadIdx.x == 0) hsm[2 * n] = (FAST ? hsm[2 * n + 1] : start) / t;
         }
         cl.sync();
         const double fac = *hfac;
