@@ -421,8 +421,8 @@ def run_adjoint(args, world, rank, local):
 
     (cfg, ms_cfg) = timed(lambda: e.adjoint_config(th), 3)
     out, dE, dL = cfg
-    ((Lk, dLk), ms_traj) = timed(lambda: e.adjoint_trajectory(th, K, C), 1)
-    (_, ms_fwd) = timed(lambda: e.adjoint_trajectory(th, K, C, grad=False), 1)
+    ((Lk, dLk), ms_traj) = timed(lambda: e.adjoint_trajectory(th, K, C), 3)
+    (_, ms_fwd) = timed(lambda: e.adjoint_trajectory(th, K, C, grad=False), 3)
 
     def fd(fn, scale=1.0):
         g = np.zeros(len(th))
@@ -552,9 +552,12 @@ def other_configs(local):
     e64 = engine.Engine(params, r, p, s, device=local, precision=engine.FP64_ANALYTIC)
     th = engine.adjoint_theta_default()
     es.adjoint_trajectory(th, 200, 20)
-    t0 = time.perf_counter()
-    es.adjoint_trajectory(th, 200, 20)
-    grad_ms = (time.perf_counter() - t0) * 1e3
+    grad_runs = []
+    for _ in range(3):   # the median of three: host-timed, so it varies from run to run
+        t0 = time.perf_counter()
+        es.adjoint_trajectory(th, 200, 20)
+        grad_runs.append((time.perf_counter() - t0) * 1e3)
+    grad_ms = float(np.median(grad_runs))
     K = 10
     _, g = e64.adjoint_trajectory(th, K, 5)
     h = np.where(th != 0.0, 1e-6 * np.abs(th), 1e-6)
@@ -661,21 +664,24 @@ def main():
             host[name] = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
             host[name].numpy()[:] = a
         k = max(5, min(args.steps, 100))
-        t0 = time.perf_counter()
-        e.set_state(host["r"].numpy(), host["p"].numpy(), host["s"].numpy())
-        for _ in range(k):
-            e.run(1)
-            e.averages()
-        for name in ("r", "p", "s"):
-            e.get(name, out=host[name].numpy().reshape(-1))
-        t1 = time.perf_counter()
+        secs = []
+        for _ in range(3):   # three samples, the median: the host's own timing varies
+            t0 = time.perf_counter()
+            e.set_state(host["r"].numpy(), host["p"].numpy(), host["s"].numpy())
+            for _ in range(k):
+                e.run(1)
+                e.averages()
+            for name in ("r", "p", "s"):
+                e.get(name, out=host[name].numpy().reshape(-1))
+            secs.append(time.perf_counter() - t0)
         nat = e.natom
-        return {"value": nat * k / (t1 - t0), "unit": "atom-steps/s",
+        return {"value": nat * k / float(np.median(secs)), "unit": "atom-steps/s",
                 "h2d_bytes_per_step": int(nat * 72 / k),
                 "d2h_bytes_per_step": int(80 + nat * 72 / k), "steps": k,
                 "note": f"per sample of {k} steps: r, p, s uploaded from pinned host memory "
                         "once (sld_set_state), sld_run(1) and the averages read back every "
-                        "step, and r, p, s read back into the pinned buffers at the end"}
+                        "step, and r, p, s read back into the pinned buffers at the end; "
+                        "the median of three samples"}
 
     main_arm = timed_form(prec, not args.no_e2e)
     fp64_arm = None
