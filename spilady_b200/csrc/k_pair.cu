@@ -716,7 +716,7 @@ __global__ void __launch_bounds__(256) k_fold_mag(Dev D, int with_f) {
     }
 }
 void launch_fold_mag(const Dev& D, cudaStream_t st) {
-    k_fold_mag<<<div_up(6 * D.natom, 256), 256, 0, st>>>(D, D.fext ? 0 : 1);
+    k_fold_mag<<<div_up(6L * D.natom, 256), 256, 0, st>>>(D, D.fext ? 0 : 1);
 }
 
 // the magnetic part from the exchange rows of the list pass that ran on the
