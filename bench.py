@@ -59,8 +59,8 @@ DESIGN_BYTES_CORE_DS = 1168
 # dram__bytes_read.sum + dram__bytes_write.sum, ncu's default cache control:
 # caches flushed before every launch, so an upper bound on the graph's own
 # traffic); profiles/step_launches_bcc128.md.
-CORE_DS_TRAFFIC_PER_ATOM = {"split": (9239.2e6 + 556.1e6) / 4194304,
-                            "fp64": (11194.7e6 + 556.1e6) / 4194304}
+CORE_DS_TRAFFIC_PER_ATOM = {"split": (9236.3e6 + 555.8e6) / 4194304,
+                            "fp64": (11178.4e6 + 556.0e6) / 4194304}
 CORE_DS_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum over one step's 72 "
                           "sweep and 2 visit-record launches at 128^3, caches flushed before "
                           "each launch")
